@@ -1,0 +1,263 @@
+/*
+ * mpdpft_gpu.h -- C ABI of the B200 self-consistent DPFT engine.
+ *
+ * This is the drop-in boundary for mpDPFT's self-consistent (SC) loop.  The
+ * reference exposes that loop as free C++ functions over one mutable
+ * `datastruct&` (mpDPFT.h:71-93); every entry point below replaces one of
+ * them and names it.  All arrays crossing this boundary are IEEE double, the
+ * reference's storage type, whatever precision the engine computes in.
+ *
+ * Grids.  The engine stores every field on the periodic grid of s^D points
+ * (s = steps), x-major (index = (i*s + j)*s + k, x = -L/2 + i*dx, dx = L/s).
+ * The reference stores (s+1)^D points whose last plane along each axis
+ * duplicates plane 0 (mpDPFT.cpp:863, refilled by fftParallel
+ * mpDPFT.cpp:8266-8324).  Pass MPDPFT_LAYOUT_REFERENCE to exchange arrays in
+ * that layout: inputs drop the duplicate planes, outputs refill them.
+ *
+ * Memory.  MPDPFT_MEM_HOST pointers are copied through pinned staging
+ * buffers on the context stream; MPDPFT_MEM_DEVICE pointers must be device
+ * memory on the context's GPU.
+ *
+ * Errors.  Every call returns an mpdpft_status.  Nothing calls exit(); the
+ * text of the last error on the calling host thread is returned by
+ * mpdpft_last_error().  A context is not re-entrant; distinct contexts are
+ * independent and may be driven from different host threads.
+ */
+#ifndef MPDPFT_GPU_H
+#define MPDPFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPDPFT_ABI_VERSION 1
+#define MPDPFT_MAX_SPECIES 4
+#define MPDPFT_MAX_INTERACTIONS 8
+#define MPDPFT_MAX_PULAY 12
+
+typedef enum {
+  MPDPFT_OK = 0,
+  MPDPFT_ERR_ARG = 1,           /* invalid argument or unsupported option      */
+  MPDPFT_ERR_CUDA = 2,          /* CUDA runtime error                          */
+  MPDPFT_ERR_NONFINITE = 3,     /* non-finite value in an input or a result    */
+  MPDPFT_ERR_MU_BRACKET = 4,    /* mu bracket not found; mu reset (warning)    */
+  MPDPFT_ERR_PULAY_SINGULAR = 5,/* Pulay Gram matrix rejected; linear mixing   */
+  MPDPFT_ERR_TIMEOUT = 6,       /* a device loop reached its iteration cap     */
+  MPDPFT_ERR_NOT_CONVERGED = 7, /* maxSCcount reached before convergence       */
+  MPDPFT_ERR_NO_DEVICE = 8      /* no usable sm_100 device                     */
+} mpdpft_status;
+
+enum { MPDPFT_FP64 = 0, MPDPFT_MIXED = 1 };
+enum { MPDPFT_LAYOUT_PERIODIC = 0, MPDPFT_LAYOUT_REFERENCE = 1 };
+enum { MPDPFT_MEM_HOST = 0, MPDPFT_MEM_DEVICE = 1 };
+
+/* Density functionals, numbered as the reference's DensityExpression
+ * (mpDPFT.input line 15, dispatcher mpDPFT.cpp:2142-2238). */
+enum {
+  MPDPFT_DENS_TF_INSPIRED = 1,   /* GetTFinspireddensity T=0   mpDPFT.cpp:3318-3347 */
+  MPDPFT_DENS_TF_INSPIRED_T = 2, /* GetTFinspireddensity T>0   mpDPFT.cpp:3340-3345 */
+  MPDPFT_DENS_GRADIENT = 5,      /* getDenEnAt small-gradient branch, T->0 form
+                                    mpDPFT.cpp:3376-3388; needs DelField        */
+  MPDPFT_DENS_TF = 7             /* GetTFdensity               mpDPFT.cpp:4415-4436 */
+};
+
+/* Interaction types, numbered as the reference's getVint (mpDPFT.cpp:2240-2318). */
+enum {
+  MPDPFT_INT_NONE = 0,
+  MPDPFT_INT_CONTACT_MUTUAL = 1, /* V_s = beta * sum_{s'!=s} n_s'          :2247-2253 */
+  MPDPFT_INT_HARTREE = 8,        /* V_s = gammaH * Coulomb[n_s]           :2677-2715 */
+  MPDPFT_INT_CONTACT_SELF = 10,  /* V = 2 beta n_0                        :2261-2264 */
+  MPDPFT_INT_DIRAC = 11,         /* V_s = -gammaH (3 n_s/pi)^(1/3)       :2759-2772 */
+  MPDPFT_INT_HARTREE_INTER = 21, /* V_s = gammaH * sum_{s'!=s} Coulomb[n_s'] :2273-2285 */
+  MPDPFT_INT_COULOMB_CHARGED = 100 /* no reference counterpart: V_s = q_s gammaH
+                                      Coulomb[sum_s' q_s' n_s'] (charged species) */
+};
+
+/* Coulomb kernels for the Hartree solve. */
+enum {
+  MPDPFT_COULOMB_REGULARISED = 0, /* reference kernel: (n~ - n~0 e^{-k^2})/k^2 plus
+                                     n~0 erf(r/2)/r, mpDPFT.cpp:2677-2715          */
+  MPDPFT_COULOMB_TRUNCATED = 1    /* spherical cutoff 4 pi (1 - cos kR)/k^2         */
+};
+
+/* Parameters of one SC solve.  Field names follow mpDPFT.input
+ * (parser mpDPFT.cpp:633-690); the line number is given for each. */
+typedef struct {
+  int dim;                  /* line 5  DIM: 2 or 3                                  */
+  int steps;                /* line 8  steps s (even; FFT sizes 2^a 3^b)            */
+  int species;              /* line 9  S                                            */
+  double edge;              /* line 7  box edge L, box [-L/2, L/2]^D                */
+  double abundances[MPDPFT_MAX_SPECIES]; /* line 10 target particle numbers N*_s    */
+  double rel_acc;           /* line 11 RelAcc of the mu search                      */
+  int density_expression;   /* line 15 one of MPDPFT_DENS_*                         */
+  double tau[MPDPFT_MAX_SPECIES];   /* line 18 tauVec (TF-inspired densities)       */
+  double temperature[MPDPFT_MAX_SPECIES]; /* line 20 TVec                          */
+  int n_interactions;       /* line 26 Interactions                                 */
+  int interactions[MPDPFT_MAX_INTERACTIONS];
+  double incremental_v;     /* line 27 incrementalV ramp per SC iteration (1 = off) */
+  double mu[MPDPFT_MAX_SPECIES];    /* line 28 muVec: initial chemical potentials   */
+  double deltamu_modifier;  /* line 29 DeltamuModifier                              */
+  int mixer;                /* line 30 Mixer[0]: 0 linear, 1 Pulay                  */
+  int pulay_scope;          /* line 30 Mixer[1]: Pulay history length (<= MAX)      */
+  double theta[MPDPFT_MAX_SPECIES]; /* line 31 thetaVec admixtures                  */
+  double sc_criterion;      /* line 32 SCcriterion                                  */
+  int max_sc_count;         /* line 33 maxSCcount                                   */
+  int schedule;             /* line 37 Schedule: 0 none, 5 adaptive theta, 9 ramp   */
+  double beta;              /* line 40 contact strength                             */
+  double gamma_h;           /* line 42 gammaH Coulomb prefactor                     */
+  double degeneracy;        /* line 43 g                                            */
+  double regularization_threshold; /* line 45 RegularizationThreshold (taper radius
+                                      fraction of the edge)                         */
+  /* hard-coded values of the reference, exposed with the reference defaults */
+  int taper_off;            /* TaperOff = 1 (mpDPFT.h:79; DelField :7251-7264)      */
+  double smearing_extent;   /* Gaussian smoothing width; <= 0 means 6*dx (:1105)    */
+  /* options of this engine */
+  double charges[MPDPFT_MAX_SPECIES]; /* species charges for MPDPFT_INT_COULOMB_CHARGED */
+  int coulomb_kernel;       /* MPDPFT_COULOMB_*                                     */
+  double coulomb_cutoff;    /* truncated kernel radius R; <= 0 means L/2            */
+  double gradient_floor;    /* floor on mu - V in the (mu-V)^{-1/2} and ^{-3/2}
+                               gradient terms of MPDPFT_DENS_GRADIENT               */
+  double gradient_grad2;    /* coefficient of the |grad V|^2 term (0: reference
+                               small-gradient branch; 1: second-order
+                               Wigner-Kirkwood)                                    */
+  double potential_tol;     /* extra exit test: rms(V_new - V_old) <= tol (0: off)  */
+  int precision;            /* MPDPFT_FP64 or MPDPFT_MIXED                          */
+} mpdpft_params;
+
+/* Per-iteration record of mpdpft_sc_run (the reference prints SCcount, CC,
+ * mu and abundances per iteration, mpDPFT.cpp:4862). */
+typedef struct {
+  int sc_count;
+  int mu_trials;            /* density evaluations spent in the mu search          */
+  int pulay_used;           /* 1 if Pulay mixing was applied                       */
+  int status_bits;          /* bit k set = status k raised during this iteration    */
+  double cc;                /* convergence criterion, CheckConvergence :4759-4782   */
+  double v_residual;        /* rms of V between consecutive iterations             */
+  double mu[MPDPFT_MAX_SPECIES];
+  double abundance[MPDPFT_MAX_SPECIES];
+  double theta[MPDPFT_MAX_SPECIES];
+  double ms;                /* device time of the iteration                        */
+} mpdpft_iter_log;
+
+typedef struct {
+  int iterations;           /* SC iterations run                                   */
+  int converged;            /* 1 if the exit rule was met                          */
+  int total_mu_trials;
+  double cc;
+  double v_residual;
+  double mu[MPDPFT_MAX_SPECIES];
+  double abundance[MPDPFT_MAX_SPECIES];
+  double e_total;
+  double e_kinetic[MPDPFT_MAX_SPECIES];
+  double e_external[MPDPFT_MAX_SPECIES];
+  double e_interaction[MPDPFT_MAX_INTERACTIONS];
+  double seconds;           /* wall time of the solve                              */
+} mpdpft_result;
+
+typedef struct mpdpft_ctx mpdpft_ctx;
+typedef struct mpdpft_batch mpdpft_batch;
+
+/* Fill *p with the reference defaults (mpDPFT.input sample values and the
+ * hard-coded defaults of InitializeHardCodedParameters, mpDPFT.cpp:858-1115). */
+void mpdpft_params_default(mpdpft_params* p);
+
+int mpdpft_abi_version(void);
+/* sizeof(mpdpft_params), sizeof(mpdpft_result), sizeof(mpdpft_iter_log) for
+ * which = 0, 1, 2 (binding checks); 0 for any other value. */
+size_t mpdpft_struct_size(int which);
+const char* mpdpft_last_error(void);
+const char* mpdpft_status_string(int status);
+
+/* Context: device buffers, FFT plans and the SC state of one solve.
+ * Replaces the allocation half of GetData's initialisation
+ * (AllocateDensityMemory :6392, InitializeGlobalFFTWplans :6313,
+ * AllocateTMPmemory :6337, InitializePulayMixer :7029). */
+int mpdpft_ctx_create(const mpdpft_params* params, int device, mpdpft_ctx** out);
+int mpdpft_ctx_destroy(mpdpft_ctx* ctx);
+int mpdpft_ctx_sync(mpdpft_ctx* ctx);
+/* The context's cudaStream_t, as an opaque pointer. */
+void* mpdpft_ctx_stream(mpdpft_ctx* ctx);
+
+/* External potential V_ext of species s.  Replaces GetEnv (mpDPFT.cpp:1385). */
+int mpdpft_set_external_potential(mpdpft_ctx* ctx, int s, const double* v_ext,
+                                  int layout, int mem);
+
+/* n[V] of species s at chemical potential mu, and N = Integrate(n).
+ * Replaces GetDensity (mpDPFT.cpp:2142) followed by Integrate (:7970).
+ * For MPDPFT_DENS_GRADIENT the derivatives of V come from DelField. */
+int mpdpft_density(mpdpft_ctx* ctx, int s, const double* v, double mu,
+                   double* n_out, double* abundance_out, int layout, int mem);
+
+/* V_int[n] of one interaction type for focal species s.  `n` holds the
+ * densities of all species, each a pointer to one grid.  Replaces getVint
+ * (mpDPFT.cpp:2240), which writes data.TmpField2. */
+int mpdpft_vint(mpdpft_ctx* ctx, int type, int s, const double* const* n,
+                double* v_out, int layout, int mem);
+
+/* V_s = V_ext,s + incremental * sum_a V_int,a[n] for every species.
+ * Replaces UpdateV (mpDPFT.cpp:4815). */
+int mpdpft_update_v(mpdpft_ctx* ctx, const double* const* n, double incremental,
+                    double* const* v_out, int layout, int mem);
+
+/* Particle-number constraint for species s: find mu with
+ * |N(mu) - N*| / (2 N*) <= rel_acc.  Replaces EnforceConstraints
+ * (mpDPFT.cpp:4569-4743) for one species.  *mu_io holds the starting mu on
+ * entry and the result on exit; the final density is left in n_out when it
+ * is not NULL.  Returns MPDPFT_ERR_MU_BRACKET (mu reset to the start value)
+ * when no bracket is found, as the reference does. */
+int mpdpft_mu_search(mpdpft_ctx* ctx, int s, const double* v, double n_target,
+                     double* mu_io, double* abundance_out, int* trials_out,
+                     double* n_out, int layout, int mem);
+
+/* Spectral derivatives of f with Gaussian smoothing (method 5) and the
+ * boundary taper.  Writes |grad f|^2 (smoothed, clamped >= 0) and the
+ * Laplacian (smoothed).  Replaces DelField(f, s, 5, data) (mpDPFT.cpp:7243-7582). */
+int mpdpft_delfield(mpdpft_ctx* ctx, const double* f, double* grad2_out,
+                    double* laplacian_out, int layout, int mem);
+
+/* Centred-k complex DFT with the reference's conventions: forward
+ * f~(k) = dx^D sum_x f(x) e^{-ikx}, backward f(x) = L^-D sum_k f~(k) e^{ikx},
+ * k = -pi/dx + m dk.  Interleaved complex, periodic layout s^D.
+ * Replaces fftParallel (mpDPFT.cpp:8173-8335); sign = -1 forward, +1 backward. */
+int mpdpft_fft(mpdpft_ctx* ctx, int sign, const double* in, double* out, int mem);
+
+/* Trapezoid integral over the box.  Replaces Integrate(method 1)
+ * (Riemann, mpDPFT.cpp:7981-8026). */
+int mpdpft_integrate(mpdpft_ctx* ctx, const double* f, double* out, int layout, int mem);
+
+/* Density mixing for all species.  mixer 1 runs PulayMixer
+ * (mpDPFT.cpp:5005-5167) with its history kept on the device and falls back
+ * to linear mixing (AdmixDensities :4921-4992) when the Gram matrix is
+ * rejected or on the first call after mpdpft_pulay_reset.  coeffs_out
+ * (may be NULL) receives up to MPDPFT_MAX_PULAY coefficients. */
+int mpdpft_pulay_reset(mpdpft_ctx* ctx);
+int mpdpft_admix(mpdpft_ctx* ctx, const double* const* n_in, const double* const* n_out,
+                 const double* theta, double* const* n_mixed, double* coeffs_out,
+                 int* n_coeffs_out, int layout, int mem);
+
+/* Full SC solve (GetData's loop, mpDPFT.cpp:210-229).  v0 (may be NULL: start
+ * from V_ext) holds the starting potentials of all species.  The per-iteration
+ * log is written when log != NULL (at most log_cap records).  The final
+ * densities and potentials stay in the context (mpdpft_get_field). */
+int mpdpft_sc_run(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem,
+                  mpdpft_result* result, mpdpft_iter_log* log, int log_cap);
+
+/* One SC iteration on the current state (captured as a CUDA graph after the
+ * first call when graph != 0).  Used by benchmarks and the batch engine. */
+int mpdpft_sc_step(mpdpft_ctx* ctx, int graph, mpdpft_iter_log* log);
+int mpdpft_sc_init(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem);
+
+enum { MPDPFT_FIELD_DENSITY = 0, MPDPFT_FIELD_POTENTIAL = 1, MPDPFT_FIELD_GRAD2 = 2,
+       MPDPFT_FIELD_LAPLACIAN = 3, MPDPFT_FIELD_EXTERNAL = 4 };
+int mpdpft_get_field(mpdpft_ctx* ctx, int which, int s, double* out, int layout, int mem);
+
+/* Energies of the current state (GetEnergy, mpDPFT.cpp:5414-5436). */
+int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPDPFT_GPU_H */

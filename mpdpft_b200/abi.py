@@ -1,0 +1,188 @@
+"""ctypes mirror of include/mpdpft_gpu.h (ABI version 1).
+
+Only declarations live here: the parameter, result and log structs, the
+status codes and the enum values.  ``mpdpft_b200.engine`` binds the CUDA
+library against these declarations.
+"""
+import ctypes as C
+
+ABI_VERSION = 1
+MAX_SPECIES = 4
+MAX_INTERACTIONS = 8
+MAX_PULAY = 12
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_NONFINITE = 3
+ERR_MU_BRACKET = 4
+ERR_PULAY_SINGULAR = 5
+ERR_TIMEOUT = 6
+ERR_NOT_CONVERGED = 7
+ERR_NO_DEVICE = 8
+
+FP64 = 0
+MIXED = 1
+LAYOUT_PERIODIC = 0
+LAYOUT_REFERENCE = 1
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+DENS_TF_INSPIRED = 1
+DENS_TF_INSPIRED_T = 2
+DENS_GRADIENT = 5
+DENS_TF = 7
+
+INT_NONE = 0
+INT_CONTACT_MUTUAL = 1
+INT_HARTREE = 8
+INT_CONTACT_SELF = 10
+INT_DIRAC = 11
+INT_HARTREE_INTER = 21
+INT_COULOMB_CHARGED = 100
+
+COULOMB_REGULARISED = 0
+COULOMB_TRUNCATED = 1
+
+FIELD_DENSITY = 0
+FIELD_POTENTIAL = 1
+FIELD_GRAD2 = 2
+FIELD_LAPLACIAN = 3
+FIELD_EXTERNAL = 4
+
+_D4 = C.c_double * MAX_SPECIES
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int),
+        ("steps", C.c_int),
+        ("species", C.c_int),
+        ("edge", C.c_double),
+        ("abundances", _D4),
+        ("rel_acc", C.c_double),
+        ("density_expression", C.c_int),
+        ("tau", _D4),
+        ("temperature", _D4),
+        ("n_interactions", C.c_int),
+        ("interactions", C.c_int * MAX_INTERACTIONS),
+        ("incremental_v", C.c_double),
+        ("mu", _D4),
+        ("deltamu_modifier", C.c_double),
+        ("mixer", C.c_int),
+        ("pulay_scope", C.c_int),
+        ("theta", _D4),
+        ("sc_criterion", C.c_double),
+        ("max_sc_count", C.c_int),
+        ("schedule", C.c_int),
+        ("beta", C.c_double),
+        ("gamma_h", C.c_double),
+        ("degeneracy", C.c_double),
+        ("regularization_threshold", C.c_double),
+        ("taper_off", C.c_int),
+        ("smearing_extent", C.c_double),
+        ("charges", _D4),
+        ("coulomb_kernel", C.c_int),
+        ("coulomb_cutoff", C.c_double),
+        ("gradient_floor", C.c_double),
+        ("gradient_grad2", C.c_double),
+        ("potential_tol", C.c_double),
+        ("precision", C.c_int),
+    ]
+
+    def grid_points(self, layout=LAYOUT_PERIODIC):
+        n = self.steps + (1 if layout == LAYOUT_REFERENCE else 0)
+        return n ** self.dim
+
+    def copy(self):
+        other = Params()
+        C.memmove(C.byref(other), C.byref(self), C.sizeof(Params))
+        return other
+
+
+class IterLog(C.Structure):
+    _fields_ = [
+        ("sc_count", C.c_int),
+        ("mu_trials", C.c_int),
+        ("pulay_used", C.c_int),
+        ("status_bits", C.c_int),
+        ("cc", C.c_double),
+        ("v_residual", C.c_double),
+        ("mu", _D4),
+        ("abundance", _D4),
+        ("theta", _D4),
+        ("ms", C.c_double),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("converged", C.c_int),
+        ("total_mu_trials", C.c_int),
+        ("cc", C.c_double),
+        ("v_residual", C.c_double),
+        ("mu", _D4),
+        ("abundance", _D4),
+        ("e_total", C.c_double),
+        ("e_kinetic", _D4),
+        ("e_external", _D4),
+        ("e_interaction", C.c_double * MAX_INTERACTIONS),
+        ("seconds", C.c_double),
+    ]
+
+
+def make_params(**kw):
+    """Params with the reference defaults, overridden by keyword arguments.
+
+    Defaults follow the sample mpDPFT.input and the hard-coded values of
+    InitializeHardCodedParameters (mpDPFT.cpp:858-1115).  Array fields accept
+    Python sequences.
+    """
+    p = Params()
+    p.dim = 3
+    p.steps = 64
+    p.species = 1
+    p.edge = 16.0
+    p.rel_acc = 1.0e-10
+    p.density_expression = DENS_TF
+    for s in range(MAX_SPECIES):
+        p.abundances[s] = 1.0
+        p.tau[s] = 1.0
+        p.temperature[s] = 1.0
+        p.mu[s] = 5.5
+        p.theta[s] = 0.3
+        p.charges[s] = 1.0
+    p.n_interactions = 0
+    p.incremental_v = 1.0
+    p.deltamu_modifier = -3.0
+    p.mixer = 1
+    p.pulay_scope = 5
+    p.sc_criterion = 1.0e-12
+    p.max_sc_count = 200
+    p.schedule = 0
+    p.beta = 0.0
+    p.gamma_h = 0.0
+    p.degeneracy = 1.0
+    p.regularization_threshold = 0.375
+    p.taper_off = 1
+    p.smearing_extent = 0.0
+    p.coulomb_kernel = COULOMB_REGULARISED
+    p.coulomb_cutoff = 0.0
+    p.gradient_floor = 1.0e-3
+    p.gradient_grad2 = 0.0
+    p.potential_tol = 0.0
+    p.precision = FP64
+    for key, val in kw.items():
+        if key == "interactions":
+            p.n_interactions = len(val)
+            for i, v in enumerate(val):
+                p.interactions[i] = int(v)
+            continue
+        field = getattr(p, key)
+        if isinstance(field, C.Array):
+            for i, v in enumerate(val):
+                field[i] = v
+        else:
+            setattr(p, key, val)
+    return p

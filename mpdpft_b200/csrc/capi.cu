@@ -1,0 +1,247 @@
+// capi.cu -- extern "C" entry points of include/mpdpft_gpu.h.
+#include <cstring>
+#include <new>
+
+#include "../../include/mpdpft_gpu.h"
+#include "engine.h"
+
+using mpdpft::Ctx;
+using mpdpft::set_error;
+
+struct mpdpft_ctx {
+  Ctx impl;
+};
+
+#define CHECK_CTX(c) \
+  if (!(c)) return set_error(MPDPFT_ERR_ARG, "null context")
+
+extern "C" {
+
+void mpdpft_params_default(mpdpft_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->dim = 3;
+  p->steps = 64;
+  p->species = 1;
+  p->edge = 16.0;
+  p->rel_acc = 1.0e-10;
+  p->density_expression = MPDPFT_DENS_TF;
+  for (int s = 0; s < MPDPFT_MAX_SPECIES; ++s) {
+    p->abundances[s] = 1.0;
+    p->tau[s] = 1.0;
+    p->temperature[s] = 1.0;
+    p->mu[s] = 5.5;
+    p->theta[s] = 0.3;
+    p->charges[s] = 1.0;
+  }
+  p->incremental_v = 1.0;
+  p->deltamu_modifier = -3.0;
+  p->mixer = 1;
+  p->pulay_scope = 5;
+  p->sc_criterion = 1.0e-12;
+  p->max_sc_count = 200;
+  p->degeneracy = 1.0;
+  p->regularization_threshold = 0.375;
+  p->taper_off = 1;
+  p->coulomb_kernel = MPDPFT_COULOMB_REGULARISED;
+  p->gradient_floor = 1.0e-3;
+  p->precision = MPDPFT_FP64;
+}
+
+int mpdpft_abi_version(void) { return MPDPFT_ABI_VERSION; }
+
+size_t mpdpft_struct_size(int which) {
+  switch (which) {
+    case 0: return sizeof(mpdpft_params);
+    case 1: return sizeof(mpdpft_result);
+    case 2: return sizeof(mpdpft_iter_log);
+    default: return 0;
+  }
+}
+
+const char* mpdpft_last_error(void) { return mpdpft::g_last_error.c_str(); }
+
+const char* mpdpft_status_string(int status) {
+  switch (status) {
+    case MPDPFT_OK: return "ok";
+    case MPDPFT_ERR_ARG: return "invalid argument";
+    case MPDPFT_ERR_CUDA: return "CUDA error";
+    case MPDPFT_ERR_NONFINITE: return "non-finite value";
+    case MPDPFT_ERR_MU_BRACKET: return "mu bracket not found";
+    case MPDPFT_ERR_PULAY_SINGULAR: return "Pulay matrix rejected";
+    case MPDPFT_ERR_TIMEOUT: return "device loop cap reached";
+    case MPDPFT_ERR_NOT_CONVERGED: return "not converged";
+    case MPDPFT_ERR_NO_DEVICE: return "no usable device";
+    default: return "unknown status";
+  }
+}
+
+int mpdpft_ctx_create(const mpdpft_params* params, int device, mpdpft_ctx** out) {
+  if (!params || !out) return set_error(MPDPFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  mpdpft_ctx* c = new (std::nothrow) mpdpft_ctx;
+  if (!c) return set_error(MPDPFT_ERR_ARG, "out of host memory");
+  int st = c->impl.init(*params, device);
+  if (!st) st = c->impl.fft_setup();
+  if (st) {
+    delete c;
+    return st;
+  }
+  *out = c;
+  return MPDPFT_OK;
+}
+
+int mpdpft_ctx_destroy(mpdpft_ctx* ctx) {
+  if (!ctx) return MPDPFT_OK;
+  cudaSetDevice(ctx->impl.device);
+  cudaStreamSynchronize(ctx->impl.stream);
+  ctx->impl.fft_release();
+  delete ctx;
+  return MPDPFT_OK;
+}
+
+int mpdpft_ctx_sync(mpdpft_ctx* ctx) {
+  CHECK_CTX(ctx);
+  cudaError_t e = cudaStreamSynchronize(ctx->impl.stream);
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, cudaGetErrorString(e));
+  return MPDPFT_OK;
+}
+
+void* mpdpft_ctx_stream(mpdpft_ctx* ctx) { return ctx ? (void*)ctx->impl.stream : nullptr; }
+
+int mpdpft_set_external_potential(mpdpft_ctx* ctx, int s, const double* v_ext, int layout, int mem) {
+  CHECK_CTX(ctx);
+  Ctx& c = ctx->impl;
+  if (s < 0 || s >= c.S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  cudaSetDevice(c.device);
+  return c.import_field(v_ext, (char*)c.d_vext + (size_t)s * c.geom.n * c.rsize, layout, mem);
+}
+
+int mpdpft_density(mpdpft_ctx* ctx, int s, const double* v, double mu, double* n_out, double* abundance_out,
+                   int layout, int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_density(s, v, mu, n_out, abundance_out, layout, mem);
+}
+
+int mpdpft_vint(mpdpft_ctx* ctx, int type, int s, const double* const* n, double* v_out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_vint(type, s, n, v_out, layout, mem);
+}
+
+int mpdpft_update_v(mpdpft_ctx* ctx, const double* const* n, double incremental, double* const* v_out, int layout,
+                    int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_update_v(n, incremental, v_out, layout, mem);
+}
+
+int mpdpft_mu_search(mpdpft_ctx* ctx, int s, const double* v, double n_target, double* mu_io,
+                     double* abundance_out, int* trials_out, double* n_out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  if (!mu_io) return set_error(MPDPFT_ERR_ARG, "null mu");
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_mu_search(s, v, n_target, mu_io, abundance_out, trials_out, n_out, layout, mem);
+}
+
+int mpdpft_delfield(mpdpft_ctx* ctx, const double* f, double* grad2_out, double* laplacian_out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_delfield(f, grad2_out, laplacian_out, layout, mem);
+}
+
+int mpdpft_fft(mpdpft_ctx* ctx, int sign, const double* in, double* out, int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_fft(sign, in, out, mem);
+}
+
+int mpdpft_integrate(mpdpft_ctx* ctx, const double* f, double* out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  if (!out) return set_error(MPDPFT_ERR_ARG, "null output");
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_integrate(f, out, layout, mem);
+}
+
+int mpdpft_pulay_reset(mpdpft_ctx* ctx) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.reset_state();
+}
+
+int mpdpft_admix(mpdpft_ctx* ctx, const double* const* n_in, const double* const* n_out, const double* theta,
+                 double* const* n_mixed, double* coeffs_out, int* n_coeffs_out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  if (!n_in || !n_out || !n_mixed) return set_error(MPDPFT_ERR_ARG, "null density arrays");
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.op_admix(n_in, n_out, theta, n_mixed, coeffs_out, n_coeffs_out, layout, mem);
+}
+
+int mpdpft_sc_init(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.sc_init(v0, layout, mem);
+}
+
+int mpdpft_sc_step(mpdpft_ctx* ctx, int graph, mpdpft_iter_log* log) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  int st = ctx->impl.sc_step(graph);
+  if (st || !log) return st;
+  mpdpft::ScState h;
+  if ((st = ctx->impl.read_state(&h))) return st;
+  int idx = h.sc_count - 1;
+  if (idx < 0 || idx >= ctx->impl.log_cap) return MPDPFT_OK;
+  cudaError_t e = cudaMemcpy(log, ctx->impl.d_log + idx, sizeof(mpdpft_iter_log), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, cudaGetErrorString(e));
+  return ctx->impl.status_from_state(h);
+}
+
+int mpdpft_sc_run(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem, mpdpft_result* result,
+                  mpdpft_iter_log* log, int log_cap) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  int st = ctx->impl.sc_init(v0, layout, mem);
+  if (st) return st;
+  return ctx->impl.sc_run(result, log, log_cap, /*use_graph=*/1);
+}
+
+int mpdpft_get_field(mpdpft_ctx* ctx, int which, int s, double* out, int layout, int mem) {
+  CHECK_CTX(ctx);
+  Ctx& c = ctx->impl;
+  if (s < 0 || s >= c.S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  cudaSetDevice(c.device);
+  const size_t off = (size_t)s * c.geom.n * c.rsize;
+  const void* src = nullptr;
+  if (which == MPDPFT_FIELD_DENSITY) {
+    mpdpft::ScState h;
+    int st = c.read_state(&h);
+    if (st) return st;
+    src = (char*)c.d_nin + (size_t)h.slot * c.S * c.geom.n * c.rsize + off;
+  } else if (which == MPDPFT_FIELD_POTENTIAL) {
+    src = (char*)c.d_V + off;
+  } else if (which == MPDPFT_FIELD_EXTERNAL) {
+    src = (char*)c.d_vext + off;
+  } else if (which == MPDPFT_FIELD_GRAD2 && c.d_g2) {
+    src = (char*)c.d_g2 + off;
+  } else if (which == MPDPFT_FIELD_LAPLACIAN && c.d_lap) {
+    src = (char*)c.d_lap + off;
+  } else {
+    return set_error(MPDPFT_ERR_ARG, "field not available");
+  }
+  return c.export_field(src, out, layout, mem);
+}
+
+int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result) {
+  CHECK_CTX(ctx);
+  if (!result) return set_error(MPDPFT_ERR_ARG, "null result");
+  cudaSetDevice(ctx->impl.device);
+  mpdpft::ScState h;
+  int st = ctx->impl.read_state(&h);
+  if (st) return st;
+  std::memset(result, 0, sizeof(*result));
+  return ctx->impl.fill_result(result, h);
+}
+
+}  // extern "C"

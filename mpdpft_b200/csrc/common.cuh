@@ -1,0 +1,186 @@
+// common.cuh -- shared device helpers of the B200 DPFT engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "../../include/mpdpft_gpu.h"
+
+namespace mpdpft {
+
+constexpr double kPi = 3.141592653589793;
+constexpr int kThreads = 256;
+constexpr int kMaxS = MPDPFT_MAX_SPECIES;
+constexpr int kMaxP = MPDPFT_MAX_PULAY;
+constexpr int kMuCand = 16;          // candidates per mu-search pass
+constexpr int kMuMaxPasses = 24;     // device mu-search pass cap
+constexpr int kMaxBlocks = 148 * 8;  // 148 SMs x 8 resident 256-thread blocks
+
+// Device error bits (ScState::status_bits), bit k = mpdpft_status k.
+constexpr int kBitNonfinite = 1 << MPDPFT_ERR_NONFINITE;
+constexpr int kBitBracket = 1 << MPDPFT_ERR_MU_BRACKET;
+constexpr int kBitPulay = 1 << MPDPFT_ERR_PULAY_SINGULAR;
+constexpr int kBitTimeout = 1 << MPDPFT_ERR_TIMEOUT;
+
+inline int grid_blocks(long n) {
+  long b = (n + kThreads - 1) / kThreads;
+  if (b > kMaxBlocks) b = kMaxBlocks;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Geometry of the periodic grid.
+struct Geom {
+  int dim;
+  int s;
+  long n;       // s^dim
+  double L, dx, dk;
+  double dvol;  // dx^dim: trapezoid weight of every periodic point
+};
+
+// Multiplicity of a periodic point in the reference's (s+1)^D storage: plane
+// 0 of every axis is stored twice (mpDPFT.cpp:863), so VecMult over that
+// storage (mpDPFT.cpp:7103-7107) counts it twice.
+__device__ __forceinline__ double ref_multiplicity(long p, int s, int dim) {
+  int k = (int)(p % s);
+  long q = p / s;
+  int j = (int)(q % s);
+  double w = (k == 0 ? 2.0 : 1.0) * (j == 0 ? 2.0 : 1.0);
+  if (dim == 3) {
+    int i = (int)(q / s);
+    w *= (i == 0 ? 2.0 : 1.0);
+  }
+  return w;
+}
+
+__device__ __forceinline__ void point_coords(long p, const Geom& g, double& x, double& y, double& z) {
+  int k = (int)(p % g.s);
+  long q = p / g.s;
+  if (g.dim == 3) {
+    int j = (int)(q % g.s), i = (int)(q / g.s);
+    x = -0.5 * g.L + g.dx * i; y = -0.5 * g.L + g.dx * j; z = -0.5 * g.L + g.dx * k;
+  } else {
+    int i = (int)q;
+    x = -0.5 * g.L + g.dx * i; y = -0.5 * g.L + g.dx * k; z = 0.0;
+  }
+}
+
+// ---------------------------------------------------------- reductions --
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Reduce NV per-thread accumulators over the block; thread t < NV writes
+// the block total of accumulator t to out[t].  Deterministic order.
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[NV], double* out) {
+  __shared__ double sh[32][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // a previous call may still be reading sh
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double t = warp_sum(acc[v]);
+    if (lane == 0) sh[warp][v] = t;
+  }
+  __syncthreads();
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w][v];
+    out[v] = t;
+  }
+}
+
+// Pairwise sum of n partial values (one block, deterministic), returned to
+// every thread of the block.
+__device__ inline double block_sum_partials(const double* part, int n, int stride) {
+  __shared__ double sh[kThreads];
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t += part[(long)i * stride];
+  sh[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------- density functionals --
+// Parameters of n[V] for one species.  Numbering follows DensityExpression.
+struct DensParams {
+  int expr;
+  int dim;
+  double g;        // degeneracy
+  double tau;      // tauVec (TF-inspired)
+  double T;        // temperature (TF-inspired T>0, gradient 2D)
+  double floor_u;  // floor of mu - V in the 3D gradient terms
+  double c2;       // |grad V|^2 coefficient (3D gradient form)
+};
+
+// Pointwise density at u = mu - V (R = float or double arithmetic).
+//  7: GetTFdensity (mpDPFT.cpp:4415-4436)
+//  1/2: GetTFinspireddensity (mpDPFT.cpp:3318-3347)
+//  5: small-gradient branch of getDenEnAt (mpDPFT.cpp:3376-3388): finite-T
+//     form in 2D; its T -> 0 limit in 3D,
+//     n = g (2u)^{3/2}/(6 pi^2) - g sqrt2/(48 pi^2) [lap u^{-1/2} + c2/4 |gradV|^2 u^{-3/2}],
+//     with the singular factors continued linearly to 0 below u = floor.
+template <typename R>
+__device__ __forceinline__ R density_at(const DensParams& d, R u, R lap, R g2) {
+  if (d.expr == MPDPFT_DENS_TF) {
+    if (!(u > R(0))) return R(0);
+    if (d.dim == 3) return R(1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * u * sqrt(u);
+    return R(d.g / (2.0 * kPi)) * u;
+  }
+  if (d.expr == MPDPFT_DENS_TF_INSPIRED) {
+    R t = u / R(d.tau);
+    if (!(t > R(0))) return R(0);
+    if (d.dim == 3) return t * sqrt(t) * R(sqrt(d.tau));
+    return t;
+  }
+  if (d.expr == MPDPFT_DENS_TF_INSPIRED_T) {
+    R pref = R(1.0 / d.tau);
+    R t = u * pref;
+    R t2 = t / R(d.T);
+    if (fabs(t2) < R(40)) return pref * R(d.T) * log(R(1) + exp(t2));
+    if (t2 <= R(-40) || t2 != t2) return R(0);
+    return pref * t;
+  }
+  // MPDPFT_DENS_GRADIENT
+  if (d.dim == 2) {
+    const R tau = R(1.0 / d.T);
+    const R arg = tau * u;  // -tau (V - mu)
+    R zeta, LOG;
+    if (arg > R(700)) zeta = R(0);
+    else zeta = exp(-arg);
+    if (arg < R(-100)) LOG = R(1) / zeta;
+    else if (arg > R(100)) LOG = arg;
+    else LOG = log(R(1) + R(1) / zeta);
+    R opz = R(1) + zeta;
+    R r = R(d.g / (2.0 * kPi)) * (LOG / tau - tau * lap / R(12) * zeta / (opz * opz));
+    return (r != r) ? R(0) : r;
+  }
+  if (!(u > R(0))) return R(0);
+  const R f = R(d.floor_u);
+  R m1, m3;
+  if (u >= f) { m1 = R(1) / sqrt(u); m3 = m1 / u; }
+  else { m1 = u * R(1.0 / (d.floor_u * sqrt(d.floor_u))); m3 = m1 / f; }
+  const R ctf = R(2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi));
+  const R cg = R(1.4142135623730951 * d.g / (48.0 * kPi * kPi));
+  R r = ctf * u * sqrt(u) - cg * (lap * m1 + R(0.25) * R(d.c2) * g2 * m3);
+  return r > R(0) ? r : R(0);
+}
+
+// d n / d mu at u (used to place mu candidates; accuracy is not critical).
+template <typename R>
+__device__ __forceinline__ R density_slope(const DensParams& d, R u) {
+  if (!(u > R(0))) return R(0);
+  if (d.dim == 3) return R(1.5 * 1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * sqrt(u);
+  return R(d.g / (2.0 * kPi));
+}
+
+}  // namespace mpdpft

@@ -1,0 +1,665 @@
+// engine.cu -- host side of the B200 DPFT engine and its C ABI.
+//
+// A context owns every device buffer of one SC solve on one GPU: fields are
+// stored on the periodic s^D grid in the compute precision (double for
+// MPDPFT_FP64, float for MPDPFT_MIXED); the particle-number integrals, the
+// convergence dots, the Pulay Gram matrix and solve, and the energies are
+// accumulated in double in every mode.  All work is issued on the context's
+// stream; the SC iteration is one persistent kernel (plus the FFT kernels for
+// Coulomb and gradient terms) and is replayed as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mpdpft_gpu.h"
+#include "common.cuh"
+#include "engine.h"
+#include "sc_step.cuh"
+
+namespace mpdpft {
+
+thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+#define CU(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return set_error(MPDPFT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------- kernels ----
+template <typename R>
+__global__ void k_import(const double* __restrict__ src, R* __restrict__ dst, Geom g, int layout) {
+  const long n = g.n;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    long q = p;
+    if (layout == MPDPFT_LAYOUT_REFERENCE) {
+      const long el = g.s + 1;
+      int k = (int)(p % g.s);
+      long t = p / g.s;
+      if (g.dim == 3) {
+        int j = (int)(t % g.s), i = (int)(t / g.s);
+        q = ((long)i * el + j) * el + k;
+      } else {
+        q = t * el + k;
+      }
+    }
+    dst[p] = (R)src[q];
+  }
+}
+
+template <typename R>
+__global__ void k_export(const R* __restrict__ src, double* __restrict__ dst, Geom g, int layout) {
+  long total = g.n;
+  const long el = g.s + 1;
+  if (layout == MPDPFT_LAYOUT_REFERENCE) total = (g.dim == 3) ? el * el * el : el * el;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    long p = q;
+    if (layout == MPDPFT_LAYOUT_REFERENCE) {
+      int k = (int)(q % el) % g.s;
+      long t = q / el;
+      if (g.dim == 3) {
+        int j = (int)(t % el) % g.s, i = (int)(t / el) % g.s;
+        p = ((long)i * g.s + j) * g.s + k;
+      } else {
+        p = (t % g.s) * g.s + k;
+      }
+    }
+    dst[q] = (double)src[p];
+  }
+}
+
+// Energy integrands (GetEnergy, mpDPFT.cpp:5414-5436), one block partial per
+// accumulator: per species [0] int (mu-V)_+^{(D+2)/2}, [1] int Vext n,
+// [2] int n^2, [3] int n_+^{1+1/D}, [4] int n vh/2; pairs [16+...] int n_s n_s'.
+constexpr int kNEnergy = 5 * kMaxS + kMaxS * kMaxS;
+template <typename R>
+__global__ void k_energy(Geom g, int S, const R* V, const R* vext, const R* dens, const R* vh,
+                         const double* mu, double* part) {
+  double acc[kNEnergy];
+#pragma unroll
+  for (int j = 0; j < kNEnergy; ++j) acc[j] = 0.0;
+  const long n = g.n;
+  const double ex = 0.5 * (g.dim + 2);
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    for (int s = 0; s < S; ++s) {
+      const long q = (long)s * n + p;
+      double u = mu[s] - (double)V[q];
+      double ns = (double)dens[q];
+      acc[5 * s + 0] += u > 0.0 ? pow(u, ex) : 0.0;
+      acc[5 * s + 1] += (double)vext[q] * ns;
+      acc[5 * s + 2] += ns * ns;
+      acc[5 * s + 3] += ns > 0.0 ? pow(ns, 1.0 + 1.0 / g.dim) : 0.0;
+      if (vh) acc[5 * s + 4] += 0.5 * ns * (double)vh[q];
+      for (int t = s + 1; t < S; ++t) acc[5 * kMaxS + s * kMaxS + t] += ns * (double)dens[(long)t * n + p];
+    }
+  }
+  block_reduce_store<kNEnergy>(acc, part + (long)blockIdx.x * kNEnergy);
+}
+
+template <typename R>
+__global__ void k_integrate(Geom g, const R* f, double* part) {
+  double acc[1] = {0.0};
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x)
+    acc[0] += (double)f[p];
+  block_reduce_store<1>(acc, part + blockIdx.x);
+}
+
+// n[V] at a fixed mu (GetDensity), no reduction.
+template <typename R>
+__global__ void k_density(Geom g, DensParams d, double mu, const R* V, const R* lap, const R* g2, R* out) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x)
+    out[p] = density_at<R>(d, R(mu) - V[p], lap ? lap[p] : R(0), g2 ? g2[p] : R(0));
+}
+
+// ---------------------------------------------------------- the context --
+Ctx::~Ctx() { release(); }
+
+void Ctx::release() {
+  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  for (void* p : allocations) cudaFree(p);
+  allocations.clear();
+  if (pinned) { cudaFreeHost(pinned); pinned = nullptr; }
+  if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
+}
+
+int Ctx::alloc(void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  allocations.push_back(*p);
+  return MPDPFT_OK;
+}
+
+static int check_params(const mpdpft_params& p) {
+  if (p.dim != 2 && p.dim != 3) return set_error(MPDPFT_ERR_ARG, "dim must be 2 or 3");
+  if (p.steps < 4 || (p.steps & 1)) return set_error(MPDPFT_ERR_ARG, "steps must be even and >= 4");
+  if (p.species < 1 || p.species > MPDPFT_MAX_SPECIES) return set_error(MPDPFT_ERR_ARG, "species out of range");
+  if (!(p.edge > 0.0)) return set_error(MPDPFT_ERR_ARG, "edge must be positive");
+  if (p.mixer < 0 || p.mixer > 1) return set_error(MPDPFT_ERR_ARG, "mixer must be 0 (linear) or 1 (Pulay)");
+  if (p.mixer == 1 && (p.pulay_scope < 1 || p.pulay_scope > MPDPFT_MAX_PULAY))
+    return set_error(MPDPFT_ERR_ARG, "pulay_scope out of range");
+  if (p.n_interactions < 0 || p.n_interactions > MPDPFT_MAX_INTERACTIONS)
+    return set_error(MPDPFT_ERR_ARG, "n_interactions out of range");
+  int de = p.density_expression;
+  if (de != MPDPFT_DENS_TF && de != MPDPFT_DENS_TF_INSPIRED && de != MPDPFT_DENS_TF_INSPIRED_T &&
+      de != MPDPFT_DENS_GRADIENT)
+    return set_error(MPDPFT_ERR_ARG, "unsupported density_expression");
+  for (int a = 0; a < p.n_interactions; ++a) {
+    int t = p.interactions[a];
+    if (t != 0 && t != 1 && t != 8 && t != 10 && t != 11 && t != 21 && t != 100)
+      return set_error(MPDPFT_ERR_ARG, "unsupported interaction type " + std::to_string(t));
+    if ((t == 8 || t == 21 || t == 100) && p.dim != 3)
+      return set_error(MPDPFT_ERR_ARG, "Coulomb interactions need dim 3");
+  }
+  if (p.precision != MPDPFT_FP64 && p.precision != MPDPFT_MIXED) return set_error(MPDPFT_ERR_ARG, "bad precision");
+  if (p.max_sc_count < 0) return set_error(MPDPFT_ERR_ARG, "max_sc_count < 0");
+  return MPDPFT_OK;
+}
+
+bool Ctx::has_interaction(int t) const {
+  for (int a = 0; a < P.n_interactions; ++a)
+    if (P.interactions[a] == t) return true;
+  return false;
+}
+
+KParams Ctx::kparams() const {
+  KParams k;
+  std::memset(&k, 0, sizeof(k));
+  k.geom = geom;
+  k.S = P.species;
+  for (int s = 0; s < P.species; ++s) {
+    DensParams& d = k.dens[s];
+    d.expr = P.density_expression;
+    d.dim = P.dim;
+    d.g = P.degeneracy;
+    d.tau = P.tau[s];
+    d.T = temperature[s];
+    d.floor_u = P.gradient_floor;
+    d.c2 = P.gradient_grad2;
+    k.abundance[s] = P.abundances[s];
+    k.charges[s] = P.charges[s];
+  }
+  k.rel_acc = P.rel_acc;
+  k.beta = P.beta;
+  k.gamma_h = P.gamma_h;
+  k.contact_self = has_interaction(MPDPFT_INT_CONTACT_SELF);
+  k.contact_mutual = has_interaction(MPDPFT_INT_CONTACT_MUTUAL);
+  k.dirac = has_interaction(MPDPFT_INT_DIRAC);
+  k.has_coulomb = has_coulomb;
+  k.mixer = P.mixer;
+  k.scope = P.mixer ? P.pulay_scope : 1;
+  k.ring = ring;
+  k.sc_criterion = P.sc_criterion;
+  k.max_sc = P.max_sc_count;
+  k.schedule = P.schedule;
+  k.pot_tol = P.potential_tol;
+  k.inc_v0 = P.incremental_v;
+  return k;
+}
+
+int Ctx::init(const mpdpft_params& params, int dev) {
+  int st = check_params(params);
+  if (st) return st;
+  P = params;
+  device = dev;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(MPDPFT_ERR_NO_DEVICE, "no CUDA device");
+  if (dev < 0 || dev >= ndev) return set_error(MPDPFT_ERR_ARG, "device index out of range");
+  CU(cudaSetDevice(dev));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) return set_error(MPDPFT_ERR_NO_DEVICE, "needs an sm_100 (Blackwell) device");
+  num_sms = prop.multiProcessorCount;
+  CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  geom.dim = P.dim;
+  geom.s = P.steps;
+  geom.n = 1;
+  for (int d = 0; d < P.dim; ++d) geom.n *= P.steps;
+  geom.L = P.edge;
+  geom.dx = P.edge / P.steps;
+  geom.dk = 2.0 * kPi / P.edge;
+  geom.dvol = std::pow(geom.dx, (double)P.dim);
+  n_ref = 1;
+  for (int d = 0; d < P.dim; ++d) n_ref *= (P.steps + 1);
+  rsize = P.precision == MPDPFT_FP64 ? sizeof(double) : sizeof(float);
+  S = P.species;
+  ring = (P.mixer ? P.pulay_scope : 1) + 1;
+  gradient = P.density_expression == MPDPFT_DENS_GRADIENT;
+  has_coulomb = has_interaction(MPDPFT_INT_HARTREE) || has_interaction(MPDPFT_INT_HARTREE_INTER) ||
+                has_interaction(MPDPFT_INT_COULOMB_CHARGED);
+  for (int s = 0; s < S; ++s) temperature[s] = P.temperature[s];
+  const size_t field = (size_t)geom.n * rsize;
+  if ((st = alloc(&d_vext, field * S))) return st;
+  if ((st = alloc(&d_V, field * S))) return st;
+  if ((st = alloc(&d_nin, field * S * ring))) return st;
+  if ((st = alloc(&d_res, field * S * ring))) return st;
+  if ((st = alloc(&d_tmp, field * S))) return st;
+  if (gradient) {
+    if ((st = alloc(&d_lap, field * S))) return st;
+    if ((st = alloc(&d_g2, field * S))) return st;
+  }
+  if (has_coulomb) {
+    if ((st = alloc(&d_vh, field * S))) return st;
+  }
+  if ((st = alloc((void**)&d_io, sizeof(double) * (size_t)std::max(n_ref, geom.n) * 2))) return st;
+  if ((st = alloc((void**)&d_state, sizeof(ScState)))) return st;
+  log_cap = P.max_sc_count + 2;
+  if ((st = alloc((void**)&d_log, sizeof(mpdpft_iter_log) * log_cap))) return st;
+  // persistent-kernel grid: co-resident blocks only
+  int occ = 0;
+  cudaError_t e = P.precision == MPDPFT_FP64
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sc_step_kernel<double>, kStepThreads, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sc_step_kernel<float>, kStepThreads, 0);
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+  if (occ < 1) return set_error(MPDPFT_ERR_CUDA, "step kernel cannot be resident");
+  step_blocks = num_sms * std::min(occ, 2);
+  long useful = (geom.n + kStepThreads - 1) / kStepThreads;
+  if (step_blocks > useful) step_blocks = (int)std::max(1L, useful);
+  part_vals = std::max(kNPart, kNEnergy);
+  if ((st = alloc((void**)&d_part, sizeof(double) * (size_t)std::max(step_blocks, kMaxBlocks) * part_vals))) return st;
+  pinned_bytes = sizeof(double) * (size_t)std::max(n_ref, geom.n) * 2;
+  CU(cudaMallocHost(&pinned, pinned_bytes));
+  CU(cudaMemsetAsync(d_V, 0, field * S, stream));
+  CU(cudaMemsetAsync(d_vext, 0, field * S, stream));
+  CU(cudaMemsetAsync(d_nin, 0, field * S * ring, stream));
+  CU(cudaMemsetAsync(d_res, 0, field * S * ring, stream));
+  CU(cudaMemsetAsync(d_log, 0, sizeof(mpdpft_iter_log) * log_cap, stream));
+  return reset_state();
+}
+
+int Ctx::reset_state() {
+  ScState h;
+  std::memset(&h, 0, sizeof(h));
+  for (int s = 0; s < S; ++s) {
+    h.mu[s] = h.prev_mu[s] = h.old_mu[s] = P.mu[s];
+    h.theta[s] = h.theta0[s] = h.theta_mix[s] = P.theta[s];
+  }
+  h.dmm = P.deltamu_modifier;
+  h.inc_v = P.incremental_v;
+  h.cc = 0.0;
+  h.old_cc = 0.0;  // the reference leaves data.CC indeterminate before iteration 0
+  CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  return MPDPFT_OK;
+}
+
+int Ctx::read_state(ScState* h) {
+  CU(cudaMemcpyAsync(h, d_state, sizeof(ScState), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  return MPDPFT_OK;
+}
+
+// Copy one grid (host or device double pointer, either layout) into the
+// compute-precision device array dst.
+int Ctx::import_field(const double* src, void* dst, int layout, int mem) {
+  if (!src) return set_error(MPDPFT_ERR_ARG, "null input array");
+  const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
+  const double* dsrc = src;
+  if (mem == MPDPFT_MEM_HOST) {
+    std::memcpy(pinned, src, sizeof(double) * cnt);
+    CU(cudaMemcpyAsync(d_io, pinned, sizeof(double) * cnt, cudaMemcpyHostToDevice, stream));
+    dsrc = d_io;
+  }
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double)) k_import<double><<<blocks, kThreads, 0, stream>>>(dsrc, (double*)dst, geom, layout);
+  else k_import<float><<<blocks, kThreads, 0, stream>>>(dsrc, (float*)dst, geom, layout);
+  CU(cudaGetLastError());
+  if (mem == MPDPFT_MEM_HOST) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
+  return MPDPFT_OK;
+}
+
+int Ctx::export_field(const void* src, double* dst, int layout, int mem) {
+  if (!dst) return set_error(MPDPFT_ERR_ARG, "null output array");
+  const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
+  double* ddst = mem == MPDPFT_MEM_HOST ? d_io : dst;
+  const int blocks = grid_blocks(cnt);
+  if (rsize == sizeof(double)) k_export<double><<<blocks, kThreads, 0, stream>>>((const double*)src, ddst, geom, layout);
+  else k_export<float><<<blocks, kThreads, 0, stream>>>((const float*)src, ddst, geom, layout);
+  CU(cudaGetLastError());
+  if (mem == MPDPFT_MEM_HOST) {
+    CU(cudaMemcpyAsync(pinned, d_io, sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    std::memcpy(dst, pinned, sizeof(double) * cnt);
+  }
+  return MPDPFT_OK;
+}
+
+template <typename R>
+StepArgs<R> Ctx::step_args(int mode) {
+  StepArgs<R> a;
+  std::memset(&a, 0, sizeof(a));
+  a.kp = kparams();
+  a.st = d_state;
+  a.vext = (const R*)d_vext;
+  a.V = (R*)d_V;
+  a.lap = gradient ? (const R*)d_lap : nullptr;
+  a.g2 = gradient ? (const R*)d_g2 : nullptr;
+  a.vh = has_coulomb ? (const R*)d_vh : nullptr;
+  a.nin = (R*)d_nin;
+  a.res = (R*)d_res;
+  a.part = d_part;
+  a.vres_part = vres_part_ext;
+  a.vres_blocks = vres_blocks_ext;
+  a.log = d_log;
+  a.log_cap = log_cap;
+  a.assemble_v = assemble_in_step;
+  a.mode = mode;
+  return a;
+}
+
+int Ctx::launch_step(int mode) {
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(step_blocks);
+  cfg.blockDim = dim3(kStepThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  if (rsize == sizeof(double)) e = cudaLaunchKernelEx(&cfg, sc_step_kernel<double>, step_args<double>(mode));
+  else e = cudaLaunchKernelEx(&cfg, sc_step_kernel<float>, step_args<float>(mode));
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("sc_step launch: ") + cudaGetErrorString(e));
+  return MPDPFT_OK;
+}
+
+// Everything of one SC iteration, issued on the stream (graph-capturable).
+int Ctx::issue_iteration() {
+  int st;
+  if (has_coulomb || gradient) {
+    if ((st = issue_fft_terms())) return st;
+  }
+  return launch_step(0);
+}
+
+int Ctx::status_from_state(const ScState& h) {
+  if (h.abort) return set_error(MPDPFT_ERR_TIMEOUT, "grid barrier timed out in the SC step kernel");
+  return MPDPFT_OK;
+}
+
+int Ctx::sc_init(const double* const* v0, int layout, int mem) {
+  int st;
+  if ((st = reset_state())) return st;
+  for (int s = 0; s < S; ++s) {
+    void* dst = (char*)d_V + (size_t)s * geom.n * rsize;
+    if (v0 && v0[s]) {
+      if ((st = import_field(v0[s], dst, layout, mem))) return st;
+    } else {
+      CU(cudaMemcpyAsync(dst, (char*)d_vext + (size_t)s * geom.n * rsize, geom.n * rsize,
+                         cudaMemcpyDeviceToDevice, stream));
+    }
+  }
+  // automatic temperature (PreparationsForSCdensity, mpDPFT.cpp:4523-4528)
+  bool need_t = false;
+  for (int s = 0; s < S; ++s) need_t |= temperature[s] < 0.0;
+  if (need_t) {
+    std::vector<double> h(geom.n);
+    for (int s = 0; s < S; ++s) {
+      if (temperature[s] >= 0.0) continue;
+      if ((st = export_field((char*)d_V + (size_t)s * geom.n * rsize, h.data(), MPDPFT_LAYOUT_PERIODIC, MPDPFT_MEM_HOST))) return st;
+      double vmin = h[0], vmax = h[0];
+      for (double x : h) { vmin = std::min(vmin, x); vmax = std::max(vmax, x); }
+      temperature[s] = std::max(std::fabs(P.mu[s] - vmin), std::fabs(P.mu[s] - vmax)) / 50.0;
+    }
+  }
+  if (gradient) {
+    if ((st = issue_delfield_of_V())) return st;
+  }
+  if ((st = launch_step(1))) return st;  // initial densities (mpDPFT.cpp:195)
+  CU(cudaStreamSynchronize(stream));
+  ScState h;
+  if ((st = read_state(&h))) return st;
+  if ((st = status_from_state(h))) return st;
+  initialised = true;
+  return MPDPFT_OK;
+}
+
+int Ctx::sc_step(int use_graph) {
+  if (!initialised) return set_error(MPDPFT_ERR_ARG, "sc_init has not been called");
+  int st;
+  if (!use_graph) return issue_iteration();
+  if (!graph_exec) {
+    CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    st = issue_iteration();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    graph = g;
+    CU(cudaGraphInstantiate(&graph_exec, graph, 0));
+  }
+  CU(cudaGraphLaunch(graph_exec, stream));
+  return MPDPFT_OK;
+}
+
+int Ctx::sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph) {
+  auto t0 = std::chrono::steady_clock::now();
+  int st;
+  ScState h;
+  const int chunk = 4;
+  int issued = 0;
+  for (;;) {
+    for (int c = 0; c < chunk; ++c, ++issued)
+      if ((st = sc_step(use_graph))) return st;
+    CU(cudaStreamSynchronize(stream));
+    if ((st = read_state(&h))) return st;
+    if ((st = status_from_state(h))) return st;
+    if (h.exit_loop || issued > P.max_sc_count + 2) break;
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  if (result) {
+    std::memset(result, 0, sizeof(*result));
+    if ((st = fill_result(result, h))) return st;
+    result->seconds = std::chrono::duration<double>(t1 - t0).count();
+  }
+  if (log && cap > 0) {
+    int nlog = std::min(cap, std::min(h.sc_count, log_cap));
+    CU(cudaMemcpy(log, d_log, sizeof(mpdpft_iter_log) * nlog, cudaMemcpyDeviceToHost));
+  }
+  if (h.status_bits & kBitTimeout) return set_error(MPDPFT_ERR_TIMEOUT, "mu search reached its pass cap");
+  if (!h.exit_loop || h.exit_count < 3) return set_error(MPDPFT_ERR_NOT_CONVERGED, "maxSCcount reached");
+  return MPDPFT_OK;
+}
+
+int Ctx::fill_result(mpdpft_result* r, const ScState& h) {
+  r->iterations = h.sc_count;
+  r->converged = h.exit_count >= 3 ? 1 : 0;
+  r->total_mu_trials = h.mu_passes_total;
+  r->cc = h.cc;
+  r->v_residual = h.v_res;
+  for (int s = 0; s < S; ++s) { r->mu[s] = h.mu[s]; r->abundance[s] = h.ab[s]; }
+  return energy(r, h);
+}
+
+// Energies of the current state (GetEnergy, mpDPFT.cpp:5414-5436): the
+// densities are the mixed densities of the last iteration, V and mu those
+// of the last density evaluation, as in the reference's ExportData.
+int Ctx::energy(mpdpft_result* r, const ScState& h) {
+  int st;
+  double* d_mu = d_io;  // scratch
+  CU(cudaMemcpyAsync(d_mu, h.mu, sizeof(double) * kMaxS, cudaMemcpyHostToDevice, stream));
+  const void* dens = (char*)d_nin + (size_t)h.slot * S * geom.n * rsize;
+  if (has_coulomb) {
+    if ((st = issue_coulomb(dens, d_vh, /*for_energy=*/1))) return st;
+  }
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double))
+    k_energy<double><<<blocks, kThreads, 0, stream>>>(geom, S, (const double*)d_V, (const double*)d_vext,
+                                                       (const double*)dens, has_coulomb ? (const double*)d_vh : nullptr,
+                                                       d_mu, d_part);
+  else
+    k_energy<float><<<blocks, kThreads, 0, stream>>>(geom, S, (const float*)d_V, (const float*)d_vext,
+                                                     (const float*)dens, has_coulomb ? (const float*)d_vh : nullptr,
+                                                     d_mu, d_part);
+  CU(cudaGetLastError());
+  std::vector<double> hp((size_t)blocks * kNEnergy);
+  CU(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  double E[kNEnergy] = {0};
+  for (int b = 0; b < blocks; ++b)
+    for (int j = 0; j < kNEnergy; ++j) E[j] += hp[(size_t)b * kNEnergy + j];
+  for (int j = 0; j < kNEnergy; ++j) E[j] *= geom.dvol;
+  const double D = P.dim;
+  double etot = 0.0;
+  for (int a = 0; a < P.n_interactions; ++a) {
+    const int t = P.interactions[a];
+    double e = 0.0;
+    if (t == MPDPFT_INT_CONTACT_MUTUAL) {
+      for (int s = 0; s < S; ++s)
+        for (int q = s + 1; q < S; ++q) e += E[5 * kMaxS + s * kMaxS + q];
+      e *= P.beta;
+    } else if (t == MPDPFT_INT_CONTACT_SELF) {
+      e = P.beta * E[2];
+    } else if (t == MPDPFT_INT_HARTREE || t == MPDPFT_INT_HARTREE_INTER || t == MPDPFT_INT_COULOMB_CHARGED) {
+      for (int s = 0; s < S; ++s) e += E[5 * s + 4];
+    } else if (t == MPDPFT_INT_DIRAC) {
+      const double cXD = 2.0 * std::sqrt(4.0 * kPi) / ((D - 1.0) * kPi) *
+                         std::pow(0.5 * std::pow(0.75 * std::sqrt(kPi), D - 2.0), 1.0 / D);
+      for (int s = 0; s < S; ++s) e += -P.gamma_h * cXD * D / (1.0 + D) * E[5 * s + 3];
+    }
+    r->e_interaction[a] = e;
+    etot += e;
+  }
+  const double AF = P.dim == 2 ? 2.0 * kPi : 4.0 * kPi;
+  for (int s = 0; s < S; ++s) {
+    double ekin;
+    if (P.dim == 2 && (P.density_expression == MPDPFT_DENS_TF_INSPIRED ||
+                       P.density_expression == MPDPFT_DENS_TF_INSPIRED_T))
+      ekin = 0.5 * P.tau[s] * E[5 * s + 2];
+    else
+      ekin = P.degeneracy * AF * std::pow(2.0, (D + 2.0) / 2.0) / (std::pow(2.0 * kPi, D) * (2.0 * D + 4.0)) *
+             E[5 * s + 0];
+    r->e_kinetic[s] = ekin;
+    r->e_external[s] = E[5 * s + 1];
+    etot += ekin + E[5 * s + 1];
+  }
+  r->e_total = etot;
+  return MPDPFT_OK;
+}
+
+// -------------------------------------------------- standalone operators --
+int Ctx::op_mu_search(int s, const double* v, double target, double* mu_io, double* ab_out, int* trials,
+                      double* n_out, int layout, int mem) {
+  if (s < 0 || s >= S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  int st;
+  if ((st = reset_state())) return st;
+  // the kernel searches every species; others get their own target N from
+  // P and the same V, which is harmless (only species s is reported)
+  for (int q = 0; q < S; ++q)
+    if ((st = import_field(v, (char*)d_V + (size_t)q * geom.n * rsize, layout, mem))) return st;
+  ScState h;
+  if ((st = read_state(&h))) return st;
+  for (int q = 0; q < S; ++q) h.mu[q] = *mu_io;
+  P.abundances[s] = target;
+  CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  if (gradient && (st = issue_delfield_of_V())) return st;
+  if ((st = launch_step(1))) return st;
+  CU(cudaStreamSynchronize(stream));
+  if ((st = read_state(&h))) return st;
+  if ((st = status_from_state(h))) return st;
+  *mu_io = h.mu[s];
+  if (ab_out) *ab_out = h.ab[s];
+  if (trials) *trials = h.mu_passes;
+  if (n_out) {
+    const void* src = (char*)d_nin + ((size_t)h.slot * S + s) * geom.n * rsize;
+    if ((st = export_field(src, n_out, layout, mem))) return st;
+  }
+  if (h.status_bits & kBitBracket) return set_error(MPDPFT_ERR_MU_BRACKET, "mu bracket not found; mu reset");
+  if (h.status_bits & kBitTimeout) return set_error(MPDPFT_ERR_TIMEOUT, "mu search reached its pass cap");
+  return MPDPFT_OK;
+}
+
+int Ctx::op_density(int s, const double* v, double mu, double* n_out, double* ab_out, int layout, int mem) {
+  if (s < 0 || s >= S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  int st;
+  void* Vs = (char*)d_V + (size_t)s * geom.n * rsize;
+  if ((st = import_field(v, Vs, layout, mem))) return st;
+  if (gradient && (st = issue_delfield_of_V())) return st;
+  DensParams d = kparams().dens[s];
+  const int blocks = grid_blocks(geom.n);
+  void* lap = gradient ? (char*)d_lap + (size_t)s * geom.n * rsize : nullptr;
+  void* g2 = gradient ? (char*)d_g2 + (size_t)s * geom.n * rsize : nullptr;
+  if (rsize == sizeof(double))
+    k_density<double><<<blocks, kThreads, 0, stream>>>(geom, d, mu, (const double*)Vs, (const double*)lap,
+                                                        (const double*)g2, (double*)d_tmp);
+  else
+    k_density<float><<<blocks, kThreads, 0, stream>>>(geom, d, mu, (const float*)Vs, (const float*)lap,
+                                                      (const float*)g2, (float*)d_tmp);
+  CU(cudaGetLastError());
+  if (ab_out && (st = integrate_device(d_tmp, ab_out))) return st;
+  if (n_out && (st = export_field(d_tmp, n_out, layout, mem))) return st;
+  return MPDPFT_OK;
+}
+
+int Ctx::integrate_device(const void* f, double* out) {
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double)) k_integrate<double><<<blocks, kThreads, 0, stream>>>(geom, (const double*)f, d_part);
+  else k_integrate<float><<<blocks, kThreads, 0, stream>>>(geom, (const float*)f, d_part);
+  CU(cudaGetLastError());
+  std::vector<double> hp(blocks);
+  CU(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * blocks, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  double t = 0.0;
+  for (double x : hp) t += x;
+  *out = t * geom.dvol;
+  return MPDPFT_OK;
+}
+
+int Ctx::op_integrate(const double* f, double* out, int layout, int mem) {
+  int st;
+  if ((st = import_field(f, d_tmp, layout, mem))) return st;
+  return integrate_device(d_tmp, out);
+}
+
+int Ctx::op_admix(const double* const* n_in, const double* const* n_out, const double* theta, double* const* n_mixed,
+                  double* coeffs, int* ncoeff, int layout, int mem) {
+  int st;
+  ScState h;
+  if ((st = read_state(&h))) return st;
+  const int cur = h.slot;
+  for (int s = 0; s < S; ++s) {
+    void* dst = (char*)d_nin + ((size_t)cur * S + s) * geom.n * rsize;
+    if ((st = import_field(n_in[s], dst, layout, mem))) return st;
+    void* dv = (char*)d_V + (size_t)s * geom.n * rsize;  // n_out staged in V
+    if ((st = import_field(n_out[s], dv, layout, mem))) return st;
+    if (theta) { h.theta[s] = theta[s]; }
+  }
+  h.ab[0] = h.ab[0];
+  CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  admix_only = true;
+  st = launch_step(2);
+  admix_only = false;
+  if (st) return st;
+  CU(cudaStreamSynchronize(stream));
+  if ((st = read_state(&h))) return st;
+  if ((st = status_from_state(h))) return st;
+  for (int s = 0; s < S; ++s) {
+    const void* src = (char*)d_nin + ((size_t)h.slot * S + s) * geom.n * rsize;
+    if ((st = export_field(src, n_mixed[s], layout, mem))) return st;
+  }
+  if (ncoeff) *ncoeff = h.ncoeff;
+  if (coeffs)
+    for (int i = 0; i < h.ncoeff; ++i) coeffs[i] = h.coeff[i];
+  if (h.iter_bits & kBitPulay) return set_error(MPDPFT_ERR_PULAY_SINGULAR, "Pulay Gram matrix rejected; linear mixing");
+  return MPDPFT_OK;
+}
+
+}  // namespace mpdpft

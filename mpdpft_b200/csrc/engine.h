@@ -1,0 +1,108 @@
+// engine.h -- the context object behind the C ABI (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mpdpft_gpu.h"
+#include "common.cuh"
+#include "sc_step.cuh"
+
+namespace mpdpft {
+
+int set_error(int status, const std::string& msg);
+extern thread_local std::string g_last_error;
+
+struct FftPlan;  // fft.cu
+
+struct Ctx {
+  mpdpft_params P;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  Geom geom;
+  long n_ref = 0;
+  size_t rsize = 8;
+  int S = 1;
+  int ring = 2;
+  bool gradient = false;
+  int has_coulomb = 0;
+  double temperature[kMaxS];
+  bool initialised = false;
+  bool admix_only = false;
+
+  // device buffers (compute precision unless noted)
+  void* d_vext = nullptr;  // [S][n]
+  void* d_V = nullptr;     // [S][n]
+  void* d_nin = nullptr;   // [ring][S][n]
+  void* d_res = nullptr;   // [ring][S][n]
+  void* d_tmp = nullptr;   // [S][n]
+  void* d_lap = nullptr;   // [S][n]
+  void* d_g2 = nullptr;    // [S][n]
+  void* d_vh = nullptr;    // [S][n] Coulomb terms of V
+  double* d_io = nullptr;  // staging, double
+  double* d_part = nullptr;
+  int part_vals = 0;
+  ScState* d_state = nullptr;
+  mpdpft_iter_log* d_log = nullptr;
+  int log_cap = 0;
+  int step_blocks = 0;
+  int assemble_in_step = 1;
+  const double* vres_part_ext = nullptr;
+  int vres_blocks_ext = 0;
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  std::vector<void*> allocations;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  FftPlan* fft = nullptr;
+
+  ~Ctx();
+  void release();
+  int alloc(void** p, size_t bytes);
+  int init(const mpdpft_params& params, int dev);
+  int reset_state();
+  int read_state(ScState* h);
+  int status_from_state(const ScState& h);
+  bool has_interaction(int t) const;
+  KParams kparams() const;
+  int import_field(const double* src, void* dst, int layout, int mem);
+  int export_field(const void* src, double* dst, int layout, int mem);
+  template <typename R>
+  StepArgs<R> step_args(int mode);
+  int launch_step(int mode);
+  int issue_iteration();
+  int sc_init(const double* const* v0, int layout, int mem);
+  int sc_step(int use_graph);
+  int sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph);
+  int fill_result(mpdpft_result* r, const ScState& h);
+  int energy(mpdpft_result* r, const ScState& h);
+  int integrate_device(const void* f, double* out);
+  // standalone operators
+  int op_mu_search(int s, const double* v, double target, double* mu_io, double* ab_out, int* trials,
+                   double* n_out, int layout, int mem);
+  int op_density(int s, const double* v, double mu, double* n_out, double* ab_out, int layout, int mem);
+  int op_integrate(const double* f, double* out, int layout, int mem);
+  int op_admix(const double* const* n_in, const double* const* n_out, const double* theta, double* const* n_mixed,
+               double* coeffs, int* ncoeff, int layout, int mem);
+  // FFT-based terms (fft.cu)
+  int fft_setup();
+  void fft_release();
+  int issue_fft_terms();                      // Coulomb terms + V assembly + DelField(V)
+  int issue_coulomb(const void* dens, void* out, int for_energy);
+  int issue_delfield_of_V();
+  int op_vint(int type, int s, const double* const* n, double* v_out, int layout, int mem);
+  int op_update_v(const double* const* n, double incremental, double* const* v_out, int layout, int mem);
+  int op_delfield(const double* f, double* grad2, double* lap, int layout, int mem);
+  int op_fft(int sign, const double* in, double* out, int mem);
+  // helpers (fft.cu)
+  int scale_copy(const void* src, void* dst, double a);
+  int axpy(const void* x, void* y, double a, int accumulate);
+  int copy_current_density();
+  int pointwise_vint(int type, int s, void* out);
+  int full_c2c(void* buf, int sign);
+  int alloc_io(long doubles);
+};
+
+}  // namespace mpdpft

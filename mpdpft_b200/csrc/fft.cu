@@ -1,0 +1,1153 @@
+// fft.cu -- FFT kernels and the FFT-based operators of the engine:
+// Coulomb (Hartree) potentials, DelField (spectral gradient, Laplacian and
+// Gaussian smoothing with the boundary taper) and the reference-convention
+// complex transform of fftParallel.
+//
+// A D-dimensional real transform is split into passes over global memory:
+//   Z  R2C along the contiguous axis (s reals -> s/2+1 complex per row), with
+//      a fused prologue (taper, species charge sum) and the row sums needed
+//      for the k = 0 mode;
+//   Y  C2C along y (3D only), in place, batched over fields;
+//   X  C2C along x as a round trip: forward FFT, k-space multiplier(s),
+//      inverse FFT, without leaving shared memory;
+//   Y  inverse, then Z C2R with a fused epilogue (|grad f|^2 + Laplacian,
+//      positivity clamp, Coulomb compensation term).
+// The half spectrum is stored [x][y][kz], kz = 0..s/2.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "fft.cuh"
+
+namespace mpdpft {
+
+#define CU(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return set_error(MPDPFT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kFftThreads = 256;
+
+// ------------------------------------------------------------ plan ------
+static bool factor(int len, RadixPlan& p) {
+  p.len = len;
+  p.n = 0;
+  int m = len;
+  while (m % 4 == 0 && p.n < kMaxRadixStages) { p.r[p.n++] = 4; m /= 4; }
+  while (m % 2 == 0 && p.n < kMaxRadixStages) { p.r[p.n++] = 2; m /= 2; }
+  while (m % 3 == 0 && p.n < kMaxRadixStages) { p.r[p.n++] = 3; m /= 3; }
+  return m == 1;
+}
+
+struct FftPlan {
+  int dim, s, M, H;     // M = s/2, H = s/2 + 1
+  long rows;            // s^{dim-1} rows of the contiguous axis
+  long nspec;           // complex elements of one half spectrum
+  RadixPlan plan_s, plan_m;
+  void* tw_s_f = nullptr;  // forward / inverse twiddles of length s (compute precision)
+  void* tw_s_b = nullptr;
+  void* tw_m_f = nullptr;  // of length M
+  void* tw_m_b = nullptr;
+  void* tw_n_f = nullptr;  // e^{-2 pi i q/s}, q < s  (R2C split)
+  int zl;                  // rows per block in the Z passes
+  int tk;                  // lines per tile in the Y/X passes
+  void* spec[4] = {nullptr, nullptr, nullptr, nullptr};  // half spectra
+  void* rtmp = nullptr;    // real scratch field
+  double* zpart = nullptr; // per-block sums of the Z pass input
+  int zblocks = 0;
+  unsigned long long* vmax = nullptr;  // ordered-bits max of the taper shell
+  double* vres_part = nullptr;         // V assembly |dV|^2 partials
+  int vblocks = 0;
+  void* cbuf = nullptr;    // complex s^D field for the fftParallel op
+};
+
+// --------------------------------------------------- ordered max of doubles --
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
+  b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+  return __longlong_as_double((long long)b);
+}
+
+// ---------------------------------------------------------- prologues ----
+enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
+enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3 };
+enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3 };
+
+template <typename R>
+struct ZArgs {
+  Geom g;
+  int M, H, zl;
+  long rows;
+  RadixPlan plan;
+  const typename Cx<R>::T* tw_m;  // length-M table (forward for R2C, inverse for C2R)
+  const typename Cx<R>::T* tw_n;  // e^{-2 pi i q/s}
+  // R2C
+  const R* in;                    // real input [nsrc][n] (PRO_CHARGE sums nsrc)
+  int nsrc;
+  double qcoef[kMaxS];
+  int pro;
+  double taper_r0, taper_a;       // taper: r > r0 -> * exp(a (r - r0)^2)
+  const unsigned long long* vmax; // shift for the taper
+  typename Cx<R>::T* out;         // half spectrum
+  double* part;                   // per-block input sums (may be null)
+  // C2R
+  const typename Cx<R>::T* cin[4];
+  int nin;
+  int epi;
+  R* rout[2];
+  double scale;
+  double coul_coef;               // Coulomb epilogue: out = coef (x + f0 erf(r/2)/(4 pi r))
+  const double* f0_part;          // Z-pass partials giving f0 = dvol * sum(input)
+  int f0_blocks;
+};
+
+// R2C along the contiguous axis.  Block = zl rows; each row of s reals is
+// read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
+// into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
+template <typename R>
+__global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
+  using C = typename Cx<R>::T;
+  extern __shared__ unsigned char smem_raw[];
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + a.M * a.zl;
+  const long row0 = (long)blockIdx.x * a.zl;
+  const int s = a.g.s;
+  double shift = 0.0;  // no shell points: no shift
+  if (a.pro == PRO_TAPER && *a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
+  double rowsum = 0.0;
+  for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
+    const int l = w / a.M, m = w % a.M;
+    const long row = row0 + l;
+    C z = {R(0), R(0)};
+    if (row < a.rows) {
+      const long p0 = row * s + 2 * m;
+      R x0, x1;
+      if (a.pro == PRO_CHARGE) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int q = 0; q < a.nsrc; ++q) {
+          t0 += a.qcoef[q] * (double)a.in[(long)q * a.g.n + p0];
+          t1 += a.qcoef[q] * (double)a.in[(long)q * a.g.n + p0 + 1];
+        }
+        x0 = R(t0); x1 = R(t1);
+      } else {
+        x0 = a.in[p0];
+        x1 = a.in[p0 + 1];
+      }
+      if (a.pro == PRO_TAPER) {  // DelField boundary taper (mpDPFT.cpp:7251-7264)
+        double x, y, zc;
+        point_coords(p0, a.g, x, y, zc);
+        double r2a = x * x + y * y, za = zc, zb = zc + a.g.dx;
+        double ra = sqrt(r2a + za * za), rb = sqrt(r2a + zb * zb);
+        double fa = (double)x0 - shift, fb = (double)x1 - shift;
+        if (ra > a.taper_r0) fa *= exp(a.taper_a * (ra - a.taper_r0) * (ra - a.taper_r0));
+        if (rb > a.taper_r0) fb *= exp(a.taper_a * (rb - a.taper_r0) * (rb - a.taper_r0));
+        x0 = R(fa); x1 = R(fb);
+      }
+      rowsum += (double)x0 + (double)x1;
+      z = {x0, x1};
+    }
+    A[m * a.zl + l] = z;
+  }
+  if (a.part) {
+    double acc[1] = {rowsum};
+    block_reduce_store<1>(acc, a.part + blockIdx.x);
+  }
+  __syncthreads();
+  C* Z = tile_fft<C>(A, B, a.plan, a.zl, a.tw_m, -1);
+  for (int w = threadIdx.x; w < a.H * a.zl; w += blockDim.x) {
+    const int l = w / a.H, q = w % a.H;
+    const long row = row0 + l;
+    if (row >= a.rows) continue;
+    C zq = Z[(q % a.M) * a.zl + l];
+    C zc = cconj(Z[((a.M - q) % a.M) * a.zl + l]);
+    C E = cscale(cadd(zq, zc), R(0.5));
+    C D = csub(zq, zc);             // 2 i O_q
+    C O = {D.y * R(0.5), -D.x * R(0.5)};
+    C t = a.tw_n[q];               // e^{-2 pi i q/s}, q <= M < s
+    a.out[row * a.H + q] = cadd(E, cmul(t, O));
+  }
+}
+
+// C2R along the contiguous axis for nin half-spectrum rows, with epilogue.
+template <typename R>
+__global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
+  using C = typename Cx<R>::T;
+  extern __shared__ unsigned char smem_raw[];
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + a.M * a.zl;
+  R* acc = reinterpret_cast<R*>(B + a.M * a.zl);  // [zl][s]
+  const long row0 = (long)blockIdx.x * a.zl;
+  const int s = a.g.s;
+  double f0 = 0.0;
+  if (a.epi == EPI_COULOMB) {
+    double t = 0.0;
+    for (int b = 0; b < a.f0_blocks; ++b) t += a.f0_part[b];
+    f0 = t * a.g.dvol;
+  }
+  for (int f = 0; f < a.nin; ++f) {
+    const C* X = a.cin[f];
+    for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
+      const int l = w / a.M, q = w % a.M;
+      const long row = row0 + l;
+      C z = {R(0), R(0)};
+      if (row < a.rows) {
+        C xq = X[row * a.H + q];
+        C xc = cconj(X[row * a.H + (a.M - q)]);
+        C E = cadd(xq, xc);   // 2 E_q
+        C D = csub(xq, xc);   // 2 e^{-2 pi i q/s} O_q
+        C t = cconj(a.tw_n[q]);
+        C O = cmul(t, D);     // 2 O_q
+        z = {E.x - O.y, E.y + O.x};  // 2 (E_q + i O_q)
+      }
+      A[q * a.zl + l] = z;
+    }
+    __syncthreads();
+    C* Z = tile_fft<C>(A, B, a.plan, a.zl, a.tw_m, +1);
+    for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
+      const int l = w / a.M, m = w % a.M;
+      C z = Z[m * a.zl + l];
+      R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
+      R* dst = acc + (long)l * s + 2 * m;
+      if (a.epi == EPI_GRAD) {
+        if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
+        else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
+        else {
+          const long row = row0 + l;
+          if (row < a.rows) {
+            a.rout[0][row * s + 2 * m] = dst[0];
+            a.rout[0][row * s + 2 * m + 1] = dst[1];
+            a.rout[1][row * s + 2 * m] = x0;
+            a.rout[1][row * s + 2 * m + 1] = x1;
+          }
+        }
+      } else {
+        dst[0] = x0;
+        dst[1] = x1;
+      }
+    }
+    __syncthreads();
+  }
+  if (a.epi == EPI_GRAD) return;
+  for (int w = threadIdx.x; w < s * a.zl; w += blockDim.x) {
+    const int l = w / s, k = w % s;
+    const long row = row0 + l;
+    if (row >= a.rows) continue;
+    const long p = row * s + k;
+    R v = acc[(long)l * s + k];
+    if (a.epi == EPI_POS) {
+      v = v > R(0) ? v : R(0);
+    } else if (a.epi == EPI_COULOMB) {  // mpDPFT.cpp:2704-2711
+      double x, y, z;
+      point_coords(p, a.g, x, y, z);
+      double r = sqrt(x * x + y * y + z * z);
+      double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
+      v = R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
+    }
+    a.rout[0][p] = v;
+  }
+}
+
+// Y or X pass arguments.  Lines run along an axis of stride `astride`
+// (complex elements); a line is identified by (outer, col) with base
+// outer * ostride + col, col in [0, H).  Blocks [0, nbulk) take tk adjacent
+// columns of one outer index; the remaining blocks take the Nyquist column
+// col = M of tk consecutive outer indices.
+template <typename R>
+struct AxisArgs {
+  int s, M, H, tk, dim;
+  long nouter, ostride, astride;
+  int ntile;   // column tiles per outer index (M / tk)
+  long nbulk;  // nouter * ntile
+  RadixPlan plan;
+  const typename Cx<R>::T* twf;
+  const typename Cx<R>::T* twb;
+  typename Cx<R>::T* data[4];  // Y pass: per field (blockIdx.y); X pass: input in data[0]
+  int dir;                     // Y pass direction
+  // X round trip
+  int nout;
+  typename Cx<R>::T* out[4];
+  int mul;
+  double sigma_c;       // Gaussian smoothing exponent (k^2 multiplier)
+  double scale;         // 1 / s^D
+  double dk;
+  double cutoff;        // truncated Coulomb radius
+  const double* f0_part;  // Z-pass input sums (Coulomb, k = 0 mode)
+  int f0_blocks;
+};
+
+template <typename R>
+__device__ __forceinline__ bool axis_line(const AxisArgs<R>& a, int l, long& base, long& outer, int& col) {
+  const long b = blockIdx.x;
+  if (b < a.nbulk) {
+    outer = b / a.ntile;
+    col = (int)(b % a.ntile) * a.tk + l;
+  } else {
+    outer = (b - a.nbulk) * a.tk + l;
+    col = a.M;
+    if (l > 0 && a.nouter == 1) return false;
+  }
+  if (outer >= a.nouter) return false;
+  base = outer * a.ostride + col;
+  return true;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
+  using C = typename Cx<R>::T;
+  extern __shared__ unsigned char smem_raw[];
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + a.s * a.tk;
+  C* data = a.data[blockIdx.y];
+  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
+    const int t = w / a.tk, l = w % a.tk;
+    long base, outer;
+    int col;
+    C v = {R(0), R(0)};
+    if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+    A[t * a.tk + l] = v;
+  }
+  __syncthreads();
+  C* res = tile_fft<C>(A, B, a.plan, a.tk, a.dir < 0 ? a.twf : a.twb, a.dir);
+  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
+    const int t = w / a.tk, l = w % a.tk;
+    long base, outer;
+    int col;
+    if (axis_line(a, l, base, outer, col)) data[base + t * a.astride] = res[t * a.tk + l];
+  }
+}
+
+// Signed frequency of stored index t of a length-s axis: t < s/2 -> t,
+// else t - s.  The reference's k grid runs over -s/2 .. s/2 - 1, so the
+// Nyquist index s/2 carries k = -pi/dx (mpDPFT.cpp:889-895).
+__device__ __forceinline__ int signed_freq(int t, int s) { return t < s / 2 ? t : t - s; }
+
+template <typename R>
+__global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
+  using C = typename Cx<R>::T;
+  extern __shared__ unsigned char smem_raw[];
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + a.s * a.tk;
+  C* W = B + a.s * a.tk;
+  __shared__ double s_f0;
+  if (a.mul == MUL_COULOMB_REG) {
+    if (threadIdx.x < 32) {
+      double t = 0.0;
+      for (int b = threadIdx.x; b < a.f0_blocks; b += 32) t += a.f0_part[b];
+      t = warp_sum(t);
+      if (threadIdx.x == 0) s_f0 = t;  // unnormalised k = 0 mode: sum of the input
+    }
+  }
+  C* data = a.data[0];
+  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
+    const int t = w / a.tk, l = w % a.tk;
+    long base, outer;
+    int col;
+    C v = {R(0), R(0)};
+    if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+    A[t * a.tk + l] = v;
+  }
+  __syncthreads();
+  C* F = tile_fft<C>(A, B, a.plan, a.tk, a.twf, -1);
+  C* spare = (F == A) ? B : A;  // two free buffers: spare and W
+  for (int o = 0; o < a.nout; ++o) {
+    for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
+      const int t = w / a.tk, l = w % a.tk;
+      long base, outer;
+      int col;
+      C v = F[t * a.tk + l];
+      if (!axis_line(a, l, base, outer, col)) { spare[t * a.tk + l] = v; continue; }
+      const int qx = signed_freq(t, a.s);
+      const int qy = a.dim == 3 ? signed_freq((int)outer, a.s) : 0;
+      const int qz = col;  // 0..M; M is the Nyquist column
+      const double kx = a.dk * (t == a.s / 2 ? -(double)(a.s / 2) : (double)qx);
+      const double ky = a.dk * (double)qy;
+      const double kz = a.dk * (col == a.M ? -(double)a.M : (double)qz);
+      const double k2 = kx * kx + ky * ky + (a.dim == 3 ? kz * kz : 0.0);
+      double fr = 0.0;  // real multiplier
+      bool imag = false;
+      if (a.mul == MUL_COULOMB_REG) {
+        // (n~ - n~0 e^{-k^2})/k^2, k = 0 -> n~0 (mpDPFT.cpp:2686-2701); the
+        // centred transform's phase (-1)^{qx+qy+qz} carries over to the
+        // subtracted Gaussian in this frame
+        if (k2 > 1.0e-6 * a.dk * a.dk) {
+          const int par = ((t + (int)outer * (a.dim == 3) + col) & 1);
+          const double g = exp(-k2) * s_f0 * (par ? -1.0 : 1.0);
+          v = {R(((double)v.x - g) / k2 * a.scale), R((double)v.y / k2 * a.scale)};
+        } else {
+          v = {R(s_f0 * a.scale), R(0)};
+        }
+        spare[t * a.tk + l] = v;
+        continue;
+      } else if (a.mul == MUL_COULOMB_TRUNC) {
+        fr = k2 > 0.0 ? (1.0 - cos(sqrt(k2) * a.cutoff)) / k2 : 0.5 * a.cutoff * a.cutoff;
+      } else if (a.mul == MUL_SMOOTH) {
+        fr = exp(a.sigma_c * k2);
+      } else {  // MUL_DERIV: outputs d/dx, d/dy, d/dz (or 2D: d/dx, d/dy), Laplacian
+        const double sm = exp(a.sigma_c * k2);
+        const int nd = a.dim;
+        if (o < nd) {
+          // i k_j: the reference takes Im of IFT(-k f~), which drops the
+          // Nyquist index of axis j (mpDPFT.cpp:7442-7444)
+          double kj;
+          if (a.dim == 3) kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (o == 1 ? ((int)outer == a.s / 2 ? 0.0 : ky) : (col == a.M ? 0.0 : kz));
+          else kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (col == a.M ? 0.0 : kz);
+          fr = kj * sm;
+          imag = true;
+        } else {
+          fr = -k2 * sm * sm;  // Laplacian smoothed twice (mpDPFT.cpp:7477, 7577)
+        }
+      }
+      fr *= a.scale;
+      if (imag) v = {R(-fr * (double)v.y), R(fr * (double)v.x)};
+      else v = {R(fr * (double)v.x), R(fr * (double)v.y)};
+      spare[t * a.tk + l] = v;
+    }
+    __syncthreads();
+    C* res = tile_fft<C>(spare, W, a.plan, a.tk, a.twb, +1);
+    C* dst = a.out[o];
+    for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
+      const int t = w / a.tk, l = w % a.tk;
+      long base, outer;
+      int col;
+      if (axis_line(a, l, base, outer, col)) dst[base + t * a.astride] = res[t * a.tk + l];
+    }
+    __syncthreads();
+  }
+}
+
+// V assembly (UpdateV, mpDPFT.cpp:4815-4838) when Coulomb terms exist:
+// V_s = Vext_s + incV (vh_s + contact + Dirac); partial sums of |dV|^2 and
+// the maximum of V over the taper shell (DelField, mpDPFT.cpp:7253-7259).
+template <typename R>
+__global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const R* vh, const R* nin_ring, R* V,
+                             double* vres_part, unsigned long long* vmax, double shell_r, double shell_w) {
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  if (__ldcg(&st->exit_loop)) return;
+  const int cur = __ldcg(&st->slot);
+  const double incv = __ldcg(&st->inc_v);
+  const double fac = incv < 1.0 ? incv : 1.0;
+  const R* nin = nin_ring + (long)cur * S * n;
+  double acc[kMaxS];
+  for (int s = 0; s < kMaxS; ++s) acc[s] = 0.0;
+  double vm = -1.0e300;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    double x, y, z;
+    point_coords(p, kp.geom, x, y, z);
+    const bool shell = fabs(sqrt(x * x + y * y + z * z) - shell_r) < shell_w;
+    for (int s = 0; s < S; ++s) {
+      R vi = vh ? vh[(long)s * n + p] : R(0);
+      if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];
+      if (kp.contact_mutual) {
+        R t = R(0);
+        for (int q = 0; q < S; ++q)
+          if (q != s) t += nin[(long)q * n + p];
+        vi += R(kp.beta) * t;
+      }
+      if (kp.dirac) {
+        R ns = nin[(long)s * n + p];
+        ns = ns > R(0) ? ns : R(0);
+        if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+        else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+      }
+      R vnew = vext[(long)s * n + p] + R(fac) * vi;
+      double d = (double)vnew - (double)V[(long)s * n + p];
+      acc[s] += d * d;
+      V[(long)s * n + p] = vnew;
+      if (s == 0 && shell) vm = fmax(vm, (double)vnew);
+    }
+  }
+  block_reduce_store<kMaxS>(acc, vres_part + (long)blockIdx.x * kMaxS);
+  // block max -> global ordered max (order independent, so deterministic)
+  __shared__ double sm[32];
+  double t = vm;
+  for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = sm[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, sm[w]);
+    if (b > -1.0e300) atomicMax(vmax, ordered_bits(b));
+  }
+}
+
+// Shell maximum of a standalone field (the DelField entry point).
+template <typename R>
+__global__ void k_shell_max(Geom g, const R* f, unsigned long long* vmax, double shell_r, double shell_w) {
+  double vm = -1.0e300;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x) {
+    double x, y, z;
+    point_coords(p, g, x, y, z);
+    if (fabs(sqrt(x * x + y * y + z * z) - shell_r) < shell_w) vm = fmax(vm, (double)f[p]);
+  }
+  for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if ((threadIdx.x & 31) == 0 && vm > -1.0e300) atomicMax(vmax, ordered_bits(vm));
+}
+
+// fftParallel phase factors on an s^D complex field: multiply by
+// c * (-1)^{i+j+k}, c complex.
+template <typename R>
+__global__ void k_alternate(typename Cx<R>::T* f, Geom g, double cr, double ci) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x) {
+    int k = (int)(p % g.s);
+    long q = p / g.s;
+    int par = k + (int)(q % g.s) + (g.dim == 3 ? (int)(q / g.s) : 0);
+    double sg = (par & 1) ? -1.0 : 1.0;
+    typename Cx<R>::T v = f[p];
+    double x = (double)v.x, y = (double)v.y;
+    f[p] = {R(sg * (cr * x - ci * y)), R(sg * (cr * y + ci * x))};
+  }
+}
+
+template <typename R>
+__global__ void k_cx_import(const double* src, typename Cx<R>::T* dst, long n) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
+    dst[p] = {R(src[2 * p]), R(src[2 * p + 1])};
+}
+template <typename R>
+__global__ void k_cx_export(const typename Cx<R>::T* src, double* dst, long n) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    dst[2 * p] = (double)src[p].x;
+    dst[2 * p + 1] = (double)src[p].y;
+  }
+}
+
+template <typename R>
+__global__ void k_scale_copy(const R* src, R* dst, long n, double a) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
+    dst[p] = R(a * (double)src[p]);
+}
+
+template <typename R>
+__global__ void k_axpy(const R* x, R* y, long n, double a, int accumulate) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
+    y[p] = accumulate ? R((double)y[p] + a * (double)x[p]) : R(a * (double)x[p]);
+}
+
+// ------------------------------------------------------------ host side --
+template <typename R>
+static int make_twiddles(Ctx& c, FftPlan& f) {
+  using C = typename Cx<R>::T;
+  auto table = [&](int len, int sign, void** dst) -> int {
+    std::vector<C> h(len);
+    for (int t = 0; t < len; ++t) {
+      double a = 2.0 * kPi * (double)t / (double)len;
+      h[t] = C{R(std::cos(a)), R(sign * std::sin(a))};
+    }
+    int st = c.alloc(dst, sizeof(C) * len);
+    if (st) return st;
+    CU(cudaMemcpy(*dst, h.data(), sizeof(C) * len, cudaMemcpyHostToDevice));
+    return MPDPFT_OK;
+  };
+  int st;
+  if ((st = table(f.s, -1, &f.tw_s_f))) return st;
+  if ((st = table(f.s, +1, &f.tw_s_b))) return st;
+  if ((st = table(f.M, -1, &f.tw_m_f))) return st;
+  if ((st = table(f.M, +1, &f.tw_m_b))) return st;
+  if ((st = table(f.s, -1, &f.tw_n_f))) return st;
+  return MPDPFT_OK;
+}
+
+int Ctx::fft_setup() {
+  fft = new FftPlan;
+  FftPlan& f = *fft;
+  f.dim = P.dim;
+  f.s = P.steps;
+  f.M = P.steps / 2;
+  f.H = f.M + 1;
+  f.rows = geom.n / P.steps;
+  f.nspec = f.rows * f.H;
+  if (!factor(f.s, f.plan_s) || !factor(f.M, f.plan_m))
+    return set_error(MPDPFT_ERR_ARG, "steps must factor into 2s and 3s for the FFT");
+  int st = rsize == sizeof(double) ? make_twiddles<double>(*this, f) : make_twiddles<float>(*this, f);
+  if (st) return st;
+  const size_t csz = 2 * rsize;
+  f.tk = rsize == sizeof(double) ? 8 : 16;
+  while (f.tk > 1 && f.M % f.tk) f.tk /= 2;
+  f.zl = 16;
+  f.zblocks = (int)((f.rows + f.zl - 1) / f.zl);
+  const bool need = has_coulomb || gradient;
+  const int nspec_buf = gradient ? 4 : 1;
+  for (int i = 0; i < nspec_buf; ++i)
+    if ((st = alloc(&f.spec[i], csz * f.nspec))) return st;
+  if ((st = alloc(&f.rtmp, rsize * geom.n))) return st;
+  if ((st = alloc((void**)&f.zpart, sizeof(double) * (f.zblocks + 1)))) return st;
+  if ((st = alloc((void**)&f.vmax, sizeof(unsigned long long)))) return st;
+  f.vblocks = grid_blocks(geom.n);
+  if ((st = alloc((void**)&f.vres_part, sizeof(double) * f.vblocks * kMaxS))) return st;
+  (void)need;
+  // shared memory opt-in for the largest tiles
+  const int max_smem = 200 * 1024;
+  if (rsize == sizeof(double)) {
+    CU(cudaFuncSetAttribute(k_z_r2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_z_c2r<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_axis_c2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_x_roundtrip<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  } else {
+    CU(cudaFuncSetAttribute(k_z_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_z_c2r<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_axis_c2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(cudaFuncSetAttribute(k_x_roundtrip<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  }
+  return MPDPFT_OK;
+}
+
+void Ctx::fft_release() {
+  delete fft;
+  fft = nullptr;
+}
+
+// --- pass launchers ---------------------------------------------------------
+template <typename R>
+static ZArgs<R> zargs(Ctx& c) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = c.geom;
+  a.M = f.M;
+  a.H = f.H;
+  a.zl = f.zl;
+  a.rows = f.rows;
+  a.plan = f.plan_m;
+  a.tw_n = (const typename Cx<R>::T*)f.tw_n_f;
+  a.nsrc = 1;
+  return a;
+}
+
+template <typename R>
+static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qcoef, void* out, bool sums) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = zargs<R>(c);
+  a.tw_m = (const typename Cx<R>::T*)f.tw_m_f;
+  a.in = in;
+  a.pro = pro;
+  a.nsrc = nsrc;
+  for (int q = 0; q < nsrc && qcoef; ++q) a.qcoef[q] = qcoef[q];
+  a.vmax = f.vmax;
+  a.taper_r0 = c.P.regularization_threshold * c.P.edge;
+  a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
+  a.out = (typename Cx<R>::T*)out;
+  a.part = sums ? f.zpart : nullptr;
+  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.M * f.zl;
+  k_z_r2c<R><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+template <typename R>
+static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* out1, double coul_coef) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = zargs<R>(c);
+  a.tw_m = (const typename Cx<R>::T*)f.tw_m_b;
+  for (int i = 0; i < nin; ++i) a.cin[i] = (const typename Cx<R>::T*)in[i];
+  a.nin = nin;
+  a.epi = epi;
+  a.rout[0] = out0;
+  a.rout[1] = out1;
+  a.scale = 1.0;
+  a.coul_coef = coul_coef;
+  a.f0_part = f.zpart;
+  a.f0_blocks = f.zblocks;
+  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.M * f.zl + sizeof(R) * (size_t)f.s * f.zl;
+  k_z_c2r<R><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+template <typename R>
+static AxisArgs<R> axis_args(Ctx& c, int axis) {
+  FftPlan& f = *c.fft;
+  AxisArgs<R> a;
+  std::memset(&a, 0, sizeof(a));
+  a.s = f.s;
+  a.M = f.M;
+  a.H = f.H;
+  a.tk = f.tk;
+  a.dim = f.dim;
+  a.plan = f.plan_s;
+  a.twf = (const typename Cx<R>::T*)f.tw_s_f;
+  a.twb = (const typename Cx<R>::T*)f.tw_s_b;
+  if (f.dim == 3 && axis == 1) {        // Y: outer = x index, lines along y
+    a.nouter = f.s;
+    a.ostride = (long)f.s * f.H;
+    a.astride = f.H;
+  } else if (f.dim == 3) {              // X: outer = y index, lines along x
+    a.nouter = f.s;
+    a.ostride = f.H;
+    a.astride = (long)f.s * f.H;
+  } else {                              // 2D X: single outer
+    a.nouter = 1;
+    a.ostride = 0;
+    a.astride = f.H;
+  }
+  a.ntile = f.M / f.tk;
+  a.nbulk = a.nouter * a.ntile;
+  a.dk = c.geom.dk;
+  a.scale = 1.0 / (double)c.geom.n;
+  return a;
+}
+
+template <typename R>
+static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
+  FftPlan& f = *c.fft;
+  AxisArgs<R> a = axis_args<R>(c, 1);
+  for (int i = 0; i < nfield; ++i) a.data[i] = (typename Cx<R>::T*)data[i];
+  a.dir = dir;
+  const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
+  dim3 grid((unsigned)(a.nbulk + nyq_blocks), nfield);
+  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.s * f.tk;
+  k_axis_c2c<R><<<grid, kFftThreads, smem, c.stream>>>(a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+template <typename R>
+static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, double sigma_c) {
+  FftPlan& f = *c.fft;
+  AxisArgs<R> a = axis_args<R>(c, 0);
+  a.data[0] = (typename Cx<R>::T*)in;
+  for (int i = 0; i < nout; ++i) a.out[i] = (typename Cx<R>::T*)out[i];
+  a.nout = nout;
+  a.mul = mul;
+  a.sigma_c = sigma_c;
+  a.cutoff = c.P.coulomb_cutoff > 0.0 ? c.P.coulomb_cutoff : 0.5 * c.P.edge;
+  a.f0_part = f.zpart;
+  a.f0_blocks = f.zblocks;
+  const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
+  const size_t smem = 3 * sizeof(typename Cx<R>::T) * f.s * f.tk;
+  k_x_roundtrip<R><<<(unsigned)(a.nbulk + nyq_blocks), kFftThreads, smem, c.stream>>>(a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+// Coulomb potential of `src` (nsrc species combined with weights qcoef)
+// into out: out = coef * phi, phi = int rho(r')/|r - r'|.
+template <typename R>
+static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* out, double coef) {
+  FftPlan& f = *c.fft;
+  int st;
+  const int pro = nsrc > 1 || (qcoef && qcoef[0] != 1.0) ? PRO_CHARGE : PRO_NONE;
+  if ((st = launch_z_r2c<R>(c, src, pro, nsrc, qcoef, f.spec[0], true))) return st;
+  if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, -1))) return st;
+  const int mul = c.P.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED ? MUL_COULOMB_TRUNC : MUL_COULOMB_REG;
+  if ((st = launch_x<R>(c, f.spec[0], &f.spec[0], 1, mul, 0.0))) return st;
+  if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, +1))) return st;
+  // regularised: V = 4 pi gammaH (x + f0 erf(r/2)/(4 pi r)); truncated: V = 4 pi gammaH x
+  if (mul == MUL_COULOMB_REG)
+    return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_COULOMB, out, nullptr, 4.0 * kPi * coef);
+  // truncated kernel: out = 4 pi coef x
+  if ((st = launch_z_c2r<R>(c, &f.spec[0], 1, EPI_STORE, (R*)f.rtmp, nullptr, 0.0))) return st;
+  return c.scale_copy(f.rtmp, out, 4.0 * kPi * coef);
+}
+
+
+int Ctx::scale_copy(const void* src, void* dst, double a) {
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double)) k_scale_copy<double><<<blocks, kThreads, 0, stream>>>((const double*)src, (double*)dst, geom.n, a);
+  else k_scale_copy<float><<<blocks, kThreads, 0, stream>>>((const float*)src, (float*)dst, geom.n, a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+// Coulomb terms of every species for densities `dens` ([S][n]) into out
+// ([S][n]): types 8, 21 and 100 (mpDPFT.cpp:2266-2285).
+template <typename R>
+static int coulomb_terms(Ctx& c, const R* dens, R* out) {
+  const long n = c.geom.n;
+  const int S = c.S;
+  int st;
+  std::vector<int> touched(S, 0);
+  for (int a = 0; a < c.P.n_interactions; ++a) {
+    const int t = c.P.interactions[a];
+    if (t == MPDPFT_INT_HARTREE) {
+      for (int s = 0; s < S; ++s) {
+        double one = 1.0;
+        if ((st = coulomb_into<R>(c, dens + (long)s * n, 1, &one, (R*)c.fft->rtmp, c.P.gamma_h))) return st;
+        if ((st = c.axpy(c.fft->rtmp, out + (long)s * n, 1.0, touched[s]))) return st;
+        touched[s] = 1;
+      }
+    } else if (t == MPDPFT_INT_HARTREE_INTER) {
+      for (int s = 0; s < S; ++s)
+        for (int q = 0; q < S; ++q) {
+          if (q == s) continue;
+          double one = 1.0;
+          if ((st = coulomb_into<R>(c, dens + (long)q * n, 1, &one, (R*)c.fft->rtmp, c.P.gamma_h))) return st;
+          if ((st = c.axpy(c.fft->rtmp, out + (long)s * n, 1.0, touched[s]))) return st;
+          touched[s] = 1;
+        }
+    } else if (t == MPDPFT_INT_COULOMB_CHARGED) {
+      if ((st = coulomb_into<R>(c, dens, S, c.P.charges, (R*)c.fft->rtmp, c.P.gamma_h))) return st;
+      for (int s = 0; s < S; ++s) {
+        if ((st = c.axpy(c.fft->rtmp, out + (long)s * n, c.P.charges[s], touched[s]))) return st;
+        touched[s] = 1;
+      }
+    }
+  }
+  for (int s = 0; s < S; ++s)
+    if (!touched[s]) CU(cudaMemsetAsync(out + (long)s * n, 0, sizeof(R) * n, c.stream));
+  return MPDPFT_OK;
+}
+
+
+int Ctx::axpy(const void* x, void* y, double a, int accumulate) {
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double)) k_axpy<double><<<blocks, kThreads, 0, stream>>>((const double*)x, (double*)y, geom.n, a, accumulate);
+  else k_axpy<float><<<blocks, kThreads, 0, stream>>>((const float*)x, (float*)y, geom.n, a, accumulate);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+// DelField of species-0 field f (already in compute precision): g2 and lap.
+template <typename R>
+static int delfield_into(Ctx& c, const R* f, R* g2, R* lap) {
+  FftPlan& F = *c.fft;
+  int st;
+  const double smear = c.P.smearing_extent > 0.0 ? c.P.smearing_extent : 6.0 * c.geom.dx;
+  const double sigma_c = -0.5 * smear * smear;  // ConvolutionSigma (mpDPFT.cpp:1106)
+  const int pro = c.P.taper_off ? PRO_TAPER : PRO_NONE;
+  if ((st = launch_z_r2c<R>(c, f, pro, 1, nullptr, F.spec[0], false))) return st;
+  if (F.dim == 3 && (st = launch_y<R>(c, &F.spec[0], 1, -1))) return st;
+  const int nout = F.dim + 1;  // gradients + Laplacian
+  void* outs[4] = {F.spec[0], F.spec[1], F.spec[2], F.spec[3]};
+  if (F.dim == 2) { outs[0] = F.spec[1]; outs[1] = F.spec[2]; outs[2] = F.spec[3]; }
+  if ((st = launch_x<R>(c, F.spec[0], outs, nout, MUL_DERIV, sigma_c))) return st;
+  if (F.dim == 3 && (st = launch_y<R>(c, outs, nout, +1))) return st;
+  // |grad f|^2 (raw) -> rtmp, Laplacian -> lap
+  if ((st = launch_z_c2r<R>(c, outs, nout, EPI_GRAD, (R*)F.rtmp, lap, 0.0))) return st;
+  // smooth |grad f|^2 and clamp at 0 (mpDPFT.cpp:7550-7560)
+  if ((st = launch_z_r2c<R>(c, (const R*)F.rtmp, PRO_NONE, 1, nullptr, F.spec[0], false))) return st;
+  if (F.dim == 3 && (st = launch_y<R>(c, &F.spec[0], 1, -1))) return st;
+  if ((st = launch_x<R>(c, F.spec[0], &F.spec[0], 1, MUL_SMOOTH, sigma_c))) return st;
+  if (F.dim == 3 && (st = launch_y<R>(c, &F.spec[0], 1, +1))) return st;
+  if ((st = launch_z_c2r<R>(c, &F.spec[0], 1, EPI_POS, g2, nullptr, 0.0))) return st;
+  return MPDPFT_OK;
+}
+
+static double shell_width(const Ctx& c) { return 2.0 * c.geom.dx; }
+static double shell_radius(const Ctx& c) { return c.P.edge * c.P.regularization_threshold; }
+
+template <typename R>
+static int fft_terms_impl(Ctx& c) {
+  FftPlan& F = *c.fft;
+  int st;
+  const long n = c.geom.n;
+  // current input densities live in ring slot state.slot; the slot index is
+  // only known on the device, so the Coulomb transform reads them through a
+  // gather into rtmp-sized staging: use the kernel-side slot via a copy.
+  const R* dens = (const R*)c.d_tmp;
+  if ((st = c.copy_current_density())) return st;
+  if (c.has_coulomb) {
+    if ((st = coulomb_terms<R>(c, dens, (R*)c.d_vh))) return st;
+  }
+  CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+  KParams kp = c.kparams();
+  k_assemble_v<R><<<F.vblocks, kThreads, 0, c.stream>>>(kp, c.d_state, (const R*)c.d_vext,
+                                                         c.has_coulomb ? (const R*)c.d_vh : nullptr,
+                                                         (const R*)c.d_nin, (R*)c.d_V, F.vres_part, F.vmax,
+                                                         shell_radius(c), shell_width(c));
+  CU(cudaGetLastError());
+  c.assemble_in_step = 0;
+  c.vres_part_ext = F.vres_part;
+  c.vres_blocks_ext = F.vblocks;
+  if (c.gradient) {
+    for (int s = 0; s < c.S; ++s) {
+      if (s > 0) {  // taper shift of species s
+        CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+        k_shell_max<R><<<grid_blocks(n), kThreads, 0, c.stream>>>(c.geom, (const R*)c.d_V + (long)s * n, F.vmax,
+                                                                  shell_radius(c), shell_width(c));
+        CU(cudaGetLastError());
+      }
+      if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
+                                 (R*)c.d_lap + (long)s * n)))
+        return st;
+    }
+  }
+  return MPDPFT_OK;
+}
+
+// Copy the current input densities (ring slot held on the device) into
+// d_tmp, so FFT passes can read them from a fixed address.
+template <typename R>
+__global__ void k_copy_slot(const ScState* st, const R* ring, R* dst, long count) {
+  if (__ldcg(&st->exit_loop)) return;
+  const int cur = __ldcg(&st->slot);
+  const R* src = ring + (long)cur * count;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < count; p += (long)gridDim.x * blockDim.x)
+    dst[p] = src[p];
+}
+
+int Ctx::copy_current_density() {
+  const long cnt = geom.n * S;
+  const int blocks = grid_blocks(cnt);
+  if (rsize == sizeof(double)) k_copy_slot<double><<<blocks, kThreads, 0, stream>>>(d_state, (const double*)d_nin, (double*)d_tmp, cnt);
+  else k_copy_slot<float><<<blocks, kThreads, 0, stream>>>(d_state, (const float*)d_nin, (float*)d_tmp, cnt);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+int Ctx::issue_fft_terms() {
+  return rsize == sizeof(double) ? fft_terms_impl<double>(*this) : fft_terms_impl<float>(*this);
+}
+
+int Ctx::issue_coulomb(const void* dens, void* out, int for_energy) {
+  (void)for_energy;
+  if (rsize == sizeof(double)) return coulomb_terms<double>(*this, (const double*)dens, (double*)out);
+  return coulomb_terms<float>(*this, (const float*)dens, (float*)out);
+}
+
+template <typename R>
+static int delfield_of_v_impl(Ctx& c) {
+  FftPlan& F = *c.fft;
+  const long n = c.geom.n;
+  int st;
+  for (int s = 0; s < c.S; ++s) {
+    CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+    k_shell_max<R><<<grid_blocks(n), kThreads, 0, c.stream>>>(c.geom, (const R*)c.d_V + (long)s * n, F.vmax,
+                                                              shell_radius(c), shell_width(c));
+    CU(cudaGetLastError());
+    if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n, (R*)c.d_lap + (long)s * n)))
+      return st;
+  }
+  return MPDPFT_OK;
+}
+
+int Ctx::issue_delfield_of_V() {
+  return rsize == sizeof(double) ? delfield_of_v_impl<double>(*this) : delfield_of_v_impl<float>(*this);
+}
+
+// ------------------------------------------------- standalone operators --
+int Ctx::op_delfield(const double* f, double* grad2, double* lap, int layout, int mem) {
+  if (!gradient) return set_error(MPDPFT_ERR_ARG, "context was not created with density_expression 5");
+  int st;
+  void* V0 = d_V;  // species 0 slot is used as staging
+  if ((st = import_field(f, V0, layout, mem))) return st;
+  const int S_save = S;
+  S = 1;
+  st = issue_delfield_of_V();
+  S = S_save;
+  if (st) return st;
+  if (grad2 && (st = export_field(d_g2, grad2, layout, mem))) return st;
+  if (lap && (st = export_field(d_lap, lap, layout, mem))) return st;
+  return MPDPFT_OK;
+}
+
+int Ctx::op_vint(int type, int s, const double* const* nn, double* v_out, int layout, int mem) {
+  if (s < 0 || s >= S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  if (!nn || !v_out) return set_error(MPDPFT_ERR_ARG, "null arrays");
+  int st;
+  for (int q = 0; q < S; ++q)
+    if ((st = import_field(nn[q], (char*)d_tmp + (size_t)q * geom.n * rsize, layout, mem))) return st;
+  const mpdpft_params saved = P;
+  P.n_interactions = 1;
+  P.interactions[0] = type;
+  P.incremental_v = 1.0;
+  const bool coul = type == MPDPFT_INT_HARTREE || type == MPDPFT_INT_HARTREE_INTER || type == MPDPFT_INT_COULOMB_CHARGED;
+  if (coul && (!fft || !fft->spec[0] || geom.dim != 3)) {
+    P = saved;
+    return set_error(MPDPFT_ERR_ARG, "Coulomb terms need a 3D context created with a Coulomb interaction");
+  }
+  void* out = (char*)d_V + (size_t)s * geom.n * rsize;  // staging
+  if (coul) {
+    st = rsize == sizeof(double) ? coulomb_terms<double>(*this, (const double*)d_tmp, (double*)d_vh)
+                                 : coulomb_terms<float>(*this, (const float*)d_tmp, (float*)d_vh);
+    if (!st) st = export_field((char*)d_vh + (size_t)s * geom.n * rsize, v_out, layout, mem);
+  } else if (type == MPDPFT_INT_CONTACT_SELF || type == MPDPFT_INT_CONTACT_MUTUAL || type == MPDPFT_INT_DIRAC ||
+             type == MPDPFT_INT_NONE) {
+    st = pointwise_vint(type, s, out);
+    if (!st) st = export_field(out, v_out, layout, mem);
+  } else {
+    st = set_error(MPDPFT_ERR_ARG, "unsupported interaction type");
+  }
+  P = saved;
+  return st;
+}
+
+template <typename R>
+__global__ void k_pointwise_vint(KParams kp, int type, int s, const R* dens, R* out) {
+  const long n = kp.geom.n;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    R v = R(0);
+    if (type == MPDPFT_INT_CONTACT_SELF) v = R(2.0 * kp.beta) * dens[p];
+    else if (type == MPDPFT_INT_CONTACT_MUTUAL) {
+      R t = R(0);
+      for (int q = 0; q < kp.S; ++q)
+        if (q != s) t += dens[(long)q * n + p];
+      v = R(kp.beta) * t;
+    } else if (type == MPDPFT_INT_DIRAC) {
+      R ns = dens[(long)s * n + p];
+      ns = ns > R(0) ? ns : R(0);
+      if (kp.geom.dim == 3) v = R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+      else v = R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+    }
+    out[p] = v;
+  }
+}
+
+int Ctx::pointwise_vint(int type, int s, void* out) {
+  KParams kp = kparams();
+  const int blocks = grid_blocks(geom.n);
+  if (rsize == sizeof(double)) k_pointwise_vint<double><<<blocks, kThreads, 0, stream>>>(kp, type, s, (const double*)d_tmp, (double*)out);
+  else k_pointwise_vint<float><<<blocks, kThreads, 0, stream>>>(kp, type, s, (const float*)d_tmp, (float*)out);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+int Ctx::op_update_v(const double* const* nn, double incremental, double* const* v_out, int layout, int mem) {
+  if (!nn || !v_out) return set_error(MPDPFT_ERR_ARG, "null arrays");
+  int st;
+  ScState h;
+  if ((st = read_state(&h))) return st;
+  const int cur = h.slot;
+  for (int q = 0; q < S; ++q)
+    if ((st = import_field(nn[q], (char*)d_nin + ((size_t)cur * S + q) * geom.n * rsize, layout, mem))) return st;
+  h.inc_v = incremental;
+  h.exit_loop = 0;
+  CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  if (has_coulomb || gradient) {
+    if ((st = issue_fft_terms())) return st;
+  } else {
+    const int blocks = grid_blocks(geom.n);
+    KParams kp = kparams();
+    if (!fft) return set_error(MPDPFT_ERR_ARG, "no FFT plan");
+    if (rsize == sizeof(double))
+      k_assemble_v<double><<<fft->vblocks, kThreads, 0, stream>>>(kp, d_state, (const double*)d_vext, nullptr,
+                                                                  (const double*)d_nin, (double*)d_V, fft->vres_part,
+                                                                  fft->vmax, 0.0, -1.0);
+    else
+      k_assemble_v<float><<<fft->vblocks, kThreads, 0, stream>>>(kp, d_state, (const float*)d_vext, nullptr,
+                                                                 (const float*)d_nin, (float*)d_V, fft->vres_part,
+                                                                 fft->vmax, 0.0, -1.0);
+    (void)blocks;
+    CU(cudaGetLastError());
+  }
+  for (int s = 0; s < S; ++s)
+    if ((st = export_field((char*)d_V + (size_t)s * geom.n * rsize, v_out[s], layout, mem))) return st;
+  return MPDPFT_OK;
+}
+
+// fftParallel semantics on an interleaved complex s^D field (see header).
+int Ctx::op_fft(int sign, const double* in, double* out, int mem) {
+  if (sign != -1 && sign != 1) return set_error(MPDPFT_ERR_ARG, "sign must be -1 or +1");
+  if (!in || !out) return set_error(MPDPFT_ERR_ARG, "null arrays");
+  FftPlan& F = *fft;
+  int st;
+  if (!F.cbuf && (st = alloc(&F.cbuf, 2 * rsize * geom.n))) return st;
+  const long n = geom.n;
+  double* din = d_io;
+  double* dout = d_io;
+  std::vector<double> stage;
+  if (mem == MPDPFT_MEM_HOST) {
+    if ((st = alloc_io(2 * n))) return st;
+    CU(cudaMemcpyAsync(d_io, in, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, stream));
+  } else {
+    din = (double*)in;
+    dout = out;
+  }
+  const int blocks = grid_blocks(n);
+  const double D = geom.dim;
+  const double ph = -0.5 * D * kPi * geom.s;  // e^{-i D pi s/2} (mpDPFT.cpp:8228-8262)
+  double cr_pre = 1.0, ci_pre = 0.0, cr_post, ci_post;
+  if (sign < 0) {
+    const double fac = std::pow(geom.dx, D);
+    cr_post = fac * std::cos(ph);
+    ci_post = fac * std::sin(ph);
+  } else {
+    const double fac = std::pow(1.0 / geom.L, D);
+    cr_post = fac * std::cos(-ph);
+    ci_post = fac * std::sin(-ph);
+  }
+  if (rsize == sizeof(double)) {
+    using C = double2;
+    k_cx_import<double><<<blocks, kThreads, 0, stream>>>(din, (C*)F.cbuf, n);
+    k_alternate<double><<<blocks, kThreads, 0, stream>>>((C*)F.cbuf, geom, cr_pre, ci_pre);
+    st = full_c2c(F.cbuf, sign);
+    if (st) return st;
+    k_alternate<double><<<blocks, kThreads, 0, stream>>>((C*)F.cbuf, geom, cr_post, ci_post);
+    k_cx_export<double><<<blocks, kThreads, 0, stream>>>((const C*)F.cbuf, dout, n);
+  } else {
+    using C = float2;
+    k_cx_import<float><<<blocks, kThreads, 0, stream>>>(din, (C*)F.cbuf, n);
+    k_alternate<float><<<blocks, kThreads, 0, stream>>>((C*)F.cbuf, geom, cr_pre, ci_pre);
+    st = full_c2c(F.cbuf, sign);
+    if (st) return st;
+    k_alternate<float><<<blocks, kThreads, 0, stream>>>((C*)F.cbuf, geom, cr_post, ci_post);
+    k_cx_export<float><<<blocks, kThreads, 0, stream>>>((const C*)F.cbuf, dout, n);
+  }
+  CU(cudaGetLastError());
+  if (mem == MPDPFT_MEM_HOST) {
+    CU(cudaMemcpyAsync(out, d_io, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+  }
+  return MPDPFT_OK;
+}
+
+// Unnormalised full complex transform of an s^D field along every axis,
+// using the tile kernel with all s columns of each axis.
+template <typename R>
+static int full_c2c_impl(Ctx& c, void* buf, int sign) {
+  FftPlan& F = *c.fft;
+  const int s = F.s;
+  const int dim = F.dim;
+  for (int axis = 0; axis < dim; ++axis) {
+    AxisArgs<R> a;
+    std::memset(&a, 0, sizeof(a));
+    a.s = s;
+    a.tk = F.tk;
+    a.dim = dim;
+    a.plan = F.plan_s;
+    a.twf = (const typename Cx<R>::T*)F.tw_s_f;
+    a.twb = (const typename Cx<R>::T*)F.tw_s_b;
+    a.dir = sign;
+    a.data[0] = (typename Cx<R>::T*)buf;
+    // treat the field as H = s columns with no separate Nyquist column
+    a.M = s;  // columns 0..s-1 are all bulk
+    a.H = s;
+    long astride, ostride, nouter;
+    if (dim == 3) {
+      if (axis == 0) { astride = (long)s * s; ostride = s; nouter = s; }       // lines along x: (y, z)
+      else if (axis == 1) { astride = s; ostride = (long)s * s; nouter = s; }  // along y: (x, z)
+      else { astride = 1; ostride = s; nouter = (long)s * s; }                 // along z: rows
+    } else {
+      if (axis == 0) { astride = s; ostride = 0; nouter = 1; }
+      else { astride = 1; ostride = s; nouter = s; }
+    }
+    a.astride = astride;
+    a.ostride = ostride;
+    a.nouter = nouter;
+    if ((dim == 3 && axis == 2) || (dim == 2 && axis == 1)) {
+      // contiguous lines: one column per outer row
+      a.M = 1;
+      a.ntile = 1;
+      a.tk = 1;
+    } else {
+      a.ntile = s / a.tk;
+      a.M = s;
+    }
+    a.nbulk = a.nouter * a.ntile;
+    const size_t smem = 2 * sizeof(typename Cx<R>::T) * s * a.tk;
+    // no Nyquist blocks: columns cover 0..s-1
+    k_axis_c2c<R><<<dim3((unsigned)a.nbulk, 1), kFftThreads, smem, c.stream>>>(a);
+    CU(cudaGetLastError());
+  }
+  return MPDPFT_OK;
+}
+
+int Ctx::full_c2c(void* buf, int sign) {
+  return rsize == sizeof(double) ? full_c2c_impl<double>(*this, buf, sign) : full_c2c_impl<float>(*this, buf, sign);
+}
+
+int Ctx::alloc_io(long doubles) {
+  (void)doubles;  // d_io holds 2 * max(n_ref, n) doubles, enough for one complex field
+  return MPDPFT_OK;
+}
+
+}  // namespace mpdpft

@@ -1,0 +1,660 @@
+// sc_step.cuh -- one SC iteration of the DPFT loop as a persistent kernel.
+//
+// The reference iteration (GetData loop, mpDPFT.cpp:213-224) is
+//   StoreCurrentIteration; UpdateV; GetDensities (n[V] + EnforceConstraints);
+//   CheckConvergence; Intercept; AdmixDensities; InjectSchedule;
+//   PrepareNextIteration.
+// Every step that is pointwise or a reduction runs here, in one cooperative
+// launch whose phases are separated by bounded grid barriers; the scalar
+// logic (mu decisions, convergence test, Pulay solve, schedules) runs on
+// block 0 and lives in device memory, so an iteration needs no host
+// synchronisation and can be captured in a CUDA graph.  FFT-based terms
+// (Hartree, DelField) are produced by the FFT kernels before this launch.
+#pragma once
+#include "common.cuh"
+
+namespace mpdpft {
+
+constexpr int kStepThreads = 512;
+constexpr int kNPart = 4 * kMaxS + kMaxP > kMaxS * kMuCand ? 4 * kMaxS + kMaxP : kMaxS * kMuCand;
+constexpr long kBarrierSpinLimit = 20000000;  // ~ seconds with nanosleep backoff
+
+// Constant parameters of one solve (kernel argument, by value).
+struct KParams {
+  Geom geom;
+  int S;
+  DensParams dens[kMaxS];
+  double abundance[kMaxS];
+  double rel_acc;
+  double beta, gamma_h;
+  double charges[kMaxS];
+  int contact_self, contact_mutual, dirac;  // pointwise V_int terms present
+  int has_coulomb;                          // vh holds the Coulomb terms
+  int mixer, scope, ring;                   // ring = scope + 1 slots
+  double sc_criterion;
+  int max_sc;
+  int schedule;
+  double pot_tol;
+  double inc_v0;
+};
+
+struct MuState {
+  double start, prev_abs, delta0, delta1, lo, hi, Nlo, Nhi;
+  int have_lo, have_hi, done, active, pass;
+  int ncand;
+  int dir;     // -1: N(start) > N*, step down; +1: step up (reference order)
+  int next_c;  // next reference bracket step to place
+  double cand[kMuCand];
+  double best_mu, best_N, best_err;
+};
+
+// SC loop state, resident in device memory.
+struct ScState {
+  double mu[kMaxS], prev_mu[kMaxS], old_mu[kMaxS];
+  double ab[kMaxS], old_ab[kMaxS];
+  double theta[kMaxS], theta0[kMaxS], theta_mix[kMaxS];
+  double dmm, cc, old_cc, inc_v, v_res;
+  int sc_count, exit_count, exit_loop, halted;
+  int status_bits, iter_bits;
+  int slot;      // ring slot of the current input density
+  int mix_src;   // slot the last mix read from
+  int hist;      // Pulay history length
+  int pulay_used;
+  int ncoeff;
+  double gram[kMaxP * kMaxP];
+  double coeff[kMaxP];
+  int mu_passes;
+  int mu_passes_total;
+  MuState ms[kMaxS];
+  unsigned bar_count, bar_gen;
+  int abort;
+};
+
+template <typename R>
+struct StepArgs {
+  KParams kp;
+  ScState* st;
+  const R* vext;  // [S][n]
+  R* V;           // [S][n]
+  const R* lap;   // [S][n] or null
+  const R* g2;    // [S][n] or null
+  const R* vh;    // [S][n] Coulomb terms or null
+  R* nin;         // [ring][S][n]
+  R* res;         // [ring][S][n]
+  double* part;   // [gridDim.x][kNPart]
+  const double* vres_part;  // partials of |V_new - V_old|^2 from an external
+  int vres_blocks;          //   V assembly (when assemble_v == 0), or null
+  mpdpft_iter_log* log;
+  int log_cap;
+  int assemble_v;  // 1: phase A assembles V from vext, n_in and vh
+  int mode;        // 0: SC iteration; 1: densities of the current V only;
+                   // 2: admix only (V holds the output densities)
+};
+
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
+
+// Bounded sense-free generation barrier over all blocks of a cooperative
+// launch.  Returns false (and raises the abort flag) if a block does not
+// arrive within the spin limit; every block then leaves its loop.
+__device__ inline bool grid_barrier(ScState* st) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned* gen = &st->bar_gen;
+    unsigned g = *gen;
+    __threadfence();
+    unsigned arrived = atomicAdd(&st->bar_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      long spins = 0;
+      while (*gen == g) {
+        if (*(volatile int*)&st->abort) { ok = 0; break; }
+        if (++spins > kBarrierSpinLimit) {
+          atomicExch(&st->abort, 1);
+          atomicOr(&st->status_bits, kBitTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// ---------------------------------------------------------- mu search ----
+// The reference brackets mu by steps Delta_c = e^{DeltamuModifier} (1 + c)
+// |mu_prev| away from the start (mpDPFT.cpp:4603, 4633), adapting
+// DeltamuModifier once after the first step (:4613, :4643), for at most 20
+// steps (:4584), and then bisects.  Here each pass evaluates N(mu) for up to
+// kMuCand candidates in one sweep: pass 0 holds the start, the first step in
+// both directions and a few close and wider points; later passes place the
+// reference's remaining bracket steps (with the adapted modifier), and once
+// mu is bracketed the candidates cluster around the regula-falsi estimate,
+// which shrinks the bracket by at least half per pass.  The search ends, as
+// the reference's, when |N - N*| / (2 N*) <= RelAcc.
+__device__ __forceinline__ double tri(int c) { return 0.5 * (double)c * (double)(c + 1); }
+
+// Offset of the reference's c-th bracket step from the start.
+__device__ __forceinline__ double step_offset(const MuState& m, int c) {
+  return m.delta0 + m.delta1 * (tri(c) - 1.0);
+}
+
+__device__ inline void mu_begin(MuState& m, double mu, double prev_abs, double dmm, int active) {
+  m.start = mu;
+  m.prev_abs = prev_abs;
+  m.delta0 = exp(dmm) * prev_abs;
+  m.delta1 = m.delta0;
+  m.have_lo = m.have_hi = 0;
+  m.done = active ? 0 : 1;
+  m.active = active;
+  m.pass = 0;
+  m.dir = 0;
+  m.next_c = 2;
+  m.best_mu = mu;
+  m.best_N = 0.0;
+  m.best_err = 1e300;
+  m.ncand = 0;
+  m.cand[m.ncand++] = mu;
+  m.cand[m.ncand++] = mu - m.delta0;  // first reference step, both directions
+  m.cand[m.ncand++] = mu + m.delta0;
+  const double am = fabs(mu) > 1e-300 ? fabs(mu) : prev_abs;
+  const double eps[3] = {1e-8, 1e-6, 1e-4};
+  for (int e = 0; e < 3; ++e) {
+    m.cand[m.ncand++] = mu - eps[e] * am;
+    m.cand[m.ncand++] = mu + eps[e] * am;
+  }
+  for (int c = 2; c <= 4; ++c) {
+    m.cand[m.ncand++] = mu - step_offset(m, c);
+    m.cand[m.ncand++] = mu + step_offset(m, c);
+  }
+}
+
+// Evaluate a pass (block 0, thread 0): update bracket and best point, choose
+// the next candidates or finish.
+__device__ inline void mu_decide(MuState& m, const double* N, double target, double rel_acc,
+                                 double& dmm, int& bits) {
+  const double denom = fabs(2.0 * target);
+  for (int c = 0; c < m.ncand; ++c) {
+    double mu = m.cand[c], n = N[c];
+    if (!isfinite(n)) { bits |= kBitNonfinite; continue; }
+    double err = fabs(n - target) / denom;
+    if (err < m.best_err) { m.best_err = err; m.best_mu = mu; m.best_N = n; }
+    if (n < target) {
+      if (!m.have_lo || mu > m.lo) { m.lo = mu; m.Nlo = n; m.have_lo = 1; }
+    } else if (n > target) {
+      if (!m.have_hi || mu < m.hi) { m.hi = mu; m.Nhi = n; m.have_hi = 1; }
+    }
+  }
+  if (m.pass == 0) {
+    const double N0 = N[0];
+    const double diff0 = fabs(N0 - target);
+    m.dir = N0 > target ? -1 : 1;
+    if (diff0 / denom > rel_acc) {  // DeltamuModifier adaptation (:4613, :4643)
+      const double n1 = m.dir < 0 ? N[1] : N[2];
+      const double diff1 = fabs(n1 - target);
+      dmm -= (diff1 - diff0 < 0.0 ? -1.0 : 1.0) * 0.1 * fabs(dmm);
+      m.delta1 = exp(dmm) * m.prev_abs;
+    }
+  }
+  m.pass++;
+  if (m.best_err <= rel_acc) { m.done = 1; return; }
+  if (m.pass >= kMuMaxPasses) { m.done = 1; bits |= kBitTimeout; return; }
+  m.ncand = 0;
+  if (!m.have_lo || !m.have_hi) {
+    // continue the reference's bracket steps towards the target
+    const int d = m.have_hi ? -1 : 1;  // missing lower end: step down
+    while (m.next_c <= 20 && m.ncand < kMuCand) m.cand[m.ncand++] = m.start + d * step_offset(m, m.next_c++);
+    if (m.ncand == 0) {  // no bracket within 20 steps: reset mu (:4657-4662)
+      m.done = 1;
+      m.best_mu = m.start;
+      m.best_err = 1e300;
+      bits |= kBitBracket;
+    }
+    return;
+  }
+  const double w = m.hi - m.lo;
+  if (!(w > 1.0e-12)) { m.done = 1; return; }  // Deltamu below MP (:4711)
+  double rf = m.lo + (target - m.Nlo) * w / (m.Nhi - m.Nlo);
+  if (!(rf > m.lo && rf < m.hi)) rf = 0.5 * (m.lo + m.hi);
+  m.cand[m.ncand++] = rf;
+  m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
+  double f = 0.25;
+  for (int j = 0; j < 7; ++j) {
+    m.cand[m.ncand++] = rf - (rf - m.lo) * f;
+    m.cand[m.ncand++] = rf + (m.hi - rf) * f;
+    f *= 0.125;
+  }
+}
+
+// ---------------------------------------------------------- small solve --
+// Inverse of an n x n matrix (n <= kMaxP) by Gauss-Jordan elimination with
+// full pivoting.  Rank test as Eigen's FullPivHouseholderQR::isInvertible
+// (threshold eps * n * max|pivot|), which the reference uses (mpDPFT.cpp:5089).
+__device__ inline bool small_inverse(int n, const double* A, double* inv) {
+  double M[kMaxP * kMaxP];
+  int colperm[kMaxP];
+  double piv[kMaxP];
+  for (int i = 0; i < n * n; ++i) { M[i] = A[i]; inv[i] = 0.0; }
+  for (int i = 0; i < n; ++i) { inv[i * n + i] = 1.0; colperm[i] = i; }
+  double maxpiv = 0.0;
+  for (int c = 0; c < n; ++c) {
+    int pr = c, pc = c;
+    double best = -1.0;
+    for (int i = c; i < n; ++i)
+      for (int j = c; j < n; ++j)
+        if (fabs(M[i * n + j]) > best) { best = fabs(M[i * n + j]); pr = i; pc = j; }
+    if (pr != c)
+      for (int j = 0; j < n; ++j) {
+        double t = M[pr * n + j]; M[pr * n + j] = M[c * n + j]; M[c * n + j] = t;
+        t = inv[pr * n + j]; inv[pr * n + j] = inv[c * n + j]; inv[c * n + j] = t;
+      }
+    if (pc != c) {
+      for (int i = 0; i < n; ++i) { double t = M[i * n + pc]; M[i * n + pc] = M[i * n + c]; M[i * n + c] = t; }
+      int t = colperm[pc]; colperm[pc] = colperm[c]; colperm[c] = t;
+    }
+    piv[c] = M[c * n + c];
+    if (fabs(piv[c]) > maxpiv) maxpiv = fabs(piv[c]);
+    if (piv[c] == 0.0) return false;
+    double ip = 1.0 / piv[c];
+    for (int j = 0; j < n; ++j) { M[c * n + j] *= ip; inv[c * n + j] *= ip; }
+    for (int i = 0; i < n; ++i) {
+      if (i == c) continue;
+      double f = M[i * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) { M[i * n + j] -= f * M[c * n + j]; inv[i * n + j] -= f * inv[c * n + j]; }
+    }
+  }
+  const double thr = 2.220446049250313e-16 * (double)n * maxpiv;
+  for (int c = 0; c < n; ++c)
+    if (fabs(piv[c]) <= thr) return false;
+  double out[kMaxP * kMaxP];
+  for (int c = 0; c < n; ++c)
+    for (int j = 0; j < n; ++j) out[colperm[c] * n + j] = inv[c * n + j];
+  for (int i = 0; i < n * n; ++i) inv[i] = out[i];
+  return true;
+}
+
+// Reduce kNPart partials over blocks into red[] (block 0 only).
+__device__ inline void reduce_partials(const double* part, int nblocks, int nvals, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = warp; j < nvals; j += nw) {
+    double t = 0.0;
+    for (int b = lane; b < nblocks; b += 32) t += __ldcg(part + (long)b * kNPart + j);
+    t = warp_sum(t);
+    if (lane == 0) red[j] = t;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------ the kernel --
+// mode 0: one SC iteration.  mode 1: GetDensities of the current V (mu
+// search + n[V]), written into the current ring slot; used for the initial
+// densities (mpDPFT.cpp:195) and the standalone mu-search entry point.
+template <typename R>
+__global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long nthreads = (long)gridDim.x * blockDim.x;
+  __shared__ double red[kNPart];
+  __shared__ double s_mu[kMaxS];
+  __shared__ int s_flag;
+  __shared__ MuState s_ms[kMaxS];
+
+  if (a.mode != 1 && ldcg(&st->exit_loop)) return;
+  const int cur = ldcg(&st->slot);
+  const int ring = kp.ring;
+  const int next = (cur + 1) % ring;
+  double* mypart = a.part + (long)blockIdx.x * kNPart;
+
+  // ---- phase A: UpdateV (mpDPFT.cpp:4815-4838) --------------------------
+  if (a.mode == 0 && a.assemble_v) {
+    const double incv = ldcg(&st->inc_v);
+    const double fac = incv < 1.0 ? incv : 1.0;
+    double acc[kMaxS];
+    for (int s = 0; s < kMaxS; ++s) acc[s] = 0.0;
+    const R* nin = a.nin + (long)cur * S * n;
+    for (long p = tid; p < n; p += nthreads) {
+      for (int s = 0; s < S; ++s) {
+        R vi = R(0);
+        if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];  // type 10 (:2261)
+        if (kp.contact_mutual) {                                  // type 1 (:2247)
+          R t = R(0);
+          for (int q = 0; q < S; ++q)
+            if (q != s) t += nin[(long)q * n + p];
+          vi += R(kp.beta) * t;
+        }
+        if (kp.dirac) {  // type 11 (:2768): -gammaH 2 (D n+/pi)^{1/D}/(D-1)
+          R ns = nin[(long)s * n + p];
+          ns = ns > R(0) ? ns : R(0);
+          if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+          else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+        }
+        if (a.vh) vi += a.vh[(long)s * n + p];
+        R vnew = a.vext[(long)s * n + p] + R(fac) * vi;
+        R vold = a.V[(long)s * n + p];
+        double d = (double)vnew - (double)vold;
+        acc[s] += d * d;
+        a.V[(long)s * n + p] = vnew;
+      }
+    }
+    block_reduce_store<kMaxS>(acc, mypart);
+  }
+
+  // ---- phase B: mu search (GetDensities + EnforceConstraints) ----------
+  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
+  if (threadIdx.x == 0) {  // every block derives the pass-0 candidates itself
+    double dmm = ldcg(&st->dmm);
+    double pn = 0.0;
+    for (int s = 0; s < S; ++s) { double pm = ldcg(&st->mu[s]); pn += pm * pm; }
+    for (int s = 0; s < S; ++s) {
+      double mu = ldcg(&st->mu[s]);
+      double pa = sqrt(pn) < 1.0e-12 ? 1.0e-12 : fabs(mu);
+      mu_begin(s_ms[s], mu, pa, dmm, active);
+    }
+  }
+  __syncthreads();
+  if (!grid_barrier(st)) return;
+  if (blockIdx.x == 0) {
+    if (a.mode == 0 && (a.assemble_v || a.vres_part)) {
+      const double* vp = a.assemble_v ? a.part : a.vres_part;
+      const int nb = a.assemble_v ? (int)gridDim.x : a.vres_blocks;
+      const int stride = a.assemble_v ? kNPart : kMaxS;
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      if (warp < S) {
+        double t = 0.0;
+        for (int b = lane; b < nb; b += 32) t += __ldcg(vp + (long)b * stride + warp);
+        t = warp_sum(t);
+        if (lane == 0) red[warp] = t;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double w = 0.0;
+        for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red[s] / (double)n));
+        st->v_res = w;
+      }
+    }
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < S; ++s) { st->ms[s] = s_ms[s]; st->prev_mu[s] = s_ms[s].start; }
+      st->mu_passes = 0;
+      st->iter_bits = 0;
+    }
+  }
+  if (!grid_barrier(st)) return;
+
+  const R* V = a.V;
+  for (int pass = 0; pass < kMuMaxPasses && a.mode != 2; ++pass) {
+    if (pass > 0 && threadIdx.x < S) {
+      const int s = threadIdx.x;
+      s_ms[s].done = ldcg(&st->ms[s].done);
+      s_ms[s].ncand = ldcg(&st->ms[s].ncand);
+      for (int c = 0; c < s_ms[s].ncand; ++c) s_ms[s].cand[c] = ldcg(&st->ms[s].cand[c]);
+    }
+    __syncthreads();
+    int any = 0;
+    for (int s = 0; s < S; ++s) any |= !s_ms[s].done;
+    if (!any) break;
+    for (int s = 0; s < S; ++s) {
+      if (s_ms[s].done) continue;
+      double acc[kMuCand];
+#pragma unroll
+      for (int c = 0; c < kMuCand; ++c) acc[c] = 0.0;
+      // n(mu) is evaluated in double from the stored fields (FP32 in mixed
+      // mode): the particle-number integral and the mu search are FP64.
+      const DensParams d = kp.dens[s];
+      const int nc = s_ms[s].ncand;
+      double cmu[kMuCand];
+#pragma unroll
+      for (int c = 0; c < kMuCand; ++c) cmu[c] = c < nc ? s_ms[s].cand[c] : 0.0;
+      const R* Vs = V + (long)s * n;
+      const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
+      const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
+      for (long p = tid; p < n; p += nthreads) {
+        const double v = (double)Vs[p];
+        const double l = Ls ? (double)Ls[p] : 0.0;
+        const double g = Gs ? (double)Gs[p] : 0.0;
+#pragma unroll
+        for (int c = 0; c < kMuCand; ++c)
+          if (c < nc) acc[c] += density_at<double>(d, cmu[c] - v, l, g);
+      }
+      block_reduce_store<kMuCand>(acc, mypart + s * kMuCand);
+    }
+    if (!grid_barrier(st)) return;
+    if (blockIdx.x == 0) {
+      reduce_partials(a.part, gridDim.x, S * kMuCand, red);
+      if (threadIdx.x == 0) {
+        double dmm = st->dmm;
+        int bits = 0;
+        for (int s = 0; s < S; ++s) {
+          if (s_ms[s].done) continue;
+          MuState ms = st->ms[s];
+          double N[kMuCand];
+          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuCand + c] * kp.geom.dvol;
+          mu_decide(ms, N, kp.abundance[s], kp.rel_acc, dmm, bits);
+          st->ms[s] = ms;
+        }
+        st->dmm = dmm;
+        st->iter_bits |= bits;
+        st->mu_passes++;
+      }
+    }
+    if (!grid_barrier(st)) return;
+  }
+
+  // ---- phase C: final densities, residual, CC dots, Gram row -----------
+  if (threadIdx.x < S) {
+    const int s = threadIdx.x;
+    double mu = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
+    s_mu[s] = mu;
+  }
+  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
+  __syncthreads();
+  const int pulay_now = s_flag;
+  const int hist = ldcg(&st->hist);
+  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
+  {
+    constexpr int NF = 4 * kMaxS + kMaxP;
+    double acc[NF];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) acc[j] = 0.0;
+    R* nin = a.nin + (long)cur * S * n;
+    R* rcur = a.res + (long)cur * S * n;
+    for (long p = tid; p < n; p += nthreads) {
+      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
+      for (int s = 0; s < S; ++s) {
+        const long q = (long)s * n + p;
+        const R v = V[q];
+        const double l = a.lap ? (double)a.lap[q] : 0.0;
+        const double g = a.g2 ? (double)a.g2[q] : 0.0;
+        // mode 2 (admix only): V holds the output densities
+        const double nod = a.mode == 2 ? (double)v : density_at<double>(kp.dens[s], s_mu[s] - (double)v, l, g);
+        const R no = R(nod);
+        acc[4 * s + 0] += nod;
+        if (a.mode == 1) { nin[q] = no; continue; }
+        R ni = nin[q];
+        R r = no - ni;
+        rcur[q] = r;
+        const double dno = (double)no, dni = (double)ni, dr = (double)r;
+        acc[4 * s + 1] += w * dno * dni;
+        acc[4 * s + 2] += w * dno * dno;
+        acc[4 * s + 3] += w * dni * dni;
+        for (int j = 0; j < I; ++j) {
+          int slot = (cur - (I - 1) + j + ring) % ring;
+          double rj = (j == I - 1) ? dr : (double)a.res[((long)slot * S + s) * n + p];
+          acc[4 * kMaxS + j] += w * dr * rj;
+        }
+      }
+    }
+    block_reduce_store<NF>(acc, mypart);
+  }
+  if (!grid_barrier(st)) return;
+
+  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
+  if (blockIdx.x == 0) {
+    reduce_partials(a.part, gridDim.x, 4 * kMaxS + kMaxP, red);
+    if (threadIdx.x == 0) {
+      const int sc = st->sc_count;
+      double tot = 0.0;
+      for (int s = 0; s < S; ++s) {
+        st->mu[s] = s_mu[s];
+        st->ab[s] = red[4 * s] * kp.geom.dvol;
+        if (!isfinite(st->ab[s])) st->iter_bits |= kBitNonfinite;
+        tot += st->ab[s];
+      }
+      if (a.mode == 1) {
+        st->status_bits |= st->iter_bits;
+        st->mu_passes_total += st->mu_passes;
+      } else {
+        // CheckConvergence (mpDPFT.cpp:4759-4782)
+        const double mp = 100.0 * 1.0e-16;
+        if (sc > 0) {
+          double cc = 0.0, maxtest = 0.0;
+          for (int s = 0; s < S; ++s) {
+            double oi = red[4 * s + 1], oo = red[4 * s + 2], ii = red[4 * s + 3];
+            double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
+            double t = rd * st->ab[s] / tot;
+            if (t > maxtest) { maxtest = t; cc = maxtest; }
+          }
+          st->cc = cc;
+          double dab = 0.0, dmu = 0.0;
+          for (int s = 0; s < S; ++s) {
+            dab += (st->ab[s] - st->old_ab[s]) * (st->ab[s] - st->old_ab[s]);
+            dmu += (st->mu[s] - st->old_mu[s]) * (st->mu[s] - st->old_mu[s]);
+          }
+          int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
+          double avth = 0.0;
+          for (int s = 0; s < S; ++s) avth += st->theta[s] / (double)S;
+          bool vok = !(kp.pot_tol > 0.0) || st->v_res <= kp.pot_tol;
+          if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
+              (cc < kp.sc_criterion || steady) && vok)
+            st->exit_count++;
+          else
+            st->exit_count = 0;
+          if (st->exit_count >= 3) st->exit_loop = 1;
+        } else {
+          st->cc = 1.2345678901234567890;
+        }
+        if (sc == kp.max_sc) st->exit_loop = 1;  // Intercept (:4866)
+        // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167)
+        int used = 0;
+        if (pulay_now) {
+          const int shift = (hist + 1 > kp.scope) ? 1 : 0;
+          double G[kMaxP * kMaxP];
+          for (int i = 0; i < I; ++i)
+            for (int j = 0; j < I; ++j) {
+              double v;
+              if (i == I - 1) v = red[4 * kMaxS + j];
+              else if (j == I - 1) v = red[4 * kMaxS + i];
+              else v = st->gram[(i + shift) * kMaxP + (j + shift)];
+              G[i * I + j] = v;
+            }
+          for (int i = 0; i < I; ++i)
+            for (int j = 0; j < I; ++j) st->gram[i * kMaxP + j] = G[i * I + j];
+          st->hist = I;
+          double inv[kMaxP * kMaxP];
+          if (small_inverse(I, G, inv)) {
+            double test = 0.0;
+            for (int i = 0; i < I; ++i)
+              for (int j = 0; j < I; ++j) {
+                double t = 0.0;
+                for (int k = 0; k < I; ++k) t += inv[i * I + k] * G[k * I + j];
+                t -= (i == j) ? 1.0 : 0.0;
+                test += t * t;
+              }
+            if (test <= 1.0e-8) {
+              double x[kMaxP], A = 0.0;
+              for (int i = 0; i < I; ++i) {
+                x[i] = 0.0;
+                for (int k = 0; k < I; ++k) x[i] += inv[i * I + k];
+                A += x[i];
+              }
+              for (int i = 0; i < I; ++i) st->coeff[i] = x[i] / A;
+              used = 1;
+            }
+          }
+          if (!used) st->iter_bits |= kBitPulay;
+        }
+        st->pulay_used = used;
+        st->ncoeff = used ? I : 0;
+        for (int s = 0; s < S; ++s) st->theta_mix[s] = st->theta[s];
+        // InjectSchedule (mpDPFT.cpp:5229-5315)
+        if (kp.schedule == 5) {
+          for (int s = 0; s < S; ++s) {
+            double th = st->theta[s] * (st->cc < st->old_cc ? 1.1 : 0.5);
+            th = fmin(0.8, th);
+            th = fmax(10.0 / (double)kp.max_sc, th);
+            st->theta[s] = th;
+          }
+        } else if (kp.schedule == 9) {
+          for (int s = 0; s < S; ++s)
+            if (st->theta[s] < 0.2)
+              st->theta[s] = st->theta0[s] + (0.2 - st->theta0[s]) * (double)sc / (double)kp.max_sc;
+        }
+        if (a.log && sc < a.log_cap) {
+          mpdpft_iter_log& L = a.log[sc];
+          L.sc_count = sc;
+          L.mu_trials = st->mu_passes;
+          L.pulay_used = used;
+          L.status_bits = st->iter_bits;
+          L.cc = st->cc;
+          L.v_residual = st->v_res;
+          for (int s = 0; s < kMaxS; ++s) {
+            L.mu[s] = s < S ? st->mu[s] : 0.0;
+            L.abundance[s] = s < S ? st->ab[s] : 0.0;
+            L.theta[s] = s < S ? st->theta_mix[s] : 0.0;
+          }
+          L.ms = 0.0;
+        }
+        st->status_bits |= st->iter_bits;
+        st->mu_passes_total += st->mu_passes;
+        // StoreCurrentIteration of the next iteration; PrepareNextIteration
+        for (int s = 0; s < S; ++s) { st->old_mu[s] = st->mu[s]; st->old_ab[s] = st->ab[s]; }
+        st->old_cc = st->cc;
+        if (sc > 0) st->inc_v = fmin(1.0, st->inc_v + kp.inc_v0);  // (:4833)
+        st->mix_src = cur;
+        st->slot = next;
+        st->sc_count = sc + 1;
+      }
+    }
+  }
+  if (a.mode == 1) return;
+  if (!grid_barrier(st)) return;
+
+  // ---- phase E: mixed density -> ring[next] ----------------------------
+  {
+    const int used = ldcg(&st->pulay_used);
+    const int nc = ldcg(&st->ncoeff);
+    double coeff[kMaxP];
+    for (int i = 0; i < nc; ++i) coeff[i] = ldcg(&st->coeff[i]);
+    double th[kMaxS];
+    for (int s = 0; s < S; ++s) th[s] = ldcg(&st->theta_mix[s]);
+    R* out = a.nin + (long)next * S * n;
+    for (long p = tid; p < n; p += nthreads)
+      for (int s = 0; s < S; ++s) {
+        double v = 0.0;
+        if (used) {
+          for (int j = 0; j < nc; ++j) {
+            int slot = (cur - (nc - 1) + j + ring) % ring;
+            const long q = ((long)slot * S + s) * n + p;
+            v += coeff[j] * ((double)a.nin[q] + th[s] * (double)a.res[q]);
+          }
+        } else {
+          const long q = ((long)cur * S + s) * n + p;
+          v = (double)a.nin[q] + th[s] * (double)a.res[q];
+        }
+        out[(long)s * n + p] = R(v);
+      }
+  }
+}
+
+}  // namespace mpdpft

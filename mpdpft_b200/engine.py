@@ -1,0 +1,262 @@
+"""ctypes binding of libmpdpft_b200.so (the C ABI of include/mpdpft_gpu.h).
+
+This is the harness-side host layer: it names the operators after the
+reference functions they replace (GetDensity, getVint, EnforceConstraints,
+DelField, fftParallel, Integrate, AdmixDensities, GetData loop) and raises
+MpdpftError with the library's message when a call returns a non-zero
+status.  There is no fallback: if the CUDA library is missing or no sm_100
+device is present, construction fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpdpft_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_dpp = C.POINTER(_dp)
+_lib = None
+
+EXPORTS = [
+    "mpdpft_params_default", "mpdpft_abi_version", "mpdpft_struct_size", "mpdpft_last_error",
+    "mpdpft_status_string",
+    "mpdpft_ctx_create", "mpdpft_ctx_destroy", "mpdpft_ctx_sync", "mpdpft_ctx_stream",
+    "mpdpft_set_external_potential", "mpdpft_density", "mpdpft_vint", "mpdpft_update_v",
+    "mpdpft_mu_search", "mpdpft_delfield", "mpdpft_fft", "mpdpft_integrate", "mpdpft_pulay_reset",
+    "mpdpft_admix", "mpdpft_sc_run", "mpdpft_sc_step", "mpdpft_sc_init", "mpdpft_get_field",
+    "mpdpft_energy",
+]
+
+
+class MpdpftError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d): %s" % (_status_name(status), status, msg))
+        self.status = status
+
+
+def _status_name(st):
+    names = {v: k for k, v in vars(abi).items() if k.startswith("ERR_") or k == "OK"}
+    return names.get(st, "status")
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MpdpftError(abi.ERR_NO_DEVICE, "CUDA library %s not built (python -m mpdpft_b200.build)" % path)
+    L = C.CDLL(path)
+    P = C.POINTER(abi.Params)
+    vp = C.c_void_p
+    L.mpdpft_params_default.argtypes = [P]
+    L.mpdpft_params_default.restype = None
+    L.mpdpft_abi_version.restype = C.c_int
+    L.mpdpft_last_error.restype = C.c_char_p
+    L.mpdpft_status_string.restype = C.c_char_p
+    L.mpdpft_status_string.argtypes = [C.c_int]
+    L.mpdpft_ctx_create.argtypes = [P, C.c_int, C.POINTER(vp)]
+    L.mpdpft_ctx_destroy.argtypes = [vp]
+    L.mpdpft_ctx_sync.argtypes = [vp]
+    L.mpdpft_ctx_stream.argtypes = [vp]
+    L.mpdpft_ctx_stream.restype = vp
+    L.mpdpft_set_external_potential.argtypes = [vp, C.c_int, _dp, C.c_int, C.c_int]
+    L.mpdpft_density.argtypes = [vp, C.c_int, _dp, C.c_double, _dp, _dp, C.c_int, C.c_int]
+    L.mpdpft_vint.argtypes = [vp, C.c_int, C.c_int, _dpp, _dp, C.c_int, C.c_int]
+    L.mpdpft_update_v.argtypes = [vp, _dpp, C.c_double, _dpp, C.c_int, C.c_int]
+    L.mpdpft_mu_search.argtypes = [vp, C.c_int, _dp, C.c_double, _dp, _dp, C.POINTER(C.c_int), _dp,
+                                   C.c_int, C.c_int]
+    L.mpdpft_delfield.argtypes = [vp, _dp, _dp, _dp, C.c_int, C.c_int]
+    L.mpdpft_fft.argtypes = [vp, C.c_int, _dp, _dp, C.c_int]
+    L.mpdpft_integrate.argtypes = [vp, _dp, _dp, C.c_int, C.c_int]
+    L.mpdpft_pulay_reset.argtypes = [vp]
+    L.mpdpft_admix.argtypes = [vp, _dpp, _dpp, _dp, _dpp, _dp, C.POINTER(C.c_int), C.c_int, C.c_int]
+    L.mpdpft_sc_run.argtypes = [vp, _dpp, C.c_int, C.c_int, C.POINTER(abi.Result), C.POINTER(abi.IterLog), C.c_int]
+    L.mpdpft_sc_step.argtypes = [vp, C.c_int, C.POINTER(abi.IterLog)]
+    L.mpdpft_sc_init.argtypes = [vp, _dpp, C.c_int, C.c_int]
+    L.mpdpft_get_field.argtypes = [vp, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
+    L.mpdpft_energy.argtypes = [vp, C.POINTER(abi.Result)]
+    for name in EXPORTS:
+        getattr(L, name)
+    _lib = L
+    return L
+
+
+def _arr(x, n=None):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    if n is not None and a.size != n:
+        raise ValueError("expected %d values, got %d" % (n, a.size))
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _ptrs(arrays):
+    return (_dp * len(arrays))(*[_ptr(a) for a in arrays])
+
+
+class Engine:
+    """One SC solve context on one GPU (mpdpft_ctx)."""
+
+    def __init__(self, params, device=0):
+        self.lib = load()
+        self.params = params.copy()
+        h = C.c_void_p()
+        self._check(self.lib.mpdpft_ctx_create(C.byref(self.params), device, C.byref(h)))
+        self.h = h
+        self.S = params.species
+        self.n = params.steps ** params.dim
+
+    def _check(self, st):
+        if st != abi.OK:
+            raise MpdpftError(st, self.lib.mpdpft_last_error().decode())
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpdpft_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _count(self, layout):
+        return self.params.grid_points(layout)
+
+    # --- operators ------------------------------------------------------
+    def set_external_potential(self, s, vext, layout=abi.LAYOUT_PERIODIC):
+        a = _arr(vext, self._count(layout))
+        self._check(self.lib.mpdpft_set_external_potential(self.h, s, _ptr(a), layout, abi.MEM_HOST))
+
+    def GetDensity(self, s, v, mu, layout=abi.LAYOUT_PERIODIC):
+        """n[V] at mu and N = Integrate(n)."""
+        a = _arr(v, self._count(layout))
+        out = np.empty(self._count(layout))
+        N = C.c_double()
+        self._check(self.lib.mpdpft_density(self.h, s, _ptr(a), mu, _ptr(out), C.byref(N), layout, abi.MEM_HOST))
+        return out, N.value
+
+    def getVint(self, type_, s, dens, layout=abi.LAYOUT_PERIODIC):
+        arrs = [_arr(d, self._count(layout)) for d in dens]
+        out = np.empty(self._count(layout))
+        self._check(self.lib.mpdpft_vint(self.h, type_, s, _ptrs(arrs), _ptr(out), layout, abi.MEM_HOST))
+        return out
+
+    def UpdateV(self, dens, incremental=1.0, layout=abi.LAYOUT_PERIODIC):
+        arrs = [_arr(d, self._count(layout)) for d in dens]
+        outs = [np.empty(self._count(layout)) for _ in range(self.S)]
+        self._check(self.lib.mpdpft_update_v(self.h, _ptrs(arrs), incremental, _ptrs(outs), layout, abi.MEM_HOST))
+        return outs
+
+    def EnforceConstraints(self, s, v, n_target, mu, layout=abi.LAYOUT_PERIODIC, check=True):
+        a = _arr(v, self._count(layout))
+        mu_io = C.c_double(mu)
+        N = C.c_double()
+        tr = C.c_int()
+        out = np.empty(self._count(layout))
+        st = self.lib.mpdpft_mu_search(self.h, s, _ptr(a), n_target, C.byref(mu_io), C.byref(N), C.byref(tr),
+                                       _ptr(out), layout, abi.MEM_HOST)
+        if check:
+            self._check(st)
+        return mu_io.value, N.value, tr.value, out, st
+
+    def DelField(self, f, layout=abi.LAYOUT_PERIODIC):
+        a = _arr(f, self._count(layout))
+        g2 = np.empty(self._count(layout))
+        lap = np.empty(self._count(layout))
+        self._check(self.lib.mpdpft_delfield(self.h, _ptr(a), _ptr(g2), _ptr(lap), layout, abi.MEM_HOST))
+        return g2, lap
+
+    def fftParallel(self, sign, field):
+        f = np.asarray(field, dtype=np.complex128).reshape(-1)
+        if f.size != self.n:
+            raise ValueError("field size")
+        buf = np.ascontiguousarray(np.stack([f.real, f.imag], axis=-1).reshape(-1))
+        out = np.empty_like(buf)
+        self._check(self.lib.mpdpft_fft(self.h, sign, _ptr(buf), _ptr(out), abi.MEM_HOST))
+        return out[0::2] + 1j * out[1::2]
+
+    def Integrate(self, f, layout=abi.LAYOUT_PERIODIC):
+        a = _arr(f, self._count(layout))
+        out = C.c_double()
+        self._check(self.lib.mpdpft_integrate(self.h, _ptr(a), C.byref(out), layout, abi.MEM_HOST))
+        return out.value
+
+    def PulayReset(self):
+        self._check(self.lib.mpdpft_pulay_reset(self.h))
+
+    def AdmixDensities(self, n_in, n_out, theta=None, layout=abi.LAYOUT_PERIODIC, check=True):
+        ai = [_arr(x, self._count(layout)) for x in n_in]
+        ao = [_arr(x, self._count(layout)) for x in n_out]
+        outs = [np.empty(self._count(layout)) for _ in range(self.S)]
+        th = None if theta is None else _arr(theta)
+        coeffs = np.zeros(abi.MAX_PULAY)
+        nc = C.c_int(0)
+        st = self.lib.mpdpft_admix(self.h, _ptrs(ai), _ptrs(ao), None if th is None else _ptr(th), _ptrs(outs),
+                                   _ptr(coeffs), C.byref(nc), layout, abi.MEM_HOST)
+        if check and st not in (abi.OK, abi.ERR_PULAY_SINGULAR):
+            self._check(st)
+        return outs, coeffs[:nc.value].copy(), st
+
+    # --- SC loop ----------------------------------------------------------
+    def sc_run(self, vext, v0=None, layout=abi.LAYOUT_PERIODIC, log_cap=None, check=True):
+        for s in range(self.S):
+            self.set_external_potential(s, vext[s], layout)
+        v0p = None
+        if v0 is not None:
+            arrs = [_arr(x, self._count(layout)) for x in v0]
+            self._keep = arrs
+            v0p = _ptrs(arrs)
+        cap = log_cap or (self.params.max_sc_count + 2)
+        res = abi.Result()
+        log = (abi.IterLog * cap)()
+        st = self.lib.mpdpft_sc_run(self.h, v0p, layout, abi.MEM_HOST, C.byref(res), log, cap)
+        if check and st not in (abi.OK, abi.ERR_NOT_CONVERGED):
+            self._check(st)
+        return res, list(log[:min(res.iterations, cap)]), st
+
+    def sc_init(self, vext, v0=None, layout=abi.LAYOUT_PERIODIC):
+        for s in range(self.S):
+            self.set_external_potential(s, vext[s], layout)
+        v0p = None
+        if v0 is not None:
+            arrs = [_arr(x, self._count(layout)) for x in v0]
+            self._keep = arrs
+            v0p = _ptrs(arrs)
+        self._check(self.lib.mpdpft_sc_init(self.h, v0p, layout, abi.MEM_HOST))
+
+    def sc_step(self, graph=True, want_log=False):
+        log = abi.IterLog()
+        self._check(self.lib.mpdpft_sc_step(self.h, 1 if graph else 0, C.byref(log) if want_log else None))
+        return log if want_log else None
+
+    def sync(self):
+        self._check(self.lib.mpdpft_ctx_sync(self.h))
+
+    def stream(self):
+        return self.lib.mpdpft_ctx_stream(self.h)
+
+    def field(self, which, s, layout=abi.LAYOUT_PERIODIC):
+        out = np.empty(self._count(layout))
+        self._check(self.lib.mpdpft_get_field(self.h, which, s, _ptr(out), layout, abi.MEM_HOST))
+        return out
+
+    def energy(self):
+        r = abi.Result()
+        self._check(self.lib.mpdpft_energy(self.h, C.byref(r)))
+        return r

@@ -1,0 +1,117 @@
+"""Grid helpers and the synthetic workloads the engine is measured on.
+
+Every field is generated on the periodic s^D grid (x_i = -L/2 + i*dx,
+dx = L/s) and expanded to the reference's (s+1)^D layout by copying plane 0
+into plane s along each axis, which is what mpDPFT's fftParallel refill does
+(mpDPFT.cpp:8266-8324).  Inputs are seeded (numpy PCG64, seed base
+20261203); there is no dataset behind any of them.
+
+Workloads (one SC solve each unless stated):
+  harmonic_tf     3D trapped Fermi gas, TF density, contact g n, 64^3
+  argon_atom      Z=18 Gaussian nucleus, TF + gradient correction, Hartree,
+                  Dirac exchange, 128^3
+  sweep_2d        256 two-species 2D trapped gases, uneven grids (batched)
+  cluster_adjoint 13 Z=3 nuclei on an icosahedron, 192^3, adjoint loss
+  eh_plasma       two opposite-charge species on 256^3 in a random potential
+"""
+import math
+
+import numpy as np
+
+from . import abi
+
+SEED_BASE = 20261203
+
+
+def axis(steps, edge):
+    """Periodic-grid coordinates along one axis (rGrid, mpDPFT.cpp:7130)."""
+    dx = edge / steps
+    return -0.5 * edge + dx * np.arange(steps, dtype=np.float64)
+
+
+def radius2(dim, steps, edge):
+    x = axis(steps, edge)
+    if dim == 3:
+        return x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2
+    return x[:, None] ** 2 + x[None, :] ** 2
+
+
+def to_reference(f, dim):
+    """Periodic s^D array (any trailing shape flattened) -> (s+1)^D layout."""
+    f = np.asarray(f)
+    s = round(f.size ** (1.0 / dim)) if f.ndim == 1 else f.shape[0]
+    g = f.reshape((s,) * dim)
+    return np.pad(g, [(0, 1)] * dim, mode="wrap").reshape(-1)
+
+
+def to_periodic(f, dim):
+    """(s+1)^D layout -> periodic s^D (drops the duplicate planes)."""
+    f = np.asarray(f)
+    el = round(f.size ** (1.0 / dim))
+    g = f.reshape((el,) * dim)
+    sl = tuple(slice(0, el - 1) for _ in range(dim))
+    return np.ascontiguousarray(g[sl]).reshape(-1)
+
+
+def noise(shape, amplitude, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-amplitude, amplitude, size=shape)
+
+
+def gaussian_nucleus(dim, steps, edge, charge, sigma, centre=(0.0, 0.0, 0.0)):
+    """V = -Z erf(|r-R|/(sqrt(2) sigma))/|r-R|, the potential of a Gaussian
+    charge of width sigma (finite at r=R: -Z sqrt(2/pi)/sigma)."""
+    from scipy.special import erf
+
+    x = axis(steps, edge)
+    X, Y, Z = np.meshgrid(x - centre[0], x - centre[1], x - centre[2], indexing="ij")
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    out = np.empty_like(r)
+    small = r < 1e-12
+    out[~small] = -charge * erf(r[~small] / (math.sqrt(2.0) * sigma)) / r[~small]
+    out[small] = -charge * math.sqrt(2.0 / math.pi) / sigma
+    return out.reshape(-1)
+
+
+# ---------------------------------------------------------------- configs --
+
+def harmonic_tf(steps=64, edge=24.0, precision=abi.FP64, seed=SEED_BASE + 1, **over):
+    """3D harmonically trapped Fermi gas (hbar = m = omega = 1), N = 1000,
+    TF density, contact repulsion V = g n with g = 0.5 (type 10, beta = 0.25),
+    Pulay history 5, theta 0.3; V_0 = V_ext + U(-1e-3, 1e-3)."""
+    n_target = 1000.0
+    mu0 = (6.0 * n_target) ** (1.0 / 3.0)  # noninteracting TF estimate
+    kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[n_target],
+              rel_acc=1e-10, density_expression=abi.DENS_TF, degeneracy=1.0,
+              interactions=[abi.INT_CONTACT_SELF], beta=0.25, mu=[mu0],
+              mixer=1, pulay_scope=5, theta=[0.3], sc_criterion=1e-12,
+              max_sc_count=400, potential_tol=1e-8, precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    vext = 0.5 * radius2(3, steps, edge).reshape(-1)
+    v0 = vext + noise(vext.shape, 1e-3, seed)
+    return p, [vext], [v0]
+
+
+def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **over):
+    """Neutral atom Z = 18: Gaussian nucleus (sigma 0.1 bohr) at the centre of
+    [-10, 10]^3, TF + gradient correction (spectral grad V and Laplacian,
+    each smoothed by a Gaussian of width 0.2 bohr), Hartree by FFT Poisson,
+    Dirac exchange, g = 2, atomic units (gammaH = 1)."""
+    z = 18.0
+    kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z],
+              rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
+              interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
+              mu=[-0.5], mixer=1, pulay_scope=5, theta=[0.3], sc_criterion=1e-8,
+              max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
+              gradient_floor=5e-2, gradient_grad2=1.0, potential_tol=0.0,
+              precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    vext = gaussian_nucleus(3, steps, edge, z, 0.1)
+    v0 = vext + noise(vext.shape, 1e-3, seed)
+    return p, [vext], [v0]
+
+
+def workload_names():
+    return ["harmonic_tf", "argon_atom"]
