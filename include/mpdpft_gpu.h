@@ -257,6 +257,35 @@ int mpdpft_get_field(mpdpft_ctx* ctx, int which, int s, double* out, int layout,
 /* Energies of the current state (GetEnergy, mpDPFT.cpp:5414-5436). */
 int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result);
 
+/* Stage timing (the reference's StartTimer/EndTimer per routine,
+ * mpDPFT.cpp:11997-12003): launch one stage `reps` times on the context
+ * stream, timed with CUDA events; returns the mean device time per launch
+ * and the algorithmic bytes one launch must move (its own inputs and
+ * outputs, each field counted once).  MPDPFT_STAGE_SC_STEP runs real SC
+ * iterations on the current state (after mpdpft_sc_init); the FFT stages
+ * transform a zeroed scratch spectrum. */
+enum {
+  MPDPFT_STAGE_SC_STEP = 0,   /* persistent SC-step kernel (mu search .. mix) */
+  MPDPFT_STAGE_FFT_Z_R2C = 1, /* R2C pass along the contiguous axis           */
+  MPDPFT_STAGE_FFT_Y = 2,     /* C2C pass along y (3D)                        */
+  MPDPFT_STAGE_FFT_X = 3,     /* x-axis round trip with one k-space multiplier */
+  MPDPFT_STAGE_FFT_Z_C2R = 4, /* C2R pass along the contiguous axis           */
+  MPDPFT_STAGE_ITERATION = 5  /* one whole SC iteration (graph replay)        */
+};
+int mpdpft_profile_stage(mpdpft_ctx* ctx, int stage, int reps, double* ms_per_launch,
+                         double* bytes_per_launch);
+
+/* Kernel launches in one SC iteration as captured in its CUDA graph:
+ * counts[i] for i = MPDPFT_STAGE_SC_STEP .. MPDPFT_STAGE_FFT_Z_C2R, counts[5]
+ * for the remaining (pointwise) kernels; *total = their sum.  Valid after
+ * the first graph-mode mpdpft_sc_step. */
+int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
+
+/* Phase durations (microseconds, block 0 of the grid) of the last SC-step
+ * kernel: [0] V update, [1] mu search, [2] densities/residual/Gram row,
+ * [3] convergence test and Pulay solve, [4] grid barrier, [5] mix. */
+int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n);
+
 #ifdef __cplusplus
 }
 #endif

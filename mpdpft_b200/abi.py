@@ -50,6 +50,13 @@ FIELD_GRAD2 = 2
 FIELD_LAPLACIAN = 3
 FIELD_EXTERNAL = 4
 
+STAGE_SC_STEP = 0
+STAGE_FFT_Z_R2C = 1
+STAGE_FFT_Y = 2
+STAGE_FFT_X = 3
+STAGE_FFT_Z_C2R = 4
+STAGE_ITERATION = 5
+
 _D4 = C.c_double * MAX_SPECIES
 
 

@@ -244,4 +244,33 @@ int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result) {
   return ctx->impl.fill_result(result, h);
 }
 
+int mpdpft_profile_stage(mpdpft_ctx* ctx, int stage, int reps, double* ms_per_launch, double* bytes_per_launch) {
+  CHECK_CTX(ctx);
+  if (reps < 1 || !ms_per_launch) return set_error(MPDPFT_ERR_ARG, "bad profile arguments");
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.profile_stage(stage, reps, ms_per_launch, bytes_per_launch);
+}
+
+int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total) {
+  CHECK_CTX(ctx);
+  int t = 0;
+  for (int i = 0; i < 6; ++i) {
+    if (counts) counts[i] = ctx->impl.iter_cnt[i];
+    t += ctx->impl.iter_cnt[i];
+  }
+  if (total) *total = t;
+  return MPDPFT_OK;
+}
+
+int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n) {
+  CHECK_CTX(ctx);
+  if (!us || n < 1) return set_error(MPDPFT_ERR_ARG, "bad arguments");
+  cudaSetDevice(ctx->impl.device);
+  mpdpft::ScState h;
+  int st = ctx->impl.read_state(&h);
+  if (st) return st;
+  for (int i = 0; i < n && i < 6; ++i) us[i] = 1e-3 * (double)(h.tphase[i + 1] - h.tphase[i]);
+  return MPDPFT_OK;
+}
+
 }  // extern "C"

@@ -175,6 +175,69 @@ __device__ __forceinline__ R density_at(const DensParams& d, R u, R lap, R g2) {
   return r > R(0) ? r : R(0);
 }
 
+// 1/sqrt(u) for u > 0 to double precision: FP32 hardware estimate refined by
+// two Newton steps r <- r (3 - u r^2)/2 in double (the error squares each
+// step: ~2^-23 -> ~2^-46 -> below double rounding).  Inputs below the FP32
+// normal range fall back to the library division.
+__device__ __forceinline__ double rsqrt_d(double u) {
+  if (u < 1.0e-30 || u > 1.0e30) return 1.0 / sqrt(u);
+  double r = (double)rsqrtf((float)u);
+  double h = 0.5 * u;
+  r = r * fma(-h * r, r, 1.5);
+  r = r * fma(-h * r, r, 1.5);
+  return r;
+}
+
+// The density functionals in double, for the particle-number integral and
+// the mu search (same formulas as density_at; square roots via rsqrt_d).
+__device__ __forceinline__ double density_at_d(const DensParams& d, double u, double lap, double g2) {
+  if (d.expr == MPDPFT_DENS_TF) {
+    if (!(u > 0.0)) return 0.0;
+    if (d.dim == 3) return (1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * u * u * rsqrt_d(u);
+    return (d.g / (2.0 * kPi)) * u;
+  }
+  if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 3) {
+    if (!(u > 0.0)) return 0.0;
+    const double ctf = 2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi);
+    const double cg = 1.4142135623730951 * d.g / (48.0 * kPi * kPi);
+    const double r = rsqrt_d(u);
+    double m1, m3;
+    if (u >= d.floor_u) { m1 = r; m3 = r * r * r; }
+    else {
+      const double rf = rsqrt_d(d.floor_u);
+      m1 = u * rf / d.floor_u;
+      m3 = m1 / d.floor_u;
+    }
+    const double v = ctf * u * u * r - cg * (lap * m1 + 0.25 * d.c2 * g2 * m3);
+    return v > 0.0 ? v : 0.0;
+  }
+  return density_at<double>(d, u, lap, g2);
+}
+
+// FP32 evaluation for the mixed-precision mu search: u is formed in double
+// from the double candidate mu and then rounded once, so N(mu) keeps the
+// resolution of double mu (a staircase of 2M per-point steps of relative size
+// ~1e-7 / 2M, far below RelAcc); the sum is accumulated in double.
+__device__ __forceinline__ float density_at_f(const DensParams& d, float u, float lap, float g2) {
+  if (d.expr == MPDPFT_DENS_TF) {
+    if (!(u > 0.f)) return 0.f;
+    if (d.dim == 3) return float(1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * u * u * rsqrtf(u);
+    return float(d.g / (2.0 * kPi)) * u;
+  }
+  if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 3) {
+    if (!(u > 0.f)) return 0.f;
+    const float ctf = float(2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi));
+    const float cg = float(1.4142135623730951 * d.g / (48.0 * kPi * kPi));
+    const float fl = float(d.floor_u);
+    float m1, m3;
+    if (u >= fl) { m1 = rsqrtf(u); m3 = m1 * m1 * m1; }
+    else { m1 = u * float(1.0 / (d.floor_u * sqrt(d.floor_u))); m3 = m1 / fl; }
+    const float v = ctf * u * u * rsqrtf(u) - cg * (lap * m1 + 0.25f * float(d.c2) * g2 * m3);
+    return v > 0.f ? v : 0.f;
+  }
+  return density_at<float>(d, u, lap, g2);
+}
+
 // d n / d mu at u (used to place mu candidates; accuracy is not critical).
 template <typename R>
 __device__ __forceinline__ R density_slope(const DensParams& d, R u) {

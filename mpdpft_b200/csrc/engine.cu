@@ -375,6 +375,7 @@ int Ctx::launch_step(int mode) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e;
+  cnt[MPDPFT_STAGE_SC_STEP]++;
   if (rsize == sizeof(double)) e = cudaLaunchKernelEx(&cfg, sc_step_kernel<double>, step_args<double>(mode));
   else e = cudaLaunchKernelEx(&cfg, sc_step_kernel<float>, step_args<float>(mode));
   if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("sc_step launch: ") + cudaGetErrorString(e));
@@ -438,7 +439,9 @@ int Ctx::sc_step(int use_graph) {
   if (!use_graph) return issue_iteration();
   if (!graph_exec) {
     CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < 6; ++i) cnt[i] = 0;
     st = issue_iteration();
+    for (int i = 0; i < 6; ++i) iter_cnt[i] = cnt[i];
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (st) { if (g) cudaGraphDestroy(g); return st; }

@@ -57,6 +57,8 @@ struct Ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   FftPlan* fft = nullptr;
+  int cnt[6] = {0, 0, 0, 0, 0, 0};       // launches issued, by stage
+  int iter_cnt[6] = {0, 0, 0, 0, 0, 0};  // launches in the captured iteration
 
   ~Ctx();
   void release();
@@ -103,6 +105,7 @@ struct Ctx {
   int pointwise_vint(int type, int s, void* out);
   int full_c2c(void* buf, int sign);
   int alloc_io(long doubles);
+  int profile_stage(int stage, int reps, double* ms, double* bytes);
 };
 
 }  // namespace mpdpft

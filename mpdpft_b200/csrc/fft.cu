@@ -17,6 +17,8 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -33,6 +35,25 @@ namespace mpdpft {
   } while (0)
 
 constexpr int kFftThreads = 256;
+
+// Raise a kernel's dynamic shared memory limit to the device's per-block
+// opt-in maximum minus the kernel's static shared memory (once per kernel).
+template <typename F>
+static cudaError_t smem_optin(F* fn) {
+  static std::mutex mu;
+  static std::set<const void*> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count((const void*)fn)) return cudaSuccess;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes at;
+  if ((e = cudaFuncGetAttributes(&at, fn)) != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)at.sharedSizeBytes);
+  if (e == cudaSuccess) done.insert((const void*)fn);
+  return e;
+}
 
 // ------------------------------------------------------------ plan ------
 static bool factor(int len, RadixPlan& p) {
@@ -113,79 +134,132 @@ struct ZArgs {
 // R2C along the contiguous axis.  Block = zl rows; each row of s reals is
 // read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
 // into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
+// Input value of the R2C pass at element p (prologue: taper or charge sum).
 template <typename R>
+__device__ __forceinline__ R z_input(const ZArgs<R>& a, long p, double shift) {
+  R x;
+  if (a.pro == PRO_CHARGE) {
+    double t = 0.0;
+    for (int q = 0; q < a.nsrc; ++q) t += a.qcoef[q] * (double)a.in[(long)q * a.g.n + p];
+    x = R(t);
+  } else {
+    x = a.in[p];
+  }
+  if (a.pro == PRO_TAPER) {  // DelField boundary taper (mpDPFT.cpp:7251-7264)
+    double px, py, pz;
+    point_coords(p, a.g, px, py, pz);
+    const double r = sqrt(px * px + py * py + pz * pz);
+    double f = (double)x - shift;
+    if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
+    x = R(f);
+  }
+  return x;
+}
+
+// R2C along the contiguous axis.  Block = zl rows; each row of s reals is
+// read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
+// into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
+template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  C* A = reinterpret_cast<C*>(smem_raw);
-  C* B = A + a.M * a.zl;
-  const long row0 = (long)blockIdx.x * a.zl;
+  const int M = NC > 0 ? NC : a.M;
+  const int zl = NC > 0 ? NL : a.zl;
+  const int H = M + 1;
+  const long row0 = (long)blockIdx.x * zl;
   const int s = a.g.s;
   double shift = 0.0;  // no shell points: no shift
   if (a.pro == PRO_TAPER && *a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
   double rowsum = 0.0;
-  for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
-    const int l = w / a.M, m = w % a.M;
-    const long row = row0 + l;
-    C z = {R(0), R(0)};
-    if (row < a.rows) {
+  C* Z;
+  if constexpr (NC > 0) {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + NC * NL;
+    Z = B + NC * NL;
+    C* tws = Z + NC * NL;
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = a.tw_m[i];
+    __syncthreads();
+    auto load = [&](int m, int l) -> C {
+      const long row = row0 + l;
+      if (row >= a.rows) return C{R(0), R(0)};
       const long p0 = row * s + 2 * m;
       R x0, x1;
-      if (a.pro == PRO_CHARGE) {
-        double t0 = 0.0, t1 = 0.0;
-        for (int q = 0; q < a.nsrc; ++q) {
-          t0 += a.qcoef[q] * (double)a.in[(long)q * a.g.n + p0];
-          t1 += a.qcoef[q] * (double)a.in[(long)q * a.g.n + p0 + 1];
-        }
-        x0 = R(t0); x1 = R(t1);
+      if (a.pro == PRO_NONE) {
+        const C v = *reinterpret_cast<const C*>(a.in + p0);  // 2 reals, aligned (s even)
+        x0 = v.x;
+        x1 = v.y;
       } else {
-        x0 = a.in[p0];
-        x1 = a.in[p0 + 1];
-      }
-      if (a.pro == PRO_TAPER) {  // DelField boundary taper (mpDPFT.cpp:7251-7264)
-        double x, y, zc;
-        point_coords(p0, a.g, x, y, zc);
-        double r2a = x * x + y * y, za = zc, zb = zc + a.g.dx;
-        double ra = sqrt(r2a + za * za), rb = sqrt(r2a + zb * zb);
-        double fa = (double)x0 - shift, fb = (double)x1 - shift;
-        if (ra > a.taper_r0) fa *= exp(a.taper_a * (ra - a.taper_r0) * (ra - a.taper_r0));
-        if (rb > a.taper_r0) fb *= exp(a.taper_a * (rb - a.taper_r0) * (rb - a.taper_r0));
-        x0 = R(fa); x1 = R(fb);
+        x0 = z_input<R>(a, p0, shift);
+        x1 = z_input<R>(a, p0 + 1, shift);
       }
       rowsum += (double)x0 + (double)x1;
-      z = {x0, x1};
+      return C{x0, x1};
+    };
+    auto store = [&](int m, int l, C v) { Z[m * NL + l] = v; };
+    fft_lines<C, NC, NL, true>(A, B, tws, -1, load, store);
+    if (a.part) {
+      double acc[1] = {rowsum};
+      block_reduce_store<1>(acc, a.part + blockIdx.x);
     }
-    A[m * a.zl + l] = z;
+  } else {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + M * zl;
+    for (int w = threadIdx.x; w < M * zl; w += blockDim.x) {
+      const int l = w / M, m = w % M;
+      const long row = row0 + l;
+      C z = {R(0), R(0)};
+      if (row < a.rows) {
+        const long p0 = row * s + 2 * m;
+        R x0 = z_input<R>(a, p0, shift), x1 = z_input<R>(a, p0 + 1, shift);
+        rowsum += (double)x0 + (double)x1;
+        z = {x0, x1};
+      }
+      A[m * zl + l] = z;
+    }
+    if (a.part) {
+      double acc[1] = {rowsum};
+      block_reduce_store<1>(acc, a.part + blockIdx.x);
+    }
+    __syncthreads();
+    Z = tile_fft<C>(A, B, a.plan, zl, a.tw_m, -1);
   }
-  if (a.part) {
-    double acc[1] = {rowsum};
-    block_reduce_store<1>(acc, a.part + blockIdx.x);
-  }
-  __syncthreads();
-  C* Z = tile_fft<C>(A, B, a.plan, a.zl, a.tw_m, -1);
-  for (int w = threadIdx.x; w < a.H * a.zl; w += blockDim.x) {
-    const int l = w / a.H, q = w % a.H;
+  for (int w = threadIdx.x; w < H * zl; w += blockDim.x) {
+    const int l = w / H, q = w % H;
     const long row = row0 + l;
     if (row >= a.rows) continue;
-    C zq = Z[(q % a.M) * a.zl + l];
-    C zc = cconj(Z[((a.M - q) % a.M) * a.zl + l]);
+    C zq = Z[(q % M) * zl + l];
+    C zc = cconj(Z[((M - q) % M) * zl + l]);
     C E = cscale(cadd(zq, zc), R(0.5));
     C D = csub(zq, zc);             // 2 i O_q
     C O = {D.y * R(0.5), -D.x * R(0.5)};
     C t = a.tw_n[q];               // e^{-2 pi i q/s}, q <= M < s
-    a.out[row * a.H + q] = cadd(E, cmul(t, O));
+    a.out[row * H + q] = cadd(E, cmul(t, O));
   }
 }
 
-// C2R along the contiguous axis for nin half-spectrum rows, with epilogue.
+// Epilogue value of the C2R pass at element p (single-field epilogues).
 template <typename R>
+__device__ __forceinline__ R z_output(const ZArgs<R>& a, long p, R v, double f0) {
+  if (a.epi == EPI_POS) return v > R(0) ? v : R(0);
+  if (a.epi == EPI_COULOMB) {  // mpDPFT.cpp:2704-2711
+    double x, y, z;
+    point_coords(p, a.g, x, y, z);
+    const double r = sqrt(x * x + y * y + z * z);
+    const double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
+    return R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
+  }
+  return v;
+}
+
+// C2R along the contiguous axis for nin half-spectrum rows, with epilogue.
+template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  C* A = reinterpret_cast<C*>(smem_raw);
-  C* B = A + a.M * a.zl;
-  R* acc = reinterpret_cast<R*>(B + a.M * a.zl);  // [zl][s]
-  const long row0 = (long)blockIdx.x * a.zl;
+  const int M = NC > 0 ? NC : a.M;
+  const int zl = NC > 0 ? NL : a.zl;
+  const int H = M + 1;
+  const long row0 = (long)blockIdx.x * zl;
   const int s = a.g.s;
   double f0 = 0.0;
   if (a.epi == EPI_COULOMB) {
@@ -193,66 +267,98 @@ __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
     for (int b = 0; b < a.f0_blocks; ++b) t += a.f0_part[b];
     f0 = t * a.g.dvol;
   }
-  for (int f = 0; f < a.nin; ++f) {
-    const C* X = a.cin[f];
-    for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
-      const int l = w / a.M, q = w % a.M;
-      const long row = row0 + l;
-      C z = {R(0), R(0)};
-      if (row < a.rows) {
-        C xq = X[row * a.H + q];
-        C xc = cconj(X[row * a.H + (a.M - q)]);
+  if constexpr (NC > 0) {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + NC * NL;
+    C* tws = B + NC * NL;
+    R* acc = reinterpret_cast<R*>(tws + NC);  // [NL][s] (EPI_GRAD)
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = a.tw_m[i];
+    __syncthreads();
+    for (int f = 0; f < a.nin; ++f) {
+      const C* X = a.cin[f];
+      auto load = [&](int q, int l) -> C {
+        const long row = row0 + l;
+        if (row >= a.rows) return C{R(0), R(0)};
+        C xq = X[row * H + q];
+        C xc = cconj(X[row * H + (NC - q)]);
         C E = cadd(xq, xc);   // 2 E_q
         C D = csub(xq, xc);   // 2 e^{-2 pi i q/s} O_q
-        C t = cconj(a.tw_n[q]);
-        C O = cmul(t, D);     // 2 O_q
-        z = {E.x - O.y, E.y + O.x};  // 2 (E_q + i O_q)
-      }
-      A[q * a.zl + l] = z;
-    }
-    __syncthreads();
-    C* Z = tile_fft<C>(A, B, a.plan, a.zl, a.tw_m, +1);
-    for (int w = threadIdx.x; w < a.M * a.zl; w += blockDim.x) {
-      const int l = w / a.M, m = w % a.M;
-      C z = Z[m * a.zl + l];
-      R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
-      R* dst = acc + (long)l * s + 2 * m;
-      if (a.epi == EPI_GRAD) {
-        if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
-        else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
-        else {
-          const long row = row0 + l;
-          if (row < a.rows) {
-            a.rout[0][row * s + 2 * m] = dst[0];
-            a.rout[0][row * s + 2 * m + 1] = dst[1];
-            a.rout[1][row * s + 2 * m] = x0;
-            a.rout[1][row * s + 2 * m + 1] = x1;
+        C O = cmul(cconj(a.tw_n[q]), D);  // 2 O_q
+        return C{E.x - O.y, E.y + O.x};   // 2 (E_q + i O_q)
+      };
+      auto store = [&](int m, int l, C z) {
+        const long row = row0 + l;
+        if (row >= a.rows) return;
+        const R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
+        const long p0 = row * s + 2 * m;
+        if (a.epi == EPI_GRAD) {
+          R* dst = acc + (long)l * s + 2 * m;
+          if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
+          else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
+          else {
+            *reinterpret_cast<C*>(a.rout[0] + p0) = C{dst[0], dst[1]};
+            *reinterpret_cast<C*>(a.rout[1] + p0) = C{x0, x1};
           }
+        } else {
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{z_output<R>(a, p0, x0, f0), z_output<R>(a, p0 + 1, x1, f0)};
         }
-      } else {
-        dst[0] = x0;
-        dst[1] = x1;
+      };
+      fft_lines<C, NC, NL, true>(A, B, tws, +1, load, store);
+    }
+  } else {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + M * zl;
+    R* acc = reinterpret_cast<R*>(B + M * zl);  // [zl][s]
+    for (int f = 0; f < a.nin; ++f) {
+      const C* X = a.cin[f];
+      for (int w = threadIdx.x; w < M * zl; w += blockDim.x) {
+        const int l = w / M, q = w % M;
+        const long row = row0 + l;
+        C z = {R(0), R(0)};
+        if (row < a.rows) {
+          C xq = X[row * H + q];
+          C xc = cconj(X[row * H + (M - q)]);
+          C E = cadd(xq, xc);
+          C D = csub(xq, xc);
+          C O = cmul(cconj(a.tw_n[q]), D);
+          z = {E.x - O.y, E.y + O.x};
+        }
+        A[q * zl + l] = z;
       }
+      __syncthreads();
+      C* Z = tile_fft<C>(A, B, a.plan, zl, a.tw_m, +1);
+      for (int w = threadIdx.x; w < M * zl; w += blockDim.x) {
+        const int l = w / M, m = w % M;
+        C z = Z[m * zl + l];
+        R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
+        R* dst = acc + (long)l * s + 2 * m;
+        if (a.epi == EPI_GRAD) {
+          if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
+          else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
+          else {
+            const long row = row0 + l;
+            if (row < a.rows) {
+              a.rout[0][row * s + 2 * m] = dst[0];
+              a.rout[0][row * s + 2 * m + 1] = dst[1];
+              a.rout[1][row * s + 2 * m] = x0;
+              a.rout[1][row * s + 2 * m + 1] = x1;
+            }
+          }
+        } else {
+          dst[0] = x0;
+          dst[1] = x1;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
-  }
-  if (a.epi == EPI_GRAD) return;
-  for (int w = threadIdx.x; w < s * a.zl; w += blockDim.x) {
-    const int l = w / s, k = w % s;
-    const long row = row0 + l;
-    if (row >= a.rows) continue;
-    const long p = row * s + k;
-    R v = acc[(long)l * s + k];
-    if (a.epi == EPI_POS) {
-      v = v > R(0) ? v : R(0);
-    } else if (a.epi == EPI_COULOMB) {  // mpDPFT.cpp:2704-2711
-      double x, y, z;
-      point_coords(p, a.g, x, y, z);
-      double r = sqrt(x * x + y * y + z * z);
-      double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
-      v = R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
+    if (a.epi == EPI_GRAD) return;
+    for (int w = threadIdx.x; w < s * zl; w += blockDim.x) {
+      const int l = w / s, k = w % s;
+      const long row = row0 + l;
+      if (row >= a.rows) continue;
+      const long p = row * s + k;
+      a.rout[0][p] = z_output<R>(a, p, acc[(long)l * s + k], f0);
     }
-    a.rout[0][p] = v;
   }
 }
 
@@ -300,28 +406,55 @@ __device__ __forceinline__ bool axis_line(const AxisArgs<R>& a, int l, long& bas
   return true;
 }
 
-template <typename R>
+template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  C* A = reinterpret_cast<C*>(smem_raw);
-  C* B = A + a.s * a.tk;
   C* data = a.data[blockIdx.y];
-  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
-    const int t = w / a.tk, l = w % a.tk;
-    long base, outer;
-    int col;
-    C v = {R(0), R(0)};
-    if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
-    A[t * a.tk + l] = v;
-  }
-  __syncthreads();
-  C* res = tile_fft<C>(A, B, a.plan, a.tk, a.dir < 0 ? a.twf : a.twb, a.dir);
-  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
-    const int t = w / a.tk, l = w % a.tk;
-    long base, outer;
-    int col;
-    if (axis_line(a, l, base, outer, col)) data[base + t * a.astride] = res[t * a.tk + l];
+  const C* twg = a.dir < 0 ? a.twf : a.twb;
+  if constexpr (NC > 0) {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + NC * NL;
+    C* tws = B + NC * NL;
+    __shared__ long s_base[NL];
+    __shared__ int s_ok[NL];
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = twg[i];
+    if (threadIdx.x < NL) {
+      long base, outer;
+      int col;
+      s_ok[threadIdx.x] = axis_line(a, threadIdx.x, base, outer, col) ? 1 : 0;
+      s_base[threadIdx.x] = base;
+    }
+    __syncthreads();
+    const long as = a.astride;
+    auto load = [&](int t, int l) -> C {
+      return s_ok[l] ? data[s_base[l] + t * as] : C{R(0), R(0)};
+    };
+    auto store = [&](int t, int l, C v) {
+      if (s_ok[l]) data[s_base[l] + t * as] = v;
+    };
+    fft_lines<C, NC, NL, false>(A, B, tws, a.dir, load, store);
+  } else {
+    const int n = a.s;
+    const int tk = a.tk;
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + n * tk;
+    for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
+      const int t = w / tk, l = w % tk;
+      long base, outer;
+      int col;
+      C v = {R(0), R(0)};
+      if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+      A[t * tk + l] = v;
+    }
+    __syncthreads();
+    C* res = tile_fft<C>(A, B, a.plan, tk, twg, a.dir);
+    for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
+      const int t = w / tk, l = w % tk;
+      long base, outer;
+      int col;
+      if (axis_line(a, l, base, outer, col)) data[base + t * a.astride] = res[t * tk + l];
+    }
   }
 }
 
@@ -330,13 +463,59 @@ __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
 // Nyquist index s/2 carries k = -pi/dx (mpDPFT.cpp:889-895).
 __device__ __forceinline__ int signed_freq(int t, int s) { return t < s / 2 ? t : t - s; }
 
+// k-space multiplier of the x round trip for element (t along x, line of
+// outer index `outer`, column `col`) and output o; v is the forward
+// transform value, the return value what the inverse transform receives.
 template <typename R>
+__device__ __forceinline__ typename Cx<R>::T apply_multiplier(const AxisArgs<R>& a, typename Cx<R>::T v, int t,
+                                                             long outer, int col, int o, double f0) {
+  using C = typename Cx<R>::T;
+  const int qx = signed_freq(t, a.s);
+  const int qy = a.dim == 3 ? signed_freq((int)outer, a.s) : 0;
+  const double kx = a.dk * (t == a.s / 2 ? -(double)(a.s / 2) : (double)qx);
+  const double ky = a.dk * (double)qy;
+  const double kz = a.dk * (col == a.M ? -(double)a.M : (double)col);  // col M: Nyquist
+  const double k2 = kx * kx + ky * ky + (a.dim == 3 ? kz * kz : 0.0);
+  if (a.mul == MUL_COULOMB_REG) {
+    // (n~ - n~0 e^{-k^2})/k^2, k = 0 -> n~0 (mpDPFT.cpp:2686-2701); the
+    // centred transform's phase (-1)^{qx+qy+qz} carries over to the
+    // subtracted Gaussian in this frame
+    if (k2 > 1.0e-6 * a.dk * a.dk) {
+      const int par = (t + (int)outer * (a.dim == 3) + col) & 1;
+      const double g = exp(-k2) * f0 * (par ? -1.0 : 1.0);
+      return C{R(((double)v.x - g) / k2 * a.scale), R((double)v.y / k2 * a.scale)};
+    }
+    return C{R(f0 * a.scale), R(0)};
+  }
+  double fr;
+  bool imag = false;
+  if (a.mul == MUL_COULOMB_TRUNC) {
+    fr = k2 > 0.0 ? (1.0 - cos(sqrt(k2) * a.cutoff)) / k2 : 0.5 * a.cutoff * a.cutoff;
+  } else if (a.mul == MUL_SMOOTH) {
+    fr = exp(a.sigma_c * k2);
+  } else {  // MUL_DERIV: outputs d/dx, d/dy (, d/dz), Laplacian
+    const double sm = exp(a.sigma_c * k2);
+    if (o < a.dim) {
+      // i k_j: the reference takes Im of IFT(-k f~), which drops the
+      // Nyquist index of axis j (mpDPFT.cpp:7442-7444)
+      double kj;
+      if (a.dim == 3) kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (o == 1 ? ((int)outer == a.s / 2 ? 0.0 : ky) : (col == a.M ? 0.0 : kz));
+      else kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (col == a.M ? 0.0 : kz);
+      fr = kj * sm;
+      imag = true;
+    } else {
+      fr = -k2 * sm * sm;  // Laplacian smoothed twice (mpDPFT.cpp:7477, 7577)
+    }
+  }
+  fr *= a.scale;
+  if (imag) return C{R(-fr * (double)v.y), R(fr * (double)v.x)};
+  return C{R(fr * (double)v.x), R(fr * (double)v.y)};
+}
+
+template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  C* A = reinterpret_cast<C*>(smem_raw);
-  C* B = A + a.s * a.tk;
-  C* W = B + a.s * a.tk;
   __shared__ double s_f0;
   if (a.mul == MUL_COULOMB_REG) {
     if (threadIdx.x < 32) {
@@ -347,80 +526,78 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
     }
   }
   C* data = a.data[0];
-  for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
-    const int t = w / a.tk, l = w % a.tk;
-    long base, outer;
-    int col;
-    C v = {R(0), R(0)};
-    if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
-    A[t * a.tk + l] = v;
-  }
-  __syncthreads();
-  C* F = tile_fft<C>(A, B, a.plan, a.tk, a.twf, -1);
-  C* spare = (F == A) ? B : A;  // two free buffers: spare and W
-  for (int o = 0; o < a.nout; ++o) {
-    for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
-      const int t = w / a.tk, l = w % a.tk;
+  if constexpr (NC > 0) {
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + NC * NL;
+    C* F = B + NC * NL;
+    C* twf = F + NC * NL;
+    C* twb = twf + NC;
+    __shared__ long s_base[NL];
+    __shared__ long s_outer[NL];
+    __shared__ int s_col[NL];
+    __shared__ int s_ok[NL];
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) { twf[i] = a.twf[i]; twb[i] = a.twb[i]; }
+    if (threadIdx.x < NL) {
       long base, outer;
       int col;
-      C v = F[t * a.tk + l];
-      if (!axis_line(a, l, base, outer, col)) { spare[t * a.tk + l] = v; continue; }
-      const int qx = signed_freq(t, a.s);
-      const int qy = a.dim == 3 ? signed_freq((int)outer, a.s) : 0;
-      const int qz = col;  // 0..M; M is the Nyquist column
-      const double kx = a.dk * (t == a.s / 2 ? -(double)(a.s / 2) : (double)qx);
-      const double ky = a.dk * (double)qy;
-      const double kz = a.dk * (col == a.M ? -(double)a.M : (double)qz);
-      const double k2 = kx * kx + ky * ky + (a.dim == 3 ? kz * kz : 0.0);
-      double fr = 0.0;  // real multiplier
-      bool imag = false;
-      if (a.mul == MUL_COULOMB_REG) {
-        // (n~ - n~0 e^{-k^2})/k^2, k = 0 -> n~0 (mpDPFT.cpp:2686-2701); the
-        // centred transform's phase (-1)^{qx+qy+qz} carries over to the
-        // subtracted Gaussian in this frame
-        if (k2 > 1.0e-6 * a.dk * a.dk) {
-          const int par = ((t + (int)outer * (a.dim == 3) + col) & 1);
-          const double g = exp(-k2) * s_f0 * (par ? -1.0 : 1.0);
-          v = {R(((double)v.x - g) / k2 * a.scale), R((double)v.y / k2 * a.scale)};
-        } else {
-          v = {R(s_f0 * a.scale), R(0)};
-        }
-        spare[t * a.tk + l] = v;
-        continue;
-      } else if (a.mul == MUL_COULOMB_TRUNC) {
-        fr = k2 > 0.0 ? (1.0 - cos(sqrt(k2) * a.cutoff)) / k2 : 0.5 * a.cutoff * a.cutoff;
-      } else if (a.mul == MUL_SMOOTH) {
-        fr = exp(a.sigma_c * k2);
-      } else {  // MUL_DERIV: outputs d/dx, d/dy, d/dz (or 2D: d/dx, d/dy), Laplacian
-        const double sm = exp(a.sigma_c * k2);
-        const int nd = a.dim;
-        if (o < nd) {
-          // i k_j: the reference takes Im of IFT(-k f~), which drops the
-          // Nyquist index of axis j (mpDPFT.cpp:7442-7444)
-          double kj;
-          if (a.dim == 3) kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (o == 1 ? ((int)outer == a.s / 2 ? 0.0 : ky) : (col == a.M ? 0.0 : kz));
-          else kj = (o == 0) ? (t == a.s / 2 ? 0.0 : kx) : (col == a.M ? 0.0 : kz);
-          fr = kj * sm;
-          imag = true;
-        } else {
-          fr = -k2 * sm * sm;  // Laplacian smoothed twice (mpDPFT.cpp:7477, 7577)
-        }
+      s_ok[threadIdx.x] = axis_line(a, threadIdx.x, base, outer, col) ? 1 : 0;
+      s_base[threadIdx.x] = base;
+      s_outer[threadIdx.x] = outer;
+      s_col[threadIdx.x] = col;
+    }
+    __syncthreads();
+    const long as = a.astride;
+    auto gload = [&](int t, int l) -> C { return s_ok[l] ? data[s_base[l] + t * as] : C{R(0), R(0)}; };
+    auto fstore = [&](int t, int l, C v) { F[t * NL + l] = v; };
+    fft_lines<C, NC, NL, false>(A, B, twf, -1, gload, fstore);
+    const double f0 = a.mul == MUL_COULOMB_REG ? s_f0 : 0.0;
+    for (int o = 0; o < a.nout; ++o) {
+      C* dst = a.out[o];
+      auto mload = [&](int t, int l) -> C {
+        C v = F[t * NL + l];
+        return s_ok[l] ? apply_multiplier<R>(a, v, t, s_outer[l], s_col[l], o, f0) : v;
+      };
+      auto gstore = [&](int t, int l, C v) { if (s_ok[l]) dst[s_base[l] + t * as] = v; };
+      fft_lines<C, NC, NL, false>(A, B, twb, +1, mload, gstore);
+    }
+  } else {
+    const int n = a.s;
+    const int tk = a.tk;
+    C* A = reinterpret_cast<C*>(smem_raw);
+    C* B = A + n * tk;
+    C* W = B + n * tk;
+    for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
+      const int t = w / tk, l = w % tk;
+      long base, outer;
+      int col;
+      C v = {R(0), R(0)};
+      if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+      A[t * tk + l] = v;
+    }
+    __syncthreads();
+    C* F = tile_fft<C>(A, B, a.plan, tk, a.twf, -1);
+    C* spare = (F == A) ? B : A;  // two free buffers: spare and W
+    const double f0 = a.mul == MUL_COULOMB_REG ? s_f0 : 0.0;
+    for (int o = 0; o < a.nout; ++o) {
+      for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
+        const int t = w / tk, l = w % tk;
+        long base, outer;
+        int col;
+        C v = F[t * tk + l];
+        if (axis_line(a, l, base, outer, col)) v = apply_multiplier<R>(a, v, t, outer, col, o, f0);
+        spare[t * tk + l] = v;
       }
-      fr *= a.scale;
-      if (imag) v = {R(-fr * (double)v.y), R(fr * (double)v.x)};
-      else v = {R(fr * (double)v.x), R(fr * (double)v.y)};
-      spare[t * a.tk + l] = v;
+      __syncthreads();
+      C* res = tile_fft<C>(spare, W, a.plan, tk, a.twb, +1);
+      C* dst = a.out[o];
+      for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
+        const int t = w / tk, l = w % tk;
+        long base, outer;
+        int col;
+        if (axis_line(a, l, base, outer, col)) dst[base + t * a.astride] = res[t * tk + l];
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    C* res = tile_fft<C>(spare, W, a.plan, a.tk, a.twb, +1);
-    C* dst = a.out[o];
-    for (int w = threadIdx.x; w < a.s * a.tk; w += blockDim.x) {
-      const int t = w / a.tk, l = w % a.tk;
-      long base, outer;
-      int col;
-      if (axis_line(a, l, base, outer, col)) dst[base + t * a.astride] = res[t * a.tk + l];
-    }
-    __syncthreads();
   }
 }
 
@@ -533,6 +710,72 @@ __global__ void k_axpy(const R* x, R* y, long n, double a, int accumulate) {
     y[p] = accumulate ? R((double)y[p] + a * (double)x[p]) : R(a * (double)x[p]);
 }
 
+// ------------------------------------------------- size dispatch --------
+// Compile-time instantiations for the grid sizes the engine is run at; any
+// other size uses the runtime radix plan (tile_fft).  NL is the tile width:
+// 16 lines in FP32 and 8 in FP64 (128-byte rows).
+
+#define MPDPFT_CT_LENGTHS(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+
+template <typename R, int NL>
+static bool launch_z_r2c_ct(int M, unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  switch (M) {
+#define CASE(N)                                                                                   \
+  case N:                                                                                         \
+    smem_optin(k_z_r2c<R, N, NL>); \
+    k_z_r2c<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R, int NL>
+static bool launch_z_c2r_ct(int M, unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  switch (M) {
+#define CASE(N)                                                                                   \
+  case N:                                                                                         \
+    smem_optin(k_z_c2r<R, N, NL>); \
+    k_z_c2r<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R, int NL>
+static bool launch_axis_ct(int n, dim3 grid, size_t smem, cudaStream_t st, const AxisArgs<R>& a) {
+  switch (n) {
+#define CASE(N)                                                                                      \
+  case N:                                                                                            \
+    smem_optin(k_axis_c2c<R, N, NL>); \
+    k_axis_c2c<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R, int NL>
+static bool launch_x_ct(int n, unsigned grid, size_t smem, cudaStream_t st, const AxisArgs<R>& a) {
+  switch (n) {
+#define CASE(N)                                                                                         \
+  case N:                                                                                               \
+    smem_optin(k_x_roundtrip<R, N, NL>); \
+    k_x_roundtrip<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R>
+constexpr int ct_width() { return sizeof(R) == sizeof(double) ? 8 : 16; }
+
 // ------------------------------------------------------------ host side --
 template <typename R>
 static int make_twiddles(Ctx& c, FftPlan& f) {
@@ -585,18 +828,17 @@ int Ctx::fft_setup() {
   f.vblocks = grid_blocks(geom.n);
   if ((st = alloc((void**)&f.vres_part, sizeof(double) * f.vblocks * kMaxS))) return st;
   (void)need;
-  // shared memory opt-in for the largest tiles
-  const int max_smem = 200 * 1024;
+  // shared memory opt-in of the runtime-plan kernels (any grid size)
   if (rsize == sizeof(double)) {
-    CU(cudaFuncSetAttribute(k_z_r2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_z_c2r<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_axis_c2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_x_roundtrip<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(smem_optin(k_z_r2c<double, 0, 0>));
+    CU(smem_optin(k_z_c2r<double, 0, 0>));
+    CU(smem_optin(k_axis_c2c<double, 0, 0>));
+    CU(smem_optin(k_x_roundtrip<double, 0, 0>));
   } else {
-    CU(cudaFuncSetAttribute(k_z_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_z_c2r<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_axis_c2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    CU(cudaFuncSetAttribute(k_x_roundtrip<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    CU(smem_optin(k_z_r2c<float, 0, 0>));
+    CU(smem_optin(k_z_c2r<float, 0, 0>));
+    CU(smem_optin(k_axis_c2c<float, 0, 0>));
+    CU(smem_optin(k_x_roundtrip<float, 0, 0>));
   }
   return MPDPFT_OK;
 }
@@ -637,8 +879,10 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
   a.out = (typename Cx<R>::T*)out;
   a.part = sums ? f.zpart : nullptr;
-  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.M * f.zl;
-  k_z_r2c<R><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+  const size_t smem = (3 * (size_t)f.M * f.zl + f.M) * sizeof(typename Cx<R>::T);
+  c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
+  if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
+    k_z_r2c<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -657,8 +901,10 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   a.coul_coef = coul_coef;
   a.f0_part = f.zpart;
   a.f0_blocks = f.zblocks;
-  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.M * f.zl + sizeof(R) * (size_t)f.s * f.zl;
-  k_z_c2r<R><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+  const size_t smem = (2 * (size_t)f.M * f.zl + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
+  c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
+  if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
+    k_z_c2r<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -704,8 +950,10 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   a.dir = dir;
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
   dim3 grid((unsigned)(a.nbulk + nyq_blocks), nfield);
-  const size_t smem = 2 * sizeof(typename Cx<R>::T) * f.s * f.tk;
-  k_axis_c2c<R><<<grid, kFftThreads, smem, c.stream>>>(a);
+  const size_t smem = (2 * (size_t)f.s * f.tk + f.s) * sizeof(typename Cx<R>::T);
+  c.cnt[MPDPFT_STAGE_FFT_Y]++;
+  if (f.tk != ct_width<R>() || !launch_axis_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
+    k_axis_c2c<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -723,8 +971,11 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   a.f0_part = f.zpart;
   a.f0_blocks = f.zblocks;
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
-  const size_t smem = 3 * sizeof(typename Cx<R>::T) * f.s * f.tk;
-  k_x_roundtrip<R><<<(unsigned)(a.nbulk + nyq_blocks), kFftThreads, smem, c.stream>>>(a);
+  const size_t smem = (3 * (size_t)f.s * f.tk + 2 * f.s) * sizeof(typename Cx<R>::T);
+  const unsigned grid = (unsigned)(a.nbulk + nyq_blocks);
+  c.cnt[MPDPFT_STAGE_FFT_X]++;
+  if (f.tk != ct_width<R>() || !launch_x_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
+    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -752,6 +1003,7 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
 
 int Ctx::scale_copy(const void* src, void* dst, double a) {
   const int blocks = grid_blocks(geom.n);
+  cnt[5]++;
   if (rsize == sizeof(double)) k_scale_copy<double><<<blocks, kThreads, 0, stream>>>((const double*)src, (double*)dst, geom.n, a);
   else k_scale_copy<float><<<blocks, kThreads, 0, stream>>>((const float*)src, (float*)dst, geom.n, a);
   CU(cudaGetLastError());
@@ -800,6 +1052,7 @@ static int coulomb_terms(Ctx& c, const R* dens, R* out) {
 
 int Ctx::axpy(const void* x, void* y, double a, int accumulate) {
   const int blocks = grid_blocks(geom.n);
+  cnt[5]++;
   if (rsize == sizeof(double)) k_axpy<double><<<blocks, kThreads, 0, stream>>>((const double*)x, (double*)y, geom.n, a, accumulate);
   else k_axpy<float><<<blocks, kThreads, 0, stream>>>((const float*)x, (float*)y, geom.n, a, accumulate);
   CU(cudaGetLastError());
@@ -850,6 +1103,7 @@ static int fft_terms_impl(Ctx& c) {
   }
   CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
   KParams kp = c.kparams();
+  c.cnt[5]++;
   k_assemble_v<R><<<F.vblocks, kThreads, 0, c.stream>>>(kp, c.d_state, (const R*)c.d_vext,
                                                          c.has_coulomb ? (const R*)c.d_vh : nullptr,
                                                          (const R*)c.d_nin, (R*)c.d_V, F.vres_part, F.vmax,
@@ -862,6 +1116,7 @@ static int fft_terms_impl(Ctx& c) {
     for (int s = 0; s < c.S; ++s) {
       if (s > 0) {  // taper shift of species s
         CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+        c.cnt[5]++;
         k_shell_max<R><<<grid_blocks(n), kThreads, 0, c.stream>>>(c.geom, (const R*)c.d_V + (long)s * n, F.vmax,
                                                                   shell_radius(c), shell_width(c));
         CU(cudaGetLastError());
@@ -886,10 +1141,11 @@ __global__ void k_copy_slot(const ScState* st, const R* ring, R* dst, long count
 }
 
 int Ctx::copy_current_density() {
-  const long cnt = geom.n * S;
-  const int blocks = grid_blocks(cnt);
-  if (rsize == sizeof(double)) k_copy_slot<double><<<blocks, kThreads, 0, stream>>>(d_state, (const double*)d_nin, (double*)d_tmp, cnt);
-  else k_copy_slot<float><<<blocks, kThreads, 0, stream>>>(d_state, (const float*)d_nin, (float*)d_tmp, cnt);
+  const long count = geom.n * S;
+  const int blocks = grid_blocks(count);
+  cnt[5]++;
+  if (rsize == sizeof(double)) k_copy_slot<double><<<blocks, kThreads, 0, stream>>>(d_state, (const double*)d_nin, (double*)d_tmp, count);
+  else k_copy_slot<float><<<blocks, kThreads, 0, stream>>>(d_state, (const float*)d_nin, (float*)d_tmp, count);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1135,7 +1391,7 @@ static int full_c2c_impl(Ctx& c, void* buf, int sign) {
     a.nbulk = a.nouter * a.ntile;
     const size_t smem = 2 * sizeof(typename Cx<R>::T) * s * a.tk;
     // no Nyquist blocks: columns cover 0..s-1
-    k_axis_c2c<R><<<dim3((unsigned)a.nbulk, 1), kFftThreads, smem, c.stream>>>(a);
+    k_axis_c2c<R, 0, 0><<<dim3((unsigned)a.nbulk, 1), kFftThreads, smem, c.stream>>>(a);
     CU(cudaGetLastError());
   }
   return MPDPFT_OK;
@@ -1143,6 +1399,70 @@ static int full_c2c_impl(Ctx& c, void* buf, int sign) {
 
 int Ctx::full_c2c(void* buf, int sign) {
   return rsize == sizeof(double) ? full_c2c_impl<double>(*this, buf, sign) : full_c2c_impl<float>(*this, buf, sign);
+}
+
+// Stage timing with CUDA events (see mpdpft_profile_stage).
+template <typename R>
+static int profile_impl(Ctx& c, int stage, int reps, double* ms, double* bytes) {
+  FftPlan& F = *c.fft;
+  const double n = (double)c.geom.n;
+  const double spec = (double)F.nspec * 2.0 * c.rsize;
+  const double field = n * c.rsize;
+  const int S = c.S;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  int st = MPDPFT_OK;
+  double b = 0.0;
+  if (stage != MPDPFT_STAGE_SC_STEP && stage != MPDPFT_STAGE_ITERATION) {
+    if (!F.spec[0]) return set_error(MPDPFT_ERR_ARG, "context has no FFT buffers");
+    CU(cudaMemsetAsync(F.spec[0], 0, (size_t)spec, c.stream));
+    CU(cudaMemsetAsync(F.rtmp, 0, (size_t)field, c.stream));
+  }
+  auto one = [&]() -> int {
+    switch (stage) {
+      case MPDPFT_STAGE_SC_STEP: return c.launch_step(0);
+      case MPDPFT_STAGE_FFT_Z_R2C: return launch_z_r2c<R>(c, (const R*)F.rtmp, PRO_NONE, 1, nullptr, F.spec[0], false);
+      case MPDPFT_STAGE_FFT_Y: return F.dim == 3 ? launch_y<R>(c, &F.spec[0], 1, -1) : set_error(MPDPFT_ERR_ARG, "no y pass in 2D");
+      case MPDPFT_STAGE_FFT_X: return launch_x<R>(c, F.spec[0], &F.spec[0], 1, MUL_SMOOTH, -0.01);
+      case MPDPFT_STAGE_FFT_Z_C2R: return launch_z_c2r<R>(c, &F.spec[0], 1, EPI_STORE, (R*)F.rtmp, nullptr, 0.0);
+      case MPDPFT_STAGE_ITERATION: return c.sc_step(1);
+      default: return set_error(MPDPFT_ERR_ARG, "unknown stage");
+    }
+  };
+  if ((st = one())) return st;  // warm-up (and graph instantiation)
+  CU(cudaEventRecord(e0, c.stream));
+  for (int r = 0; r < reps && !st; ++r) st = one();
+  CU(cudaEventRecord(e1, c.stream));
+  CU(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CU(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  *ms = (double)t / reps;
+  const int I = c.P.mixer ? c.P.pulay_scope : 1;
+  switch (stage) {
+    case MPDPFT_STAGE_SC_STEP:
+      // V (+ Laplacian, |grad V|^2) read once by the mu search, n_in read,
+      // residual written, I-1 older residuals read for the Gram row, 2I
+      // history fields read and 1 written by the mix
+      b = field * S * ((c.gradient ? 3 : 1) + 1 + 1 + (I - 1) + 2 * I + 1);
+      if (c.assemble_in_step) b += field * S * 3;
+      break;
+    case MPDPFT_STAGE_FFT_Z_R2C: b = field + spec; break;
+    case MPDPFT_STAGE_FFT_Y: b = 2.0 * spec; break;
+    case MPDPFT_STAGE_FFT_X: b = 2.0 * spec; break;
+    case MPDPFT_STAGE_FFT_Z_C2R: b = spec + field; break;
+    default: b = 0.0; break;
+  }
+  if (bytes) *bytes = b;
+  return MPDPFT_OK;
+}
+
+int Ctx::profile_stage(int stage, int reps, double* ms, double* bytes) {
+  return rsize == sizeof(double) ? profile_impl<double>(*this, stage, reps, ms, bytes)
+                                 : profile_impl<float>(*this, stage, reps, ms, bytes);
 }
 
 int Ctx::alloc_io(long doubles) {

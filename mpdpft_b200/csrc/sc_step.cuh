@@ -46,6 +46,7 @@ struct MuState {
   int next_c;  // next reference bracket step to place
   double cand[kMuCand];
   double best_mu, best_N, best_err;
+  double dens_mu;  // mu at which the final density is evaluated
 };
 
 // SC loop state, resident in device memory.
@@ -68,6 +69,7 @@ struct ScState {
   MuState ms[kMaxS];
   unsigned bar_count, bar_gen;
   int abort;
+  unsigned long long tphase[8];  // %globaltimer at phase boundaries (block 0)
 };
 
 template <typename R>
@@ -90,6 +92,14 @@ struct StepArgs {
   int mode;        // 0: SC iteration; 1: densities of the current V only;
                    // 2: admix only (V holds the output densities)
 };
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+#define MPDPFT_TSTAMP(k) \
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[k] = globaltimer()
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
@@ -159,6 +169,7 @@ __device__ inline void mu_begin(MuState& m, double mu, double prev_abs, double d
   m.dir = 0;
   m.next_c = 2;
   m.best_mu = mu;
+  m.dens_mu = mu;
   m.best_N = 0.0;
   m.best_err = 1e300;
   m.ncand = 0;
@@ -205,6 +216,7 @@ __device__ inline void mu_decide(MuState& m, const double* N, double target, dou
     }
   }
   m.pass++;
+  m.dens_mu = m.best_mu;
   if (m.best_err <= rel_acc) { m.done = 1; return; }
   if (m.pass >= kMuMaxPasses) { m.done = 1; bits |= kBitTimeout; return; }
   m.ncand = 0;
@@ -212,11 +224,15 @@ __device__ inline void mu_decide(MuState& m, const double* N, double target, dou
     // continue the reference's bracket steps towards the target
     const int d = m.have_hi ? -1 : 1;  // missing lower end: step down
     while (m.next_c <= 20 && m.ncand < kMuCand) m.cand[m.ncand++] = m.start + d * step_offset(m, m.next_c++);
-    if (m.ncand == 0) {  // no bracket within 20 steps: reset mu (:4657-4662)
+    if (m.ncand == 0) {
+      // no bracket within 20 steps: the reference resets mu to its start
+      // value but keeps the density of its last trial step (:4657-4662)
       m.done = 1;
+      m.dens_mu = m.start + d * step_offset(m, 20);
       m.best_mu = m.start;
       m.best_err = 1e300;
       bits |= kBitBracket;
+      return;
     }
     return;
   }
@@ -235,50 +251,75 @@ __device__ inline void mu_decide(MuState& m, const double* N, double target, dou
 }
 
 // ---------------------------------------------------------- small solve --
-// Inverse of an n x n matrix (n <= kMaxP) by Gauss-Jordan elimination with
-// full pivoting.  Rank test as Eigen's FullPivHouseholderQR::isInvertible
+// Inverse of the Pulay Gram matrix by Gauss-Jordan elimination with full
+// pivoting; rank test as Eigen's FullPivHouseholderQR::isInvertible
 // (threshold eps * n * max|pivot|), which the reference uses (mpDPFT.cpp:5089).
-__device__ inline bool small_inverse(int n, const double* A, double* inv) {
-  double M[kMaxP * kMaxP];
-  int colperm[kMaxP];
-  double piv[kMaxP];
-  for (int i = 0; i < n * n; ++i) { M[i] = A[i]; inv[i] = 0.0; }
-  for (int i = 0; i < n; ++i) { inv[i * n + i] = 1.0; colperm[i] = i; }
-  double maxpiv = 0.0;
+// One warp, matrices in shared memory; pivots are the first maximum in
+// row-major order, as in a serial scan.
+// G is n x n (row-major, stride n); inv receives the inverse.  Returns the
+// rank-test result on every lane.
+__device__ inline bool warp_inverse(int n, const double* G, double* M, double* inv, double* fac, int* colperm) {
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < n * n; i += 32) { M[i] = G[i]; inv[i] = 0.0; }
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) { inv[i * n + i] = 1.0; colperm[i] = i; }
+  __syncwarp();
+  double maxpiv = 0.0, minpiv = 1e300;
   for (int c = 0; c < n; ++c) {
-    int pr = c, pc = c;
+    const int w = n - c;
     double best = -1.0;
-    for (int i = c; i < n; ++i)
-      for (int j = c; j < n; ++j)
-        if (fabs(M[i * n + j]) > best) { best = fabs(M[i * n + j]); pr = i; pc = j; }
+    int bidx = c * n + c;
+    for (int e = lane; e < w * w; e += 32) {
+      const int i = c + e / w, j = c + e % w;
+      const double v = fabs(M[i * n + j]);
+      if (v > best) { best = v; bidx = i * n + j; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+      if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
+    }
+    const int pr = bidx / n, pc = bidx % n;
     if (pr != c)
-      for (int j = 0; j < n; ++j) {
+      for (int j = lane; j < n; j += 32) {
         double t = M[pr * n + j]; M[pr * n + j] = M[c * n + j]; M[c * n + j] = t;
         t = inv[pr * n + j]; inv[pr * n + j] = inv[c * n + j]; inv[c * n + j] = t;
       }
+    __syncwarp();
     if (pc != c) {
-      for (int i = 0; i < n; ++i) { double t = M[i * n + pc]; M[i * n + pc] = M[i * n + c]; M[i * n + c] = t; }
-      int t = colperm[pc]; colperm[pc] = colperm[c]; colperm[c] = t;
+      for (int i = lane; i < n; i += 32) { double t = M[i * n + pc]; M[i * n + pc] = M[i * n + c]; M[i * n + c] = t; }
+      if (lane == 0) { int t = colperm[pc]; colperm[pc] = colperm[c]; colperm[c] = t; }
     }
-    piv[c] = M[c * n + c];
-    if (fabs(piv[c]) > maxpiv) maxpiv = fabs(piv[c]);
-    if (piv[c] == 0.0) return false;
-    double ip = 1.0 / piv[c];
-    for (int j = 0; j < n; ++j) { M[c * n + j] *= ip; inv[c * n + j] *= ip; }
-    for (int i = 0; i < n; ++i) {
+    __syncwarp();
+    const double piv = M[c * n + c];
+    maxpiv = fmax(maxpiv, fabs(piv));
+    minpiv = fmin(minpiv, fabs(piv));
+    if (piv == 0.0) return false;
+    const double ip = 1.0 / piv;
+    __syncwarp();
+    for (int j = lane; j < n; j += 32) { M[c * n + j] *= ip; inv[c * n + j] *= ip; }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) fac[i] = M[i * n + c];
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) {
+      const int i = e / n, j = e % n;
       if (i == c) continue;
-      double f = M[i * n + c];
+      const double f = fac[i];
       if (f == 0.0) continue;
-      for (int j = 0; j < n; ++j) { M[i * n + j] -= f * M[c * n + j]; inv[i * n + j] -= f * inv[c * n + j]; }
+      M[i * n + j] -= f * M[c * n + j];
+      inv[i * n + j] -= f * inv[c * n + j];
     }
+    __syncwarp();
   }
-  const double thr = 2.220446049250313e-16 * (double)n * maxpiv;
-  for (int c = 0; c < n; ++c)
-    if (fabs(piv[c]) <= thr) return false;
-  double out[kMaxP * kMaxP];
-  for (int c = 0; c < n; ++c)
-    for (int j = 0; j < n; ++j) out[colperm[c] * n + j] = inv[c * n + j];
-  for (int i = 0; i < n * n; ++i) inv[i] = out[i];
+  if (minpiv <= 2.220446049250313e-16 * (double)n * maxpiv) return false;
+  // undo the column permutation: row c of the result goes to row colperm[c]
+  for (int e = lane; e < n * n; e += 32) M[e] = inv[e];
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) {
+    const int c = e / n, j = e % n;
+    inv[colperm[c] * n + j] = M[e];
+  }
+  __syncwarp();
   return true;
 }
 
@@ -307,15 +348,20 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
   const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long nthreads = (long)gridDim.x * blockDim.x;
   __shared__ double red[kNPart];
-  __shared__ double s_mu[kMaxS];
+  __shared__ double s_mu[kMaxS];      // mu of the final density
+  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
   __shared__ int s_flag;
   __shared__ MuState s_ms[kMaxS];
+  __shared__ double s_G[kMaxP * kMaxP], s_M[kMaxP * kMaxP], s_inv[kMaxP * kMaxP], s_fac[kMaxP];
+  __shared__ int s_perm[kMaxP];
+  __shared__ int s_ok;
 
   if (a.mode != 1 && ldcg(&st->exit_loop)) return;
   const int cur = ldcg(&st->slot);
   const int ring = kp.ring;
   const int next = (cur + 1) % ring;
   double* mypart = a.part + (long)blockIdx.x * kNPart;
+  MPDPFT_TSTAMP(0);
 
   // ---- phase A: UpdateV (mpDPFT.cpp:4815-4838) --------------------------
   if (a.mode == 0 && a.assemble_v) {
@@ -393,6 +439,7 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
   if (!grid_barrier(st)) return;
 
   const R* V = a.V;
+  MPDPFT_TSTAMP(1);
   for (int pass = 0; pass < kMuMaxPasses && a.mode != 2; ++pass) {
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
@@ -419,13 +466,24 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
       const R* Vs = V + (long)s * n;
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
-      for (long p = tid; p < n; p += nthreads) {
-        const double v = (double)Vs[p];
-        const double l = Ls ? (double)Ls[p] : 0.0;
-        const double g = Gs ? (double)Gs[p] : 0.0;
+      if (sizeof(R) == sizeof(double)) {
+        for (long p = tid; p < n; p += nthreads) {
+          const double v = (double)Vs[p];
+          const double l = Ls ? (double)Ls[p] : 0.0;
+          const double g = Gs ? (double)Gs[p] : 0.0;
 #pragma unroll
-        for (int c = 0; c < kMuCand; ++c)
-          if (c < nc) acc[c] += density_at<double>(d, cmu[c] - v, l, g);
+          for (int c = 0; c < kMuCand; ++c)
+            if (c < nc) acc[c] += density_at_d(d, cmu[c] - v, l, g);
+        }
+      } else {
+        for (long p = tid; p < n; p += nthreads) {
+          const double v = (double)Vs[p];
+          const float l = Ls ? (float)Ls[p] : 0.f;
+          const float g = Gs ? (float)Gs[p] : 0.f;
+#pragma unroll
+          for (int c = 0; c < kMuCand; ++c)
+            if (c < nc) acc[c] += (double)density_at_f(d, (float)(cmu[c] - v), l, g);
+        }
       }
       block_reduce_store<kMuCand>(acc, mypart + s * kMuCand);
     }
@@ -451,11 +509,12 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
     if (!grid_barrier(st)) return;
   }
 
+  MPDPFT_TSTAMP(2);
   // ---- phase C: final densities, residual, CC dots, Gram row -----------
   if (threadIdx.x < S) {
     const int s = threadIdx.x;
-    double mu = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
-    s_mu[s] = mu;
+    s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
+    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
   }
   if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
   __syncthreads();
@@ -477,7 +536,10 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
         const double l = a.lap ? (double)a.lap[q] : 0.0;
         const double g = a.g2 ? (double)a.g2[q] : 0.0;
         // mode 2 (admix only): V holds the output densities
-        const double nod = a.mode == 2 ? (double)v : density_at<double>(kp.dens[s], s_mu[s] - (double)v, l, g);
+        const double nod = a.mode == 2 ? (double)v
+                           : (sizeof(R) == sizeof(double)
+                                  ? density_at_d(kp.dens[s], s_mu[s] - (double)v, l, g)
+                                  : (double)density_at_f(kp.dens[s], (float)(s_mu[s] - (double)v), (float)l, (float)g));
         const R no = R(nod);
         acc[4 * s + 0] += nod;
         if (a.mode == 1) { nin[q] = no; continue; }
@@ -500,13 +562,14 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
   if (!grid_barrier(st)) return;
 
   // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
+  MPDPFT_TSTAMP(3);
   if (blockIdx.x == 0) {
     reduce_partials(a.part, gridDim.x, 4 * kMaxS + kMaxP, red);
     if (threadIdx.x == 0) {
       const int sc = st->sc_count;
       double tot = 0.0;
       for (int s = 0; s < S; ++s) {
-        st->mu[s] = s_mu[s];
+        st->mu[s] = s_mu_rep[s];
         st->ab[s] = red[4 * s] * kp.geom.dvol;
         if (!isfinite(st->ab[s])) st->iter_bits |= kBitNonfinite;
         tot += st->ab[s];
@@ -545,42 +608,57 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
           st->cc = 1.2345678901234567890;
         }
         if (sc == kp.max_sc) st->exit_loop = 1;  // Intercept (:4866)
-        // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167)
-        int used = 0;
+        // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): assemble the
+        // Gram matrix (last row/column new, the rest shifted from before)
         if (pulay_now) {
           const int shift = (hist + 1 > kp.scope) ? 1 : 0;
-          double G[kMaxP * kMaxP];
           for (int i = 0; i < I; ++i)
             for (int j = 0; j < I; ++j) {
               double v;
               if (i == I - 1) v = red[4 * kMaxS + j];
               else if (j == I - 1) v = red[4 * kMaxS + i];
               else v = st->gram[(i + shift) * kMaxP + (j + shift)];
-              G[i * I + j] = v;
+              s_G[i * I + j] = v;
             }
           for (int i = 0; i < I; ++i)
-            for (int j = 0; j < I; ++j) st->gram[i * kMaxP + j] = G[i * I + j];
+            for (int j = 0; j < I; ++j) st->gram[i * kMaxP + j] = s_G[i * I + j];
           st->hist = I;
-          double inv[kMaxP * kMaxP];
-          if (small_inverse(I, G, inv)) {
-            double test = 0.0;
-            for (int i = 0; i < I; ++i)
-              for (int j = 0; j < I; ++j) {
-                double t = 0.0;
-                for (int k = 0; k < I; ++k) t += inv[i * I + k] * G[k * I + j];
-                t -= (i == j) ? 1.0 : 0.0;
-                test += t * t;
-              }
-            if (test <= 1.0e-8) {
-              double x[kMaxP], A = 0.0;
-              for (int i = 0; i < I; ++i) {
-                x[i] = 0.0;
-                for (int k = 0; k < I; ++k) x[i] += inv[i * I + k];
-                A += x[i];
-              }
-              for (int i = 0; i < I; ++i) st->coeff[i] = x[i] / A;
-              used = 1;
+        }
+      }
+    }
+    __syncthreads();
+    // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
+    // reference, mpDPFT.cpp:5089-5107)
+    if (a.mode != 1 && pulay_now && threadIdx.x < 32) {
+      bool ok = warp_inverse(I, s_G, s_M, s_inv, s_fac, s_perm);
+      double test = 0.0;
+      if (ok) {
+        for (int e = threadIdx.x; e < I * I; e += 32) {
+          const int i = e / I, j = e % I;
+          double t = 0.0;
+          for (int k = 0; k < I; ++k) t += s_inv[i * I + k] * s_G[k * I + j];
+          t -= (i == j) ? 1.0 : 0.0;
+          test += t * t;
+        }
+        test = warp_sum(test);
+      }
+      if (threadIdx.x == 0) s_ok = ok && test <= 1.0e-8;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int sc = st->sc_count;
+      if (a.mode != 1) {
+        int used = 0;
+        if (pulay_now) {
+          if (s_ok) {
+            double x[kMaxP], A = 0.0;
+            for (int i = 0; i < I; ++i) {
+              x[i] = 0.0;
+              for (int k = 0; k < I; ++k) x[i] += s_inv[i * I + k];
+              A += x[i];
             }
+            for (int i = 0; i < I; ++i) st->coeff[i] = x[i] / A;
+            used = 1;
           }
           if (!used) st->iter_bits |= kBitPulay;
         }
@@ -628,33 +706,61 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
     }
   }
   if (a.mode == 1) return;
+  MPDPFT_TSTAMP(4);
   if (!grid_barrier(st)) return;
+  MPDPFT_TSTAMP(5);
 
   // ---- phase E: mixed density -> ring[next] ----------------------------
+  // n = sum_j c_j (n_in,j + theta r_j) (Pulay) or n_in + theta r (linear),
+  // AdmixDensities mpDPFT.cpp:4946-4955 / :4987
   {
-    const int used = ldcg(&st->pulay_used);
-    const int nc = ldcg(&st->ncoeff);
-    double coeff[kMaxP];
-    for (int i = 0; i < nc; ++i) coeff[i] = ldcg(&st->coeff[i]);
-    double th[kMaxS];
-    for (int s = 0; s < S; ++s) th[s] = ldcg(&st->theta_mix[s]);
-    R* out = a.nin + (long)next * S * n;
-    for (long p = tid; p < n; p += nthreads)
-      for (int s = 0; s < S; ++s) {
-        double v = 0.0;
-        if (used) {
-          for (int j = 0; j < nc; ++j) {
-            int slot = (cur - (nc - 1) + j + ring) % ring;
-            const long q = ((long)slot * S + s) * n + p;
-            v += coeff[j] * ((double)a.nin[q] + th[s] * (double)a.res[q]);
-          }
-        } else {
-          const long q = ((long)cur * S + s) * n + p;
-          v = (double)a.nin[q] + th[s] * (double)a.res[q];
-        }
-        out[(long)s * n + p] = R(v);
+    __shared__ long s_off[kMaxP];
+    __shared__ double s_c[kMaxP];
+    __shared__ int s_nc;
+    if (threadIdx.x == 0) {
+      const int used = ldcg(&st->pulay_used);
+      const int nc = used ? ldcg(&st->ncoeff) : 1;
+      s_nc = nc;
+      for (int j = 0; j < nc; ++j) {
+        const int slot = (cur - (nc - 1) + j + ring) % ring;
+        s_off[j] = (long)slot * S * n;
+        s_c[j] = used ? ldcg(&st->coeff[j]) : 1.0;
       }
+    }
+    __syncthreads();
+    const int nc = s_nc;
+    for (int s = 0; s < S; ++s) {
+      const double th = ldcg(&st->theta_mix[s]);
+      R* out = a.nin + (long)next * S * n + (long)s * n;
+      if (sizeof(R) == sizeof(float) && (n & 3) == 0) {
+        const long n4 = n >> 2;
+        for (long p4 = tid; p4 < n4; p4 += nthreads) {
+          double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+          for (int j = 0; j < nc; ++j) {
+            const long q = s_off[j] + (long)s * n + 4 * p4;
+            const float4 ni = *reinterpret_cast<const float4*>(a.nin + q);
+            const float4 ri = *reinterpret_cast<const float4*>(a.res + q);
+            const double c = s_c[j];
+            v0 += c * ((double)ni.x + th * (double)ri.x);
+            v1 += c * ((double)ni.y + th * (double)ri.y);
+            v2 += c * ((double)ni.z + th * (double)ri.z);
+            v3 += c * ((double)ni.w + th * (double)ri.w);
+          }
+          *reinterpret_cast<float4*>(out + 4 * p4) = make_float4((float)v0, (float)v1, (float)v2, (float)v3);
+        }
+      } else {
+        for (long p = tid; p < n; p += nthreads) {
+          double v = 0.0;
+          for (int j = 0; j < nc; ++j) {
+            const long q = s_off[j] + (long)s * n + p;
+            v += s_c[j] * ((double)a.nin[q] + th * (double)a.res[q]);
+          }
+          out[p] = R(v);
+        }
+      }
+    }
   }
+  MPDPFT_TSTAMP(6);
 }
 
 }  // namespace mpdpft

@@ -28,7 +28,7 @@ EXPORTS = [
     "mpdpft_set_external_potential", "mpdpft_density", "mpdpft_vint", "mpdpft_update_v",
     "mpdpft_mu_search", "mpdpft_delfield", "mpdpft_fft", "mpdpft_integrate", "mpdpft_pulay_reset",
     "mpdpft_admix", "mpdpft_sc_run", "mpdpft_sc_step", "mpdpft_sc_init", "mpdpft_get_field",
-    "mpdpft_energy",
+    "mpdpft_energy", "mpdpft_profile_stage", "mpdpft_iteration_launches", "mpdpft_step_phase_times",
 ]
 
 
@@ -80,6 +80,9 @@ def load(path=LIB_PATH):
     L.mpdpft_sc_init.argtypes = [vp, _dpp, C.c_int, C.c_int]
     L.mpdpft_get_field.argtypes = [vp, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
     L.mpdpft_energy.argtypes = [vp, C.POINTER(abi.Result)]
+    L.mpdpft_profile_stage.argtypes = [vp, C.c_int, C.c_int, _dp, _dp]
+    L.mpdpft_iteration_launches.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.mpdpft_step_phase_times.argtypes = [vp, _dp, C.c_int]
     for name in EXPORTS:
         getattr(L, name)
     _lib = L
@@ -255,6 +258,34 @@ class Engine:
         out = np.empty(self._count(layout))
         self._check(self.lib.mpdpft_get_field(self.h, which, s, _ptr(out), layout, abi.MEM_HOST))
         return out
+
+    def profile_stage(self, stage, reps=20):
+        """(ms per launch, algorithmic bytes per launch) of one stage."""
+        ms = C.c_double()
+        b = C.c_double()
+        self._check(self.lib.mpdpft_profile_stage(self.h, stage, reps, C.byref(ms), C.byref(b)))
+        return ms.value, b.value
+
+    def _launches(self):
+        counts = (C.c_int * 6)()
+        total = C.c_int()
+        self._check(self.lib.mpdpft_iteration_launches(self.h, counts, C.byref(total)))
+        return list(counts), total.value
+
+    def iteration_kernels(self):
+        """Kernel launches in one captured SC iteration."""
+        return self._launches()[1]
+
+    def stage_launch_counts(self):
+        c, _ = self._launches()
+        return {"sc_step": c[0], "z_r2c": c[1], "y": c[2], "x": c[3], "z_c2r": c[4], "other": c[5]}
+
+    def step_phase_times(self):
+        """Phase durations (us) of the last SC-step kernel: V update, mu
+        search, densities/Gram, solve, barrier, mix."""
+        us = np.zeros(6)
+        self._check(self.lib.mpdpft_step_phase_times(self.h, _ptr(us), 6))
+        return us
 
     def energy(self):
         r = abi.Result()

@@ -97,14 +97,19 @@ def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **
     """Neutral atom Z = 18: Gaussian nucleus (sigma 0.1 bohr) at the centre of
     [-10, 10]^3, TF + gradient correction (spectral grad V and Laplacian,
     each smoothed by a Gaussian of width 0.2 bohr), Hartree by FFT Poisson,
-    Dirac exchange, g = 2, atomic units (gammaH = 1)."""
+    Dirac exchange, g = 2, atomic units (gammaH = 1).  The gradient
+    terms' singular factors are floored at mu - V = 0.5 hartree, the order of the
+    Airy energy 1/2 |grad V|^{2/3} below which the small-gradient expansion
+    fails (the reference switches to its Airy branch there).  The start mu = -30
+    lies within the reference's 20 bracket steps of the bare-nucleus root
+    (the first density is computed in V_ext alone)."""
     z = 18.0
     kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z],
               rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
               interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
-              mu=[-0.5], mixer=1, pulay_scope=5, theta=[0.3], sc_criterion=1e-8,
+              mu=[-30.0], mixer=1, pulay_scope=5, theta=[0.5], sc_criterion=1e-8,
               max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
-              gradient_floor=5e-2, gradient_grad2=1.0, potential_tol=0.0,
+              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0,
               precision=precision)
     kw.update(over)
     p = abi.make_params(**kw)

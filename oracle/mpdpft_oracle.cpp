@@ -19,6 +19,7 @@
 // known-answer tests (Gaussian transform pair, harmonic-oscillator TF mu and
 // energy, Poisson of a Gaussian charge, Pulay on a linear map) in tests/.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -1059,6 +1060,7 @@ int oracle_sc_run(const mpdpft_params* p, const double* vext, const double* v0,
   while (!st.exit_loop) {
     st.status_bits = 0;
     long trials0 = st.mu_trials;
+    auto t_iter = std::chrono::steady_clock::now();
     st.OldDen = st.Den; st.OldV = st.V;   // StoreCurrentIteration MD:4804
     st.old_mu = st.mu; st.old_ab = st.tmp_ab; st.old_cc = st.cc;
     update_v(st);
@@ -1077,6 +1079,7 @@ int oracle_sc_run(const mpdpft_params* p, const double* vext, const double* v0,
       L.status_bits = st.status_bits;
       L.cc = st.cc;
       L.v_residual = vres;
+      L.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_iter).count();
       for (int q = 0; q < st.S; ++q) { L.mu[q] = st.mu[q]; L.abundance[q] = st.tmp_ab[q]; L.theta[q] = st.theta[q]; }
     }
     result->v_residual = vres;
