@@ -214,6 +214,54 @@ __device__ __forceinline__ double density_at_d(const DensParams& d, double u, do
   return density_at<double>(d, u, lap, g2);
 }
 
+// dn/dmu (= dn/du) of each functional, in double, for the Newton placement
+// of mu candidates.  Zero where the density is clamped at 0.
+__device__ __forceinline__ double density_slope_d(const DensParams& d, double u, double lap, double g2) {
+  if (d.expr == MPDPFT_DENS_TF) {
+    if (!(u > 0.0)) return 0.0;
+    if (d.dim == 3) return 1.5 * (1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * u * rsqrt_d(u);
+    return d.g / (2.0 * kPi);
+  }
+  if (d.expr == MPDPFT_DENS_TF_INSPIRED) {
+    const double t = u / d.tau;
+    if (!(t > 0.0)) return 0.0;
+    if (d.dim == 3) return 1.5 * t * rsqrt_d(t) * sqrt(d.tau) / d.tau;
+    return 1.0 / d.tau;
+  }
+  if (d.expr == MPDPFT_DENS_TF_INSPIRED_T) {
+    const double t2 = u / (d.tau * d.T);
+    if (t2 <= -40.0 || t2 != t2) return 0.0;
+    if (t2 >= 40.0) return 1.0 / (d.tau * d.tau);
+    return 1.0 / (1.0 + exp(-t2)) / (d.tau * d.tau);
+  }
+  // gradient-corrected
+  if (d.dim == 2) {
+    const double tau = 1.0 / d.T;
+    const double arg = tau * u;
+    if (arg > 700.0) return d.g / (2.0 * kPi);
+    if (arg < -700.0) return 0.0;
+    const double z = exp(-arg), opz = 1.0 + z;
+    const double r = d.g / (2.0 * kPi) * (1.0 / opz + tau * tau * lap / 12.0 * z * (1.0 - z) / (opz * opz * opz));
+    return r == r ? r : 0.0;
+  }
+  if (!(u > 0.0)) return 0.0;
+  const double ctf = 2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi);
+  const double cg = 1.4142135623730951 * d.g / (48.0 * kPi * kPi);
+  const double r = rsqrt_d(u);
+  double m1, m3, dm1, dm3;
+  if (u >= d.floor_u) {
+    m1 = r; m3 = r * r * r;
+    dm1 = -0.5 * m3; dm3 = -1.5 * m3 * r * r;
+  } else {
+    const double rf = rsqrt_d(d.floor_u);
+    dm1 = rf / d.floor_u; m1 = u * dm1;
+    dm3 = dm1 / d.floor_u; m3 = u * dm3;
+  }
+  const double n = ctf * u * u * r - cg * (lap * m1 + 0.25 * d.c2 * g2 * m3);
+  if (!(n > 0.0)) return 0.0;
+  return 1.5 * ctf * u * r - cg * (lap * dm1 + 0.25 * d.c2 * g2 * dm3);
+}
+
 // FP32 evaluation for the mixed-precision mu search: u is formed in double
 // from the double candidate mu and then rounded once, so N(mu) keeps the
 // resolution of double mu (a staircase of 2M per-point steps of relative size

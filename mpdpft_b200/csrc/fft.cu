@@ -174,9 +174,9 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
   C* Z;
   if constexpr (NC > 0) {
     C* A = reinterpret_cast<C*>(smem_raw);
-    C* B = A + NC * NL;
-    Z = B + NC * NL;
-    C* tws = Z + NC * NL;
+    C* B = A + NC * (NL + 1);
+    Z = B + NC * (NL + 1);
+    C* tws = Z + NC * (NL + 1);
     for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = a.tw_m[i];
     __syncthreads();
     auto load = [&](int m, int l) -> C {
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
       rowsum += (double)x0 + (double)x1;
       return C{x0, x1};
     };
-    auto store = [&](int m, int l, C v) { Z[m * NL + l] = v; };
+    auto store = [&](int m, int l, C v) { Z[m * (NL + 1) + l] = v; };
     fft_lines<C, NC, NL, true>(A, B, tws, -1, load, store);
     if (a.part) {
       double acc[1] = {rowsum};
@@ -223,12 +223,13 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
     __syncthreads();
     Z = tile_fft<C>(A, B, a.plan, zl, a.tw_m, -1);
   }
+  const int zld = NC > 0 ? NL + 1 : zl;  // row stride of the Z tile
   for (int w = threadIdx.x; w < H * zl; w += blockDim.x) {
     const int l = w / H, q = w % H;
     const long row = row0 + l;
     if (row >= a.rows) continue;
-    C zq = Z[(q % M) * zl + l];
-    C zc = cconj(Z[((M - q) % M) * zl + l]);
+    C zq = Z[(q % M) * zld + l];
+    C zc = cconj(Z[((M - q) % M) * zld + l]);
     C E = cscale(cadd(zq, zc), R(0.5));
     C D = csub(zq, zc);             // 2 i O_q
     C O = {D.y * R(0.5), -D.x * R(0.5)};
@@ -269,8 +270,8 @@ __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
   }
   if constexpr (NC > 0) {
     C* A = reinterpret_cast<C*>(smem_raw);
-    C* B = A + NC * NL;
-    C* tws = B + NC * NL;
+    C* B = A + NC * (NL + 1);
+    C* tws = B + NC * (NL + 1);
     R* acc = reinterpret_cast<R*>(tws + NC);  // [NL][s] (EPI_GRAD)
     for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = a.tw_m[i];
     __syncthreads();
@@ -414,8 +415,8 @@ __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
   const C* twg = a.dir < 0 ? a.twf : a.twb;
   if constexpr (NC > 0) {
     C* A = reinterpret_cast<C*>(smem_raw);
-    C* B = A + NC * NL;
-    C* tws = B + NC * NL;
+    C* B = A + NC * (NL + 1);
+    C* tws = B + NC * (NL + 1);
     __shared__ long s_base[NL];
     __shared__ int s_ok[NL];
     for (int i = threadIdx.x; i < NC; i += blockDim.x) tws[i] = twg[i];
@@ -475,7 +476,7 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier(const AxisArgs<R>&
   const double kx = a.dk * (t == a.s / 2 ? -(double)(a.s / 2) : (double)qx);
   const double ky = a.dk * (double)qy;
   const double kz = a.dk * (col == a.M ? -(double)a.M : (double)col);  // col M: Nyquist
-  const double k2 = kx * kx + ky * ky + (a.dim == 3 ? kz * kz : 0.0);
+  const double k2 = kx * kx + ky * ky + kz * kz;  // 2D: ky = 0, kz is the contiguous axis
   if (a.mul == MUL_COULOMB_REG) {
     // (n~ - n~0 e^{-k^2})/k^2, k = 0 -> n~0 (mpDPFT.cpp:2686-2701); the
     // centred transform's phase (-1)^{qx+qy+qz} carries over to the
@@ -512,6 +513,50 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier(const AxisArgs<R>&
   return C{R(fr * (double)v.x), R(fr * (double)v.y)};
 }
 
+// Separable factors of the multipliers for one tile: per x index t (kx,
+// e^{sigma kx^2}, e^{-kx^2}) and per line (ky, kz, the y-z parts of k^2,
+// e^{sigma k^2} and e^{-k^2}, and the parity of qy + qz).
+template <typename R, int NC, int NL>
+struct MulTables {
+  R kx[NC], ex[NC], gx[NC];
+  R ky[NL], kz[NL], k2yz[NL], eyz[NL], gyz[NL];
+  int par[NL];
+};
+
+template <typename R, int NC, int NL>
+__device__ __forceinline__ typename Cx<R>::T apply_multiplier_tab(const AxisArgs<R>& a, const MulTables<R, NC, NL>& T,
+                                                                 typename Cx<R>::T v, int t, int l, int o, double f0,
+                                                                 long outer, int col) {
+  using C = typename Cx<R>::T;
+  const R sc = R(a.scale);
+  if (a.mul == MUL_COULOMB_TRUNC) return apply_multiplier<R>(a, v, t, outer, col, o, f0);
+  const R kx = T.kx[t];
+  const R k2 = kx * kx + T.k2yz[l];
+  if (a.mul == MUL_COULOMB_REG) {
+    if ((double)k2 > 1.0e-6 * a.dk * a.dk) {
+      const int par = (t + T.par[l]) & 1;
+      const R g = T.gx[t] * T.gyz[l] * R(f0) * (par ? R(-1) : R(1));
+      const R ik = sc / k2;
+      return C{(v.x - g) * ik, v.y * ik};
+    }
+    return C{R(f0) * sc, R(0)};
+  }
+  const R e = T.ex[t] * T.eyz[l];  // e^{sigma k^2}
+  if (a.mul == MUL_SMOOTH) return C{v.x * e * sc, v.y * e * sc};
+  // MUL_DERIV: i k_j e^{sigma k^2} (Nyquist of axis j dropped), Laplacian
+  // -k^2 e^{2 sigma k^2}
+  if (o < a.dim) {
+    R kj;
+    if (o == 0) kj = (t == a.s / 2) ? R(0) : kx;
+    else if (o == 1 && a.dim == 3) kj = T.ky[l];
+    else kj = T.kz[l];
+    const R fr = kj * e * sc;
+    return C{-fr * v.y, fr * v.x};
+  }
+  const R fr = -k2 * e * e * sc;
+  return C{fr * v.x, fr * v.y};
+}
+
 template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
   using C = typename Cx<R>::T;
@@ -528,34 +573,55 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
   C* data = a.data[0];
   if constexpr (NC > 0) {
     C* A = reinterpret_cast<C*>(smem_raw);
-    C* B = A + NC * NL;
-    C* F = B + NC * NL;
-    C* twf = F + NC * NL;
+    C* B = A + NC * (NL + 1);
+    C* F = B + NC * (NL + 1);
+    C* twf = F + NC * (NL + 1);
     C* twb = twf + NC;
     __shared__ long s_base[NL];
     __shared__ long s_outer[NL];
     __shared__ int s_col[NL];
     __shared__ int s_ok[NL];
-    for (int i = threadIdx.x; i < NC; i += blockDim.x) { twf[i] = a.twf[i]; twb[i] = a.twb[i]; }
+    __shared__ MulTables<R, NC, NL> T;
+    for (int i = threadIdx.x; i < NC; i += blockDim.x) {
+      twf[i] = a.twf[i];
+      twb[i] = a.twb[i];
+      const double kx = a.dk * (i == NC / 2 ? -(double)(NC / 2) : (double)signed_freq(i, NC));
+      T.kx[i] = R(kx);
+      T.ex[i] = R(exp(a.sigma_c * kx * kx));
+      T.gx[i] = R(exp(-kx * kx));
+    }
     if (threadIdx.x < NL) {
+      const int l = threadIdx.x;
       long base, outer;
       int col;
-      s_ok[threadIdx.x] = axis_line(a, threadIdx.x, base, outer, col) ? 1 : 0;
-      s_base[threadIdx.x] = base;
-      s_outer[threadIdx.x] = outer;
-      s_col[threadIdx.x] = col;
+      s_ok[l] = axis_line(a, l, base, outer, col) ? 1 : 0;
+      s_base[l] = base;
+      s_outer[l] = outer;
+      s_col[l] = col;
+      const double ky = a.dim == 3 ? a.dk * (double)signed_freq((int)outer, a.s) : 0.0;
+      const double kz = a.dk * (col == a.M ? -(double)a.M : (double)col);  // col M: Nyquist
+      const double k2 = ky * ky + (a.dim == 3 ? kz * kz : 0.0);
+      // 2D: the single-outer layout puts the contiguous axis in col (its k
+      // is "kz" here); the y slot is unused
+      const double kyy = a.dim == 3 ? ky : kz;
+      T.ky[l] = R(a.dim == 3 ? (((int)outer == a.s / 2) ? 0.0 : ky) : 0.0);
+      T.kz[l] = R(col == a.M ? 0.0 : kz);
+      T.k2yz[l] = R(a.dim == 3 ? k2 : kyy * kyy);
+      T.eyz[l] = R(exp(a.sigma_c * (a.dim == 3 ? k2 : kyy * kyy)));
+      T.gyz[l] = R(exp(-(a.dim == 3 ? k2 : kyy * kyy)));
+      T.par[l] = ((a.dim == 3 ? (int)outer : 0) + col) & 1;
     }
     __syncthreads();
     const long as = a.astride;
     auto gload = [&](int t, int l) -> C { return s_ok[l] ? data[s_base[l] + t * as] : C{R(0), R(0)}; };
-    auto fstore = [&](int t, int l, C v) { F[t * NL + l] = v; };
+    auto fstore = [&](int t, int l, C v) { F[t * (NL + 1) + l] = v; };
     fft_lines<C, NC, NL, false>(A, B, twf, -1, gload, fstore);
     const double f0 = a.mul == MUL_COULOMB_REG ? s_f0 : 0.0;
     for (int o = 0; o < a.nout; ++o) {
       C* dst = a.out[o];
       auto mload = [&](int t, int l) -> C {
-        C v = F[t * NL + l];
-        return s_ok[l] ? apply_multiplier<R>(a, v, t, s_outer[l], s_col[l], o, f0) : v;
+        C v = F[t * (NL + 1) + l];
+        return s_ok[l] ? apply_multiplier_tab<R, NC, NL>(a, T, v, t, l, o, f0, s_outer[l], s_col[l]) : v;
       };
       auto gstore = [&](int t, int l, C v) { if (s_ok[l]) dst[s_base[l] + t * as] = v; };
       fft_lines<C, NC, NL, false>(A, B, twb, +1, mload, gstore);
@@ -879,7 +945,7 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
   a.out = (typename Cx<R>::T*)out;
   a.part = sums ? f.zpart : nullptr;
-  const size_t smem = (3 * (size_t)f.M * f.zl + f.M) * sizeof(typename Cx<R>::T);
+  const size_t smem = (3 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T);
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
   if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_r2c<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
@@ -901,7 +967,7 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   a.coul_coef = coul_coef;
   a.f0_part = f.zpart;
   a.f0_blocks = f.zblocks;
-  const size_t smem = (2 * (size_t)f.M * f.zl + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
+  const size_t smem = (2 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_c2r<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
@@ -950,7 +1016,7 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   a.dir = dir;
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
   dim3 grid((unsigned)(a.nbulk + nyq_blocks), nfield);
-  const size_t smem = (2 * (size_t)f.s * f.tk + f.s) * sizeof(typename Cx<R>::T);
+  const size_t smem = (2 * (size_t)f.s * (f.tk + 1) + f.s) * sizeof(typename Cx<R>::T);
   c.cnt[MPDPFT_STAGE_FFT_Y]++;
   if (f.tk != ct_width<R>() || !launch_axis_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
     k_axis_c2c<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
@@ -971,11 +1037,14 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   a.f0_part = f.zpart;
   a.f0_blocks = f.zblocks;
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
-  const size_t smem = (3 * (size_t)f.s * f.tk + 2 * f.s) * sizeof(typename Cx<R>::T);
+  const size_t csz = sizeof(typename Cx<R>::T);
+  const size_t smem_ct = (3 * (size_t)f.s * (f.tk + 1) + 2 * f.s) * csz;
+  const size_t smem_rt = 3 * (size_t)f.s * f.tk * csz;
   const unsigned grid = (unsigned)(a.nbulk + nyq_blocks);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
-  if (f.tk != ct_width<R>() || !launch_x_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
-    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
+  const bool ct_fits = smem_ct + sizeof(MulTables<R, 512, 16>) <= 227 * 1024;
+  if (f.tk != ct_width<R>() || !ct_fits || !launch_x_ct<R, ct_width<R>()>(f.s, grid, smem_ct, c.stream, a))
+    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, smem_rt, c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }

@@ -166,7 +166,9 @@ __device__ __forceinline__ void reg_dft(C (&a)[8], int dir) {
   }
 }
 
-// Stockham stages STAGE .. END-1 of a length-N transform of an NL-line tile.
+// Stockham stages STAGE .. END-1 of a length-N transform of an NL-line tile
+// stored as element (t, l) at t * (NL + 1) + l: the padded row keeps both
+// line-fastest and element-fastest accesses free of bank conflicts.
 template <typename C, int N, int NL, int STAGE, int STRIDE, int END = ct_num_stages(N)>
 __device__ __forceinline__ void ct_stages(C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw,
                                           int dir) {
@@ -181,13 +183,13 @@ __device__ __forceinline__ void ct_stages(C* __restrict__ src, C* __restrict__ d
       const int q = b / STRIDE, k = b % STRIDE;
       C a[8];
 #pragma unroll
-      for (int t = 0; t < R; ++t) a[t] = src[(k + STRIDE * (q + t * M)) * NL + l];
+      for (int t = 0; t < R; ++t) a[t] = src[(k + STRIDE * (q + t * M)) * (NL + 1) + l];
       reg_dft<R>(a, dir);
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         C v = a[u];
         if (u > 0) v = cmul(v, tw[q * u * STRIDE]);
-        dst[(k + STRIDE * (R * q + u)) * NL + l] = v;
+        dst[(k + STRIDE * (R * q + u)) * (NL + 1) + l] = v;
       }
     }
     __syncthreads();
@@ -204,7 +206,7 @@ __host__ __device__ constexpr int ct_stride_before(int n, int stage) {
 // Length-N transforms of NL lines with the first stage reading its inputs
 // from `load(t, l)` straight into registers and the last stage handing its
 // outputs to `store(t, l, v)`; only the middle stages exchange through the
-// shared-memory tile A/B (layout t * NL + l).  ELEM_FAST maps consecutive
+// shared-memory tile A/B (layout t * (NL + 1) + l).  ELEM_FAST maps consecutive
 // threads to consecutive elements of a line in the first and last stages
 // (contiguous rows); otherwise to consecutive lines (strided columns).
 // The twiddle table tw (length N) holds e^{dir 2 pi i t/N}.  Ends with
@@ -240,7 +242,7 @@ __device__ __forceinline__ void fft_lines(C* __restrict__ A, C* __restrict__ B, 
       for (int u = 0; u < R0; ++u) {
         C v = a[u];
         if (u > 0) v = cmul(v, tw[q * u]);
-        A[(R0 * q + u) * NL + l] = v;
+        A[(R0 * q + u) * (NL + 1) + l] = v;
       }
     }
     __syncthreads();
@@ -255,7 +257,7 @@ __device__ __forceinline__ void fft_lines(C* __restrict__ A, C* __restrict__ B, 
       const int k = ELEM_FAST ? w % SL : w / NL;
       C a[8];
 #pragma unroll
-      for (int t = 0; t < RL; ++t) a[t] = src[(k + SL * t) * NL + l];
+      for (int t = 0; t < RL; ++t) a[t] = src[(k + SL * t) * (NL + 1) + l];
       reg_dft<RL>(a, dir);
 #pragma unroll
       for (int u = 0; u < RL; ++u) store(k + SL * u, l, a[u]);
@@ -264,22 +266,5 @@ __device__ __forceinline__ void fft_lines(C* __restrict__ A, C* __restrict__ B, 
   }
 }
 
-// Length-N transform of the tile (A -> result); tw in shared memory holds
-// e^{dir 2 pi i t/N}.  Returns the buffer with the result.
-template <typename C, int N, int NL>
-__device__ __forceinline__ C* tile_fft_ct(C* A, C* B, const C* tw, int dir) {
-  ct_stages<C, N, NL, 0, 1>(A, B, tw, dir);
-  return (ct_num_stages(N) & 1) ? B : A;
-}
-
-// Dispatch: NC > 0 uses the compile-time path, NC == 0 the runtime plan.
-template <typename C, int NC, int NL>
-__device__ __forceinline__ C* tile_fft_any(C* A, C* B, const RadixPlan& plan, int nl, const C* tw, int dir) {
-  if constexpr (NC > 0) {
-    return tile_fft_ct<C, NC, NL>(A, B, tw, dir);
-  } else {
-    return tile_fft<C>(A, B, plan, nl, tw, dir);
-  }
-}
 
 }  // namespace mpdpft

@@ -16,7 +16,8 @@
 namespace mpdpft {
 
 constexpr int kStepThreads = 512;
-constexpr int kNPart = 4 * kMaxS + kMaxP > kMaxS * kMuCand ? 4 * kMaxS + kMaxP : kMaxS * kMuCand;
+constexpr int kMuAcc = kMuCand + 1;  // candidate sums + dN/dmu at candidate 0
+constexpr int kNPart = 4 * kMaxS + kMaxP > kMaxS * kMuAcc ? 4 * kMaxS + kMaxP : kMaxS * kMuAcc;
 constexpr long kBarrierSpinLimit = 20000000;  // ~ seconds with nanosleep backoff
 
 // Constant parameters of one solve (kernel argument, by value).
@@ -47,6 +48,9 @@ struct MuState {
   double cand[kMuCand];
   double best_mu, best_N, best_err;
   double dens_mu;  // mu at which the final density is evaluated
+  double step;     // size of the last Newton step
+  double last_mu, last_N;     // last bracket-step position and its N
+  double cand_prev0, N_prev0; // candidate 0 of the evaluated pass and its N
 };
 
 // SC loop state, resident in device memory.
@@ -143,13 +147,16 @@ __device__ inline bool grid_barrier(ScState* st) {
 // The reference brackets mu by steps Delta_c = e^{DeltamuModifier} (1 + c)
 // |mu_prev| away from the start (mpDPFT.cpp:4603, 4633), adapting
 // DeltamuModifier once after the first step (:4613, :4643), for at most 20
-// steps (:4584), and then bisects.  Here each pass evaluates N(mu) for up to
-// kMuCand candidates in one sweep: pass 0 holds the start, the first step in
-// both directions and a few close and wider points; later passes place the
-// reference's remaining bracket steps (with the adapted modifier), and once
-// mu is bracketed the candidates cluster around the regula-falsi estimate,
-// which shrinks the bracket by at least half per pass.  The search ends, as
-// the reference's, when |N - N*| / (2 N*) <= RelAcc.
+// steps (:4584), and then bisects until |N - N*| / (2 N*) <= RelAcc.
+// Here every pass evaluates N(mu) (in double) for a few candidates in one
+// sweep over the grid, plus dN/dmu at the first candidate:
+//   pass 0   the start value and the reference's first step both ways;
+//   then     a Newton step from the first candidate with a tight pair
+//            around it (which usually brackets the root) and the bracket
+//            midpoint as a safeguard; while no bracket is known, the
+//            reference's remaining bracket steps (adapted modifier) join.
+// Every evaluated point tightens the bracket, the Newton point is clipped
+// into it, and the search ends with the reference's tolerance test.
 __device__ __forceinline__ double tri(int c) { return 0.5 * (double)c * (double)(c + 1); }
 
 // Offset of the reference's c-th bracket step from the start.
@@ -172,47 +179,67 @@ __device__ inline void mu_begin(MuState& m, double mu, double prev_abs, double d
   m.dens_mu = mu;
   m.best_N = 0.0;
   m.best_err = 1e300;
+  m.step = 0.0;
   m.ncand = 0;
   m.cand[m.ncand++] = mu;
   m.cand[m.ncand++] = mu - m.delta0;  // first reference step, both directions
   m.cand[m.ncand++] = mu + m.delta0;
-  const double am = fabs(mu) > 1e-300 ? fabs(mu) : prev_abs;
-  const double eps[3] = {1e-8, 1e-6, 1e-4};
-  for (int e = 0; e < 3; ++e) {
-    m.cand[m.ncand++] = mu - eps[e] * am;
-    m.cand[m.ncand++] = mu + eps[e] * am;
-  }
-  for (int c = 2; c <= 4; ++c) {
-    m.cand[m.ncand++] = mu - step_offset(m, c);
-    m.cand[m.ncand++] = mu + step_offset(m, c);
-  }
 }
 
-// Evaluate a pass (block 0, thread 0): update bracket and best point, choose
-// the next candidates or finish.
-__device__ inline void mu_decide(MuState& m, const double* N, double target, double rel_acc,
+// Bracket [lo, hi] of the reference: the two consecutive bracket-step
+// positions around the first crossing of N* in the search direction
+// (muVecMIN/muVecMAX, mpDPFT.cpp:4601-4654).  Only candidates inside it take
+// part in the search afterwards, so the root found is the one the
+// reference's bisection converges to when N(mu) is not monotone.
+__device__ inline void set_bracket(MuState& m, double a, double Na, double b, double Nb) {
+  if (a > b) { double t = a; a = b; b = t; t = Na; Na = Nb; Nb = t; }
+  m.lo = a; m.Nlo = Na; m.hi = b; m.Nhi = Nb;
+  m.have_lo = m.have_hi = 1;
+}
+
+// Evaluate a pass (block 0, thread 0): N[c] at the candidates, slope =
+// dN/dmu at candidate 0.  Finds the bracket, tightens it with every
+// candidate inside, and places the next candidates or finishes.
+__device__ inline void mu_decide(MuState& m, const double* N, double slope, double target, double rel_acc,
                                  double& dmm, int& bits) {
   const double denom = fabs(2.0 * target);
-  for (int c = 0; c < m.ncand; ++c) {
-    double mu = m.cand[c], n = N[c];
-    if (!isfinite(n)) { bits |= kBitNonfinite; continue; }
-    double err = fabs(n - target) / denom;
-    if (err < m.best_err) { m.best_err = err; m.best_mu = mu; m.best_N = n; }
-    if (n < target) {
-      if (!m.have_lo || mu > m.lo) { m.lo = mu; m.Nlo = n; m.have_lo = 1; }
-    } else if (n > target) {
-      if (!m.have_hi || mu < m.hi) { m.hi = mu; m.Nhi = n; m.have_hi = 1; }
-    }
-  }
+  for (int c = 0; c < m.ncand; ++c)
+    if (!isfinite(N[c])) bits |= kBitNonfinite;
+  const bool bracket_before = m.have_lo && m.have_hi;
+  m.cand_prev0 = m.cand[0];
+  m.N_prev0 = N[0];
   if (m.pass == 0) {
-    const double N0 = N[0];
+    const double mu0 = m.cand[0], N0 = N[0];
     const double diff0 = fabs(N0 - target);
+    m.best_mu = mu0; m.best_N = N0; m.best_err = diff0 / denom;
     m.dir = N0 > target ? -1 : 1;
-    if (diff0 / denom > rel_acc) {  // DeltamuModifier adaptation (:4613, :4643)
+    if (m.best_err > rel_acc) {
+      const double mu1 = m.dir < 0 ? m.cand[1] : m.cand[2];
       const double n1 = m.dir < 0 ? N[1] : N[2];
-      const double diff1 = fabs(n1 - target);
-      dmm -= (diff1 - diff0 < 0.0 ? -1.0 : 1.0) * 0.1 * fabs(dmm);
+      dmm -= (fabs(n1 - target) - diff0 < 0.0 ? -1.0 : 1.0) * 0.1 * fabs(dmm);  // (:4613, :4643)
       m.delta1 = exp(dmm) * m.prev_abs;
+      const bool cross = m.dir < 0 ? (n1 <= target) : (n1 >= target);
+      if (cross) set_bracket(m, mu0, N0, mu1, n1);
+      m.last_mu = mu1; m.last_N = n1;
+    }
+  } else if (!bracket_before) {
+    // bracket-step pass: candidates are steps next_c0 .. in the search direction
+    double pm = m.last_mu, pN = m.last_N;
+    for (int c = 0; c < m.ncand; ++c) {
+      const bool cross = m.dir < 0 ? (N[c] <= target) : (N[c] >= target);
+      if (cross) { set_bracket(m, pm, pN, m.cand[c], N[c]); break; }
+      pm = m.cand[c]; pN = N[c];
+    }
+    m.last_mu = pm; m.last_N = pN;
+  } else {
+    // inside the bracket: tighten it and track the best point
+    for (int c = 0; c < m.ncand; ++c) {
+      const double mu = m.cand[c], n = N[c];
+      if (!(mu > m.lo && mu < m.hi) || !isfinite(n)) continue;
+      const double err = fabs(n - target) / denom;
+      if (err < m.best_err) { m.best_err = err; m.best_mu = mu; m.best_N = n; }
+      if (n < target) { m.lo = mu; m.Nlo = n; }
+      else if (n > target) { m.hi = mu; m.Nhi = n; }
     }
   }
   m.pass++;
@@ -220,34 +247,52 @@ __device__ inline void mu_decide(MuState& m, const double* N, double target, dou
   if (m.best_err <= rel_acc) { m.done = 1; return; }
   if (m.pass >= kMuMaxPasses) { m.done = 1; bits |= kBitTimeout; return; }
   m.ncand = 0;
-  if (!m.have_lo || !m.have_hi) {
-    // continue the reference's bracket steps towards the target
-    const int d = m.have_hi ? -1 : 1;  // missing lower end: step down
-    while (m.next_c <= 20 && m.ncand < kMuCand) m.cand[m.ncand++] = m.start + d * step_offset(m, m.next_c++);
-    if (m.ncand == 0) {
-      // no bracket within 20 steps: the reference resets mu to its start
-      // value but keeps the density of its last trial step (:4657-4662)
+  if (!(m.have_lo && m.have_hi)) {
+    if (m.next_c > 20) {
+      // no bracket within the reference's 20 steps: it resets mu to the
+      // start value but keeps the density of its last trial (:4657-4662)
       m.done = 1;
-      m.dens_mu = m.start + d * step_offset(m, 20);
+      m.dens_mu = m.start + m.dir * step_offset(m, 20);
       m.best_mu = m.start;
       m.best_err = 1e300;
       bits |= kBitBracket;
       return;
     }
+    while (m.next_c <= 20 && m.ncand < kMuCand) m.cand[m.ncand++] = m.start + m.dir * step_offset(m, m.next_c++);
     return;
   }
-  const double w = m.hi - m.lo;
-  if (!(w > 1.0e-12)) { m.done = 1; return; }  // Deltamu below MP (:4711)
-  double rf = m.lo + (target - m.Nlo) * w / (m.Nhi - m.Nlo);
-  if (!(rf > m.lo && rf < m.hi)) rf = 0.5 * (m.lo + m.hi);
-  m.cand[m.ncand++] = rf;
-  m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
-  double f = 0.25;
-  for (int j = 0; j < 7; ++j) {
-    m.cand[m.ncand++] = rf - (rf - m.lo) * f;
-    m.cand[m.ncand++] = rf + (m.hi - rf) * f;
-    f *= 0.125;
+  if (!(m.hi - m.lo > 1.0e-12)) { m.done = 1; return; }  // Deltamu below MP (:4711)
+  if (!bracket_before) {
+    // the reference starts bisecting at the bracket midpoint (:4667-4672);
+    // its first evaluation also provides the slope for Newton steps
+    m.best_mu = 0.5 * (m.lo + m.hi);
+    m.best_err = 1e300;
+    m.step = 0.0;
+    const double rf = m.lo + (target - m.Nlo) * (m.hi - m.lo) / (m.Nhi - m.Nlo);
+    if (rf > m.lo && rf < m.hi) m.cand[m.ncand++] = rf;  // candidate 0 carries the slope
+    m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
+    return;
   }
+  // Newton from candidate 0 of this pass, clipped into the bracket; else
+  // regula falsi
+  const double mu0 = m.cand_prev0, N0 = m.N_prev0;
+  double est;
+  bool newton = slope > 0.0 && isfinite(slope) && isfinite(N0);
+  if (newton) {
+    est = mu0 + (target - N0) / slope;
+    newton = est > m.lo && est < m.hi;
+  }
+  if (!newton) est = m.lo + (target - m.Nlo) * (m.hi - m.lo) / (m.Nhi - m.Nlo);
+  if (!(est > m.lo && est < m.hi)) est = 0.5 * (m.lo + m.hi);
+  const double d = fabs(est - mu0);
+  double e = 1e-3 * d;
+  if (m.step > 0.0) e = fmax(e, 2.0 * d * d / m.step);
+  e = fmax(e, 1e-13 * fabs(est) + 1e-300);
+  m.step = d;
+  m.cand[m.ncand++] = est;
+  if (est - e > m.lo) m.cand[m.ncand++] = est - e;
+  if (est + e < m.hi) m.cand[m.ncand++] = est + e;
+  if (m.pass > 3) m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
 }
 
 // ---------------------------------------------------------- small solve --
@@ -453,11 +498,12 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
     if (!any) break;
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
-      double acc[kMuCand];
+      // N(mu) and dN/dmu are evaluated in double from the stored fields
+      // (FP32 in mixed mode): the particle-number integral and the mu search
+      // are FP64 in both modes
+      double acc[kMuAcc];
 #pragma unroll
-      for (int c = 0; c < kMuCand; ++c) acc[c] = 0.0;
-      // n(mu) is evaluated in double from the stored fields (FP32 in mixed
-      // mode): the particle-number integral and the mu search are FP64.
+      for (int c = 0; c < kMuAcc; ++c) acc[c] = 0.0;
       const DensParams d = kp.dens[s];
       const int nc = s_ms[s].ncand;
       double cmu[kMuCand];
@@ -466,30 +512,20 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
       const R* Vs = V + (long)s * n;
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
-      if (sizeof(R) == sizeof(double)) {
-        for (long p = tid; p < n; p += nthreads) {
-          const double v = (double)Vs[p];
-          const double l = Ls ? (double)Ls[p] : 0.0;
-          const double g = Gs ? (double)Gs[p] : 0.0;
+      for (long p = tid; p < n; p += nthreads) {
+        const double v = (double)Vs[p];
+        const double l = Ls ? (double)Ls[p] : 0.0;
+        const double g = Gs ? (double)Gs[p] : 0.0;
+        acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
 #pragma unroll
-          for (int c = 0; c < kMuCand; ++c)
-            if (c < nc) acc[c] += density_at_d(d, cmu[c] - v, l, g);
-        }
-      } else {
-        for (long p = tid; p < n; p += nthreads) {
-          const double v = (double)Vs[p];
-          const float l = Ls ? (float)Ls[p] : 0.f;
-          const float g = Gs ? (float)Gs[p] : 0.f;
-#pragma unroll
-          for (int c = 0; c < kMuCand; ++c)
-            if (c < nc) acc[c] += (double)density_at_f(d, (float)(cmu[c] - v), l, g);
-        }
+        for (int c = 0; c < kMuCand; ++c)
+          if (c < nc) acc[c] += density_at_d(d, cmu[c] - v, l, g);
       }
-      block_reduce_store<kMuCand>(acc, mypart + s * kMuCand);
+      block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
     }
     if (!grid_barrier(st)) return;
     if (blockIdx.x == 0) {
-      reduce_partials(a.part, gridDim.x, S * kMuCand, red);
+      reduce_partials(a.part, gridDim.x, S * kMuAcc, red);
       if (threadIdx.x == 0) {
         double dmm = st->dmm;
         int bits = 0;
@@ -497,8 +533,8 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
           if (s_ms[s].done) continue;
           MuState ms = st->ms[s];
           double N[kMuCand];
-          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuCand + c] * kp.geom.dvol;
-          mu_decide(ms, N, kp.abundance[s], kp.rel_acc, dmm, bits);
+          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuAcc + c] * kp.geom.dvol;
+          mu_decide(ms, N, red[s * kMuAcc + kMuCand] * kp.geom.dvol, kp.abundance[s], kp.rel_acc, dmm, bits);
           st->ms[s] = ms;
         }
         st->dmm = dmm;
@@ -536,10 +572,7 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
         const double l = a.lap ? (double)a.lap[q] : 0.0;
         const double g = a.g2 ? (double)a.g2[q] : 0.0;
         // mode 2 (admix only): V holds the output densities
-        const double nod = a.mode == 2 ? (double)v
-                           : (sizeof(R) == sizeof(double)
-                                  ? density_at_d(kp.dens[s], s_mu[s] - (double)v, l, g)
-                                  : (double)density_at_f(kp.dens[s], (float)(s_mu[s] - (double)v), (float)l, (float)g));
+        const double nod = a.mode == 2 ? (double)v : density_at_d(kp.dens[s], s_mu[s] - (double)v, l, g);
         const R no = R(nod);
         acc[4 * s + 0] += nod;
         if (a.mode == 1) { nin[q] = no; continue; }
