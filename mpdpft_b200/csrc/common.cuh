@@ -13,7 +13,7 @@ constexpr double kPi = 3.141592653589793;
 constexpr int kThreads = 256;
 constexpr int kMaxS = MPDPFT_MAX_SPECIES;
 constexpr int kMaxP = MPDPFT_MAX_PULAY;
-constexpr int kMuCand = 16;          // candidates per mu-search pass
+constexpr int kMuCand = 8;           // candidates per mu-search pass
 constexpr int kMuMaxPasses = 24;     // device mu-search pass cap
 constexpr int kMaxBlocks = 148 * 8;  // 148 SMs x 8 resident 256-thread blocks
 

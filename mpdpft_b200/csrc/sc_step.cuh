@@ -11,13 +11,16 @@
 // synchronisation and can be captured in a CUDA graph.  FFT-based terms
 // (Hartree, DelField) are produced by the FFT kernels before this launch.
 #pragma once
+#include <cstddef>
+
 #include "common.cuh"
 
 namespace mpdpft {
 
 constexpr int kStepThreads = 512;
 constexpr int kMuAcc = kMuCand + 1;  // candidate sums + dN/dmu at candidate 0
-constexpr int kNPart = 4 * kMaxS + kMaxP > kMaxS * kMuAcc ? 4 * kMaxS + kMaxP : kMaxS * kMuAcc;
+constexpr int kNF = 4 + kMaxP;        // per-species sums of the density/Gram pass
+constexpr int kNPart = kMaxS * kNF > kMaxS * kMuAcc ? kMaxS * kNF : kMaxS * kMuAcc;
 constexpr long kBarrierSpinLimit = 20000000;  // ~ seconds with nanosleep backoff
 
 // Constant parameters of one solve (kernel argument, by value).
@@ -106,6 +109,19 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[k] = globaltimer()
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+
+// Block-wide copy of the SC state between global and block 0's shared copy.
+// The grid-barrier fields (bar_count onwards) are never copied back.
+__device__ __forceinline__ void state_load(ScState* dst, const ScState* src) {
+  const unsigned* s = reinterpret_cast<const unsigned*>(src);
+  unsigned* d = reinterpret_cast<unsigned*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(ScState) / 4); i += blockDim.x) d[i] = __ldcg(s + i);
+}
+__device__ __forceinline__ void state_store(ScState* dst, const ScState* src) {
+  const unsigned* s = reinterpret_cast<const unsigned*>(src);
+  unsigned* d = reinterpret_cast<unsigned*>(dst);
+  for (int i = threadIdx.x; i < (int)(offsetof(ScState, bar_count) / 4); i += blockDim.x) d[i] = s[i];
+}
 __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
 
 // Bounded sense-free generation barrier over all blocks of a cooperative
@@ -268,8 +284,20 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
     m.best_mu = 0.5 * (m.lo + m.hi);
     m.best_err = 1e300;
     m.step = 0.0;
+    // Newton from candidate 0 of the bracketing pass (its slope is known)
+    if (slope > 0.0 && isfinite(slope) && isfinite(m.N_prev0)) {
+      const double est = m.cand_prev0 + (target - m.N_prev0) / slope;
+      if (est > m.lo && est < m.hi) {
+        const double d = fabs(est - m.cand_prev0);
+        const double e = fmax(1e-3 * d, 1e-13 * fabs(est) + 1e-300);
+        m.step = d;
+        m.cand[m.ncand++] = est;  // candidate 0 carries the slope
+        if (est - e > m.lo) m.cand[m.ncand++] = est - e;
+        if (est + e < m.hi) m.cand[m.ncand++] = est + e;
+      }
+    }
     const double rf = m.lo + (target - m.Nlo) * (m.hi - m.lo) / (m.Nhi - m.Nlo);
-    if (rf > m.lo && rf < m.hi) m.cand[m.ncand++] = rf;  // candidate 0 carries the slope
+    if (rf > m.lo && rf < m.hi) m.cand[m.ncand++] = rf;
     m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
     return;
   }
@@ -385,7 +413,7 @@ __device__ inline void reduce_partials(const double* part, int nblocks, int nval
 // search + n[V]), written into the current ring slot; used for the initial
 // densities (mpDPFT.cpp:195) and the standalone mu-search entry point.
 template <typename R>
-__global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kStepThreads, 2) sc_step_kernel(StepArgs<R> a) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
@@ -400,8 +428,18 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
   __shared__ double s_G[kMaxP * kMaxP], s_M[kMaxP * kMaxP], s_inv[kMaxP * kMaxP], s_fac[kMaxP];
   __shared__ int s_perm[kMaxP];
   __shared__ int s_ok;
+  __shared__ double s_grow[kMaxP];
 
   if (a.mode != 1 && ldcg(&st->exit_loop)) return;
+  // block 0 runs the scalar SC logic on a shared-memory copy of the state
+  // (global round trips would serialise it); it writes the copy back before
+  // every grid barrier after which other blocks read the state
+  __shared__ ScState s_st;
+  ScState* const ls = &s_st;
+  if (blockIdx.x == 0) {
+    state_load(ls, st);
+    __syncthreads();
+  }
   const int cur = ldcg(&st->slot);
   const int ring = kp.ring;
   const int next = (cur + 1) % ring;
@@ -472,14 +510,16 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
       if (threadIdx.x == 0) {
         double w = 0.0;
         for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red[s] / (double)n));
-        st->v_res = w;
+        ls->v_res = w;
       }
     }
     if (threadIdx.x == 0) {
-      for (int s = 0; s < S; ++s) { st->ms[s] = s_ms[s]; st->prev_mu[s] = s_ms[s].start; }
-      st->mu_passes = 0;
-      st->iter_bits = 0;
+      for (int s = 0; s < S; ++s) { ls->ms[s] = s_ms[s]; ls->prev_mu[s] = s_ms[s].start; }
+      ls->mu_passes = 0;
+      ls->iter_bits = 0;
     }
+    __syncthreads();
+    state_store(st, ls);
   }
   if (!grid_barrier(st)) return;
 
@@ -506,9 +546,7 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
       for (int c = 0; c < kMuAcc; ++c) acc[c] = 0.0;
       const DensParams d = kp.dens[s];
       const int nc = s_ms[s].ncand;
-      double cmu[kMuCand];
-#pragma unroll
-      for (int c = 0; c < kMuCand; ++c) cmu[c] = c < nc ? s_ms[s].cand[c] : 0.0;
+      const double* cmu = s_ms[s].cand;  // shared memory (broadcast reads)
       const R* Vs = V + (long)s * n;
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
@@ -527,20 +565,22 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
     if (blockIdx.x == 0) {
       reduce_partials(a.part, gridDim.x, S * kMuAcc, red);
       if (threadIdx.x == 0) {
-        double dmm = st->dmm;
+        double dmm = ls->dmm;
         int bits = 0;
         for (int s = 0; s < S; ++s) {
           if (s_ms[s].done) continue;
-          MuState ms = st->ms[s];
+          MuState ms = ls->ms[s];
           double N[kMuCand];
           for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuAcc + c] * kp.geom.dvol;
           mu_decide(ms, N, red[s * kMuAcc + kMuCand] * kp.geom.dvol, kp.abundance[s], kp.rel_acc, dmm, bits);
-          st->ms[s] = ms;
+          ls->ms[s] = ms;
         }
-        st->dmm = dmm;
-        st->iter_bits |= bits;
-        st->mu_passes++;
+        ls->dmm = dmm;
+        ls->iter_bits |= bits;
+        ls->mu_passes++;
       }
+      __syncthreads();
+      state_store(st, ls);
     }
     if (!grid_barrier(st)) return;
   }
@@ -558,89 +598,103 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
   const int hist = ldcg(&st->hist);
   const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
   {
-    constexpr int NF = 4 * kMaxS + kMaxP;
-    double acc[NF];
-#pragma unroll
-    for (int j = 0; j < NF; ++j) acc[j] = 0.0;
+    // per species: [0] N, [1] <n_out, n_in>_w, [2] <n_out, n_out>_w,
+    // [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram row, summed over
+    // species in phase D); w = multiplicity in the reference storage
+    __shared__ long s_roff[kMaxP];
+    if (threadIdx.x < I) {
+      const int j = threadIdx.x;
+      s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
+    }
+    __syncthreads();
     R* nin = a.nin + (long)cur * S * n;
     R* rcur = a.res + (long)cur * S * n;
-    for (long p = tid; p < n; p += nthreads) {
-      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
-      for (int s = 0; s < S; ++s) {
-        const long q = (long)s * n + p;
+    for (int s = 0; s < S; ++s) {
+      double acc[kNF];
+#pragma unroll
+      for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
+      const DensParams d = kp.dens[s];
+      const double mus = s_mu[s];
+      const long so = (long)s * n;
+      for (long p = tid; p < n; p += nthreads) {
+        const long q = so + p;
         const R v = V[q];
         const double l = a.lap ? (double)a.lap[q] : 0.0;
         const double g = a.g2 ? (double)a.g2[q] : 0.0;
         // mode 2 (admix only): V holds the output densities
-        const double nod = a.mode == 2 ? (double)v : density_at_d(kp.dens[s], s_mu[s] - (double)v, l, g);
+        const double nod = a.mode == 2 ? (double)v : density_at_d(d, mus - (double)v, l, g);
         const R no = R(nod);
-        acc[4 * s + 0] += nod;
+        acc[0] += nod;
         if (a.mode == 1) { nin[q] = no; continue; }
-        R ni = nin[q];
-        R r = no - ni;
+        const R ni = nin[q];
+        const R r = no - ni;
         rcur[q] = r;
-        const double dno = (double)no, dni = (double)ni, dr = (double)r;
-        acc[4 * s + 1] += w * dno * dni;
-        acc[4 * s + 2] += w * dno * dno;
-        acc[4 * s + 3] += w * dni * dni;
-        for (int j = 0; j < I; ++j) {
-          int slot = (cur - (I - 1) + j + ring) % ring;
-          double rj = (j == I - 1) ? dr : (double)a.res[((long)slot * S + s) * n + p];
-          acc[4 * kMaxS + j] += w * dr * rj;
-        }
+        const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
+        const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
+        acc[1] += w * dno * dni;
+        acc[2] += w * dno * dno;
+        acc[3] += w * dni * dni;
+        for (int j = 0; j < I - 1; ++j) acc[4 + j] += wr * (double)a.res[s_roff[j] + q];
+        if (I > 0) acc[4 + I - 1] += wr * dr;
       }
+      block_reduce_store<kNF>(acc, mypart + s * kNF);
     }
-    block_reduce_store<NF>(acc, mypart);
   }
   if (!grid_barrier(st)) return;
 
   // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
   MPDPFT_TSTAMP(3);
   if (blockIdx.x == 0) {
-    reduce_partials(a.part, gridDim.x, 4 * kMaxS + kMaxP, red);
+    reduce_partials(a.part, gridDim.x, S * kNF, red);
+    if (threadIdx.x < kMaxP) {  // Gram row summed over species
+      double t = 0.0;
+      for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
+      s_grow[threadIdx.x] = t;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-      const int sc = st->sc_count;
+      const int sc = ls->sc_count;
       double tot = 0.0;
       for (int s = 0; s < S; ++s) {
-        st->mu[s] = s_mu_rep[s];
-        st->ab[s] = red[4 * s] * kp.geom.dvol;
-        if (!isfinite(st->ab[s])) st->iter_bits |= kBitNonfinite;
-        tot += st->ab[s];
+        ls->mu[s] = s_mu_rep[s];
+        ls->ab[s] = red[s * kNF] * kp.geom.dvol;
+        if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
+        tot += ls->ab[s];
       }
       if (a.mode == 1) {
-        st->status_bits |= st->iter_bits;
-        st->mu_passes_total += st->mu_passes;
+        ls->status_bits |= ls->iter_bits;
+        ls->mu_passes_total += ls->mu_passes;
       } else {
         // CheckConvergence (mpDPFT.cpp:4759-4782)
         const double mp = 100.0 * 1.0e-16;
         if (sc > 0) {
           double cc = 0.0, maxtest = 0.0;
           for (int s = 0; s < S; ++s) {
-            double oi = red[4 * s + 1], oo = red[4 * s + 2], ii = red[4 * s + 3];
+            double oi = red[s * kNF + 1], oo = red[s * kNF + 2], ii = red[s * kNF + 3];
             double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
-            double t = rd * st->ab[s] / tot;
+            double t = rd * ls->ab[s] / tot;
             if (t > maxtest) { maxtest = t; cc = maxtest; }
           }
-          st->cc = cc;
+          ls->cc = cc;
           double dab = 0.0, dmu = 0.0;
           for (int s = 0; s < S; ++s) {
-            dab += (st->ab[s] - st->old_ab[s]) * (st->ab[s] - st->old_ab[s]);
-            dmu += (st->mu[s] - st->old_mu[s]) * (st->mu[s] - st->old_mu[s]);
+            dab += (ls->ab[s] - ls->old_ab[s]) * (ls->ab[s] - ls->old_ab[s]);
+            dmu += (ls->mu[s] - ls->old_mu[s]) * (ls->mu[s] - ls->old_mu[s]);
           }
           int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
           double avth = 0.0;
-          for (int s = 0; s < S; ++s) avth += st->theta[s] / (double)S;
-          bool vok = !(kp.pot_tol > 0.0) || st->v_res <= kp.pot_tol;
+          for (int s = 0; s < S; ++s) avth += ls->theta[s] / (double)S;
+          bool vok = !(kp.pot_tol > 0.0) || ls->v_res <= kp.pot_tol;
           if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
               (cc < kp.sc_criterion || steady) && vok)
-            st->exit_count++;
+            ls->exit_count++;
           else
-            st->exit_count = 0;
-          if (st->exit_count >= 3) st->exit_loop = 1;
+            ls->exit_count = 0;
+          if (ls->exit_count >= 3) ls->exit_loop = 1;
         } else {
-          st->cc = 1.2345678901234567890;
+          ls->cc = 1.2345678901234567890;
         }
-        if (sc == kp.max_sc) st->exit_loop = 1;  // Intercept (:4866)
+        if (sc == kp.max_sc) ls->exit_loop = 1;  // Intercept (:4866)
         // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): assemble the
         // Gram matrix (last row/column new, the rest shifted from before)
         if (pulay_now) {
@@ -648,14 +702,14 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
           for (int i = 0; i < I; ++i)
             for (int j = 0; j < I; ++j) {
               double v;
-              if (i == I - 1) v = red[4 * kMaxS + j];
-              else if (j == I - 1) v = red[4 * kMaxS + i];
-              else v = st->gram[(i + shift) * kMaxP + (j + shift)];
+              if (i == I - 1) v = s_grow[j];
+              else if (j == I - 1) v = s_grow[i];
+              else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
               s_G[i * I + j] = v;
             }
           for (int i = 0; i < I; ++i)
-            for (int j = 0; j < I; ++j) st->gram[i * kMaxP + j] = s_G[i * I + j];
-          st->hist = I;
+            for (int j = 0; j < I; ++j) ls->gram[i * kMaxP + j] = s_G[i * I + j];
+          ls->hist = I;
         }
       }
     }
@@ -679,7 +733,7 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      const int sc = st->sc_count;
+      const int sc = ls->sc_count;
       if (a.mode != 1) {
         int used = 0;
         if (pulay_now) {
@@ -690,53 +744,55 @@ __global__ void __launch_bounds__(kStepThreads) sc_step_kernel(StepArgs<R> a) {
               for (int k = 0; k < I; ++k) x[i] += s_inv[i * I + k];
               A += x[i];
             }
-            for (int i = 0; i < I; ++i) st->coeff[i] = x[i] / A;
+            for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
             used = 1;
           }
-          if (!used) st->iter_bits |= kBitPulay;
+          if (!used) ls->iter_bits |= kBitPulay;
         }
-        st->pulay_used = used;
-        st->ncoeff = used ? I : 0;
-        for (int s = 0; s < S; ++s) st->theta_mix[s] = st->theta[s];
+        ls->pulay_used = used;
+        ls->ncoeff = used ? I : 0;
+        for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
         // InjectSchedule (mpDPFT.cpp:5229-5315)
         if (kp.schedule == 5) {
           for (int s = 0; s < S; ++s) {
-            double th = st->theta[s] * (st->cc < st->old_cc ? 1.1 : 0.5);
+            double th = ls->theta[s] * (ls->cc < ls->old_cc ? 1.1 : 0.5);
             th = fmin(0.8, th);
             th = fmax(10.0 / (double)kp.max_sc, th);
-            st->theta[s] = th;
+            ls->theta[s] = th;
           }
         } else if (kp.schedule == 9) {
           for (int s = 0; s < S; ++s)
-            if (st->theta[s] < 0.2)
-              st->theta[s] = st->theta0[s] + (0.2 - st->theta0[s]) * (double)sc / (double)kp.max_sc;
+            if (ls->theta[s] < 0.2)
+              ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
         }
         if (a.log && sc < a.log_cap) {
           mpdpft_iter_log& L = a.log[sc];
           L.sc_count = sc;
-          L.mu_trials = st->mu_passes;
+          L.mu_trials = ls->mu_passes;
           L.pulay_used = used;
-          L.status_bits = st->iter_bits;
-          L.cc = st->cc;
-          L.v_residual = st->v_res;
+          L.status_bits = ls->iter_bits;
+          L.cc = ls->cc;
+          L.v_residual = ls->v_res;
           for (int s = 0; s < kMaxS; ++s) {
-            L.mu[s] = s < S ? st->mu[s] : 0.0;
-            L.abundance[s] = s < S ? st->ab[s] : 0.0;
-            L.theta[s] = s < S ? st->theta_mix[s] : 0.0;
+            L.mu[s] = s < S ? ls->mu[s] : 0.0;
+            L.abundance[s] = s < S ? ls->ab[s] : 0.0;
+            L.theta[s] = s < S ? ls->theta_mix[s] : 0.0;
           }
           L.ms = 0.0;
         }
-        st->status_bits |= st->iter_bits;
-        st->mu_passes_total += st->mu_passes;
+        ls->status_bits |= ls->iter_bits;
+        ls->mu_passes_total += ls->mu_passes;
         // StoreCurrentIteration of the next iteration; PrepareNextIteration
-        for (int s = 0; s < S; ++s) { st->old_mu[s] = st->mu[s]; st->old_ab[s] = st->ab[s]; }
-        st->old_cc = st->cc;
-        if (sc > 0) st->inc_v = fmin(1.0, st->inc_v + kp.inc_v0);  // (:4833)
-        st->mix_src = cur;
-        st->slot = next;
-        st->sc_count = sc + 1;
+        for (int s = 0; s < S; ++s) { ls->old_mu[s] = ls->mu[s]; ls->old_ab[s] = ls->ab[s]; }
+        ls->old_cc = ls->cc;
+        if (sc > 0) ls->inc_v = fmin(1.0, ls->inc_v + kp.inc_v0);  // (:4833)
+        ls->mix_src = cur;
+        ls->slot = next;
+        ls->sc_count = sc + 1;
       }
     }
+    __syncthreads();
+    state_store(st, ls);
   }
   if (a.mode == 1) return;
   MPDPFT_TSTAMP(4);
