@@ -120,7 +120,15 @@ struct DensParams {
   double T;        // temperature (TF-inspired T>0, gradient 2D)
   double floor_u;  // floor of mu - V in the 3D gradient terms
   double c2;       // |grad V|^2 coefficient (3D gradient form)
+  int cut;         // 1: n and dn/dmu vanish wherever mu - V <= 0
 };
+
+// Functionals with a classically forbidden region where n = 0 exactly (TF,
+// TF-inspired, 3D gradient-corrected); the finite-temperature forms are
+// positive everywhere.
+inline int density_has_cut(int expr, int dim) {
+  return expr == MPDPFT_DENS_TF || expr == MPDPFT_DENS_TF_INSPIRED || (expr == MPDPFT_DENS_GRADIENT && dim == 3);
+}
 
 // Pointwise density at u = mu - V (R = float or double arithmetic).
 //  7: GetTFdensity (mpDPFT.cpp:4415-4436)

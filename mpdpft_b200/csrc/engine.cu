@@ -19,7 +19,7 @@
 #include "../../include/mpdpft_gpu.h"
 #include "common.cuh"
 #include "engine.h"
-#include "sc_step.cuh"
+#include "sc_kernel.cuh"
 
 namespace mpdpft {
 
@@ -145,6 +145,8 @@ int Ctx::alloc(void** p, size_t bytes) {
 static int check_params(const mpdpft_params& p) {
   if (p.dim != 2 && p.dim != 3) return set_error(MPDPFT_ERR_ARG, "dim must be 2 or 3");
   if (p.steps < 4 || (p.steps & 1)) return set_error(MPDPFT_ERR_ARG, "steps must be even and >= 4");
+  if ((p.dim == 3 && p.steps > 1024) || (p.dim == 2 && p.steps > 32768))
+    return set_error(MPDPFT_ERR_ARG, "steps too large (grid indices are 32-bit)");
   if (p.species < 1 || p.species > MPDPFT_MAX_SPECIES) return set_error(MPDPFT_ERR_ARG, "species out of range");
   if (!(p.edge > 0.0)) return set_error(MPDPFT_ERR_ARG, "edge must be positive");
   if (p.mixer < 0 || p.mixer > 1) return set_error(MPDPFT_ERR_ARG, "mixer must be 0 (linear) or 1 (Pulay)");
@@ -188,6 +190,7 @@ KParams Ctx::kparams() const {
     d.T = temperature[s];
     d.floor_u = P.gradient_floor;
     d.c2 = P.gradient_grad2;
+    d.cut = density_has_cut(d.expr, d.dim) && (d.expr != MPDPFT_DENS_TF_INSPIRED || d.tau > 0.0);
     k.abundance[s] = P.abundances[s];
     k.charges[s] = P.charges[s];
   }
@@ -206,6 +209,9 @@ KParams Ctx::kparams() const {
   k.schedule = P.schedule;
   k.pot_tol = P.potential_tol;
   k.inc_v0 = P.incremental_v;
+  k.nseg = nseg;
+  k.seg_mul = seg_mul;
+  k.vec4 = (geom.n % 4) == 0;
   return k;
 }
 
@@ -268,6 +274,23 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   step_blocks = num_sms * std::min(occ, 2);
   long useful = (geom.n + kStepThreads - 1) / kStepThreads;
   if (step_blocks > useful) step_blocks = (int)std::max(1L, useful);
+  // sweep order: segment k -> k * seg_mul mod nseg with seg_mul near
+  // nseg / golden ratio and coprime to nseg (a bijection that scatters
+  // neighbouring k over the grid)
+  nseg = (geom.n + kSegPts - 1) / kSegPts;
+  seg_mul = 1;
+  if (nseg > 2) {
+    long m = std::max(1L, (long)std::llround(0.6180339887498949 * (double)nseg));
+    auto gcd = [](long a, long b) { while (b) { long t = a % b; a = b; b = t; } return a; };
+    while (gcd(m, nseg) != 1) ++m;
+    seg_mul = m % nseg;
+  }
+  {
+    const long warps = (long)step_blocks * kStepWarps;
+    seg_wmax = (int)((nseg + warps - 1) / warps);
+    const size_t ints = (size_t)kMaxS * ((size_t)step_blocks + (size_t)warps * seg_wmax + (size_t)nseg);
+    if ((st = alloc((void**)&d_seg, sizeof(int) * ints))) return st;
+  }
   part_vals = std::max(kNPart, kNEnergy);
   if ((st = alloc((void**)&d_part, sizeof(double) * (size_t)std::max(step_blocks, kMaxBlocks) * part_vals))) return st;
   pinned_bytes = sizeof(double) * (size_t)std::max(n_ref, geom.n) * 2;
@@ -353,6 +376,13 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.nin = (R*)d_nin;
   a.res = (R*)d_res;
   a.part = d_part;
+  {
+    const long warps = (long)step_blocks * kStepWarps;
+    a.bcount = d_seg;
+    a.wlist = d_seg + (size_t)kMaxS * step_blocks;
+    a.slist = a.wlist + (size_t)kMaxS * warps * seg_wmax;
+    a.wmax = seg_wmax;
+  }
   a.vres_part = vres_part_ext;
   a.vres_blocks = vres_blocks_ext;
   a.log = d_log;

@@ -48,6 +48,10 @@ struct Ctx {
   mpdpft_iter_log* d_log = nullptr;
   int log_cap = 0;
   int step_blocks = 0;
+  long nseg = 1;     // warp segments of the step kernel's sweeps
+  long seg_mul = 1;  // their visiting-order multiplier
+  int seg_wmax = 1;  // segments per warp in a full sweep (upper bound)
+  int* d_seg = nullptr;  // active-segment lists: bcount | wlist | slist
   int assemble_in_step = 1;
   const double* vres_part_ext = nullptr;
   int vres_blocks_ext = 0;

@@ -1,0 +1,771 @@
+// sc_kernel.cuh -- the persistent SC-iteration kernel (phases A-E) and its
+// block-level helpers.  State, parameters and the mu-search decisions are in
+// sc_step.cuh.
+//
+// Work layout.  Grid sweeps are over warp segments of kSegPts = 128
+// consecutive points (4 per lane, one 16-byte vector load per field), visited
+// in the scattered order seg = k * seg_mul mod nseg, so the costly segments
+// (points where mu - V > 0, a few per cent of an atom's box) spread evenly
+// over the warps.  The mu search of a functional that vanishes for mu <= V
+// skips segments with no point below the pass's largest candidate (a warp
+// vote on V), records the others during its first full sweep, and later
+// passes visit only that compacted list: all warps share the few costly
+// segments instead of a handful of warps carrying them.
+#pragma once
+#include "sc_step.cuh"
+
+namespace mpdpft {
+
+// ---------------------------------------------------------- small solve --
+// Inverse of the Pulay Gram matrix (n <= kMaxP) by Gauss-Jordan elimination
+// with full pivoting on one warp; rank test as Eigen's
+// FullPivHouseholderQR::isInvertible (threshold eps * n * max|pivot|), which
+// the reference uses (mpDPFT.cpp:5089).  Each pivot is the first maximum, in
+// row-major order, among the rows and columns not used yet.  Rows are never
+// swapped: lane l holds elements l, l + 32, ... of [M | R] in registers, the
+// pivot row and column pass through shared memory, and at the end row pc_k
+// of the inverse is row pr_k of R.
+constexpr int kInvQ = (kMaxP * kMaxP + 31) / 32;
+
+__device__ inline bool warp_inverse(int n, const double* G, double* inv, double* prow_m, double* prow_r,
+                                    double* pcol, int* colof) {
+  const int lane = threadIdx.x & 31;
+  const int nn = n * n;
+  double m[kInvQ], r[kInvQ];
+  int ei[kInvQ], ej[kInvQ];
+#pragma unroll
+  for (int q = 0; q < kInvQ; ++q) {
+    const int e = lane + 32 * q;
+    ei[q] = e < nn ? e / n : -1;  // -1: this slot holds no element
+    ej[q] = e < nn ? e % n : 0;
+    m[q] = e < nn ? G[e] : 0.0;
+    r[q] = (e < nn && ei[q] == ej[q]) ? 1.0 : 0.0;
+  }
+  unsigned used_r = 0u, used_c = 0u;
+  double maxpiv = 0.0, minpiv = 1e300;
+  for (int c = 0; c < n; ++c) {
+    double best = -1.0;
+    int be = 0x7fffffff;
+#pragma unroll
+    for (int q = 0; q < kInvQ; ++q) {
+      if (ei[q] < 0 || ((used_r >> ei[q]) & 1u) || ((used_c >> ej[q]) & 1u)) continue;
+      const double v = fabs(m[q]);
+      if (v > best) { best = v; be = lane + 32 * q; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oe = __shfl_xor_sync(0xffffffffu, be, o);
+      if (ob > best || (ob == best && oe < be)) { best = ob; be = oe; }
+    }
+    const int pr = be / n, pc = be % n;
+#pragma unroll
+    for (int q = 0; q < kInvQ; ++q) {
+      if (ei[q] == pr) { prow_m[ej[q]] = m[q]; prow_r[ej[q]] = r[q]; }
+      if (ei[q] >= 0 && ej[q] == pc) pcol[ei[q]] = m[q];
+    }
+    if (lane == 0) colof[pr] = pc;
+    __syncwarp();
+    const double piv = pcol[pr];
+    maxpiv = fmax(maxpiv, fabs(piv));
+    minpiv = fmin(minpiv, fabs(piv));
+    if (piv == 0.0) return false;  // same value on every lane
+    const double ip = 1.0 / piv;
+#pragma unroll
+    for (int q = 0; q < kInvQ; ++q) {
+      if (ei[q] < 0) continue;
+      if (ei[q] == pr) {
+        m[q] *= ip;
+        r[q] *= ip;
+      } else {
+        const double f = pcol[ei[q]] * ip;
+        m[q] -= f * prow_m[ej[q]];
+        r[q] -= f * prow_r[ej[q]];
+      }
+    }
+    used_r |= 1u << pr;
+    used_c |= 1u << pc;
+    __syncwarp();
+  }
+  if (minpiv <= 2.220446049250313e-16 * (double)n * maxpiv) return false;
+#pragma unroll
+  for (int q = 0; q < kInvQ; ++q)
+    if (ei[q] >= 0) inv[colof[ei[q]] * n + ej[q]] = r[q];
+  __syncwarp();
+  return true;
+}
+
+// sum_{i,j} ((inv G)_{ij} - delta_ij)^2 on one warp (the reference's
+// validation of the inverse, mpDPFT.cpp:5099-5107)
+__device__ inline double warp_inverse_defect(int n, const double* G, const double* inv) {
+  const int lane = threadIdx.x & 31;
+  double test = 0.0;
+  for (int e = lane; e < n * n; e += 32) {
+    const int i = e / n, j = e % n;
+    double t = 0.0;
+    for (int k = 0; k < n; ++k) t += inv[i * n + k] * G[k * n + j];
+    t -= (i == j) ? 1.0 : 0.0;
+    test += t * t;
+  }
+  return warp_sum(test);
+}
+
+// ------------------------------------------------------------ segments --
+template <typename R>
+__device__ __forceinline__ void load4(const R* f, long p0, long n, int vec4, R (&o)[4]) {
+  if (vec4 && p0 + 3 < n) {
+    if constexpr (sizeof(R) == sizeof(float)) {
+      const float4 t = __ldcg(reinterpret_cast<const float4*>(f + p0));
+      o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+    } else {
+      const double2 t0 = __ldcg(reinterpret_cast<const double2*>(f + p0));
+      const double2 t1 = __ldcg(reinterpret_cast<const double2*>(f + p0 + 2));
+      o[0] = t0.x; o[1] = t0.y; o[2] = t1.x; o[3] = t1.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) o[i] = (p0 + i < n) ? __ldcg(f + p0 + i) : R(0);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void store4(R* f, long p0, long n, int vec4, const R (&o)[4]) {
+  if (vec4 && p0 + 3 < n) {
+    if constexpr (sizeof(R) == sizeof(float)) {
+      *reinterpret_cast<float4*>(f + p0) = make_float4(o[0], o[1], o[2], o[3]);
+    } else {
+      *reinterpret_cast<double2*>(f + p0) = make_double2(o[0], o[1]);
+      *reinterpret_cast<double2*>(f + p0 + 2) = make_double2(o[2], o[3]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (p0 + i < n) f[p0 + i] = o[i];
+  }
+}
+
+// Reference-storage multiplicities (ref_multiplicity) of points p0 .. p0+3.
+__device__ __forceinline__ void ref_weights4(long p0, int s, int dim, double (&w)[4]) {
+  const unsigned us = (unsigned)s;
+  unsigned p = (unsigned)p0;
+  unsigned k = p % us, q = p / us;
+  unsigned j = q % us, i = q / us;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    w[t] = (k == 0 ? 2.0 : 1.0) * (j == 0 ? 2.0 : 1.0) * ((dim == 3 && i == 0) ? 2.0 : 1.0);
+    if (++k == us) {
+      k = 0;
+      if (++j == us) { j = 0; ++i; }
+    }
+  }
+}
+
+// Sums of the mu candidates over one segment (N(mu_c) and dN/dmu at
+// candidate 0), given the lane's 4 potentials.
+template <typename R>
+__device__ __forceinline__ void mu_segment(const DensParams& d, const double* cmu, int nc, double cmax,
+                                           const R (&v4)[4], const R* Ls, const R* Gs, long p0, long n, int vec4,
+                                           double (&acc)[kMuAcc]) {
+  R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
+  if (Ls) load4(Ls, p0, n, vec4, l4);
+  if (Gs) load4(Gs, p0, n, vec4, g4);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double v = (double)v4[i];
+    if (p0 + i >= n || (d.cut && !(cmax - v > 0.0))) continue;
+    const double l = (double)l4[i], g = (double)g4[i];
+    acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
+#pragma unroll
+    for (int c = 0; c < kMuCand; ++c) {
+      if (c >= nc) break;
+      acc[c] += density_at_d(d, cmu[c] - v, l, g);
+    }
+  }
+}
+
+// Sum of nb per-block partials (at base + b * stride) on one warp, several
+// loads in flight per lane.
+__device__ __forceinline__ double warp_sum_rows(const double* base, int nb, int stride) {
+  const int lane = threadIdx.x & 31;
+  double t = 0.0;
+#pragma unroll 4
+  for (int b = lane; b < nb; b += 32) t += __ldcg(base + (long)b * stride);
+  return warp_sum(t);
+}
+
+// Block-wide sums of two ints, returned to every thread.
+__device__ __forceinline__ void block_sum2(int& x, int& y) {
+  __shared__ int sh[2][kStepWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  x = __reduce_add_sync(0xffffffffu, x);
+  y = __reduce_add_sync(0xffffffffu, y);
+  __syncthreads();
+  if (lane == 0) { sh[0][w] = x; sh[1][w] = y; }
+  __syncthreads();
+  x = 0;
+  y = 0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { x += sh[0][i]; y += sh[1][i]; }
+}
+
+// ------------------------------------------------------------ the kernel --
+// mode 0: one SC iteration.  mode 1: GetDensities of the current V (mu
+// search + n[V]), written into the current ring slot; used for the initial
+// densities (mpDPFT.cpp:195) and the standalone mu-search entry point.
+// mode 2: AdmixDensities only, V holding the output densities.
+template <typename R>
+__global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a) {
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long nthreads = (long)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long gw = (long)blockIdx.x * kStepWarps + wib;
+  const long nw = (long)gridDim.x * kStepWarps;
+  const long nseg = kp.nseg;
+  const long seg_step = (nw % nseg) * kp.seg_mul % nseg;
+  const long seg_first = (gw % nseg) * kp.seg_mul % nseg;
+  __shared__ double red[kNPart];
+  __shared__ double s_mu[kMaxS];      // mu of the final density
+  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
+  __shared__ int s_flag;
+  __shared__ MuState s_ms[kMaxS];
+  __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP];
+  __shared__ double s_prm[kMaxP], s_prr[kMaxP], s_pcol[kMaxP];
+  __shared__ int s_colof[kMaxP];
+  __shared__ int s_ok;
+  __shared__ double s_grow[kMaxP];
+  // active-segment lists as this block sees them (identical in every block)
+  __shared__ int s_wcnt[kMaxS][kStepWarps];
+  __shared__ int s_full[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
+  __shared__ double s_fcap[kMaxS], s_lcap[kMaxS];
+
+  if (a.mode != 1 && ldcg(&st->exit_loop)) return;
+  // block 0 runs the scalar SC logic on a shared-memory copy of the state
+  // and writes it back before every grid barrier after which other blocks
+  // read the state
+  __shared__ ScState s_st;
+  ScState* const ls = &s_st;
+  if (blockIdx.x == 0) {
+    state_load(ls, st);
+    __syncthreads();
+  }
+  const int cur = ldcg(&st->slot);
+  const int ring = kp.ring;
+  const int next = (cur + 1) % ring;
+  double* mypart = a.part + (long)blockIdx.x * kNPart;
+  MPDPFT_TSTAMP(0);
+
+  // ---- phase A: UpdateV (mpDPFT.cpp:4815-4838) --------------------------
+  if (a.mode == 0 && a.assemble_v) {
+    const double incv = ldcg(&st->inc_v);
+    const double fac = incv < 1.0 ? incv : 1.0;
+    double acc[kMaxS];
+    for (int s = 0; s < kMaxS; ++s) acc[s] = 0.0;
+    const R* nin = a.nin + (long)cur * S * n;
+    for (long p = tid; p < n; p += nthreads) {
+      for (int s = 0; s < S; ++s) {
+        R vi = R(0);
+        if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[(long)s * n + p];  // type 10 (:2261)
+        if (kp.contact_mutual) {                                              // type 1 (:2247)
+          R t = R(0);
+          for (int q = 0; q < S; ++q)
+            if (q != s) t += nin[(long)q * n + p];
+          vi += R(kp.beta) * t;
+        }
+        if (kp.dirac) {  // type 11 (:2768): -gammaH 2 (D n+/pi)^{1/D}/(D-1)
+          R ns = nin[(long)s * n + p];
+          ns = ns > R(0) ? ns : R(0);
+          if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+          else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+        }
+        if (a.vh) vi += a.vh[(long)s * n + p];
+        R vnew = a.vext[(long)s * n + p] + R(fac) * vi;
+        R vold = a.V[(long)s * n + p];
+        double d = (double)vnew - (double)vold;
+        acc[s] += d * d;
+        a.V[(long)s * n + p] = vnew;
+      }
+    }
+    block_reduce_store<kMaxS>(acc, mypart + kVresOff);
+  }
+
+  // ---- phase B: mu search (GetDensities + EnforceConstraints) ----------
+  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
+  if (threadIdx.x == 0) {  // every block derives the pass-0 candidates itself
+    double dmm = ldcg(&st->dmm);
+    double pn = 0.0;
+    for (int s = 0; s < S; ++s) { double pm = ldcg(&st->mu[s]); pn += pm * pm; }
+    for (int s = 0; s < S; ++s) {
+      double mu = ldcg(&st->mu[s]);
+      double pa = sqrt(pn) < 1.0e-12 ? 1.0e-12 : fabs(mu);
+      mu_begin(s_ms[s], mu, pa, dmm, active);
+    }
+  }
+  if (threadIdx.x < kMaxS) {
+    s_full[threadIdx.x] = 0;
+    s_lok[threadIdx.x] = 0;
+    s_llen[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) { ls->ms[s] = s_ms[s]; ls->prev_mu[s] = s_ms[s].start; }
+    ls->mu_passes = 0;
+    ls->iter_bits = 0;
+  }
+  // V written above is read at other points below
+  if (a.mode == 0 && a.assemble_v && !grid_barrier(st)) return;
+
+  const R* V = a.V;
+  MPDPFT_TSTAMP(1);
+  for (int pass = 0; pass < kMuMaxPasses && a.mode != 2; ++pass) {
+    if (pass > 0 && threadIdx.x < S) {
+      const int s = threadIdx.x;
+      s_ms[s].done = ldcg(&st->ms[s].done);
+      s_ms[s].ncand = ldcg(&st->ms[s].ncand);
+      for (int c = 0; c < s_ms[s].ncand; ++c) s_ms[s].cand[c] = ldcg(&st->ms[s].cand[c]);
+    }
+    __syncthreads();
+    int any = 0;
+    for (int s = 0; s < S; ++s) any |= !s_ms[s].done;
+    if (!any) break;
+    for (int s = 0; s < S; ++s) {
+      if (s_ms[s].done) continue;
+      // N(mu) and dN/dmu are evaluated in double from the stored fields
+      // (FP32 in mixed mode): the particle-number integral and the mu search
+      // are FP64 in both modes
+      double acc[kMuAcc];
+#pragma unroll
+      for (int c = 0; c < kMuAcc; ++c) acc[c] = 0.0;
+      const DensParams d = kp.dens[s];
+      const int nc = s_ms[s].ncand;
+      const double* cmu = s_ms[s].cand;  // shared memory (broadcast reads)
+      double cmax = cmu[0];
+      for (int c = 1; c < nc; ++c) cmax = fmax(cmax, cmu[c]);
+      const R* Vs = V + (long)s * n;
+      const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
+      const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
+      if (d.cut && s_lok[s] && cmax <= s_lcap[s]) {
+        const int len = s_llen[s];
+        for (long j = gw; j < len; j += nw) {
+          const long p0 = (long)__ldcg(a.slist + (long)s * nseg + j) * kSegPts + 4 * lane;
+          R v4[4];
+          load4(Vs, p0, n, kp.vec4, v4);
+          mu_segment(d, cmu, nc, cmax, v4, Ls, Gs, p0, n, kp.vec4, acc);
+        }
+      } else {
+        int cnt = 0;
+        int* wl = a.wlist + ((long)s * nw + gw) * a.wmax;
+        long seg = seg_first;
+        for (long k = gw; k < nseg; k += nw) {
+          const long p0 = seg * kSegPts + 4 * lane;
+          R v4[4];
+          load4(Vs, p0, n, kp.vec4, v4);
+          bool act = true;
+          if (d.cut) {
+            bool mine = false;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (cmax - (double)v4[i] > 0.0);
+            act = __any_sync(0xffffffffu, mine);
+          }
+          if (act) {
+            mu_segment(d, cmu, nc, cmax, v4, Ls, Gs, p0, n, kp.vec4, acc);
+            if (d.cut) {
+              if (lane == 0) wl[cnt] = (int)seg;
+              ++cnt;
+            }
+          }
+          seg += seg_step;
+          if (seg >= nseg) seg -= nseg;
+        }
+        if (d.cut) {
+          if (lane == 0) s_wcnt[s][wib] = cnt;
+          if (threadIdx.x == 0) { s_full[s] = 1; s_fcap[s] = cmax; }
+        }
+      }
+      block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
+    }
+    __syncthreads();
+    if (threadIdx.x < S && s_full[threadIdx.x]) {
+      int c = 0;
+      for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
+      a.bcount[(long)threadIdx.x * gridDim.x + blockIdx.x] = c;
+    }
+    if (!grid_barrier(st)) return;
+    // compact the lists of the full sweeps: block order, then warp order
+    for (int s = 0; s < S; ++s) {
+      if (!s_full[s]) continue;
+      int before = 0, total = 0;
+      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        const int c = __ldcg(a.bcount + (long)s * gridDim.x + b);
+        total += c;
+        if (b < (int)blockIdx.x) before += c;
+      }
+      block_sum2(before, total);
+      int off = before;
+      for (int w = 0; w < wib; ++w) off += s_wcnt[s][w];
+      const int* wl = a.wlist + ((long)s * nw + gw) * a.wmax;
+      for (int i = lane; i < s_wcnt[s][wib]; i += 32) a.slist[(long)s * nseg + off + i] = __ldcg(wl + i);
+      if (threadIdx.x == 0) s_llen[s] = total;
+    }
+    __syncthreads();
+    if (threadIdx.x < S && s_full[threadIdx.x]) {
+      s_lok[threadIdx.x] = 1;
+      s_lcap[threadIdx.x] = s_fcap[threadIdx.x];
+      s_full[threadIdx.x] = 0;
+    }
+    if (blockIdx.x == 0) {
+      for (int v = wib; v < S * kMuAcc; v += kStepWarps) {
+        const double t = warp_sum_rows(a.part + v, gridDim.x, kNPart);
+        if (lane == 0) red[v] = t;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double dmm = ls->dmm;
+        int bits = 0;
+        for (int s = 0; s < S; ++s) {
+          if (s_ms[s].done) continue;
+          MuState& ms = ls->ms[s];
+          double N[kMuCand];
+          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuAcc + c] * kp.geom.dvol;
+          mu_decide(ms, N, red[s * kMuAcc + kMuCand] * kp.geom.dvol, kp.abundance[s], kp.rel_acc, dmm, bits);
+        }
+        ls->dmm = dmm;
+        ls->iter_bits |= bits;
+        ls->mu_passes++;
+      }
+      __syncthreads();
+      state_store(st, ls);
+    }
+    if (!grid_barrier(st)) return;
+  }
+
+  MPDPFT_TSTAMP(2);
+  // ---- phase C: final densities, residual, CC dots, Gram row -----------
+  if (threadIdx.x < S) {
+    const int s = threadIdx.x;
+    s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
+    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
+  }
+  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
+  __syncthreads();
+  const int pulay_now = s_flag;
+  const int hist = ldcg(&st->hist);
+  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
+  {
+    // per species: [0] N, [1] <n_out, n_in>_w, [2] <n_out, n_out>_w,
+    // [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram row, summed over
+    // species in phase D); w = multiplicity in the reference storage
+    __shared__ long s_roff[kMaxP];
+    if (threadIdx.x < I) {
+      const int j = threadIdx.x;
+      s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
+    }
+    __syncthreads();
+    R* nin = a.nin + (long)cur * S * n;
+    R* rcur = a.res + (long)cur * S * n;
+    for (int s = 0; s < S; ++s) {
+      double acc[kNF];
+#pragma unroll
+      for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
+      const DensParams d = kp.dens[s];
+      const double mus = s_mu[s];
+      const long so = (long)s * n;
+      const R* Ls = a.lap ? a.lap + so : nullptr;
+      const R* Gs = a.g2 ? a.g2 + so : nullptr;
+      long seg = seg_first;
+      for (long k = gw; k < nseg; k += nw) {
+        const long p0 = seg * kSegPts + 4 * lane;
+        seg += seg_step;
+        if (seg >= nseg) seg -= nseg;
+        R v4[4];
+        load4(V + so, p0, n, kp.vec4, v4);
+        double nod[4];
+        if (a.mode == 2) {  // admix only: V holds the output densities
+#pragma unroll
+          for (int i = 0; i < 4; ++i) nod[i] = (double)v4[i];
+        } else {
+          bool mine = !d.cut;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (mus - (double)v4[i] > 0.0);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) nod[i] = 0.0;
+          if (__any_sync(0xffffffffu, mine)) {
+            R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
+            if (Ls) load4(Ls, p0, n, kp.vec4, l4);
+            if (Gs) load4(Gs, p0, n, kp.vec4, g4);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (p0 + i < n) nod[i] = density_at_d(d, mus - (double)v4[i], (double)l4[i], (double)g4[i]);
+          }
+        }
+        if (p0 >= n) continue;
+        R no4[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          no4[i] = R(nod[i]);
+          acc[0] += nod[i];  // zero beyond n
+        }
+        if (a.mode == 1) {
+          store4(nin + so, p0, n, kp.vec4, no4);
+          continue;
+        }
+        R ni4[4], r4[4];
+        load4(nin + so, p0, n, kp.vec4, ni4);
+        double w4[4], wr4[4], dr4[4];
+        ref_weights4(p0, kp.geom.s, kp.geom.dim, w4);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          r4[i] = no4[i] - ni4[i];
+          const double w = (p0 + i < n) ? w4[i] : 0.0;
+          const double dno = (double)no4[i], dni = (double)ni4[i];
+          dr4[i] = (double)r4[i];
+          wr4[i] = w * dr4[i];
+          acc[1] += w * dno * dni;
+          acc[2] += w * dno * dno;
+          acc[3] += w * dni * dni;
+        }
+        store4(rcur + so, p0, n, kp.vec4, r4);
+#pragma unroll
+        for (int j = 0; j < kMaxP; ++j) {
+          if (j < I - 1) {
+            R rj4[4];
+            load4(a.res + s_roff[j] + so, p0, n, kp.vec4, rj4);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * (double)rj4[i];
+          } else if (j == I - 1) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * dr4[i];
+          }
+        }
+      }
+      block_reduce_store<kNF>(acc, mypart + s * kNF);
+    }
+  }
+  if (!grid_barrier(st)) return;
+
+  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
+  MPDPFT_TSTAMP(3);
+  if (blockIdx.x == 0) {
+    __shared__ double red_v[kMaxS];
+    const int nv = 4 + I;  // per species: N, three dots, Gram row
+    const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
+    for (int v = wib; v < S * nv + vres; v += kStepWarps) {
+      double t;
+      if (v < S * nv) t = warp_sum_rows(a.part + (v / nv) * kNF + (v % nv), gridDim.x, kNPart);
+      else if (a.assemble_v) t = warp_sum_rows(a.part + kVresOff + (v - S * nv), gridDim.x, kNPart);
+      else t = warp_sum_rows(a.vres_part + (v - S * nv), a.vres_blocks, kMaxS);
+      if (lane == 0) {
+        if (v < S * nv) red[(v / nv) * kNF + (v % nv)] = t;
+        else red_v[v - S * nv] = t;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < I) {  // Gram row summed over species
+      double t = 0.0;
+      for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
+      s_grow[threadIdx.x] = t;
+    }
+    __syncthreads();
+    // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): the Gram matrix,
+    // last row/column new, the rest shifted from before (warp 1) ...
+    if (pulay_now && wib == 1) {
+      const int shift = (hist + 1 > kp.scope) ? 1 : 0;
+      for (int e = lane; e < I * I; e += 32) {
+        const int i = e / I, j = e % I;
+        double v;
+        if (i == I - 1) v = s_grow[j];
+        else if (j == I - 1) v = s_grow[i];
+        else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
+        s_G[e] = v;
+      }
+      __syncwarp();
+      for (int e = lane; e < I * I; e += 32) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
+      if (lane == 0) ls->hist = I;
+    }
+    // ... while thread 0 does the scalar bookkeeping
+    if (threadIdx.x == 0) {
+      if (vres) {
+        double w = 0.0;
+        for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red_v[s] / (double)n));
+        ls->v_res = w;
+      }
+      const int sc = ls->sc_count;
+      double tot = 0.0;
+      for (int s = 0; s < S; ++s) {
+        ls->mu[s] = s_mu_rep[s];
+        ls->ab[s] = red[s * kNF] * kp.geom.dvol;
+        if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
+        tot += ls->ab[s];
+      }
+      if (a.mode == 1) {
+        ls->status_bits |= ls->iter_bits;
+        ls->mu_passes_total += ls->mu_passes;
+      } else {
+        // CheckConvergence (mpDPFT.cpp:4759-4782)
+        const double mp = 100.0 * 1.0e-16;
+        if (sc > 0) {
+          double cc = 0.0, maxtest = 0.0;
+          for (int s = 0; s < S; ++s) {
+            double oi = red[s * kNF + 1], oo = red[s * kNF + 2], ii = red[s * kNF + 3];
+            double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
+            double t = rd * ls->ab[s] / tot;
+            if (t > maxtest) { maxtest = t; cc = maxtest; }
+          }
+          ls->cc = cc;
+          double dab = 0.0, dmu = 0.0;
+          for (int s = 0; s < S; ++s) {
+            dab += (ls->ab[s] - ls->old_ab[s]) * (ls->ab[s] - ls->old_ab[s]);
+            dmu += (ls->mu[s] - ls->old_mu[s]) * (ls->mu[s] - ls->old_mu[s]);
+          }
+          int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
+          double avth = 0.0;
+          for (int s = 0; s < S; ++s) avth += ls->theta[s] / (double)S;
+          bool vok = !(kp.pot_tol > 0.0) || ls->v_res <= kp.pot_tol;
+          if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
+              (cc < kp.sc_criterion || steady) && vok)
+            ls->exit_count++;
+          else
+            ls->exit_count = 0;
+          if (ls->exit_count >= 3) ls->exit_loop = 1;
+        } else {
+          ls->cc = 1.2345678901234567890;
+        }
+        if (sc == kp.max_sc) ls->exit_loop = 1;  // Intercept (:4866)
+      }
+    }
+    __syncthreads();
+    // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
+    // reference, mpDPFT.cpp:5089-5107)
+    if (a.mode != 1 && pulay_now && wib == 0) {
+      bool ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
+      double test = ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
+      if (lane == 0) s_ok = ok && test <= 1.0e-8;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int sc = ls->sc_count;
+      if (a.mode != 1) {
+        int used = 0;
+        if (pulay_now) {
+          if (s_ok) {
+            double x[kMaxP], A = 0.0;
+            for (int i = 0; i < I; ++i) {
+              x[i] = 0.0;
+              for (int k = 0; k < I; ++k) x[i] += s_inv[i * I + k];
+              A += x[i];
+            }
+            for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
+            used = 1;
+          }
+          if (!used) ls->iter_bits |= kBitPulay;
+        }
+        ls->pulay_used = used;
+        ls->ncoeff = used ? I : 0;
+        for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
+        // InjectSchedule (mpDPFT.cpp:5229-5315)
+        if (kp.schedule == 5) {
+          for (int s = 0; s < S; ++s) {
+            double th = ls->theta[s] * (ls->cc < ls->old_cc ? 1.1 : 0.5);
+            th = fmin(0.8, th);
+            th = fmax(10.0 / (double)kp.max_sc, th);
+            ls->theta[s] = th;
+          }
+        } else if (kp.schedule == 9) {
+          for (int s = 0; s < S; ++s)
+            if (ls->theta[s] < 0.2)
+              ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
+        }
+        if (a.log && sc < a.log_cap) {
+          mpdpft_iter_log& L = a.log[sc];
+          L.sc_count = sc;
+          L.mu_trials = ls->mu_passes;
+          L.pulay_used = used;
+          L.status_bits = ls->iter_bits;
+          L.cc = ls->cc;
+          L.v_residual = ls->v_res;
+          for (int s = 0; s < kMaxS; ++s) {
+            L.mu[s] = s < S ? ls->mu[s] : 0.0;
+            L.abundance[s] = s < S ? ls->ab[s] : 0.0;
+            L.theta[s] = s < S ? ls->theta_mix[s] : 0.0;
+          }
+          L.ms = 0.0;
+        }
+        ls->status_bits |= ls->iter_bits;
+        ls->mu_passes_total += ls->mu_passes;
+        // StoreCurrentIteration of the next iteration; PrepareNextIteration
+        for (int s = 0; s < S; ++s) { ls->old_mu[s] = ls->mu[s]; ls->old_ab[s] = ls->ab[s]; }
+        ls->old_cc = ls->cc;
+        if (sc > 0) ls->inc_v = fmin(1.0, ls->inc_v + kp.inc_v0);  // (:4833)
+        ls->mix_src = cur;
+        ls->slot = next;
+        ls->sc_count = sc + 1;
+      }
+    }
+    __syncthreads();
+    state_store(st, ls);
+  }
+  if (a.mode == 1) return;
+  MPDPFT_TSTAMP(4);
+  if (!grid_barrier(st)) return;
+  MPDPFT_TSTAMP(5);
+
+  // ---- phase E: mixed density -> ring[next] ----------------------------
+  // n = sum_j c_j (n_in,j + theta r_j) (Pulay) or n_in + theta r (linear),
+  // AdmixDensities mpDPFT.cpp:4946-4955 / :4987
+  {
+    __shared__ long s_off[kMaxP];
+    __shared__ double s_c[kMaxP];
+    __shared__ int s_nc;
+    if (threadIdx.x == 0) {
+      const int used = ldcg(&st->pulay_used);
+      const int nc = used ? ldcg(&st->ncoeff) : 1;
+      s_nc = nc;
+      for (int j = 0; j < nc; ++j) {
+        const int slot = (cur - (nc - 1) + j + ring) % ring;
+        s_off[j] = (long)slot * S * n;
+        s_c[j] = used ? ldcg(&st->coeff[j]) : 1.0;
+      }
+    }
+    __syncthreads();
+    const int nc = s_nc;
+    for (int s = 0; s < S; ++s) {
+      const double th = ldcg(&st->theta_mix[s]);
+      R* out = a.nin + (long)next * S * n + (long)s * n;
+      if (kp.vec4) {
+        const long n4 = n >> 2;
+        for (long p4 = tid; p4 < n4; p4 += nthreads) {
+          const long p0 = 4 * p4;
+          double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+          for (int j = 0; j < nc; ++j) {
+            const long q = s_off[j] + (long)s * n;
+            R ni[4], ri[4];
+            load4(a.nin + q, p0, n, 1, ni);
+            load4(a.res + q, p0, n, 1, ri);
+            const double c = s_c[j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) v[i] += c * ((double)ni[i] + th * (double)ri[i]);
+          }
+          R o[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) o[i] = R(v[i]);
+          store4(out, p0, n, 1, o);
+        }
+      } else {
+        for (long p = tid; p < n; p += nthreads) {
+          double v = 0.0;
+          for (int j = 0; j < nc; ++j) {
+            const long q = s_off[j] + (long)s * n + p;
+            v += s_c[j] * ((double)__ldcg(a.nin + q) + th * (double)__ldcg(a.res + q));
+          }
+          out[p] = R(v);
+        }
+      }
+    }
+  }
+  MPDPFT_TSTAMP(6);
+}
+
+}  // namespace mpdpft

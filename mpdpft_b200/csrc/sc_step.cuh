@@ -18,9 +18,14 @@
 namespace mpdpft {
 
 constexpr int kStepThreads = 512;
+constexpr int kStepWarps = kStepThreads / 32;
+constexpr int kSegPts = 128;          // points of one warp segment (4 per lane)
 constexpr int kMuAcc = kMuCand + 1;  // candidate sums + dN/dmu at candidate 0
 constexpr int kNF = 4 + kMaxP;        // per-species sums of the density/Gram pass
-constexpr int kNPart = kMaxS * kNF > kMaxS * kMuAcc ? kMaxS * kNF : kMaxS * kMuAcc;
+// per-block partial sums: [0, kVresOff) the mu-pass or density-pass sums,
+// [kVresOff, kVresOff + kMaxS) |V_new - V_old|^2 of the in-kernel V update
+constexpr int kVresOff = kMaxS * kNF > kMaxS * kMuAcc ? kMaxS * kNF : kMaxS * kMuAcc;
+constexpr int kNPart = kVresOff + kMaxS;
 constexpr long kBarrierSpinLimit = 20000000;  // ~ seconds with nanosleep backoff
 
 // Constant parameters of one solve (kernel argument, by value).
@@ -40,6 +45,13 @@ struct KParams {
   int schedule;
   double pot_tol;
   double inc_v0;
+  // Grid sweeps visit warp segments of kSegPts consecutive points in the
+  // order seg = k * seg_mul mod nseg (seg_mul coprime to nseg), which spreads
+  // the few costly segments (inside the classically allowed region) evenly
+  // over the warps.
+  long nseg;
+  long seg_mul;
+  int vec4;  // n % 4 == 0: a lane loads its 4 points as one vector
 };
 
 struct MuState {
@@ -91,6 +103,14 @@ struct StepArgs {
   R* nin;         // [ring][S][n]
   R* res;         // [ring][S][n]
   double* part;   // [gridDim.x][kNPart]
+  // active-segment lists of the mu search (functionals that vanish for
+  // mu <= V): a full sweep records the segments holding any point below the
+  // pass's largest candidate; later passes whose candidates stay below that
+  // visit only those
+  int* bcount;  // [kMaxS][gridDim.x] active segments found by each block
+  int* wlist;   // [kMaxS][warps][wmax] their indices, per warp
+  int* slist;   // [kMaxS][nseg] compacted list (block order, then warp order)
+  int wmax;     // ceil(nseg / warps)
   const double* vres_part;  // partials of |V_new - V_old|^2 from an external
   int vres_blocks;          //   V assembly (when assemble_v == 0), or null
   mpdpft_iter_log* log;
@@ -321,535 +341,6 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
   if (est - e > m.lo) m.cand[m.ncand++] = est - e;
   if (est + e < m.hi) m.cand[m.ncand++] = est + e;
   if (m.pass > 3) m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
-}
-
-// ---------------------------------------------------------- small solve --
-// Inverse of the Pulay Gram matrix by Gauss-Jordan elimination with full
-// pivoting; rank test as Eigen's FullPivHouseholderQR::isInvertible
-// (threshold eps * n * max|pivot|), which the reference uses (mpDPFT.cpp:5089).
-// One warp, matrices in shared memory; pivots are the first maximum in
-// row-major order, as in a serial scan.
-// G is n x n (row-major, stride n); inv receives the inverse.  Returns the
-// rank-test result on every lane.
-__device__ inline bool warp_inverse(int n, const double* G, double* M, double* inv, double* fac, int* colperm) {
-  const int lane = threadIdx.x & 31;
-  for (int i = lane; i < n * n; i += 32) { M[i] = G[i]; inv[i] = 0.0; }
-  __syncwarp();
-  for (int i = lane; i < n; i += 32) { inv[i * n + i] = 1.0; colperm[i] = i; }
-  __syncwarp();
-  double maxpiv = 0.0, minpiv = 1e300;
-  for (int c = 0; c < n; ++c) {
-    const int w = n - c;
-    double best = -1.0;
-    int bidx = c * n + c;
-    for (int e = lane; e < w * w; e += 32) {
-      const int i = c + e / w, j = c + e % w;
-      const double v = fabs(M[i * n + j]);
-      if (v > best) { best = v; bidx = i * n + j; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
-      if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
-    }
-    const int pr = bidx / n, pc = bidx % n;
-    if (pr != c)
-      for (int j = lane; j < n; j += 32) {
-        double t = M[pr * n + j]; M[pr * n + j] = M[c * n + j]; M[c * n + j] = t;
-        t = inv[pr * n + j]; inv[pr * n + j] = inv[c * n + j]; inv[c * n + j] = t;
-      }
-    __syncwarp();
-    if (pc != c) {
-      for (int i = lane; i < n; i += 32) { double t = M[i * n + pc]; M[i * n + pc] = M[i * n + c]; M[i * n + c] = t; }
-      if (lane == 0) { int t = colperm[pc]; colperm[pc] = colperm[c]; colperm[c] = t; }
-    }
-    __syncwarp();
-    const double piv = M[c * n + c];
-    maxpiv = fmax(maxpiv, fabs(piv));
-    minpiv = fmin(minpiv, fabs(piv));
-    if (piv == 0.0) return false;
-    const double ip = 1.0 / piv;
-    __syncwarp();
-    for (int j = lane; j < n; j += 32) { M[c * n + j] *= ip; inv[c * n + j] *= ip; }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) fac[i] = M[i * n + c];
-    __syncwarp();
-    for (int e = lane; e < n * n; e += 32) {
-      const int i = e / n, j = e % n;
-      if (i == c) continue;
-      const double f = fac[i];
-      if (f == 0.0) continue;
-      M[i * n + j] -= f * M[c * n + j];
-      inv[i * n + j] -= f * inv[c * n + j];
-    }
-    __syncwarp();
-  }
-  if (minpiv <= 2.220446049250313e-16 * (double)n * maxpiv) return false;
-  // undo the column permutation: row c of the result goes to row colperm[c]
-  for (int e = lane; e < n * n; e += 32) M[e] = inv[e];
-  __syncwarp();
-  for (int e = lane; e < n * n; e += 32) {
-    const int c = e / n, j = e % n;
-    inv[colperm[c] * n + j] = M[e];
-  }
-  __syncwarp();
-  return true;
-}
-
-// Reduce kNPart partials over blocks into red[] (block 0 only).
-__device__ inline void reduce_partials(const double* part, int nblocks, int nvals, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j = warp; j < nvals; j += nw) {
-    double t = 0.0;
-    for (int b = lane; b < nblocks; b += 32) t += __ldcg(part + (long)b * kNPart + j);
-    t = warp_sum(t);
-    if (lane == 0) red[j] = t;
-  }
-  __syncthreads();
-}
-
-// ------------------------------------------------------------ the kernel --
-// mode 0: one SC iteration.  mode 1: GetDensities of the current V (mu
-// search + n[V]), written into the current ring slot; used for the initial
-// densities (mpDPFT.cpp:195) and the standalone mu-search entry point.
-template <typename R>
-__global__ void __launch_bounds__(kStepThreads, 2) sc_step_kernel(StepArgs<R> a) {
-  const KParams& kp = a.kp;
-  ScState* st = a.st;
-  const long n = kp.geom.n;
-  const int S = kp.S;
-  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long nthreads = (long)gridDim.x * blockDim.x;
-  __shared__ double red[kNPart];
-  __shared__ double s_mu[kMaxS];      // mu of the final density
-  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
-  __shared__ int s_flag;
-  __shared__ MuState s_ms[kMaxS];
-  __shared__ double s_G[kMaxP * kMaxP], s_M[kMaxP * kMaxP], s_inv[kMaxP * kMaxP], s_fac[kMaxP];
-  __shared__ int s_perm[kMaxP];
-  __shared__ int s_ok;
-  __shared__ double s_grow[kMaxP];
-
-  if (a.mode != 1 && ldcg(&st->exit_loop)) return;
-  // block 0 runs the scalar SC logic on a shared-memory copy of the state
-  // (global round trips would serialise it); it writes the copy back before
-  // every grid barrier after which other blocks read the state
-  __shared__ ScState s_st;
-  ScState* const ls = &s_st;
-  if (blockIdx.x == 0) {
-    state_load(ls, st);
-    __syncthreads();
-  }
-  const int cur = ldcg(&st->slot);
-  const int ring = kp.ring;
-  const int next = (cur + 1) % ring;
-  double* mypart = a.part + (long)blockIdx.x * kNPart;
-  MPDPFT_TSTAMP(0);
-
-  // ---- phase A: UpdateV (mpDPFT.cpp:4815-4838) --------------------------
-  if (a.mode == 0 && a.assemble_v) {
-    const double incv = ldcg(&st->inc_v);
-    const double fac = incv < 1.0 ? incv : 1.0;
-    double acc[kMaxS];
-    for (int s = 0; s < kMaxS; ++s) acc[s] = 0.0;
-    const R* nin = a.nin + (long)cur * S * n;
-    for (long p = tid; p < n; p += nthreads) {
-      for (int s = 0; s < S; ++s) {
-        R vi = R(0);
-        if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];  // type 10 (:2261)
-        if (kp.contact_mutual) {                                  // type 1 (:2247)
-          R t = R(0);
-          for (int q = 0; q < S; ++q)
-            if (q != s) t += nin[(long)q * n + p];
-          vi += R(kp.beta) * t;
-        }
-        if (kp.dirac) {  // type 11 (:2768): -gammaH 2 (D n+/pi)^{1/D}/(D-1)
-          R ns = nin[(long)s * n + p];
-          ns = ns > R(0) ? ns : R(0);
-          if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
-          else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
-        }
-        if (a.vh) vi += a.vh[(long)s * n + p];
-        R vnew = a.vext[(long)s * n + p] + R(fac) * vi;
-        R vold = a.V[(long)s * n + p];
-        double d = (double)vnew - (double)vold;
-        acc[s] += d * d;
-        a.V[(long)s * n + p] = vnew;
-      }
-    }
-    block_reduce_store<kMaxS>(acc, mypart);
-  }
-
-  // ---- phase B: mu search (GetDensities + EnforceConstraints) ----------
-  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
-  if (threadIdx.x == 0) {  // every block derives the pass-0 candidates itself
-    double dmm = ldcg(&st->dmm);
-    double pn = 0.0;
-    for (int s = 0; s < S; ++s) { double pm = ldcg(&st->mu[s]); pn += pm * pm; }
-    for (int s = 0; s < S; ++s) {
-      double mu = ldcg(&st->mu[s]);
-      double pa = sqrt(pn) < 1.0e-12 ? 1.0e-12 : fabs(mu);
-      mu_begin(s_ms[s], mu, pa, dmm, active);
-    }
-  }
-  __syncthreads();
-  if (!grid_barrier(st)) return;
-  if (blockIdx.x == 0) {
-    if (a.mode == 0 && (a.assemble_v || a.vres_part)) {
-      const double* vp = a.assemble_v ? a.part : a.vres_part;
-      const int nb = a.assemble_v ? (int)gridDim.x : a.vres_blocks;
-      const int stride = a.assemble_v ? kNPart : kMaxS;
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      if (warp < S) {
-        double t = 0.0;
-        for (int b = lane; b < nb; b += 32) t += __ldcg(vp + (long)b * stride + warp);
-        t = warp_sum(t);
-        if (lane == 0) red[warp] = t;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double w = 0.0;
-        for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red[s] / (double)n));
-        ls->v_res = w;
-      }
-    }
-    if (threadIdx.x == 0) {
-      for (int s = 0; s < S; ++s) { ls->ms[s] = s_ms[s]; ls->prev_mu[s] = s_ms[s].start; }
-      ls->mu_passes = 0;
-      ls->iter_bits = 0;
-    }
-    __syncthreads();
-    state_store(st, ls);
-  }
-  if (!grid_barrier(st)) return;
-
-  const R* V = a.V;
-  MPDPFT_TSTAMP(1);
-  for (int pass = 0; pass < kMuMaxPasses && a.mode != 2; ++pass) {
-    if (pass > 0 && threadIdx.x < S) {
-      const int s = threadIdx.x;
-      s_ms[s].done = ldcg(&st->ms[s].done);
-      s_ms[s].ncand = ldcg(&st->ms[s].ncand);
-      for (int c = 0; c < s_ms[s].ncand; ++c) s_ms[s].cand[c] = ldcg(&st->ms[s].cand[c]);
-    }
-    __syncthreads();
-    int any = 0;
-    for (int s = 0; s < S; ++s) any |= !s_ms[s].done;
-    if (!any) break;
-    for (int s = 0; s < S; ++s) {
-      if (s_ms[s].done) continue;
-      // N(mu) and dN/dmu are evaluated in double from the stored fields
-      // (FP32 in mixed mode): the particle-number integral and the mu search
-      // are FP64 in both modes
-      double acc[kMuAcc];
-#pragma unroll
-      for (int c = 0; c < kMuAcc; ++c) acc[c] = 0.0;
-      const DensParams d = kp.dens[s];
-      const int nc = s_ms[s].ncand;
-      const double* cmu = s_ms[s].cand;  // shared memory (broadcast reads)
-      const R* Vs = V + (long)s * n;
-      const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
-      const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
-      for (long p = tid; p < n; p += nthreads) {
-        const double v = (double)Vs[p];
-        const double l = Ls ? (double)Ls[p] : 0.0;
-        const double g = Gs ? (double)Gs[p] : 0.0;
-        acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
-#pragma unroll
-        for (int c = 0; c < kMuCand; ++c)
-          if (c < nc) acc[c] += density_at_d(d, cmu[c] - v, l, g);
-      }
-      block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
-    }
-    if (!grid_barrier(st)) return;
-    if (blockIdx.x == 0) {
-      reduce_partials(a.part, gridDim.x, S * kMuAcc, red);
-      if (threadIdx.x == 0) {
-        double dmm = ls->dmm;
-        int bits = 0;
-        for (int s = 0; s < S; ++s) {
-          if (s_ms[s].done) continue;
-          MuState ms = ls->ms[s];
-          double N[kMuCand];
-          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuAcc + c] * kp.geom.dvol;
-          mu_decide(ms, N, red[s * kMuAcc + kMuCand] * kp.geom.dvol, kp.abundance[s], kp.rel_acc, dmm, bits);
-          ls->ms[s] = ms;
-        }
-        ls->dmm = dmm;
-        ls->iter_bits |= bits;
-        ls->mu_passes++;
-      }
-      __syncthreads();
-      state_store(st, ls);
-    }
-    if (!grid_barrier(st)) return;
-  }
-
-  MPDPFT_TSTAMP(2);
-  // ---- phase C: final densities, residual, CC dots, Gram row -----------
-  if (threadIdx.x < S) {
-    const int s = threadIdx.x;
-    s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
-    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
-  }
-  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
-  __syncthreads();
-  const int pulay_now = s_flag;
-  const int hist = ldcg(&st->hist);
-  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
-  {
-    // per species: [0] N, [1] <n_out, n_in>_w, [2] <n_out, n_out>_w,
-    // [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram row, summed over
-    // species in phase D); w = multiplicity in the reference storage
-    __shared__ long s_roff[kMaxP];
-    if (threadIdx.x < I) {
-      const int j = threadIdx.x;
-      s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
-    }
-    __syncthreads();
-    R* nin = a.nin + (long)cur * S * n;
-    R* rcur = a.res + (long)cur * S * n;
-    for (int s = 0; s < S; ++s) {
-      double acc[kNF];
-#pragma unroll
-      for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
-      const DensParams d = kp.dens[s];
-      const double mus = s_mu[s];
-      const long so = (long)s * n;
-      for (long p = tid; p < n; p += nthreads) {
-        const long q = so + p;
-        const R v = V[q];
-        const double l = a.lap ? (double)a.lap[q] : 0.0;
-        const double g = a.g2 ? (double)a.g2[q] : 0.0;
-        // mode 2 (admix only): V holds the output densities
-        const double nod = a.mode == 2 ? (double)v : density_at_d(d, mus - (double)v, l, g);
-        const R no = R(nod);
-        acc[0] += nod;
-        if (a.mode == 1) { nin[q] = no; continue; }
-        const R ni = nin[q];
-        const R r = no - ni;
-        rcur[q] = r;
-        const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
-        const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
-        acc[1] += w * dno * dni;
-        acc[2] += w * dno * dno;
-        acc[3] += w * dni * dni;
-        for (int j = 0; j < I - 1; ++j) acc[4 + j] += wr * (double)a.res[s_roff[j] + q];
-        if (I > 0) acc[4 + I - 1] += wr * dr;
-      }
-      block_reduce_store<kNF>(acc, mypart + s * kNF);
-    }
-  }
-  if (!grid_barrier(st)) return;
-
-  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
-  MPDPFT_TSTAMP(3);
-  if (blockIdx.x == 0) {
-    reduce_partials(a.part, gridDim.x, S * kNF, red);
-    if (threadIdx.x < kMaxP) {  // Gram row summed over species
-      double t = 0.0;
-      for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
-      s_grow[threadIdx.x] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int sc = ls->sc_count;
-      double tot = 0.0;
-      for (int s = 0; s < S; ++s) {
-        ls->mu[s] = s_mu_rep[s];
-        ls->ab[s] = red[s * kNF] * kp.geom.dvol;
-        if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
-        tot += ls->ab[s];
-      }
-      if (a.mode == 1) {
-        ls->status_bits |= ls->iter_bits;
-        ls->mu_passes_total += ls->mu_passes;
-      } else {
-        // CheckConvergence (mpDPFT.cpp:4759-4782)
-        const double mp = 100.0 * 1.0e-16;
-        if (sc > 0) {
-          double cc = 0.0, maxtest = 0.0;
-          for (int s = 0; s < S; ++s) {
-            double oi = red[s * kNF + 1], oo = red[s * kNF + 2], ii = red[s * kNF + 3];
-            double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
-            double t = rd * ls->ab[s] / tot;
-            if (t > maxtest) { maxtest = t; cc = maxtest; }
-          }
-          ls->cc = cc;
-          double dab = 0.0, dmu = 0.0;
-          for (int s = 0; s < S; ++s) {
-            dab += (ls->ab[s] - ls->old_ab[s]) * (ls->ab[s] - ls->old_ab[s]);
-            dmu += (ls->mu[s] - ls->old_mu[s]) * (ls->mu[s] - ls->old_mu[s]);
-          }
-          int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
-          double avth = 0.0;
-          for (int s = 0; s < S; ++s) avth += ls->theta[s] / (double)S;
-          bool vok = !(kp.pot_tol > 0.0) || ls->v_res <= kp.pot_tol;
-          if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
-              (cc < kp.sc_criterion || steady) && vok)
-            ls->exit_count++;
-          else
-            ls->exit_count = 0;
-          if (ls->exit_count >= 3) ls->exit_loop = 1;
-        } else {
-          ls->cc = 1.2345678901234567890;
-        }
-        if (sc == kp.max_sc) ls->exit_loop = 1;  // Intercept (:4866)
-        // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): assemble the
-        // Gram matrix (last row/column new, the rest shifted from before)
-        if (pulay_now) {
-          const int shift = (hist + 1 > kp.scope) ? 1 : 0;
-          for (int i = 0; i < I; ++i)
-            for (int j = 0; j < I; ++j) {
-              double v;
-              if (i == I - 1) v = s_grow[j];
-              else if (j == I - 1) v = s_grow[i];
-              else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
-              s_G[i * I + j] = v;
-            }
-          for (int i = 0; i < I; ++i)
-            for (int j = 0; j < I; ++j) ls->gram[i * kMaxP + j] = s_G[i * I + j];
-          ls->hist = I;
-        }
-      }
-    }
-    __syncthreads();
-    // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
-    // reference, mpDPFT.cpp:5089-5107)
-    if (a.mode != 1 && pulay_now && threadIdx.x < 32) {
-      bool ok = warp_inverse(I, s_G, s_M, s_inv, s_fac, s_perm);
-      double test = 0.0;
-      if (ok) {
-        for (int e = threadIdx.x; e < I * I; e += 32) {
-          const int i = e / I, j = e % I;
-          double t = 0.0;
-          for (int k = 0; k < I; ++k) t += s_inv[i * I + k] * s_G[k * I + j];
-          t -= (i == j) ? 1.0 : 0.0;
-          test += t * t;
-        }
-        test = warp_sum(test);
-      }
-      if (threadIdx.x == 0) s_ok = ok && test <= 1.0e-8;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int sc = ls->sc_count;
-      if (a.mode != 1) {
-        int used = 0;
-        if (pulay_now) {
-          if (s_ok) {
-            double x[kMaxP], A = 0.0;
-            for (int i = 0; i < I; ++i) {
-              x[i] = 0.0;
-              for (int k = 0; k < I; ++k) x[i] += s_inv[i * I + k];
-              A += x[i];
-            }
-            for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
-            used = 1;
-          }
-          if (!used) ls->iter_bits |= kBitPulay;
-        }
-        ls->pulay_used = used;
-        ls->ncoeff = used ? I : 0;
-        for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
-        // InjectSchedule (mpDPFT.cpp:5229-5315)
-        if (kp.schedule == 5) {
-          for (int s = 0; s < S; ++s) {
-            double th = ls->theta[s] * (ls->cc < ls->old_cc ? 1.1 : 0.5);
-            th = fmin(0.8, th);
-            th = fmax(10.0 / (double)kp.max_sc, th);
-            ls->theta[s] = th;
-          }
-        } else if (kp.schedule == 9) {
-          for (int s = 0; s < S; ++s)
-            if (ls->theta[s] < 0.2)
-              ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
-        }
-        if (a.log && sc < a.log_cap) {
-          mpdpft_iter_log& L = a.log[sc];
-          L.sc_count = sc;
-          L.mu_trials = ls->mu_passes;
-          L.pulay_used = used;
-          L.status_bits = ls->iter_bits;
-          L.cc = ls->cc;
-          L.v_residual = ls->v_res;
-          for (int s = 0; s < kMaxS; ++s) {
-            L.mu[s] = s < S ? ls->mu[s] : 0.0;
-            L.abundance[s] = s < S ? ls->ab[s] : 0.0;
-            L.theta[s] = s < S ? ls->theta_mix[s] : 0.0;
-          }
-          L.ms = 0.0;
-        }
-        ls->status_bits |= ls->iter_bits;
-        ls->mu_passes_total += ls->mu_passes;
-        // StoreCurrentIteration of the next iteration; PrepareNextIteration
-        for (int s = 0; s < S; ++s) { ls->old_mu[s] = ls->mu[s]; ls->old_ab[s] = ls->ab[s]; }
-        ls->old_cc = ls->cc;
-        if (sc > 0) ls->inc_v = fmin(1.0, ls->inc_v + kp.inc_v0);  // (:4833)
-        ls->mix_src = cur;
-        ls->slot = next;
-        ls->sc_count = sc + 1;
-      }
-    }
-    __syncthreads();
-    state_store(st, ls);
-  }
-  if (a.mode == 1) return;
-  MPDPFT_TSTAMP(4);
-  if (!grid_barrier(st)) return;
-  MPDPFT_TSTAMP(5);
-
-  // ---- phase E: mixed density -> ring[next] ----------------------------
-  // n = sum_j c_j (n_in,j + theta r_j) (Pulay) or n_in + theta r (linear),
-  // AdmixDensities mpDPFT.cpp:4946-4955 / :4987
-  {
-    __shared__ long s_off[kMaxP];
-    __shared__ double s_c[kMaxP];
-    __shared__ int s_nc;
-    if (threadIdx.x == 0) {
-      const int used = ldcg(&st->pulay_used);
-      const int nc = used ? ldcg(&st->ncoeff) : 1;
-      s_nc = nc;
-      for (int j = 0; j < nc; ++j) {
-        const int slot = (cur - (nc - 1) + j + ring) % ring;
-        s_off[j] = (long)slot * S * n;
-        s_c[j] = used ? ldcg(&st->coeff[j]) : 1.0;
-      }
-    }
-    __syncthreads();
-    const int nc = s_nc;
-    for (int s = 0; s < S; ++s) {
-      const double th = ldcg(&st->theta_mix[s]);
-      R* out = a.nin + (long)next * S * n + (long)s * n;
-      if (sizeof(R) == sizeof(float) && (n & 3) == 0) {
-        const long n4 = n >> 2;
-        for (long p4 = tid; p4 < n4; p4 += nthreads) {
-          double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
-          for (int j = 0; j < nc; ++j) {
-            const long q = s_off[j] + (long)s * n + 4 * p4;
-            const float4 ni = *reinterpret_cast<const float4*>(a.nin + q);
-            const float4 ri = *reinterpret_cast<const float4*>(a.res + q);
-            const double c = s_c[j];
-            v0 += c * ((double)ni.x + th * (double)ri.x);
-            v1 += c * ((double)ni.y + th * (double)ri.y);
-            v2 += c * ((double)ni.z + th * (double)ri.z);
-            v3 += c * ((double)ni.w + th * (double)ri.w);
-          }
-          *reinterpret_cast<float4*>(out + 4 * p4) = make_float4((float)v0, (float)v1, (float)v2, (float)v3);
-        }
-      } else {
-        for (long p = tid; p < n; p += nthreads) {
-          double v = 0.0;
-          for (int j = 0; j < nc; ++j) {
-            const long q = s_off[j] + (long)s * n + p;
-            v += s_c[j] * ((double)a.nin[q] + th * (double)a.res[q]);
-          }
-          out[p] = R(v);
-        }
-      }
-    }
-  }
-  MPDPFT_TSTAMP(6);
 }
 
 }  // namespace mpdpft
