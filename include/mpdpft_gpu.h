@@ -37,6 +37,7 @@ extern "C" {
 #define MPDPFT_MAX_SPECIES 4
 #define MPDPFT_MAX_INTERACTIONS 8
 #define MPDPFT_MAX_PULAY 12
+#define MPDPFT_NOALLOC_MAX_POINTS 16777216 /* largest grid of mpdpft_integrate_noalloc (256^3) */
 
 typedef enum {
   MPDPFT_OK = 0,
@@ -227,6 +228,24 @@ int mpdpft_fft(mpdpft_ctx* ctx, int sign, const double* in, double* out, int mem
 /* Trapezoid integral over the box.  Replaces Integrate(method 1)
  * (Riemann, mpDPFT.cpp:7981-8026). */
 int mpdpft_integrate(mpdpft_ctx* ctx, const double* f, double* out, int layout, int mem);
+
+/* The same trapezoid integral without a context and without allocating any
+ * device memory.  It has no counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc, e.g. a plug-in whose host application
+ * owns all device memory, or a loop that must not pay cudaMalloc's implicit
+ * device synchronisation.
+ *   f      device pointer, double, periodic s^D or reference (s+1)^D layout;
+ *   out    device pointer to one double, written with the integral;
+ *   stream cudaStream_t (NULL: the default stream) on the current device.
+ * Grids of more than MPDPFT_NOALLOC_MAX_POINTS points (s > 256 in 3D,
+ * s > 4096 in 2D) are rejected with MPDPFT_ERR_ARG.  The partial sums live in
+ * one fixed 32 KiB array per GPU, kept from library load to process exit and
+ * shared by all calls: calls whose kernels overlap on one GPU (other streams,
+ * other host threads) race on it and must be serialised by the caller.  The
+ * first call on each device looks up that array's device address, so make it
+ * before any stream capture.  Returns once the work is queued on stream. */
+int mpdpft_integrate_noalloc(int dim, int steps, double edge, const double* f, double* out, int layout,
+                             void* stream);
 
 /* Density mixing for all species.  mixer 1 runs PulayMixer
  * (mpDPFT.cpp:5005-5167) with its history kept on the device and falls back
