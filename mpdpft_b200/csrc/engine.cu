@@ -209,8 +209,8 @@ KParams Ctx::kparams() const {
   k.schedule = P.schedule;
   k.pot_tol = P.potential_tol;
   k.inc_v0 = P.incremental_v;
-  k.nseg = nseg;
-  k.seg_mul = seg_mul;
+  k.chunk = chunk;
+  k.mu_blocks = step_blocks;
   k.vec4 = (geom.n % 4) == 0;
   return k;
 }
@@ -265,31 +265,39 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   log_cap = P.max_sc_count + 2;
   if ((st = alloc((void**)&d_log, sizeof(mpdpft_iter_log) * log_cap))) return st;
   // persistent-kernel grid: co-resident blocks only
-  int occ = 0;
-  cudaError_t e = P.precision == MPDPFT_FP64
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sc_step_kernel<double>, kStepThreads, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sc_step_kernel<float>, kStepThreads, 0);
-  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
-  if (occ < 1) return set_error(MPDPFT_ERR_CUDA, "step kernel cannot be resident");
-  step_blocks = num_sms * std::min(occ, 2);
+  // grids: the cooperative mu kernel holds co-resident blocks only; the
+  // density and mixing kernels fill every SM
+  auto occupancy = [&](const void* fn, int threads, int* occ) -> int {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, threads, 0);
+    if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+    if (*occ < 1) return set_error(MPDPFT_ERR_CUDA, "SC kernel cannot be resident");
+    return MPDPFT_OK;
+  };
+  const bool f64 = P.precision == MPDPFT_FP64;
+  int occ_mu = 0, occ_dens = 0, occ_mix = 0;
+  if ((st = occupancy(f64 ? (const void*)sc_mu_kernel<double> : (const void*)sc_mu_kernel<float>, kStepThreads, &occ_mu)))
+    return st;
+  if ((st = occupancy(f64 ? (const void*)sc_density_kernel<double> : (const void*)sc_density_kernel<float>,
+                      kDensThreads, &occ_dens)))
+    return st;
+  if ((st = occupancy(f64 ? (const void*)sc_mix_kernel<double> : (const void*)sc_mix_kernel<float>, kDensThreads,
+                      &occ_mix)))
+    return st;
+  step_blocks = num_sms * std::min(occ_mu, 2);
   long useful = (geom.n + kStepThreads - 1) / kStepThreads;
   if (step_blocks > useful) step_blocks = (int)std::max(1L, useful);
-  // sweep order: segment k -> k * seg_mul mod nseg with seg_mul near
-  // nseg / golden ratio and coprime to nseg (a bijection that scatters
-  // neighbouring k over the grid)
-  nseg = (geom.n + kSegPts - 1) / kSegPts;
-  seg_mul = 1;
-  if (nseg > 2) {
-    long m = std::max(1L, (long)std::llround(0.6180339887498949 * (double)nseg));
-    auto gcd = [](long a, long b) { while (b) { long t = a % b; a = b; b = t; } return a; };
-    while (gcd(m, nseg) != 1) ++m;
-    seg_mul = m % nseg;
-  }
+  const long groups = (geom.n + 3) / 4;  // the density and mixing kernels take 4 points a thread
+  const long useful_dens = (groups + kDensThreads - 1) / kDensThreads;
+  dens_blocks = (int)std::max(1L, std::min((long)num_sms * occ_dens, useful_dens));
+  mix_blocks = (int)std::max(1L, std::min((long)num_sms * occ_mix, useful_dens));
+  // the mu kernel's list sweeps: a contiguous chunk of points per warp
   {
     const long warps = (long)step_blocks * kStepWarps;
-    seg_wmax = (int)((nseg + warps - 1) / warps);
-    const size_t ints = (size_t)kMaxS * ((size_t)step_blocks + (size_t)warps * seg_wmax + (size_t)nseg);
-    if ((st = alloc((void**)&d_seg, sizeof(int) * ints))) return st;
+    chunk = (geom.n + warps - 1) / warps;
+    chunk = (chunk + kSegPts - 1) / kSegPts * kSegPts;
+    if ((st = alloc((void**)&d_bcount, sizeof(int) * (size_t)kMaxS * step_blocks))) return st;
+    if ((st = alloc((void**)&d_plist, sizeof(int) * (size_t)S * geom.n))) return st;
+    if ((st = alloc((void**)&d_part2, sizeof(double) * (size_t)dens_blocks * kNPart))) return st;
   }
   part_vals = std::max(kNPart, kNEnergy);
   if ((st = alloc((void**)&d_part, sizeof(double) * (size_t)std::max(step_blocks, kMaxBlocks) * part_vals))) return st;
@@ -376,13 +384,9 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.nin = (R*)d_nin;
   a.res = (R*)d_res;
   a.part = d_part;
-  {
-    const long warps = (long)step_blocks * kStepWarps;
-    a.bcount = d_seg;
-    a.wlist = d_seg + (size_t)kMaxS * step_blocks;
-    a.slist = a.wlist + (size_t)kMaxS * warps * seg_wmax;
-    a.wmax = seg_wmax;
-  }
+  a.part2 = d_part2;
+  a.bcount = d_bcount;
+  a.plist = d_plist;
   a.vres_part = vres_part_ext;
   a.vres_blocks = vres_blocks_ext;
   a.log = d_log;
@@ -392,23 +396,39 @@ StepArgs<R> Ctx::step_args(int mode) {
   return a;
 }
 
+// One SC iteration's kernels (mode 0), the densities of the current V
+// (mode 1: mu kernel + density kernel) or the admix step alone (mode 2:
+// density kernel + mixing kernel).
 int Ctx::launch_step(int mode) {
-  cudaLaunchConfig_t cfg;
-  std::memset(&cfg, 0, sizeof(cfg));
-  cfg.gridDim = dim3(step_blocks);
-  cfg.blockDim = dim3(kStepThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
   cudaError_t e;
+  const bool f64 = rsize == sizeof(double);
+  if (mode != 2) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(step_blocks);
+    cfg.blockDim = dim3(kStepThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cnt[MPDPFT_STAGE_SC_STEP]++;
+    if (f64) e = cudaLaunchKernelEx(&cfg, sc_mu_kernel<double>, step_args<double>(mode));
+    else e = cudaLaunchKernelEx(&cfg, sc_mu_kernel<float>, step_args<float>(mode));
+    if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("sc_mu_kernel launch: ") + cudaGetErrorString(e));
+  }
   cnt[MPDPFT_STAGE_SC_STEP]++;
-  if (rsize == sizeof(double)) e = cudaLaunchKernelEx(&cfg, sc_step_kernel<double>, step_args<double>(mode));
-  else e = cudaLaunchKernelEx(&cfg, sc_step_kernel<float>, step_args<float>(mode));
-  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("sc_step launch: ") + cudaGetErrorString(e));
+  if (f64) sc_density_kernel<double><<<dens_blocks, kDensThreads, 0, stream>>>(step_args<double>(mode));
+  else sc_density_kernel<float><<<dens_blocks, kDensThreads, 0, stream>>>(step_args<float>(mode));
+  CU(cudaGetLastError());
+  if (mode != 1) {
+    cnt[MPDPFT_STAGE_SC_STEP]++;
+    if (f64) sc_mix_kernel<double><<<mix_blocks, kDensThreads, 0, stream>>>(step_args<double>(mode));
+    else sc_mix_kernel<float><<<mix_blocks, kDensThreads, 0, stream>>>(step_args<float>(mode));
+    CU(cudaGetLastError());
+  }
   return MPDPFT_OK;
 }
 

@@ -48,10 +48,12 @@ struct Ctx {
   mpdpft_iter_log* d_log = nullptr;
   int log_cap = 0;
   int step_blocks = 0;
-  long nseg = 1;     // warp segments of the step kernel's sweeps
-  long seg_mul = 1;  // their visiting-order multiplier
-  int seg_wmax = 1;  // segments per warp in a full sweep (upper bound)
-  int* d_seg = nullptr;  // active-segment lists: bcount | wlist | slist
+  int dens_blocks = 0;   // grid of the density kernel
+  int mix_blocks = 0;    // grid of the mixing kernel
+  long chunk = kSegPts;  // points per warp in the mu kernel's list sweeps
+  int* d_bcount = nullptr;    // [kMaxS][step_blocks] active points per block
+  int* d_plist = nullptr;     // [S][n] active-point lists
+  double* d_part2 = nullptr;  // [dens_blocks][kNPart] density-kernel partial sums
   int assemble_in_step = 1;
   const double* vres_part_ext = nullptr;
   int vres_blocks_ext = 0;

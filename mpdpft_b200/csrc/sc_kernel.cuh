@@ -1,16 +1,22 @@
-// sc_kernel.cuh -- the persistent SC-iteration kernel (phases A-E) and its
-// block-level helpers.  State, parameters and the mu-search decisions are in
+// sc_kernel.cuh -- the kernels of one SC iteration and their block-level
+// helpers.  State, parameters and the mu-search decisions are in
 // sc_step.cuh.
 //
-// Work layout.  Grid sweeps are over warp segments of kSegPts = 128
-// consecutive points (4 per lane, one 16-byte vector load per field), visited
-// in the scattered order seg = k * seg_mul mod nseg, so the costly segments
-// (points where mu - V > 0, a few per cent of an atom's box) spread evenly
-// over the warps.  The mu search of a functional that vanishes for mu <= V
-// skips segments with no point below the pass's largest candidate (a warp
-// vote on V), records the others during its first full sweep, and later
-// passes visit only that compacted list: all warps share the few costly
-// segments instead of a handful of warps carrying them.
+// One iteration is three launches on the context stream:
+//   sc_mu_kernel       cooperative, one block per SM: UpdateV (when V is not
+//                      assembled by the FFT path) and the mu search, whose
+//                      passes are separated by bounded grid barriers;
+//   sc_density_kernel  all points at full occupancy: final densities,
+//                      residual, convergence dots and the Pulay Gram row; its
+//                      last block to finish runs the scalar logic
+//                      (CheckConvergence ... InjectSchedule, Pulay solve);
+//   sc_mix_kernel      all points: the mixed density into the next ring slot.
+// The mu search of a functional that vanishes for mu <= V evaluates only
+// the points below the largest candidate: a sweep over V compacts them (in
+// grid order) into a list that later passes reuse while their candidates
+// stay below the bound, and every thread of the grid takes an equal share of
+// the list.  The 3D gradient-corrected and TF functionals are evaluated in a
+// branch-free form so that all candidates of a point run side by side.
 #pragma once
 #include "sc_step.cuh"
 
@@ -160,20 +166,103 @@ __device__ __forceinline__ void ref_weights4(long p0, int s, int dim, double (&w
   }
 }
 
-// Sums of the mu candidates over one segment (N(mu_c) and dN/dmu at
-// candidate 0), given the lane's 4 potentials.
-template <typename R>
-__device__ __forceinline__ void mu_segment(const DensParams& d, const double* cmu, int nc, double cmax,
-                                           const R (&v4)[4], const R* Ls, const R* Gs, long p0, long n, int vec4,
-                                           double (&acc)[kMuAcc]) {
-  R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
-  if (Ls) load4(Ls, p0, n, vec4, l4);
-  if (Gs) load4(Gs, p0, n, vec4, g4);
+// ------------------------------------------------------- point evaluation --
+// Constants of the branch-free forms (fast = 1: 3D gradient-corrected,
+// fast = 2: 3D TF, 0: the general density_at_d / density_slope_d).
+struct EvalK {
+  int fast;
+  double ctf;     // TF prefactor
+  double cg;      // gradient prefactor (times lap)
+  double cg2;     // gradient prefactor times c2 / 4 (times |grad V|^2)
+  double floor_u, c1, c3;  // below floor: u^{-1/2} -> u c1, u^{-3/2} -> u c3
+};
+
+__device__ __forceinline__ EvalK eval_constants(const DensParams& d) {
+  EvalK k;
+  k.fast = 0;
+  k.ctf = k.cg = k.cg2 = k.floor_u = k.c1 = k.c3 = 0.0;
+  if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 3) {
+    k.fast = 1;
+    k.ctf = 2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi);
+    k.cg = 1.4142135623730951 * d.g / (48.0 * kPi * kPi);
+    k.cg2 = k.cg * 0.25 * d.c2;
+    k.floor_u = d.floor_u;
+    k.c1 = rsqrt_d(d.floor_u) / d.floor_u;
+    k.c3 = k.c1 / d.floor_u;
+  } else if (d.expr == MPDPFT_DENS_TF && d.dim == 3) {
+    k.fast = 2;
+    k.ctf = 1.4142135623730951 * d.g / (3.0 * kPi * kPi);
+  }
+  return k;
+}
+
+// rsqrt_d without its range branch (callers clamp u to [1e-30, 1e30]).
+__device__ __forceinline__ double rsqrt_nr(double u) {
+  double r = (double)rsqrtf((float)u);
+  const double h = 0.5 * u;
+  r = r * fma(-h * r, r, 1.5);
+  r = r * fma(-h * r, r, 1.5);
+  return r;
+}
+
+// n(u) of the 3D gradient-corrected form for A = cg lap, B = cg c2/4 |grad V|^2
+// (density_at_d without branches: u^{-1/2}, u^{-3/2} continued linearly below
+// the floor, n = 0 for u <= 0 or a negative value).
+__device__ __forceinline__ double grad3_n(const EvalK& k, double u, double A, double B) {
+  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const bool hi = u >= k.floor_u;
+  const double m1 = hi ? r : u * k.c1;
+  const double m3 = hi ? r * r * r : u * k.c3;
+  const double v = k.ctf * u * u * r - (A * m1 + B * m3);
+  return (u > 0.0 && v > 0.0) ? v : 0.0;
+}
+
+// dn/du of the same form (density_slope_d), zero where n is clamped.
+__device__ __forceinline__ double grad3_slope(const EvalK& k, double u, double A, double B) {
+  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const bool hi = u >= k.floor_u;
+  const double r3 = r * r * r;
+  const double m1 = hi ? r : u * k.c1;
+  const double m3 = hi ? r3 : u * k.c3;
+  const double dm1 = hi ? -0.5 * r3 : k.c1;
+  const double dm3 = hi ? -1.5 * r3 * r * r : k.c3;
+  const double v = k.ctf * u * u * r - (A * m1 + B * m3);
+  const double sl = 1.5 * k.ctf * u * r - (A * dm1 + B * dm3);
+  return (u > 0.0 && v > 0.0) ? sl : 0.0;
+}
+
+__device__ __forceinline__ double tf3_n(const EvalK& k, double u) {
+  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  return u > 0.0 ? k.ctf * u * u * r : 0.0;
+}
+
+__device__ __forceinline__ double tf3_slope(const EvalK& k, double u) {
+  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  return u > 0.0 ? 1.5 * k.ctf * u * r : 0.0;
+}
+
+// n at u = mu - V for one point.
+__device__ __forceinline__ double point_density(const DensParams& d, const EvalK& k, double u, double l, double g) {
+  if (k.fast == 1) return grad3_n(k, u, k.cg * l, k.cg2 * g);
+  if (k.fast == 2) return tf3_n(k, u);
+  return density_at_d(d, u, l, g);
+}
+
+// N(mu_c) contributions of one point for all candidates, and dN/dmu at
+// candidate 0.  Candidate slots at or beyond nc hold copies of candidate 0
+// in the fast forms (evaluated, never read).
+__device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, const double* cmu, int nc, double v,
+                                         double l, double g, double (&acc)[kMuAcc]) {
+  if (k.fast == 1) {
+    const double A = k.cg * l, B = k.cg2 * g;
+    acc[kMuCand] += grad3_slope(k, cmu[0] - v, A, B);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const double v = (double)v4[i];
-    if (p0 + i >= n || (d.cut && !(cmax - v > 0.0))) continue;
-    const double l = (double)l4[i], g = (double)g4[i];
+    for (int c = 0; c < kMuCand; ++c) acc[c] += grad3_n(k, cmu[c] - v, A, B);
+  } else if (k.fast == 2) {
+    acc[kMuCand] += tf3_slope(k, cmu[0] - v);
+#pragma unroll
+    for (int c = 0; c < kMuCand; ++c) acc[c] += tf3_n(k, cmu[c] - v);
+  } else {
     acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
 #pragma unroll
     for (int c = 0; c < kMuCand; ++c) {
@@ -207,13 +296,12 @@ __device__ __forceinline__ void block_sum2(int& x, int& y) {
   for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { x += sh[0][i]; y += sh[1][i]; }
 }
 
-// ------------------------------------------------------------ the kernel --
-// mode 0: one SC iteration.  mode 1: GetDensities of the current V (mu
-// search + n[V]), written into the current ring slot; used for the initial
-// densities (mpDPFT.cpp:195) and the standalone mu-search entry point.
-// mode 2: AdmixDensities only, V holding the output densities.
+// ------------------------------------------------------------ mu kernel --
+// mode 0: UpdateV + mu search of one SC iteration.  mode 1: mu search of the
+// current V (GetDensities for the initial densities, mpDPFT.cpp:195, and the
+// standalone mu-search entry point).  Not launched in mode 2 (admix only).
 template <typename R>
-__global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
@@ -222,29 +310,20 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
   const long nthreads = (long)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const long gw = (long)blockIdx.x * kStepWarps + wib;
-  const long nw = (long)gridDim.x * kStepWarps;
-  const long nseg = kp.nseg;
-  const long seg_step = (nw % nseg) * kp.seg_mul % nseg;
-  const long seg_first = (gw % nseg) * kp.seg_mul % nseg;
   __shared__ double red[kNPart];
-  __shared__ double s_mu[kMaxS];      // mu of the final density
-  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
-  __shared__ int s_flag;
   __shared__ MuState s_ms[kMaxS];
-  __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP];
-  __shared__ double s_prm[kMaxP], s_prr[kMaxP], s_pcol[kMaxP];
-  __shared__ int s_colof[kMaxP];
-  __shared__ int s_ok;
-  __shared__ double s_grow[kMaxP];
-  // active-segment lists as this block sees them (identical in every block)
+  // active-point lists as this block sees them (identical in every block)
   __shared__ int s_wcnt[kMaxS][kStepWarps];
-  __shared__ int s_full[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
-  __shared__ double s_fcap[kMaxS], s_lcap[kMaxS];
+  __shared__ int s_need[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
+  __shared__ double s_cap[kMaxS], s_lcap[kMaxS];
 
-  if (a.mode != 1 && ldcg(&st->exit_loop)) return;
-  // block 0 runs the scalar SC logic on a shared-memory copy of the state
-  // and writes it back before every grid barrier after which other blocks
-  // read the state
+  if (a.mode == 0) {
+    const int exited = ldcg(&st->exit_loop);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->iter_active = exited ? 0 : 1;
+    if (exited) return;
+  }
+  // block 0 runs the scalar logic on a shared-memory copy of the state and
+  // writes it back before every grid barrier after which others read it
   __shared__ ScState s_st;
   ScState* const ls = &s_st;
   if (blockIdx.x == 0) {
@@ -252,12 +331,10 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
     __syncthreads();
   }
   const int cur = ldcg(&st->slot);
-  const int ring = kp.ring;
-  const int next = (cur + 1) % ring;
   double* mypart = a.part + (long)blockIdx.x * kNPart;
   MPDPFT_TSTAMP(0);
 
-  // ---- phase A: UpdateV (mpDPFT.cpp:4815-4838) --------------------------
+  // ---- UpdateV (mpDPFT.cpp:4815-4838) -----------------------------------
   if (a.mode == 0 && a.assemble_v) {
     const double incv = ldcg(&st->inc_v);
     const double fac = incv < 1.0 ? incv : 1.0;
@@ -291,7 +368,7 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
     block_reduce_store<kMaxS>(acc, mypart + kVresOff);
   }
 
-  // ---- phase B: mu search (GetDensities + EnforceConstraints) ----------
+  // ---- mu search (GetDensities + EnforceConstraints) --------------------
   const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
   if (threadIdx.x == 0) {  // every block derives the pass-0 candidates itself
     double dmm = ldcg(&st->dmm);
@@ -301,10 +378,11 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
       double mu = ldcg(&st->mu[s]);
       double pa = sqrt(pn) < 1.0e-12 ? 1.0e-12 : fabs(mu);
       mu_begin(s_ms[s], mu, pa, dmm, active);
+      for (int c = s_ms[s].ncand; c < kMuCand; ++c) s_ms[s].cand[c] = s_ms[s].cand[0];
     }
   }
   if (threadIdx.x < kMaxS) {
-    s_full[threadIdx.x] = 0;
+    s_need[threadIdx.x] = 0;
     s_lok[threadIdx.x] = 0;
     s_llen[threadIdx.x] = 0;
   }
@@ -319,102 +397,124 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
 
   const R* V = a.V;
   MPDPFT_TSTAMP(1);
-  for (int pass = 0; pass < kMuMaxPasses && a.mode != 2; ++pass) {
+  for (int pass = 0; pass < kMuMaxPasses; ++pass) {
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
       s_ms[s].done = ldcg(&st->ms[s].done);
       s_ms[s].ncand = ldcg(&st->ms[s].ncand);
       for (int c = 0; c < s_ms[s].ncand; ++c) s_ms[s].cand[c] = ldcg(&st->ms[s].cand[c]);
+      for (int c = s_ms[s].ncand; c < kMuCand; ++c) s_ms[s].cand[c] = s_ms[s].cand[0];
     }
     __syncthreads();
-    int any = 0;
-    for (int s = 0; s < S; ++s) any |= !s_ms[s].done;
+    if (threadIdx.x < S) {
+      const int s = threadIdx.x;
+      double cmax = s_ms[s].cand[0];
+      for (int c = 1; c < s_ms[s].ncand; ++c) cmax = fmax(cmax, s_ms[s].cand[c]);
+      s_cap[s] = cmax;
+      s_need[s] = !s_ms[s].done && kp.dens[s].cut && !(s_lok[s] && cmax <= s_lcap[s]);
+    }
+    __syncthreads();
+    int any = 0, need = 0;
+    for (int s = 0; s < S; ++s) { any |= !s_ms[s].done; need |= s_need[s]; }
     if (!any) break;
+    if (need) {
+      // (re)build the active-point lists: count, offsets, write (grid order)
+      const long beg = gw * kp.chunk;
+      const long end = beg + kp.chunk < n ? beg + kp.chunk : n;
+      for (int s = 0; s < S; ++s) {
+        if (!s_need[s]) continue;
+        const R* Vs = V + (long)s * n;
+        const double cap = s_cap[s];
+        int cnt = 0;
+        for (long b = beg; b < end; b += kSegPts) {
+          const long p0 = b + 4 * lane;
+          R v4[4];
+          load4(Vs, p0, n, kp.vec4, v4);
+          int c = 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) c += (p0 + i < n && cap - (double)v4[i] > 0.0) ? 1 : 0;
+          cnt += __reduce_add_sync(0xffffffffu, c);
+        }
+        if (lane == 0) s_wcnt[s][wib] = cnt;
+      }
+      __syncthreads();
+      if (threadIdx.x < S && s_need[threadIdx.x]) {
+        int c = 0;
+        for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
+        a.bcount[(long)threadIdx.x * gridDim.x + blockIdx.x] = c;
+      }
+      if (!grid_barrier(st)) return;
+      for (int s = 0; s < S; ++s) {
+        if (!s_need[s]) continue;
+        int before = 0, total = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+          const int c = __ldcg(a.bcount + (long)s * gridDim.x + b);
+          total += c;
+          if (b < (int)blockIdx.x) before += c;
+        }
+        block_sum2(before, total);
+        int off = before;
+        for (int w = 0; w < wib; ++w) off += s_wcnt[s][w];
+        const R* Vs = V + (long)s * n;
+        int* pl = a.plist + (long)s * n;
+        const double cap = s_cap[s];
+        const unsigned lt = (1u << lane) - 1u;
+        for (long b = beg; b < end; b += kSegPts) {
+          const long p0 = b + 4 * lane;
+          R v4[4];
+          load4(Vs, p0, n, kp.vec4, v4);
+          bool f[4];
+          unsigned m[4];
+          int pos = off, tot = 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            f[i] = p0 + i < n && cap - (double)v4[i] > 0.0;
+            m[i] = __ballot_sync(0xffffffffu, f[i]);
+            pos += __popc(m[i] & lt);
+            tot += __popc(m[i]);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (f[i]) pl[pos++] = (int)(p0 + i);
+          off += tot;
+        }
+        if (threadIdx.x == 0) s_llen[s] = total;
+      }
+      __syncthreads();
+      if (threadIdx.x < S && s_need[threadIdx.x]) {
+        s_lok[threadIdx.x] = 1;
+        s_lcap[threadIdx.x] = s_cap[threadIdx.x];
+        s_need[threadIdx.x] = 0;
+      }
+      if (!grid_barrier(st)) return;  // the lists are complete
+    }
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
-      // N(mu) and dN/dmu are evaluated in double from the stored fields
-      // (FP32 in mixed mode): the particle-number integral and the mu search
-      // are FP64 in both modes
+      // N(mu) and dN/dmu in double from the stored fields (FP32 in mixed
+      // mode): the particle-number integral and the mu search are FP64 in
+      // both modes
       double acc[kMuAcc];
 #pragma unroll
       for (int c = 0; c < kMuAcc; ++c) acc[c] = 0.0;
       const DensParams d = kp.dens[s];
+      const EvalK k = eval_constants(d);
       const int nc = s_ms[s].ncand;
       const double* cmu = s_ms[s].cand;  // shared memory (broadcast reads)
-      double cmax = cmu[0];
-      for (int c = 1; c < nc; ++c) cmax = fmax(cmax, cmu[c]);
       const R* Vs = V + (long)s * n;
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
-      if (d.cut && s_lok[s] && cmax <= s_lcap[s]) {
-        const int len = s_llen[s];
-        for (long j = gw; j < len; j += nw) {
-          const long p0 = (long)__ldcg(a.slist + (long)s * nseg + j) * kSegPts + 4 * lane;
-          R v4[4];
-          load4(Vs, p0, n, kp.vec4, v4);
-          mu_segment(d, cmu, nc, cmax, v4, Ls, Gs, p0, n, kp.vec4, acc);
-        }
-      } else {
-        int cnt = 0;
-        int* wl = a.wlist + ((long)s * nw + gw) * a.wmax;
-        long seg = seg_first;
-        for (long k = gw; k < nseg; k += nw) {
-          const long p0 = seg * kSegPts + 4 * lane;
-          R v4[4];
-          load4(Vs, p0, n, kp.vec4, v4);
-          bool act = true;
-          if (d.cut) {
-            bool mine = false;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (cmax - (double)v4[i] > 0.0);
-            act = __any_sync(0xffffffffu, mine);
-          }
-          if (act) {
-            mu_segment(d, cmu, nc, cmax, v4, Ls, Gs, p0, n, kp.vec4, acc);
-            if (d.cut) {
-              if (lane == 0) wl[cnt] = (int)seg;
-              ++cnt;
-            }
-          }
-          seg += seg_step;
-          if (seg >= nseg) seg -= nseg;
-        }
-        if (d.cut) {
-          if (lane == 0) s_wcnt[s][wib] = cnt;
-          if (threadIdx.x == 0) { s_full[s] = 1; s_fcap[s] = cmax; }
-        }
+      const int* pl = a.plist + (long)s * n;
+      const long len = d.cut ? (long)s_llen[s] : n;
+      for (long j = tid; j < len; j += nthreads) {
+        const long p = d.cut ? (long)__ldcg(pl + j) : j;
+        const double v = (double)__ldcg(Vs + p);
+        const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
+        const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
+        mu_point(d, k, cmu, nc, v, l, g, acc);
       }
       block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
     }
-    __syncthreads();
-    if (threadIdx.x < S && s_full[threadIdx.x]) {
-      int c = 0;
-      for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
-      a.bcount[(long)threadIdx.x * gridDim.x + blockIdx.x] = c;
-    }
     if (!grid_barrier(st)) return;
-    // compact the lists of the full sweeps: block order, then warp order
-    for (int s = 0; s < S; ++s) {
-      if (!s_full[s]) continue;
-      int before = 0, total = 0;
-      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        const int c = __ldcg(a.bcount + (long)s * gridDim.x + b);
-        total += c;
-        if (b < (int)blockIdx.x) before += c;
-      }
-      block_sum2(before, total);
-      int off = before;
-      for (int w = 0; w < wib; ++w) off += s_wcnt[s][w];
-      const int* wl = a.wlist + ((long)s * nw + gw) * a.wmax;
-      for (int i = lane; i < s_wcnt[s][wib]; i += 32) a.slist[(long)s * nseg + off + i] = __ldcg(wl + i);
-      if (threadIdx.x == 0) s_llen[s] = total;
-    }
-    __syncthreads();
-    if (threadIdx.x < S && s_full[threadIdx.x]) {
-      s_lok[threadIdx.x] = 1;
-      s_lcap[threadIdx.x] = s_fcap[threadIdx.x];
-      s_full[threadIdx.x] = 0;
-    }
     if (blockIdx.x == 0) {
       for (int v = wib; v < S * kMuAcc; v += kStepWarps) {
         const double t = warp_sum_rows(a.part + v, gridDim.x, kNPart);
@@ -440,9 +540,40 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
     }
     if (!grid_barrier(st)) return;
   }
-
+  if (blockIdx.x == 0) {  // the pass-0 set-up when no pass ran
+    __syncthreads();
+    state_store(st, ls);
+  }
   MPDPFT_TSTAMP(2);
-  // ---- phase C: final densities, residual, CC dots, Gram row -----------
+}
+
+// ------------------------------------------------------- density kernel --
+// Final densities n_out = n[V] at the mu the search chose, residual
+// r = n_out - n_in into the ring, and per species [0] N, [1] <n_out, n_in>_w,
+// [2] <n_out, n_out>_w, [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram
+// row), w = multiplicity in the reference storage.  mode 1 writes n_out
+// into the current ring slot instead; mode 2 (admix only) takes n_out from V.
+// The last block to finish runs phase D: CheckConvergence, Intercept, the
+// Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
+template <typename R>
+__global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a) {
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  __shared__ double red[kNPart];
+  __shared__ double red_v[kMaxS];
+  __shared__ double s_mu[kMaxS];      // mu of the final density
+  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
+  __shared__ int s_flag, s_last;
+  __shared__ long s_roff[kMaxP];
+
+  if (a.mode == 0 && !ldcg(&st->iter_active)) return;
+  const int cur = ldcg(&st->slot);
+  const int ring = kp.ring;
+  const int next = (cur + 1) % ring;
+  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
   if (threadIdx.x < S) {
     const int s = threadIdx.x;
     s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
@@ -453,319 +584,322 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_step_kernel(StepArgs<R> a)
   const int pulay_now = s_flag;
   const int hist = ldcg(&st->hist);
   const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
-  {
-    // per species: [0] N, [1] <n_out, n_in>_w, [2] <n_out, n_out>_w,
-    // [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram row, summed over
-    // species in phase D); w = multiplicity in the reference storage
-    __shared__ long s_roff[kMaxP];
-    if (threadIdx.x < I) {
-      const int j = threadIdx.x;
-      s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
-    }
-    __syncthreads();
-    R* nin = a.nin + (long)cur * S * n;
-    R* rcur = a.res + (long)cur * S * n;
-    for (int s = 0; s < S; ++s) {
-      double acc[kNF];
-#pragma unroll
-      for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
-      const DensParams d = kp.dens[s];
-      const double mus = s_mu[s];
-      const long so = (long)s * n;
-      const R* Ls = a.lap ? a.lap + so : nullptr;
-      const R* Gs = a.g2 ? a.g2 + so : nullptr;
-      long seg = seg_first;
-      for (long k = gw; k < nseg; k += nw) {
-        const long p0 = seg * kSegPts + 4 * lane;
-        seg += seg_step;
-        if (seg >= nseg) seg -= nseg;
-        R v4[4];
-        load4(V + so, p0, n, kp.vec4, v4);
-        double nod[4];
-        if (a.mode == 2) {  // admix only: V holds the output densities
-#pragma unroll
-          for (int i = 0; i < 4; ++i) nod[i] = (double)v4[i];
-        } else {
-          bool mine = !d.cut;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (mus - (double)v4[i] > 0.0);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) nod[i] = 0.0;
-          if (__any_sync(0xffffffffu, mine)) {
-            R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
-            if (Ls) load4(Ls, p0, n, kp.vec4, l4);
-            if (Gs) load4(Gs, p0, n, kp.vec4, g4);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-              if (p0 + i < n) nod[i] = density_at_d(d, mus - (double)v4[i], (double)l4[i], (double)g4[i]);
-          }
-        }
-        if (p0 >= n) continue;
-        R no4[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          no4[i] = R(nod[i]);
-          acc[0] += nod[i];  // zero beyond n
-        }
-        if (a.mode == 1) {
-          store4(nin + so, p0, n, kp.vec4, no4);
-          continue;
-        }
-        R ni4[4], r4[4];
-        load4(nin + so, p0, n, kp.vec4, ni4);
-        double w4[4], wr4[4], dr4[4];
-        ref_weights4(p0, kp.geom.s, kp.geom.dim, w4);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          r4[i] = no4[i] - ni4[i];
-          const double w = (p0 + i < n) ? w4[i] : 0.0;
-          const double dno = (double)no4[i], dni = (double)ni4[i];
-          dr4[i] = (double)r4[i];
-          wr4[i] = w * dr4[i];
-          acc[1] += w * dno * dni;
-          acc[2] += w * dno * dno;
-          acc[3] += w * dni * dni;
-        }
-        store4(rcur + so, p0, n, kp.vec4, r4);
-#pragma unroll
-        for (int j = 0; j < kMaxP; ++j) {
-          if (j < I - 1) {
-            R rj4[4];
-            load4(a.res + s_roff[j] + so, p0, n, kp.vec4, rj4);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * (double)rj4[i];
-          } else if (j == I - 1) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * dr4[i];
-          }
-        }
-      }
-      block_reduce_store<kNF>(acc, mypart + s * kNF);
-    }
+  if (threadIdx.x < I) {
+    const int j = threadIdx.x;
+    s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
   }
-  if (!grid_barrier(st)) return;
-
-  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
-  MPDPFT_TSTAMP(3);
-  if (blockIdx.x == 0) {
-    __shared__ double red_v[kMaxS];
-    const int nv = 4 + I;  // per species: N, three dots, Gram row
-    const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
-    for (int v = wib; v < S * nv + vres; v += kStepWarps) {
-      double t;
-      if (v < S * nv) t = warp_sum_rows(a.part + (v / nv) * kNF + (v % nv), gridDim.x, kNPart);
-      else if (a.assemble_v) t = warp_sum_rows(a.part + kVresOff + (v - S * nv), gridDim.x, kNPart);
-      else t = warp_sum_rows(a.vres_part + (v - S * nv), a.vres_blocks, kMaxS);
-      if (lane == 0) {
-        if (v < S * nv) red[(v / nv) * kNF + (v % nv)] = t;
-        else red_v[v - S * nv] = t;
+  __syncthreads();
+  R* nin = a.nin + (long)cur * S * n;
+  R* rcur = a.res + (long)cur * S * n;
+  const long ngroups = (n + 3) / 4;
+  const long gstride = (long)gridDim.x * blockDim.x;
+  for (int s = 0; s < S; ++s) {
+    double acc[kNF];
+#pragma unroll
+    for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
+    const DensParams d = kp.dens[s];
+    const EvalK k = eval_constants(d);
+    const double mus = s_mu[s];
+    const long so = (long)s * n;
+    const R* Ls = a.lap ? a.lap + so : nullptr;
+    const R* Gs = a.g2 ? a.g2 + so : nullptr;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q - threadIdx.x < ngroups; q += gstride) {
+      // the whole warp runs every trip (the vote below needs all lanes)
+      const long p0 = 4 * q;
+      R v4[4];
+      load4(a.V + so, p0, n, kp.vec4, v4);
+      double nod[4] = {0.0, 0.0, 0.0, 0.0};
+      if (a.mode == 2) {  // admix only: V holds the output densities
+#pragma unroll
+        for (int i = 0; i < 4; ++i) nod[i] = (double)v4[i];
+      } else {
+        bool mine = !d.cut && p0 < n;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (mus - (double)v4[i] > 0.0);
+        if (__any_sync(0xffffffffu, mine) && p0 < n) {
+          R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
+          if (Ls) load4(Ls, p0, n, kp.vec4, l4);
+          if (Gs) load4(Gs, p0, n, kp.vec4, g4);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (p0 + i < n) nod[i] = point_density(d, k, mus - (double)v4[i], (double)l4[i], (double)g4[i]);
+        }
       }
-    }
-    __syncthreads();
-    if (threadIdx.x < I) {  // Gram row summed over species
-      double t = 0.0;
-      for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
-      s_grow[threadIdx.x] = t;
-    }
-    __syncthreads();
-    // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): the Gram matrix,
-    // last row/column new, the rest shifted from before (warp 1) ...
-    if (pulay_now && wib == 1) {
-      const int shift = (hist + 1 > kp.scope) ? 1 : 0;
-      for (int e = lane; e < I * I; e += 32) {
-        const int i = e / I, j = e % I;
-        double v;
-        if (i == I - 1) v = s_grow[j];
-        else if (j == I - 1) v = s_grow[i];
-        else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
-        s_G[e] = v;
-      }
-      __syncwarp();
-      for (int e = lane; e < I * I; e += 32) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
-      if (lane == 0) ls->hist = I;
-    }
-    // ... while thread 0 does the scalar bookkeeping
-    if (threadIdx.x == 0) {
-      if (vres) {
-        double w = 0.0;
-        for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red_v[s] / (double)n));
-        ls->v_res = w;
-      }
-      const int sc = ls->sc_count;
-      double tot = 0.0;
-      for (int s = 0; s < S; ++s) {
-        ls->mu[s] = s_mu_rep[s];
-        ls->ab[s] = red[s * kNF] * kp.geom.dvol;
-        if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
-        tot += ls->ab[s];
+      if (p0 >= n) continue;
+      R no4[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        no4[i] = R(nod[i]);
+        acc[0] += nod[i];  // zero beyond n
       }
       if (a.mode == 1) {
-        ls->status_bits |= ls->iter_bits;
-        ls->mu_passes_total += ls->mu_passes;
-      } else {
-        // CheckConvergence (mpDPFT.cpp:4759-4782)
-        const double mp = 100.0 * 1.0e-16;
-        if (sc > 0) {
-          double cc = 0.0, maxtest = 0.0;
-          for (int s = 0; s < S; ++s) {
-            double oi = red[s * kNF + 1], oo = red[s * kNF + 2], ii = red[s * kNF + 3];
-            double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
-            double t = rd * ls->ab[s] / tot;
-            if (t > maxtest) { maxtest = t; cc = maxtest; }
-          }
-          ls->cc = cc;
-          double dab = 0.0, dmu = 0.0;
-          for (int s = 0; s < S; ++s) {
-            dab += (ls->ab[s] - ls->old_ab[s]) * (ls->ab[s] - ls->old_ab[s]);
-            dmu += (ls->mu[s] - ls->old_mu[s]) * (ls->mu[s] - ls->old_mu[s]);
-          }
-          int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
-          double avth = 0.0;
-          for (int s = 0; s < S; ++s) avth += ls->theta[s] / (double)S;
-          bool vok = !(kp.pot_tol > 0.0) || ls->v_res <= kp.pot_tol;
-          if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
-              (cc < kp.sc_criterion || steady) && vok)
-            ls->exit_count++;
-          else
-            ls->exit_count = 0;
-          if (ls->exit_count >= 3) ls->exit_loop = 1;
-        } else {
-          ls->cc = 1.2345678901234567890;
+        store4(nin + so, p0, n, kp.vec4, no4);
+        continue;
+      }
+      R ni4[4], r4[4];
+      load4(nin + so, p0, n, kp.vec4, ni4);
+      double w4[4], wr4[4], dr4[4];
+      ref_weights4(p0, kp.geom.s, kp.geom.dim, w4);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        r4[i] = no4[i] - ni4[i];
+        const double w = (p0 + i < n) ? w4[i] : 0.0;
+        const double dno = (double)no4[i], dni = (double)ni4[i];
+        dr4[i] = (double)r4[i];
+        wr4[i] = w * dr4[i];
+        acc[1] += w * dno * dni;
+        acc[2] += w * dno * dno;
+        acc[3] += w * dni * dni;
+      }
+      store4(rcur + so, p0, n, kp.vec4, r4);
+#pragma unroll
+      for (int j = 0; j < kMaxP; ++j) {
+        if (j < I - 1) {
+          R rj4[4];
+          load4(a.res + s_roff[j] + so, p0, n, kp.vec4, rj4);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * (double)rj4[i];
+        } else if (j == I - 1) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * dr4[i];
         }
-        if (sc == kp.max_sc) ls->exit_loop = 1;  // Intercept (:4866)
       }
     }
-    __syncthreads();
-    // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
-    // reference, mpDPFT.cpp:5089-5107)
-    if (a.mode != 1 && pulay_now && wib == 0) {
-      bool ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
-      double test = ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
-      if (lane == 0) s_ok = ok && test <= 1.0e-8;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int sc = ls->sc_count;
-      if (a.mode != 1) {
-        int used = 0;
-        if (pulay_now) {
-          if (s_ok) {
-            double x[kMaxP], A = 0.0;
-            for (int i = 0; i < I; ++i) {
-              x[i] = 0.0;
-              for (int k = 0; k < I; ++k) x[i] += s_inv[i * I + k];
-              A += x[i];
-            }
-            for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
-            used = 1;
-          }
-          if (!used) ls->iter_bits |= kBitPulay;
-        }
-        ls->pulay_used = used;
-        ls->ncoeff = used ? I : 0;
-        for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
-        // InjectSchedule (mpDPFT.cpp:5229-5315)
-        if (kp.schedule == 5) {
-          for (int s = 0; s < S; ++s) {
-            double th = ls->theta[s] * (ls->cc < ls->old_cc ? 1.1 : 0.5);
-            th = fmin(0.8, th);
-            th = fmax(10.0 / (double)kp.max_sc, th);
-            ls->theta[s] = th;
-          }
-        } else if (kp.schedule == 9) {
-          for (int s = 0; s < S; ++s)
-            if (ls->theta[s] < 0.2)
-              ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
-        }
-        if (a.log && sc < a.log_cap) {
-          mpdpft_iter_log& L = a.log[sc];
-          L.sc_count = sc;
-          L.mu_trials = ls->mu_passes;
-          L.pulay_used = used;
-          L.status_bits = ls->iter_bits;
-          L.cc = ls->cc;
-          L.v_residual = ls->v_res;
-          for (int s = 0; s < kMaxS; ++s) {
-            L.mu[s] = s < S ? ls->mu[s] : 0.0;
-            L.abundance[s] = s < S ? ls->ab[s] : 0.0;
-            L.theta[s] = s < S ? ls->theta_mix[s] : 0.0;
-          }
-          L.ms = 0.0;
-        }
-        ls->status_bits |= ls->iter_bits;
-        ls->mu_passes_total += ls->mu_passes;
-        // StoreCurrentIteration of the next iteration; PrepareNextIteration
-        for (int s = 0; s < S; ++s) { ls->old_mu[s] = ls->mu[s]; ls->old_ab[s] = ls->ab[s]; }
-        ls->old_cc = ls->cc;
-        if (sc > 0) ls->inc_v = fmin(1.0, ls->inc_v + kp.inc_v0);  // (:4833)
-        ls->mix_src = cur;
-        ls->slot = next;
-        ls->sc_count = sc + 1;
-      }
-    }
-    __syncthreads();
-    state_store(st, ls);
+    block_reduce_store<kNF>(acc, a.part2 + (long)blockIdx.x * kNPart + s * kNF);
   }
-  if (a.mode == 1) return;
-  MPDPFT_TSTAMP(4);
-  if (!grid_barrier(st)) return;
-  MPDPFT_TSTAMP(5);
+  // the last block to finish takes phase D
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->k2_done, 1u) == gridDim.x - 1 ? 1 : 0;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) st->tphase[3] = globaltimer();
 
-  // ---- phase E: mixed density -> ring[next] ----------------------------
-  // n = sum_j c_j (n_in,j + theta r_j) (Pulay) or n_in + theta r (linear),
-  // AdmixDensities mpDPFT.cpp:4946-4955 / :4987
-  {
-    __shared__ long s_off[kMaxP];
-    __shared__ double s_c[kMaxP];
-    __shared__ int s_nc;
-    if (threadIdx.x == 0) {
-      const int used = ldcg(&st->pulay_used);
-      const int nc = used ? ldcg(&st->ncoeff) : 1;
-      s_nc = nc;
-      for (int j = 0; j < nc; ++j) {
-        const int slot = (cur - (nc - 1) + j + ring) % ring;
-        s_off[j] = (long)slot * S * n;
-        s_c[j] = used ? ldcg(&st->coeff[j]) : 1.0;
-      }
-    }
-    __syncthreads();
-    const int nc = s_nc;
-    for (int s = 0; s < S; ++s) {
-      const double th = ldcg(&st->theta_mix[s]);
-      R* out = a.nin + (long)next * S * n + (long)s * n;
-      if (kp.vec4) {
-        const long n4 = n >> 2;
-        for (long p4 = tid; p4 < n4; p4 += nthreads) {
-          const long p0 = 4 * p4;
-          double v[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
-          for (int j = 0; j < nc; ++j) {
-            const long q = s_off[j] + (long)s * n;
-            R ni[4], ri[4];
-            load4(a.nin + q, p0, n, 1, ni);
-            load4(a.res + q, p0, n, 1, ri);
-            const double c = s_c[j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) v[i] += c * ((double)ni[i] + th * (double)ri[i]);
-          }
-          R o[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) o[i] = R(v[i]);
-          store4(out, p0, n, 1, o);
-        }
-      } else {
-        for (long p = tid; p < n; p += nthreads) {
-          double v = 0.0;
-          for (int j = 0; j < nc; ++j) {
-            const long q = s_off[j] + (long)s * n + p;
-            v += s_c[j] * ((double)__ldcg(a.nin + q) + th * (double)__ldcg(a.res + q));
-          }
-          out[p] = R(v);
-        }
-      }
+  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
+  __shared__ ScState s_st;
+  ScState* const ls = &s_st;
+  __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP];
+  __shared__ double s_prm[kMaxP], s_prr[kMaxP], s_pcol[kMaxP];
+  __shared__ int s_colof[kMaxP];
+  __shared__ int s_ok;
+  __shared__ double s_grow[kMaxP];
+  state_load(ls, st);
+  const int nv = 4 + I;  // per species: N, three dots, Gram row
+  const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
+  for (int v = wib; v < S * nv + vres; v += nwarps) {
+    double t;
+    if (v < S * nv) t = warp_sum_rows(a.part2 + (v / nv) * kNF + (v % nv), gridDim.x, kNPart);
+    else if (a.assemble_v) t = warp_sum_rows(a.part + kVresOff + (v - S * nv), kp.mu_blocks, kNPart);
+    else t = warp_sum_rows(a.vres_part + (v - S * nv), a.vres_blocks, kMaxS);
+    if (lane == 0) {
+      if (v < S * nv) red[(v / nv) * kNF + (v % nv)] = t;
+      else red_v[v - S * nv] = t;
     }
   }
-  MPDPFT_TSTAMP(6);
+  __syncthreads();
+  if (threadIdx.x < I) {  // Gram row summed over species
+    double t = 0.0;
+    for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
+    s_grow[threadIdx.x] = t;
+  }
+  __syncthreads();
+  // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): the Gram matrix,
+  // last row/column new, the rest shifted from before (warp 1) ...
+  if (pulay_now && wib == 1) {
+    const int shift = (hist + 1 > kp.scope) ? 1 : 0;
+    for (int e = lane; e < I * I; e += 32) {
+      const int i = e / I, j = e % I;
+      double v;
+      if (i == I - 1) v = s_grow[j];
+      else if (j == I - 1) v = s_grow[i];
+      else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
+      s_G[e] = v;
+    }
+    __syncwarp();
+    for (int e = lane; e < I * I; e += 32) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
+    if (lane == 0) ls->hist = I;
+  }
+  // ... while thread 0 does the scalar bookkeeping
+  if (threadIdx.x == 0) {
+    if (vres) {
+      double w = 0.0;
+      for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red_v[s] / (double)n));
+      ls->v_res = w;
+    }
+    const int sc = ls->sc_count;
+    double tot = 0.0;
+    for (int s = 0; s < S; ++s) {
+      ls->mu[s] = s_mu_rep[s];
+      ls->ab[s] = red[s * kNF] * kp.geom.dvol;
+      if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
+      tot += ls->ab[s];
+    }
+    if (a.mode == 1) {
+      ls->status_bits |= ls->iter_bits;
+      ls->mu_passes_total += ls->mu_passes;
+    } else {
+      // CheckConvergence (mpDPFT.cpp:4759-4782)
+      const double mp = 100.0 * 1.0e-16;
+      if (sc > 0) {
+        double cc = 0.0, maxtest = 0.0;
+        for (int s = 0; s < S; ++s) {
+          double oi = red[s * kNF + 1], oo = red[s * kNF + 2], ii = red[s * kNF + 3];
+          double rd = (oo + ii > 1.0e-12) ? 1.0 - 2.0 * oi / (oo + ii) : 0.0;
+          double t = rd * ls->ab[s] / tot;
+          if (t > maxtest) { maxtest = t; cc = maxtest; }
+        }
+        ls->cc = cc;
+        double dab = 0.0, dmu = 0.0;
+        for (int s = 0; s < S; ++s) {
+          dab += (ls->ab[s] - ls->old_ab[s]) * (ls->ab[s] - ls->old_ab[s]);
+          dmu += (ls->mu[s] - ls->old_mu[s]) * (ls->mu[s] - ls->old_mu[s]);
+        }
+        int steady = (cc < mp && sqrt(dab) < mp && sqrt(dmu) < mp) ? 1 : 0;
+        double avth = 0.0;
+        for (int s = 0; s < S; ++s) avth += ls->theta[s] / (double)S;
+        bool vok = !(kp.pot_tol > 0.0) || ls->v_res <= kp.pot_tol;
+        if ((tot > mp || (tot <= mp && (double)sc * avth > 1.0)) && kp.sc_criterion >= 0.0 &&
+            (cc < kp.sc_criterion || steady) && vok)
+          ls->exit_count++;
+        else
+          ls->exit_count = 0;
+        if (ls->exit_count >= 3) ls->exit_loop = 1;
+      } else {
+        ls->cc = 1.2345678901234567890;
+      }
+      if (sc == kp.max_sc) ls->exit_loop = 1;  // Intercept (:4866)
+    }
+  }
+  __syncthreads();
+  // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
+  // reference, mpDPFT.cpp:5089-5107)
+  if (a.mode != 1 && pulay_now && wib == 0) {
+    bool ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
+    double test = ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
+    if (lane == 0) s_ok = ok && test <= 1.0e-8;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int sc = ls->sc_count;
+    if (a.mode != 1) {
+      int used = 0;
+      if (pulay_now) {
+        if (s_ok) {
+          double x[kMaxP], A = 0.0;
+          for (int i = 0; i < I; ++i) {
+            x[i] = 0.0;
+            for (int k2 = 0; k2 < I; ++k2) x[i] += s_inv[i * I + k2];
+            A += x[i];
+          }
+          for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
+          used = 1;
+        }
+        if (!used) ls->iter_bits |= kBitPulay;
+      }
+      ls->pulay_used = used;
+      ls->ncoeff = used ? I : 0;
+      for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
+      // InjectSchedule (mpDPFT.cpp:5229-5315)
+      if (kp.schedule == 5) {
+        for (int s = 0; s < S; ++s) {
+          double th = ls->theta[s] * (ls->cc < ls->old_cc ? 1.1 : 0.5);
+          th = fmin(0.8, th);
+          th = fmax(10.0 / (double)kp.max_sc, th);
+          ls->theta[s] = th;
+        }
+      } else if (kp.schedule == 9) {
+        for (int s = 0; s < S; ++s)
+          if (ls->theta[s] < 0.2)
+            ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
+      }
+      if (a.log && sc < a.log_cap) {
+        mpdpft_iter_log& L = a.log[sc];
+        L.sc_count = sc;
+        L.mu_trials = ls->mu_passes;
+        L.pulay_used = used;
+        L.status_bits = ls->iter_bits;
+        L.cc = ls->cc;
+        L.v_residual = ls->v_res;
+        for (int s = 0; s < kMaxS; ++s) {
+          L.mu[s] = s < S ? ls->mu[s] : 0.0;
+          L.abundance[s] = s < S ? ls->ab[s] : 0.0;
+          L.theta[s] = s < S ? ls->theta_mix[s] : 0.0;
+        }
+        L.ms = 0.0;
+      }
+      ls->status_bits |= ls->iter_bits;
+      ls->mu_passes_total += ls->mu_passes;
+      // StoreCurrentIteration of the next iteration; PrepareNextIteration
+      for (int s = 0; s < S; ++s) { ls->old_mu[s] = ls->mu[s]; ls->old_ab[s] = ls->ab[s]; }
+      ls->old_cc = ls->cc;
+      if (sc > 0) ls->inc_v = fmin(1.0, ls->inc_v + kp.inc_v0);  // (:4833)
+      ls->mix_src = cur;
+      ls->slot = next;
+      ls->sc_count = sc + 1;
+    }
+  }
+  __syncthreads();
+  state_store(st, ls);
+  if (threadIdx.x == 0) {
+    st->k2_done = 0u;
+    st->tphase[4] = globaltimer();
+  }
+}
+
+// ---------------------------------------------------------- mix kernel --
+// The mixed density n = sum_j c_j (n_in,j + theta r_j) (Pulay) or
+// n_in + theta r (linear) into the next ring slot (AdmixDensities,
+// mpDPFT.cpp:4946-4955 / :4987).
+template <typename R>
+__global__ void __launch_bounds__(kDensThreads) sc_mix_kernel(StepArgs<R> a) {
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  __shared__ long s_off[kMaxP];
+  __shared__ double s_c[kMaxP];
+  __shared__ int s_nc;
+  if (a.mode == 0 && !ldcg(&st->iter_active)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[5] = globaltimer();
+  const int ring = kp.ring;
+  const int cur = ldcg(&st->mix_src), next = ldcg(&st->slot);
+  if (threadIdx.x == 0) {
+    const int used = ldcg(&st->pulay_used);
+    const int nc = used ? ldcg(&st->ncoeff) : 1;
+    s_nc = nc;
+    for (int j = 0; j < nc; ++j) {
+      const int slot = (cur - (nc - 1) + j + ring) % ring;
+      s_off[j] = (long)slot * S * n;
+      s_c[j] = used ? ldcg(&st->coeff[j]) : 1.0;
+    }
+  }
+  __syncthreads();
+  const int nc = s_nc;
+  const long gstride = (long)gridDim.x * blockDim.x;
+  for (int s = 0; s < S; ++s) {
+    const double th = ldcg(&st->theta_mix[s]);
+    R* out = a.nin + (long)next * S * n + (long)s * n;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += gstride) {
+      const long p0 = 4 * q;
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+      for (int j = 0; j < nc; ++j) {
+        const long o = s_off[j] + (long)s * n;
+        R ni[4], ri[4];
+        load4(a.nin + o, p0, n, kp.vec4, ni);
+        load4(a.res + o, p0, n, kp.vec4, ri);
+        const double c = s_c[j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] += c * ((double)ni[i] + th * (double)ri[i]);
+      }
+      R o4[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) o4[i] = R(v[i]);
+      store4(out, p0, n, kp.vec4, o4);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[6] = globaltimer();
 }
 
 }  // namespace mpdpft

@@ -19,7 +19,8 @@ namespace mpdpft {
 
 constexpr int kStepThreads = 512;
 constexpr int kStepWarps = kStepThreads / 32;
-constexpr int kSegPts = 128;          // points of one warp segment (4 per lane)
+constexpr int kSegPts = 128;          // points of one warp step (4 per lane)
+constexpr int kDensThreads = 256;     // density and mixing kernels
 constexpr int kMuAcc = kMuCand + 1;  // candidate sums + dN/dmu at candidate 0
 constexpr int kNF = 4 + kMaxP;        // per-species sums of the density/Gram pass
 // per-block partial sums: [0, kVresOff) the mu-pass or density-pass sums,
@@ -45,13 +46,9 @@ struct KParams {
   int schedule;
   double pot_tol;
   double inc_v0;
-  // Grid sweeps visit warp segments of kSegPts consecutive points in the
-  // order seg = k * seg_mul mod nseg (seg_mul coprime to nseg), which spreads
-  // the few costly segments (inside the classically allowed region) evenly
-  // over the warps.
-  long nseg;
-  long seg_mul;
-  int vec4;  // n % 4 == 0: a lane loads its 4 points as one vector
+  long chunk;     // points per warp in the mu kernel's sweeps (multiple of kSegPts)
+  int mu_blocks;  // grid of the mu kernel (rows of its partial sums)
+  int vec4;       // n % 4 == 0: a lane loads 4 points as one vector
 };
 
 struct MuState {
@@ -88,6 +85,9 @@ struct ScState {
   MuState ms[kMaxS];
   unsigned bar_count, bar_gen;
   int abort;
+  // not part of the state copies (written by one kernel, read by the next)
+  int iter_active;    // 0: the loop had already exited when this iteration began
+  unsigned k2_done;   // blocks of the density kernel that have finished
   unsigned long long tphase[8];  // %globaltimer at phase boundaries (block 0)
 };
 
@@ -102,15 +102,14 @@ struct StepArgs {
   const R* vh;    // [S][n] Coulomb terms or null
   R* nin;         // [ring][S][n]
   R* res;         // [ring][S][n]
-  double* part;   // [gridDim.x][kNPart]
-  // active-segment lists of the mu search (functionals that vanish for
-  // mu <= V): a full sweep records the segments holding any point below the
-  // pass's largest candidate; later passes whose candidates stay below that
-  // visit only those
-  int* bcount;  // [kMaxS][gridDim.x] active segments found by each block
-  int* wlist;   // [kMaxS][warps][wmax] their indices, per warp
-  int* slist;   // [kMaxS][nseg] compacted list (block order, then warp order)
-  int wmax;     // ceil(nseg / warps)
+  double* part;   // [mu_blocks][kNPart]: mu-pass sums, V-update residual
+  double* part2;  // [density blocks][kNPart]: density-pass sums
+  // active-point lists of the mu search (functionals that vanish for
+  // mu <= V): the points below the largest candidate of the pass that built
+  // the list, in grid order; later passes whose candidates stay below that
+  // bound visit only those
+  int* bcount;  // [kMaxS][mu_blocks] active points found by each block
+  int* plist;   // [kMaxS][n]
   const double* vres_part;  // partials of |V_new - V_old|^2 from an external
   int vres_blocks;          //   V assembly (when assemble_v == 0), or null
   mpdpft_iter_log* log;
