@@ -42,27 +42,24 @@ struct Geom {
 // Multiplicity of a periodic point in the reference's (s+1)^D storage: plane
 // 0 of every axis is stored twice (mpDPFT.cpp:863), so VecMult over that
 // storage (mpDPFT.cpp:7103-7107) counts it twice.
+// Grid indices use 32-bit arithmetic: grids hold at most 2^30 points.
 __device__ __forceinline__ double ref_multiplicity(long p, int s, int dim) {
-  int k = (int)(p % s);
-  long q = p / s;
-  int j = (int)(q % s);
+  const unsigned us = (unsigned)s, pp = (unsigned)p;
+  const unsigned q = pp / us, k = pp - q * us;
+  const unsigned i = q / us, j = q - i * us;
   double w = (k == 0 ? 2.0 : 1.0) * (j == 0 ? 2.0 : 1.0);
-  if (dim == 3) {
-    int i = (int)(q / s);
-    w *= (i == 0 ? 2.0 : 1.0);
-  }
+  if (dim == 3) w *= (i == 0 ? 2.0 : 1.0);
   return w;
 }
 
 __device__ __forceinline__ void point_coords(long p, const Geom& g, double& x, double& y, double& z) {
-  int k = (int)(p % g.s);
-  long q = p / g.s;
+  const unsigned us = (unsigned)g.s, pp = (unsigned)p;
+  const unsigned q = pp / us, k = pp - q * us;
   if (g.dim == 3) {
-    int j = (int)(q % g.s), i = (int)(q / g.s);
+    const unsigned i = q / us, j = q - i * us;
     x = -0.5 * g.L + g.dx * i; y = -0.5 * g.L + g.dx * j; z = -0.5 * g.L + g.dx * k;
   } else {
-    int i = (int)q;
-    x = -0.5 * g.L + g.dx * i; y = -0.5 * g.L + g.dx * k; z = 0.0;
+    x = -0.5 * g.L + g.dx * q; y = -0.5 * g.L + g.dx * k; z = 0.0;
   }
 }
 

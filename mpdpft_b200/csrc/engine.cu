@@ -253,6 +253,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   if ((st = alloc(&d_nin, field * S * ring))) return st;
   if ((st = alloc(&d_res, field * S * ring))) return st;
   if ((st = alloc(&d_tmp, field * S))) return st;
+  if ((st = alloc(&d_cur, field * S))) return st;
   if (gradient) {
     if ((st = alloc(&d_lap, field * S))) return st;
     if ((st = alloc(&d_g2, field * S))) return st;
@@ -306,6 +307,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   CU(cudaMemsetAsync(d_V, 0, field * S, stream));
   CU(cudaMemsetAsync(d_vext, 0, field * S, stream));
   CU(cudaMemsetAsync(d_nin, 0, field * S * ring, stream));
+  CU(cudaMemsetAsync(d_cur, 0, field * S, stream));
   CU(cudaMemsetAsync(d_res, 0, field * S * ring, stream));
   CU(cudaMemsetAsync(d_log, 0, sizeof(mpdpft_iter_log) * log_cap, stream));
   return reset_state();
@@ -383,6 +385,7 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.vh = has_coulomb ? (const R*)d_vh : nullptr;
   a.nin = (R*)d_nin;
   a.res = (R*)d_res;
+  a.cur_copy = (R*)d_cur;
   a.part = d_part;
   a.part2 = d_part2;
   a.bcount = d_bcount;

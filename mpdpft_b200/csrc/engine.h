@@ -38,6 +38,7 @@ struct Ctx {
   void* d_nin = nullptr;   // [ring][S][n]
   void* d_res = nullptr;   // [ring][S][n]
   void* d_tmp = nullptr;   // [S][n]
+  void* d_cur = nullptr;   // [S][n] copy of the current input densities
   void* d_lap = nullptr;   // [S][n]
   void* d_g2 = nullptr;    // [S][n]
   void* d_vh = nullptr;    // [S][n] Coulomb terms of V

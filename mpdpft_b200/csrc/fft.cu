@@ -100,7 +100,7 @@ __device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
 
 // ---------------------------------------------------------- prologues ----
 enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
-enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3 };
+enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3, EPI_SCALE = 4 };
 enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3 };
 
 template <typename R>
@@ -149,9 +149,16 @@ __device__ __forceinline__ R z_input(const ZArgs<R>& a, long p, double shift) {
     double px, py, pz;
     point_coords(p, a.g, px, py, pz);
     const double r = sqrt(px * px + py * py + pz * pz);
-    double f = (double)x - shift;
-    if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
-    x = R(f);
+    if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the factor in FP32
+      float f = x - float(shift);
+      const float dr = float(r - a.taper_r0);
+      if (r > a.taper_r0) f *= expf(float(a.taper_a) * dr * dr);
+      x = R(f);
+    } else {
+      double f = (double)x - shift;
+      if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
+      x = R(f);
+    }
   }
   return x;
 }
@@ -242,12 +249,19 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
 template <typename R>
 __device__ __forceinline__ R z_output(const ZArgs<R>& a, long p, R v, double f0) {
   if (a.epi == EPI_POS) return v > R(0) ? v : R(0);
+  if (a.epi == EPI_SCALE) return R(a.coul_coef * (double)v);
   if (a.epi == EPI_COULOMB) {  // mpDPFT.cpp:2704-2711
     double x, y, z;
     point_coords(p, a.g, x, y, z);
-    const double r = sqrt(x * x + y * y + z * z);
-    const double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
-    return R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
+    if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the term in FP32
+      const float r = sqrtf(float(x * x + y * y + z * z));
+      const float zf = r > 1.0e-10f ? float(kPi) * erff(0.5f * r) / r : float(1.7724538509055159);
+      return R(float(a.coul_coef) * (v + float(f0 / (4.0 * kPi * kPi)) * zf));
+    } else {
+      const double r = sqrt(x * x + y * y + z * z);
+      const double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
+      return R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
+    }
   }
   return v;
 }
@@ -263,9 +277,15 @@ __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
   const long row0 = (long)blockIdx.x * zl;
   const int s = a.g.s;
   double f0 = 0.0;
-  if (a.epi == EPI_COULOMB) {
+  if (a.epi == EPI_COULOMB) {  // f0 = dvol * sum of the R2C pass's block sums (same order in every block)
+    __shared__ double s_f0[kFftThreads / 32];
     double t = 0.0;
-    for (int b = 0; b < a.f0_blocks; ++b) t += a.f0_part[b];
+    for (int b = threadIdx.x; b < a.f0_blocks; b += blockDim.x) t += a.f0_part[b];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) s_f0[threadIdx.x >> 5] = t;
+    __syncthreads();
+    t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_f0[w];
     f0 = t * a.g.dvol;
   }
   if constexpr (NC > 0) {
@@ -1065,8 +1085,7 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
   if (mul == MUL_COULOMB_REG)
     return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_COULOMB, out, nullptr, 4.0 * kPi * coef);
   // truncated kernel: out = 4 pi coef x
-  if ((st = launch_z_c2r<R>(c, &f.spec[0], 1, EPI_STORE, (R*)f.rtmp, nullptr, 0.0))) return st;
-  return c.scale_copy(f.rtmp, out, 4.0 * kPi * coef);
+  return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_SCALE, out, nullptr, 4.0 * kPi * coef);
 }
 
 
@@ -1092,8 +1111,12 @@ static int coulomb_terms(Ctx& c, const R* dens, R* out) {
     if (t == MPDPFT_INT_HARTREE) {
       for (int s = 0; s < S; ++s) {
         double one = 1.0;
-        if ((st = coulomb_into<R>(c, dens + (long)s * n, 1, &one, (R*)c.fft->rtmp, c.P.gamma_h))) return st;
-        if ((st = c.axpy(c.fft->rtmp, out + (long)s * n, 1.0, touched[s]))) return st;
+        if (!touched[s]) {  // first term of species s: straight into its output
+          if ((st = coulomb_into<R>(c, dens + (long)s * n, 1, &one, out + (long)s * n, c.P.gamma_h))) return st;
+        } else {
+          if ((st = coulomb_into<R>(c, dens + (long)s * n, 1, &one, (R*)c.fft->rtmp, c.P.gamma_h))) return st;
+          if ((st = c.axpy(c.fft->rtmp, out + (long)s * n, 1.0, 1))) return st;
+        }
         touched[s] = 1;
       }
     } else if (t == MPDPFT_INT_HARTREE_INTER) {
@@ -1162,11 +1185,10 @@ static int fft_terms_impl(Ctx& c) {
   FftPlan& F = *c.fft;
   int st;
   const long n = c.geom.n;
-  // current input densities live in ring slot state.slot; the slot index is
-  // only known on the device, so the Coulomb transform reads them through a
-  // gather into rtmp-sized staging: use the kernel-side slot via a copy.
-  const R* dens = (const R*)c.d_tmp;
-  if ((st = c.copy_current_density())) return st;
+  // the current input densities: the ring slot state.slot is only known on
+  // the device, so the kernels that write a new input density also store a
+  // copy at the fixed address d_cur
+  const R* dens = (const R*)c.d_cur;
   if (c.has_coulomb) {
     if ((st = coulomb_terms<R>(c, dens, (R*)c.d_vh))) return st;
   }

@@ -634,6 +634,7 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
       }
       if (a.mode == 1) {
         store4(nin + so, p0, n, kp.vec4, no4);
+        store4(a.cur_copy + so, p0, n, kp.vec4, no4);
         continue;
       }
       R ni4[4], r4[4];
@@ -897,6 +898,7 @@ __global__ void __launch_bounds__(kDensThreads) sc_mix_kernel(StepArgs<R> a) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) o4[i] = R(v[i]);
       store4(out, p0, n, kp.vec4, o4);
+      store4(a.cur_copy + (long)s * n, p0, n, kp.vec4, o4);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[6] = globaltimer();

@@ -102,6 +102,7 @@ struct StepArgs {
   const R* vh;    // [S][n] Coulomb terms or null
   R* nin;         // [ring][S][n]
   R* res;         // [ring][S][n]
+  R* cur_copy;    // [S][n] copy of the current input densities (fixed address)
   double* part;   // [mu_blocks][kNPart]: mu-pass sums, V-update residual
   double* part2;  // [density blocks][kNPart]: density-pass sums
   // active-point lists of the mu search (functionals that vanish for
