@@ -122,6 +122,25 @@ __global__ void k_density(Geom g, DensParams d, double mu, const R* V, const R* 
     out[p] = density_at<R>(d, R(mu) - V[p], lap ? lap[p] : R(0), g2 ? g2[p] : R(0));
 }
 
+// The mu kernel (which 0) and the density kernel for Pulay windows <= 5
+// (which 1) or up to kMaxP (which 2), of functional kind fk.
+template <typename R>
+static const void* sc_kernel_ptr(int which, int fk) {
+  if (which == 0) {
+    if (fk == 1) return (const void*)sc_mu_kernel<R, 1>;
+    if (fk == 2) return (const void*)sc_mu_kernel<R, 2>;
+    return (const void*)sc_mu_kernel<R, 0>;
+  }
+  if (which == 1) {  // Pulay window <= 5
+    if (fk == 1) return (const void*)sc_density_kernel<R, 1, 5>;
+    if (fk == 2) return (const void*)sc_density_kernel<R, 2, 5>;
+    return (const void*)sc_density_kernel<R, 0, 5>;
+  }
+  if (fk == 1) return (const void*)sc_density_kernel<R, 1, kMaxP>;
+  if (fk == 2) return (const void*)sc_density_kernel<R, 2, kMaxP>;
+  return (const void*)sc_density_kernel<R, 0, kMaxP>;
+}
+
 // ---------------------------------------------------------- the context --
 Ctx::~Ctx() { release(); }
 
@@ -276,10 +295,12 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   };
   const bool f64 = P.precision == MPDPFT_FP64;
   int occ_mu = 0, occ_dens = 0, occ_mix = 0;
-  if ((st = occupancy(f64 ? (const void*)sc_mu_kernel<double> : (const void*)sc_mu_kernel<float>, kStepThreads, &occ_mu)))
+  fk = functional_kind(P.density_expression, P.dim);
+  if ((st = occupancy(f64 ? sc_kernel_ptr<double>(0, fk) : sc_kernel_ptr<float>(0, fk), kStepThreads, &occ_mu)))
     return st;
-  if ((st = occupancy(f64 ? (const void*)sc_density_kernel<double> : (const void*)sc_density_kernel<float>,
-                      kDensThreads, &occ_dens)))
+  dens_which = (P.mixer ? P.pulay_scope : 1) <= 5 ? 1 : 2;
+  if ((st = occupancy(f64 ? sc_kernel_ptr<double>(dens_which, fk) : sc_kernel_ptr<float>(dens_which, fk), kDensThreads,
+                      &occ_dens)))
     return st;
   if ((st = occupancy(f64 ? (const void*)sc_mix_kernel<double> : (const void*)sc_mix_kernel<float>, kDensThreads,
                       &occ_mix)))
@@ -399,39 +420,45 @@ StepArgs<R> Ctx::step_args(int mode) {
   return a;
 }
 
-// One SC iteration's kernels (mode 0), the densities of the current V
-// (mode 1: mu kernel + density kernel) or the admix step alone (mode 2:
-// density kernel + mixing kernel).
-int Ctx::launch_step(int mode) {
-  cudaError_t e;
-  const bool f64 = rsize == sizeof(double);
+template <typename R>
+static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk) {
+  StepArgs<R> args = c.step_args<R>(mode);
+  void* params[] = {&args};
   if (mode != 2) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
-    cfg.gridDim = dim3(step_blocks);
+    cfg.gridDim = dim3(c.step_blocks);
     cfg.blockDim = dim3(kStepThreads);
     cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
+    cfg.stream = c.stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cnt[MPDPFT_STAGE_SC_STEP]++;
-    if (f64) e = cudaLaunchKernelEx(&cfg, sc_mu_kernel<double>, step_args<double>(mode));
-    else e = cudaLaunchKernelEx(&cfg, sc_mu_kernel<float>, step_args<float>(mode));
-    if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("sc_mu_kernel launch: ") + cudaGetErrorString(e));
+    c.cnt[MPDPFT_STAGE_SC_STEP]++;
+    cudaError_t e = cudaLaunchKernelExC(&cfg, sc_kernel_ptr<R>(0, fk), params);
+    if (e != cudaSuccess) return e;
   }
-  cnt[MPDPFT_STAGE_SC_STEP]++;
-  if (f64) sc_density_kernel<double><<<dens_blocks, kDensThreads, 0, stream>>>(step_args<double>(mode));
-  else sc_density_kernel<float><<<dens_blocks, kDensThreads, 0, stream>>>(step_args<float>(mode));
-  CU(cudaGetLastError());
+  c.cnt[MPDPFT_STAGE_SC_STEP]++;
+  cudaError_t e =
+      cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensThreads), params, 0, c.stream);
+  if (e != cudaSuccess) return e;
   if (mode != 1) {
-    cnt[MPDPFT_STAGE_SC_STEP]++;
-    if (f64) sc_mix_kernel<double><<<mix_blocks, kDensThreads, 0, stream>>>(step_args<double>(mode));
-    else sc_mix_kernel<float><<<mix_blocks, kDensThreads, 0, stream>>>(step_args<float>(mode));
-    CU(cudaGetLastError());
+    c.cnt[MPDPFT_STAGE_SC_STEP]++;
+    sc_mix_kernel<R><<<c.mix_blocks, kDensThreads, 0, c.stream>>>(args);
+    e = cudaGetLastError();
   }
+  return e;
+}
+
+// One SC iteration's kernels (mode 0), the densities of the current V
+// (mode 1: mu kernel + density kernel) or the admix step alone (mode 2:
+// density kernel + mixing kernel).
+int Ctx::launch_step(int mode) {
+  cudaError_t e = rsize == sizeof(double) ? launch_sc_kernels<double>(*this, mode, fk)
+                                          : launch_sc_kernels<float>(*this, mode, fk);
+  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("SC kernel launch: ") + cudaGetErrorString(e));
   return MPDPFT_OK;
 }
 

@@ -49,6 +49,8 @@ struct Ctx {
   mpdpft_iter_log* d_log = nullptr;
   int log_cap = 0;
   int step_blocks = 0;
+  int fk = 0;            // functional kind of the SC kernels (functional_kind)
+  int dens_which = 1;    // density kernel variant: 1 Pulay window <= 5, 2 up to kMaxP
   int dens_blocks = 0;   // grid of the density kernel
   int mix_blocks = 0;    // grid of the mixing kernel
   long chunk = kSegPts;  // points per warp in the mu kernel's list sweeps

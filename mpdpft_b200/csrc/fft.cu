@@ -690,6 +690,12 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
 // V assembly (UpdateV, mpDPFT.cpp:4815-4838) when Coulomb terms exist:
 // V_s = Vext_s + incV (vh_s + contact + Dirac); partial sums of |dV|^2 and
 // the maximum of V over the taper shell (DelField, mpDPFT.cpp:7253-7259).
+// |r - r0| < w from r^2, without the square root.
+__device__ __forceinline__ bool in_shell(double r2, double r0, double w) {
+  const double lo = r0 - w, hi = r0 + w;
+  return r2 < hi * hi && (lo <= 0.0 || r2 > lo * lo);
+}
+
 template <typename R>
 __global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const R* vh, const R* nin_ring, R* V,
                              double* vres_part, unsigned long long* vmax, double shell_r, double shell_w) {
@@ -706,7 +712,7 @@ __global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     double x, y, z;
     point_coords(p, kp.geom, x, y, z);
-    const bool shell = fabs(sqrt(x * x + y * y + z * z) - shell_r) < shell_w;
+    const bool shell = in_shell(x * x + y * y + z * z, shell_r, shell_w);
     for (int s = 0; s < S; ++s) {
       R vi = vh ? vh[(long)s * n + p] : R(0);
       if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];
@@ -750,7 +756,7 @@ __global__ void k_shell_max(Geom g, const R* f, unsigned long long* vmax, double
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x) {
     double x, y, z;
     point_coords(p, g, x, y, z);
-    if (fabs(sqrt(x * x + y * y + z * z) - shell_r) < shell_w) vm = fmax(vm, (double)f[p]);
+    if (in_shell(x * x + y * y + z * z, shell_r, shell_w)) vm = fmax(vm, (double)f[p]);
   }
   for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
   if ((threadIdx.x & 31) == 0 && vm > -1.0e300) atomicMax(vmax, ordered_bits(vm));

@@ -241,24 +241,35 @@ __device__ __forceinline__ double tf3_slope(const EvalK& k, double u) {
   return u > 0.0 ? 1.5 * k.ctf * u * r : 0.0;
 }
 
+// Functional kind, a template parameter of the kernels so that each
+// instantiation carries only its own evaluation code: 1 = 3D
+// gradient-corrected, 2 = 3D TF, 0 = any (density_at_d).
+inline int functional_kind(int expr, int dim) {
+  if (expr == MPDPFT_DENS_GRADIENT && dim == 3) return 1;
+  if (expr == MPDPFT_DENS_TF && dim == 3) return 2;
+  return 0;
+}
+
 // n at u = mu - V for one point.
+template <int FK>
 __device__ __forceinline__ double point_density(const DensParams& d, const EvalK& k, double u, double l, double g) {
-  if (k.fast == 1) return grad3_n(k, u, k.cg * l, k.cg2 * g);
-  if (k.fast == 2) return tf3_n(k, u);
-  return density_at_d(d, u, l, g);
+  if constexpr (FK == 1) return grad3_n(k, u, k.cg * l, k.cg2 * g);
+  else if constexpr (FK == 2) return tf3_n(k, u);
+  else return density_at_d(d, u, l, g);
 }
 
 // N(mu_c) contributions of one point for all candidates, and dN/dmu at
 // candidate 0.  Candidate slots at or beyond nc hold copies of candidate 0
 // in the fast forms (evaluated, never read).
+template <int FK>
 __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, const double* cmu, int nc, double v,
                                          double l, double g, double (&acc)[kMuAcc]) {
-  if (k.fast == 1) {
+  if constexpr (FK == 1) {
     const double A = k.cg * l, B = k.cg2 * g;
     acc[kMuCand] += grad3_slope(k, cmu[0] - v, A, B);
 #pragma unroll
     for (int c = 0; c < kMuCand; ++c) acc[c] += grad3_n(k, cmu[c] - v, A, B);
-  } else if (k.fast == 2) {
+  } else if constexpr (FK == 2) {
     acc[kMuCand] += tf3_slope(k, cmu[0] - v);
 #pragma unroll
     for (int c = 0; c < kMuCand; ++c) acc[c] += tf3_n(k, cmu[c] - v);
@@ -282,6 +293,46 @@ __device__ __forceinline__ double warp_sum_rows(const double* base, int nb, int 
   return warp_sum(t);
 }
 
+// Sums over nb per-block rows (row b of value v at
+// base[b * stride + (v / per) * pstride + v % per]) of nv values into
+// out[(v / per) * pstride + v % per], by all threads of the block with every
+// thread's loads in flight together (CH values at a time).
+__device__ inline void block_rows_sum(const double* base, int nb, int stride, int nv, int per, int pstride,
+                                      double* out) {
+  constexpr int CH = 8;
+  __shared__ double sh[32][CH];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = 0; c0 < nv; c0 += CH) {
+    double t[CH];
+    int off[CH];
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      t[u] = 0.0;
+      const int v = c0 + u < nv ? c0 + u : c0;
+      off[u] = (v / per) * pstride + v % per;
+    }
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      const double* row = base + (long)b * stride;
+#pragma unroll
+      for (int u = 0; u < CH; ++u) t[u] += __ldcg(row + off[u]);
+    }
+    __syncthreads();  // sh is free
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      const double x = warp_sum(t[u]);
+      if (lane == 0) sh[w][u] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < CH && c0 + (int)threadIdx.x < nv) {
+      double x = 0.0;
+      for (int i = 0; i < nw; ++i) x += sh[i][threadIdx.x];
+      const int v = c0 + threadIdx.x;
+      out[(v / per) * pstride + v % per] = x;
+    }
+  }
+  __syncthreads();
+}
+
 // Block-wide sums of two ints, returned to every thread.
 __device__ __forceinline__ void block_sum2(int& x, int& y) {
   __shared__ int sh[2][kStepWarps];
@@ -300,7 +351,7 @@ __device__ __forceinline__ void block_sum2(int& x, int& y) {
 // mode 0: UpdateV + mu search of one SC iteration.  mode 1: mu search of the
 // current V (GetDensities for the initial densities, mpDPFT.cpp:195, and the
 // standalone mu-search entry point).  Not launched in mode 2 (admix only).
-template <typename R>
+template <typename R, int FK>
 __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
@@ -510,7 +561,7 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
         const double v = (double)__ldcg(Vs + p);
         const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
         const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
-        mu_point(d, k, cmu, nc, v, l, g, acc);
+        mu_point<FK>(d, k, cmu, nc, v, l, g, acc);
       }
       block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
     }
@@ -555,8 +606,10 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
 // into the current ring slot instead; mode 2 (admix only) takes n_out from V.
 // The last block to finish runs phase D: CheckConvergence, Intercept, the
 // Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
-template <typename R>
-__global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a) {
+template <typename R, int FK, int PW>
+__global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R> a) {
+  // PW: the largest Pulay window this instantiation handles (<= kMaxP); a
+  // small window keeps the per-thread sums in few registers
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
@@ -591,82 +644,66 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
   __syncthreads();
   R* nin = a.nin + (long)cur * S * n;
   R* rcur = a.res + (long)cur * S * n;
-  const long ngroups = (n + 3) / 4;
   const long gstride = (long)gridDim.x * blockDim.x;
   for (int s = 0; s < S; ++s) {
-    double acc[kNF];
+    double acc[4 + PW];
 #pragma unroll
-    for (int j = 0; j < kNF; ++j) acc[j] = 0.0;
+    for (int j = 0; j < 4 + PW; ++j) acc[j] = 0.0;
     const DensParams d = kp.dens[s];
     const EvalK k = eval_constants(d);
     const double mus = s_mu[s];
     const long so = (long)s * n;
+    const R* Vs = a.V + so;
     const R* Ls = a.lap ? a.lap + so : nullptr;
     const R* Gs = a.g2 ? a.g2 + so : nullptr;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q - threadIdx.x < ngroups; q += gstride) {
-      // the whole warp runs every trip (the vote below needs all lanes)
-      const long p0 = 4 * q;
-      R v4[4];
-      load4(a.V + so, p0, n, kp.vec4, v4);
-      double nod[4] = {0.0, 0.0, 0.0, 0.0};
+    // one point per thread; every lane of a warp runs every trip (the vote
+    // below needs them all)
+    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += gstride) {
+      const long p = base + threadIdx.x;
+      const bool valid = p < n;
+      // issue the streaming loads first
+      const double v = valid ? (double)__ldcg(Vs + p) : 0.0;
+      R ni = R(0);
+      R rj[PW];
+      if (a.mode == 0 || a.mode == 2) {
+        ni = valid ? __ldcg(nin + so + p) : R(0);
+#pragma unroll
+        for (int j = 0; j < PW; ++j)
+          rj[j] = (j < I - 1 && valid) ? __ldcg(a.res + s_roff[j] + so + p) : R(0);
+      }
+      double nod = 0.0;
       if (a.mode == 2) {  // admix only: V holds the output densities
-#pragma unroll
-        for (int i = 0; i < 4; ++i) nod[i] = (double)v4[i];
+        nod = v;
       } else {
-        bool mine = !d.cut && p0 < n;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) mine |= (p0 + i < n) && (mus - (double)v4[i] > 0.0);
-        if (__any_sync(0xffffffffu, mine) && p0 < n) {
-          R l4[4] = {R(0), R(0), R(0), R(0)}, g4[4] = {R(0), R(0), R(0), R(0)};
-          if (Ls) load4(Ls, p0, n, kp.vec4, l4);
-          if (Gs) load4(Gs, p0, n, kp.vec4, g4);
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (p0 + i < n) nod[i] = point_density(d, k, mus - (double)v4[i], (double)l4[i], (double)g4[i]);
+        const bool mine = valid && (!d.cut || mus - v > 0.0);
+        if (__any_sync(0xffffffffu, mine) && mine) {
+          const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
+          const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
+          nod = point_density<FK>(d, k, mus - v, l, g);
         }
       }
-      if (p0 >= n) continue;
-      R no4[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        no4[i] = R(nod[i]);
-        acc[0] += nod[i];  // zero beyond n
-      }
+      if (!valid) continue;
+      const R no = R(nod);
+      acc[0] += nod;
       if (a.mode == 1) {
-        store4(nin + so, p0, n, kp.vec4, no4);
-        store4(a.cur_copy + so, p0, n, kp.vec4, no4);
+        nin[so + p] = no;
+        a.cur_copy[so + p] = no;
         continue;
       }
-      R ni4[4], r4[4];
-      load4(nin + so, p0, n, kp.vec4, ni4);
-      double w4[4], wr4[4], dr4[4];
-      ref_weights4(p0, kp.geom.s, kp.geom.dim, w4);
+      const R r = no - ni;
+      rcur[so + p] = r;
+      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
+      const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
+      acc[1] += w * dno * dni;
+      acc[2] += w * dno * dno;
+      acc[3] += w * dni * dni;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        r4[i] = no4[i] - ni4[i];
-        const double w = (p0 + i < n) ? w4[i] : 0.0;
-        const double dno = (double)no4[i], dni = (double)ni4[i];
-        dr4[i] = (double)r4[i];
-        wr4[i] = w * dr4[i];
-        acc[1] += w * dno * dni;
-        acc[2] += w * dno * dno;
-        acc[3] += w * dni * dni;
-      }
-      store4(rcur + so, p0, n, kp.vec4, r4);
-#pragma unroll
-      for (int j = 0; j < kMaxP; ++j) {
-        if (j < I - 1) {
-          R rj4[4];
-          load4(a.res + s_roff[j] + so, p0, n, kp.vec4, rj4);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * (double)rj4[i];
-        } else if (j == I - 1) {
-#pragma unroll
-          for (int i = 0; i < 4; ++i) acc[4 + j] += wr4[i] * dr4[i];
-        }
+      for (int j = 0; j < PW; ++j) {
+        if (j < I - 1) acc[4 + j] += wr * (double)rj[j];
+        else if (j == I - 1) acc[4 + j] += wr * dr;
       }
     }
-    block_reduce_store<kNF>(acc, a.part2 + (long)blockIdx.x * kNPart + s * kNF);
+    block_reduce_store<4 + PW>(acc, a.part2 + (long)blockIdx.x * kNPart + s * kNF);
   }
   // the last block to finish takes phase D
   __threadfence();
@@ -683,31 +720,28 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
   __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP];
   __shared__ double s_prm[kMaxP], s_prr[kMaxP], s_pcol[kMaxP];
   __shared__ int s_colof[kMaxP];
-  __shared__ int s_ok;
   __shared__ double s_grow[kMaxP];
+  __shared__ int s_pbits;
   state_load(ls, st);
+  if (threadIdx.x == 0) s_pbits = 0;
   const int nv = 4 + I;  // per species: N, three dots, Gram row
   const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
-  for (int v = wib; v < S * nv + vres; v += nwarps) {
-    double t;
-    if (v < S * nv) t = warp_sum_rows(a.part2 + (v / nv) * kNF + (v % nv), gridDim.x, kNPart);
-    else if (a.assemble_v) t = warp_sum_rows(a.part + kVresOff + (v - S * nv), kp.mu_blocks, kNPart);
-    else t = warp_sum_rows(a.vres_part + (v - S * nv), a.vres_blocks, kMaxS);
-    if (lane == 0) {
-      if (v < S * nv) red[(v / nv) * kNF + (v % nv)] = t;
-      else red_v[v - S * nv] = t;
-    }
+  block_rows_sum(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red);
+  if (vres) {
+    if (a.assemble_v) block_rows_sum(a.part + kVresOff, kp.mu_blocks, kNPart, S, S, 0, red_v);
+    else block_rows_sum(a.vres_part, a.vres_blocks, kMaxS, S, S, 0, red_v);
   }
-  __syncthreads();
   if (threadIdx.x < I) {  // Gram row summed over species
     double t = 0.0;
     for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
     s_grow[threadIdx.x] = t;
   }
   __syncthreads();
-  // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167): the Gram matrix,
-  // last row/column new, the rest shifted from before (warp 1) ...
-  if (pulay_now && wib == 1) {
+  // AdmixDensities / PulayMixer (mpDPFT.cpp:4921-5167) on warp 0: the Gram
+  // matrix (last row/column new, the rest shifted from before), its inverse
+  // (FullPivHouseholderQR + validation in the reference, :5089-5107) and the
+  // coefficients c = G^{-1} 1 / (1^T G^{-1} 1) ...
+  if (a.mode != 1 && pulay_now && wib == 0) {
     const int shift = (hist + 1 > kp.scope) ? 1 : 0;
     for (int e = lane; e < I * I; e += 32) {
       const int i = e / I, j = e % I;
@@ -719,10 +753,30 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
     }
     __syncwarp();
     for (int e = lane; e < I * I; e += 32) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
-    if (lane == 0) ls->hist = I;
+    const bool inv_ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
+    const double test = inv_ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
+    const bool used = inv_ok && test <= 1.0e-8;
+    if (used && lane < I) {  // row sums of the inverse
+      double x = 0.0;
+      for (int k2 = 0; k2 < I; ++k2) x += s_inv[lane * I + k2];
+      s_prm[lane] = x;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      ls->hist = I;
+      if (used) {
+        double A = 0.0;
+        for (int i = 0; i < I; ++i) A += s_prm[i];
+        for (int i = 0; i < I; ++i) ls->coeff[i] = s_prm[i] / A;
+      } else {
+        s_pbits = kBitPulay;
+      }
+      ls->pulay_used = used ? 1 : 0;
+      ls->ncoeff = used ? I : 0;
+    }
   }
-  // ... while thread 0 does the scalar bookkeeping
-  if (threadIdx.x == 0) {
+  // ... while warp 1 does CheckConvergence and Intercept
+  if (threadIdx.x == 32) {
     if (vres) {
       double w = 0.0;
       for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red_v[s] / (double)n));
@@ -736,10 +790,7 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
       if (!isfinite(ls->ab[s])) ls->iter_bits |= kBitNonfinite;
       tot += ls->ab[s];
     }
-    if (a.mode == 1) {
-      ls->status_bits |= ls->iter_bits;
-      ls->mu_passes_total += ls->mu_passes;
-    } else {
+    if (a.mode != 1) {
       // CheckConvergence (mpDPFT.cpp:4759-4782)
       const double mp = 100.0 * 1.0e-16;
       if (sc > 0) {
@@ -773,33 +824,15 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
     }
   }
   __syncthreads();
-  // the small inverse on warp 0 (FullPivHouseholderQR + validation in the
-  // reference, mpDPFT.cpp:5089-5107)
-  if (a.mode != 1 && pulay_now && wib == 0) {
-    bool ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
-    double test = ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
-    if (lane == 0) s_ok = ok && test <= 1.0e-8;
-  }
-  __syncthreads();
   if (threadIdx.x == 0) {
     const int sc = ls->sc_count;
-    if (a.mode != 1) {
-      int used = 0;
-      if (pulay_now) {
-        if (s_ok) {
-          double x[kMaxP], A = 0.0;
-          for (int i = 0; i < I; ++i) {
-            x[i] = 0.0;
-            for (int k2 = 0; k2 < I; ++k2) x[i] += s_inv[i * I + k2];
-            A += x[i];
-          }
-          for (int i = 0; i < I; ++i) ls->coeff[i] = x[i] / A;
-          used = 1;
-        }
-        if (!used) ls->iter_bits |= kBitPulay;
-      }
-      ls->pulay_used = used;
-      ls->ncoeff = used ? I : 0;
+    if (a.mode == 1) {
+      ls->status_bits |= ls->iter_bits;
+      ls->mu_passes_total += ls->mu_passes;
+    } else {
+      const int used = pulay_now ? ls->pulay_used : 0;
+      if (!pulay_now) { ls->pulay_used = 0; ls->ncoeff = 0; }
+      ls->iter_bits |= s_pbits;
       for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
       // InjectSchedule (mpDPFT.cpp:5229-5315)
       if (kp.schedule == 5) {
@@ -853,7 +886,7 @@ __global__ void __launch_bounds__(kDensThreads) sc_density_kernel(StepArgs<R> a)
 // n_in + theta r (linear) into the next ring slot (AdmixDensities,
 // mpDPFT.cpp:4946-4955 / :4987).
 template <typename R>
-__global__ void __launch_bounds__(kDensThreads) sc_mix_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
