@@ -86,6 +86,8 @@ struct FftPlan {
   double* vres_part = nullptr;         // V assembly |dV|^2 partials
   int vblocks = 0;
   void* cbuf = nullptr;    // complex s^D field for the fftParallel op
+  int zparts = 0;          // block sums in zpart written by the last forward pass
+  bool plane = false;      // 3D transforms by x-planes (k_plane_fwd / k_plane_inv)
 };
 
 // --------------------------------------------------- ordered max of doubles --
@@ -129,12 +131,33 @@ struct ZArgs {
   double coul_coef;               // Coulomb epilogue: out = coef (x + f0 erf(r/2)/(4 pi r))
   const double* f0_part;          // Z-pass partials giving f0 = dvol * sum(input)
   int f0_blocks;
+  // plane kernels
+  const typename Cx<R>::T* tw_s;  // length-s table for the y transforms
+  int* err;                       // raised when a bulk copy does not complete
 };
 
 // R2C along the contiguous axis.  Block = zl rows; each row of s reals is
 // read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
 // into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
 // Input value of the R2C pass at element p (prologue: taper or charge sum).
+// DelField boundary taper (mpDPFT.cpp:7251-7264) of value x at point p.
+template <typename R>
+__device__ __forceinline__ R taper_value(const ZArgs<R>& a, long p, R x, double shift) {
+  double px, py, pz;
+  point_coords(p, a.g, px, py, pz);
+  const double r = sqrt(px * px + py * py + pz * pz);
+  if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the factor in FP32
+    float f = x - float(shift);
+    const float dr = float(r - a.taper_r0);
+    if (r > a.taper_r0) f *= expf(float(a.taper_a) * dr * dr);
+    return R(f);
+  } else {
+    double f = (double)x - shift;
+    if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
+    return R(f);
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ R z_input(const ZArgs<R>& a, long p, double shift) {
   R x;
@@ -145,21 +168,7 @@ __device__ __forceinline__ R z_input(const ZArgs<R>& a, long p, double shift) {
   } else {
     x = a.in[p];
   }
-  if (a.pro == PRO_TAPER) {  // DelField boundary taper (mpDPFT.cpp:7251-7264)
-    double px, py, pz;
-    point_coords(p, a.g, px, py, pz);
-    const double r = sqrt(px * px + py * py + pz * pz);
-    if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the factor in FP32
-      float f = x - float(shift);
-      const float dr = float(r - a.taper_r0);
-      if (r > a.taper_r0) f *= expf(float(a.taper_a) * dr * dr);
-      x = R(f);
-    } else {
-      double f = (double)x - shift;
-      if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
-      x = R(f);
-    }
-  }
+  if (a.pro == PRO_TAPER) x = taper_value<R>(a, p, x, shift);
   return x;
 }
 
@@ -802,6 +811,8 @@ __global__ void k_axpy(const R* x, R* y, long n, double a, int accumulate) {
     y[p] = accumulate ? R((double)y[p] + a * (double)x[p]) : R(a * (double)x[p]);
 }
 
+#include "fft_plane.cuh"
+
 // ------------------------------------------------- size dispatch --------
 // Compile-time instantiations for the grid sizes the engine is run at; any
 // other size uses the runtime radix plan (tile_fft).  NL is the tile width:
@@ -920,6 +931,16 @@ int Ctx::fft_setup() {
   f.vblocks = grid_blocks(geom.n);
   if ((st = alloc((void**)&f.vres_part, sizeof(double) * f.vblocks * kMaxS))) return st;
   (void)need;
+  {
+    int dev = 0, optin = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const bool f64 = rsize == sizeof(double);
+    const bool inst = f64 ? plane_size_instantiated<double>(f.s) : plane_size_instantiated<float>(f.s);
+    const size_t need_smem = f64 ? plane_fwd_smem<double>(f.s, plane_nl<double>(f.s))
+                                 : plane_fwd_smem<float>(f.s, plane_nl<float>(f.s));
+    f.plane = f.dim == 3 && inst && need_smem + 1024 <= (size_t)optin;
+  }
   // shared memory opt-in of the runtime-plan kernels (any grid size)
   if (rsize == sizeof(double)) {
     CU(smem_optin(k_z_r2c<double, 0, 0>));
@@ -971,6 +992,7 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
   a.out = (typename Cx<R>::T*)out;
   a.part = sums ? f.zpart : nullptr;
+  if (sums) f.zparts = f.zblocks;
   const size_t smem = (3 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T);
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
   if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
@@ -992,7 +1014,7 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   a.scale = 1.0;
   a.coul_coef = coul_coef;
   a.f0_part = f.zpart;
-  a.f0_blocks = f.zblocks;
+  a.f0_blocks = f.zparts;
   const size_t smem = (2 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
@@ -1061,7 +1083,7 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   a.sigma_c = sigma_c;
   a.cutoff = c.P.coulomb_cutoff > 0.0 ? c.P.coulomb_cutoff : 0.5 * c.P.edge;
   a.f0_part = f.zpart;
-  a.f0_blocks = f.zblocks;
+  a.f0_blocks = f.zparts;
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
   const size_t csz = sizeof(typename Cx<R>::T);
   const size_t smem_ct = (3 * (size_t)f.s * (f.tk + 1) + 2 * f.s) * csz;
@@ -1075,6 +1097,74 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   return MPDPFT_OK;
 }
 
+// ---- plane passes (3D): instantiated (s, lines per tile) per precision ----
+template <typename R, int S, int NL>
+static void plane_fwd_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  smem_optin(k_plane_fwd<R, S, NL>);
+  k_plane_fwd<R, S, NL><<<grid, kPlaneThreads, smem, st>>>(a);
+}
+template <typename R, int S, int NL>
+static void plane_inv_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  smem_optin(k_plane_inv<R, S, NL>);
+  k_plane_inv<R, S, NL><<<grid, kPlaneThreads, smem, st>>>(a);
+}
+
+template <typename R>
+static void plane_dispatch(bool fwd, int s, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  const unsigned grid = (unsigned)s;
+  if (s == 32) { fwd ? plane_fwd_ct<R, 32, 16>(grid, smem, st, a) : plane_inv_ct<R, 32, 16>(grid, smem, st, a); }
+  else if (s == 64) { fwd ? plane_fwd_ct<R, 64, 16>(grid, smem, st, a) : plane_inv_ct<R, 64, 16>(grid, smem, st, a); }
+  else if constexpr (sizeof(R) == sizeof(float)) {
+    if (s == 128) { fwd ? plane_fwd_ct<R, 128, 32>(grid, smem, st, a) : plane_inv_ct<R, 128, 32>(grid, smem, st, a); }
+  }
+}
+
+// Forward 3D transform of `in` (prologue PRO_NONE or PRO_TAPER) into the
+// half spectrum `out`: plane pass (z R2C + y C2C); the x pass follows.
+template <typename R>
+static int launch_plane_fwd(Ctx& c, const R* in, int pro, void* out, bool sums) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = zargs<R>(c);
+  a.tw_m = (const typename Cx<R>::T*)f.tw_m_f;
+  a.tw_s = (const typename Cx<R>::T*)f.tw_s_f;
+  a.in = in;
+  a.pro = pro;
+  a.vmax = f.vmax;
+  a.taper_r0 = c.P.regularization_threshold * c.P.edge;
+  a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
+  a.out = (typename Cx<R>::T*)out;
+  a.part = sums ? f.zpart : nullptr;
+  a.err = &c.d_state->abort;
+  if (sums) f.zparts = f.s;
+  c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
+  plane_dispatch<R>(true, f.s, plane_fwd_smem<R>(f.s, plane_nl<R>(f.s)), c.stream, a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+// Inverse 3D transform after the x pass: y C2C inverse + z C2R with epilogue.
+template <typename R>
+static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, R* out1, double coul_coef) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = zargs<R>(c);
+  a.tw_m = (const typename Cx<R>::T*)f.tw_m_b;
+  a.tw_s = (const typename Cx<R>::T*)f.tw_s_b;
+  for (int i = 0; i < nin; ++i) a.cin[i] = (const typename Cx<R>::T*)in[i];
+  a.nin = nin;
+  a.epi = epi;
+  a.rout[0] = out0;
+  a.rout[1] = out1;
+  a.scale = 1.0;
+  a.coul_coef = coul_coef;
+  a.f0_part = f.zpart;
+  a.f0_blocks = f.zparts;
+  a.err = &c.d_state->abort;
+  c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
+  plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nl<R>(f.s), epi == EPI_GRAD), c.stream, a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
 // Coulomb potential of `src` (nsrc species combined with weights qcoef)
 // into out: out = coef * phi, phi = int rho(r')/|r - r'|.
 template <typename R>
@@ -1082,9 +1172,16 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
   FftPlan& f = *c.fft;
   int st;
   const int pro = nsrc > 1 || (qcoef && qcoef[0] != 1.0) ? PRO_CHARGE : PRO_NONE;
+  const int mul = c.P.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED ? MUL_COULOMB_TRUNC : MUL_COULOMB_REG;
+  if (f.plane && pro == PRO_NONE) {
+    if ((st = launch_plane_fwd<R>(c, src, pro, f.spec[0], true))) return st;
+    if ((st = launch_x<R>(c, f.spec[0], &f.spec[0], 1, mul, 0.0))) return st;
+    if (mul == MUL_COULOMB_REG)
+      return launch_plane_inv<R>(c, &f.spec[0], 1, EPI_COULOMB, out, nullptr, 4.0 * kPi * coef);
+    return launch_plane_inv<R>(c, &f.spec[0], 1, EPI_SCALE, out, nullptr, 4.0 * kPi * coef);
+  }
   if ((st = launch_z_r2c<R>(c, src, pro, nsrc, qcoef, f.spec[0], true))) return st;
   if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, -1))) return st;
-  const int mul = c.P.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED ? MUL_COULOMB_TRUNC : MUL_COULOMB_REG;
   if ((st = launch_x<R>(c, f.spec[0], &f.spec[0], 1, mul, 0.0))) return st;
   if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, +1))) return st;
   // regularised: V = 4 pi gammaH (x + f0 erf(r/2)/(4 pi r)); truncated: V = 4 pi gammaH x
@@ -1165,6 +1262,17 @@ static int delfield_into(Ctx& c, const R* f, R* g2, R* lap) {
   const double smear = c.P.smearing_extent > 0.0 ? c.P.smearing_extent : 6.0 * c.geom.dx;
   const double sigma_c = -0.5 * smear * smear;  // ConvolutionSigma (mpDPFT.cpp:1106)
   const int pro = c.P.taper_off ? PRO_TAPER : PRO_NONE;
+  if (F.plane) {
+    void* outs[4] = {F.spec[0], F.spec[1], F.spec[2], F.spec[3]};
+    if ((st = launch_plane_fwd<R>(c, f, pro, F.spec[0], false))) return st;
+    if ((st = launch_x<R>(c, F.spec[0], outs, 4, MUL_DERIV, sigma_c))) return st;
+    // |grad f|^2 (raw) -> rtmp, Laplacian -> lap
+    if ((st = launch_plane_inv<R>(c, outs, 4, EPI_GRAD, (R*)F.rtmp, lap, 0.0))) return st;
+    // smooth |grad f|^2 and clamp at 0 (mpDPFT.cpp:7550-7560)
+    if ((st = launch_plane_fwd<R>(c, (const R*)F.rtmp, PRO_NONE, F.spec[0], false))) return st;
+    if ((st = launch_x<R>(c, F.spec[0], &F.spec[0], 1, MUL_SMOOTH, sigma_c))) return st;
+    return launch_plane_inv<R>(c, &F.spec[0], 1, EPI_POS, g2, nullptr, 0.0);
+  }
   if ((st = launch_z_r2c<R>(c, f, pro, 1, nullptr, F.spec[0], false))) return st;
   if (F.dim == 3 && (st = launch_y<R>(c, &F.spec[0], 1, -1))) return st;
   const int nout = F.dim + 1;  // gradients + Laplacian

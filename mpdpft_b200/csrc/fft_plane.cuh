@@ -1,0 +1,250 @@
+// fft_plane.cuh -- 3D real transforms by x-planes: one thread block holds a
+// whole plane of the grid in shared memory.
+//
+//   k_plane_fwd  bulk-copies the real plane x = const (s^2 values, contiguous)
+//                into shared memory with one TMA transfer, applies the
+//                prologue, runs the R2C transforms along z and the C2C
+//                transforms along y in shared memory, and writes the half
+//                spectrum plane [y][kz] back with one TMA transfer;
+//   k_plane_inv  the reverse for one or more spectrum planes (inverse y,
+//                C2R along z) with the epilogues of k_z_c2r.
+// Between them the x pass (k_x_roundtrip) works on the same [x][y][kz]
+// layout, so a transform costs three passes over the field instead of five.
+// Included by fft.cu inside namespace mpdpft (needs ZArgs, z_output and the
+// Stockham helpers).
+#pragma once
+
+constexpr int kPlaneThreads = 512;
+constexpr long kTmaSpinLimit = 1L << 24;  // bounded mbarrier wait (~seconds with backoff)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One 1D bulk copy global -> shared, completing on bar (issued by one thread
+// after it armed bar with the byte count).
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase `parity` of bar.  On timeout the error word is
+// raised and the wait is retried once more (a copy may still be landing in
+// this block's shared memory); false means the data must not be used.
+__device__ inline bool mbar_wait(unsigned long long* bar, unsigned parity, int* err) {
+  for (int round = 0; round < 2; ++round) {
+    for (long i = 0; i < kTmaSpinLimit; ++i) {
+      if (mbar_try_wait(bar, parity)) return round == 0;
+      if (i > 32) __nanosleep(64);
+    }
+    if (round == 0 && err && threadIdx.x == 0) atomicExch(err, 1);
+  }
+  return false;
+}
+
+// Shared -> global bulk copy of `bytes` (one thread), waited for before the
+// block may reuse or release the source.
+__device__ __forceinline__ void tma_store_1d(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Orders this thread's generic shared-memory accesses before later
+// async-proxy (TMA) accesses of the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Tile width (lines per fft_lines call) and the instantiated sizes.
+template <typename R>
+constexpr int plane_nl(int s) { return (sizeof(R) == sizeof(float) && s >= 128) ? 32 : 16; }
+
+template <typename R>
+inline bool plane_size_instantiated(int s) {
+  return s == 32 || s == 64 || (sizeof(R) == sizeof(float) && s == 128);
+}
+
+// Shared-memory bytes of the plane kernels.
+template <typename R>
+__host__ __device__ constexpr size_t plane_fwd_smem(int S, int NL) {
+  return (size_t)S * S * sizeof(R) + ((size_t)S * (S / 2 + 1) + 2 * (size_t)S * (NL + 1) + (size_t)(S / 2) * (NL + 1) +
+                                       2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
+}
+template <typename R>
+__host__ __device__ constexpr size_t plane_inv_smem(int S, int NL, bool grad) {
+  return (grad ? (size_t)S * S * sizeof(R) : 0) +
+         ((size_t)S * (S / 2 + 1) + 2 * (size_t)S * (NL + 1) + 2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
+}
+
+// Forward: real plane -> half-spectrum plane, R2C along z and C2C along y.
+// a.in, a.out, a.pro (PRO_NONE or PRO_TAPER), a.part as for k_z_r2c; the
+// plane index is blockIdx.x.
+template <typename R, int S, int NL>
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
+  using C = typename Cx<R>::T;
+  constexpr int M = S / 2, H = M + 1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* realP = reinterpret_cast<R*>(smem_raw);  // [y][z]
+  C* plane = reinterpret_cast<C*>(realP + S * S);  // [y][kz]
+  C* A = plane + S * H;
+  C* B = A + S * (NL + 1);
+  C* Z = B + S * (NL + 1);  // M x (NL + 1): z transforms before the R2C split
+  C* tw_s = Z + M * (NL + 1);
+  C* tw_n = tw_s + S;
+  C* tw_m = tw_n + S;
+  __shared__ unsigned long long bar;
+  const int xi = blockIdx.x;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) tma_load_1d(realP, a.in + (long)xi * S * S, (unsigned)(S * S * sizeof(R)), &bar);
+  for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
+  double shift = 0.0;  // no shell points: no shift
+  if (a.pro == PRO_TAPER && *a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
+  const bool ok = __syncthreads_and(mbar_wait(&bar, 0, a.err)) != 0;
+  if (!ok) return;
+  double rowsum = 0.0;
+  // R2C along z, NL rows (y) at a time
+  for (int y0 = 0; y0 < S; y0 += NL) {
+    auto load = [&](int m, int l) -> C {
+      const int y = y0 + l;
+      R x0 = realP[y * S + 2 * m], x1 = realP[y * S + 2 * m + 1];
+      if (a.pro == PRO_TAPER) {
+        const long p0 = ((long)xi * S + y) * S + 2 * m;
+        x0 = taper_value<R>(a, p0, x0, shift);
+        x1 = taper_value<R>(a, p0 + 1, x1, shift);
+      }
+      rowsum += (double)x0 + (double)x1;
+      return C{x0, x1};
+    };
+    auto store = [&](int m, int l, C v) { Z[m * (NL + 1) + l] = v; };
+    fft_lines<C, M, NL, true>(A, B, tw_m, -1, load, store);
+    for (int w = threadIdx.x; w < H * NL; w += blockDim.x) {
+      const int l = w / H, q = w % H;
+      const C zq = Z[(q % M) * (NL + 1) + l];
+      const C zc = cconj(Z[((M - q) % M) * (NL + 1) + l]);
+      const C E = cscale(cadd(zq, zc), R(0.5));
+      const C D = csub(zq, zc);  // 2 i O_q
+      const C O = {D.y * R(0.5), -D.x * R(0.5)};
+      plane[(y0 + l) * H + q] = cadd(E, cmul(tw_n[q], O));
+    }
+    __syncthreads();
+  }
+  // C2C along y, NL columns (kz) at a time, in place
+  for (int q0 = 0; q0 < H; q0 += NL) {
+    auto load = [&](int t, int l) -> C { return q0 + l < H ? plane[t * H + q0 + l] : C{R(0), R(0)}; };
+    auto store = [&](int t, int l, C v) {
+      if (q0 + l < H) plane[t * H + q0 + l] = v;
+    };
+    fft_lines<C, S, NL, false>(A, B, tw_s, -1, load, store);
+  }
+  if (a.part) {
+    double acc[1] = {rowsum};
+    block_reduce_store<1>(acc, a.part + blockIdx.x);
+  }
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) tma_store_1d(a.out + (long)xi * S * H, plane, (unsigned)(S * H * sizeof(C)));
+}
+
+// Inverse: a.nin half-spectrum planes -> real outputs with a.epi (as
+// k_z_c2r: EPI_GRAD sums the squares of fields 0 .. nin-2 into rout[0] and
+// writes field nin-1 to rout[1]; the others write rout[0]).
+template <typename R, int S, int NL>
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
+  using C = typename Cx<R>::T;
+  constexpr int M = S / 2, H = M + 1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* plane = reinterpret_cast<C*>(smem_raw);  // [y][kz]
+  C* A = plane + S * H;
+  C* B = A + S * (NL + 1);
+  C* tw_s = B + S * (NL + 1);
+  C* tw_n = tw_s + S;
+  C* tw_m = tw_n + S;
+  R* acc = reinterpret_cast<R*>(tw_m + M);  // [y][z] (EPI_GRAD)
+  __shared__ unsigned long long bar;
+  __shared__ double s_f0[kPlaneThreads / 32];
+  const int xi = blockIdx.x;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
+  double f0 = 0.0;
+  if (a.epi == EPI_COULOMB) {  // f0 = dvol * sum of the forward pass's block sums
+    double t = 0.0;
+    for (int b = threadIdx.x; b < a.f0_blocks; b += blockDim.x) t += a.f0_part[b];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) s_f0[threadIdx.x >> 5] = t;
+  }
+  __syncthreads();
+  if (a.epi == EPI_COULOMB) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_f0[w];
+    f0 = t * a.g.dvol;
+  }
+  for (int f = 0; f < a.nin; ++f) {
+    if (threadIdx.x == 0) tma_load_1d(plane, a.cin[f] + (long)xi * S * H, (unsigned)(S * H * sizeof(C)), &bar);
+    const bool ok = __syncthreads_and(mbar_wait(&bar, (unsigned)(f & 1), a.err)) != 0;
+    if (!ok) return;
+    // inverse C2C along y, in place
+    for (int q0 = 0; q0 < H; q0 += NL) {
+      auto load = [&](int t, int l) -> C { return q0 + l < H ? plane[t * H + q0 + l] : C{R(0), R(0)}; };
+      auto store = [&](int t, int l, C v) {
+        if (q0 + l < H) plane[t * H + q0 + l] = v;
+      };
+      fft_lines<C, S, NL, false>(A, B, tw_s, +1, load, store);
+    }
+    // C2R along z, NL rows at a time, with the epilogue
+    for (int y0 = 0; y0 < S; y0 += NL) {
+      auto load = [&](int q, int l) -> C {
+        const C* X = plane + (y0 + l) * H;
+        const C xq = X[q];
+        const C xc = cconj(X[M - q]);
+        const C E = cadd(xq, xc);                  // 2 E_q
+        const C D = csub(xq, xc);                  // 2 e^{-2 pi i q/s} O_q
+        const C O = cmul(cconj(tw_n[q]), D);       // 2 O_q
+        return C{E.x - O.y, E.y + O.x};            // 2 (E_q + i O_q)
+      };
+      auto store = [&](int m, int l, C z) {
+        const int y = y0 + l;
+        const R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
+        const long p0 = ((long)xi * S + y) * S + 2 * m;
+        if (a.epi == EPI_GRAD) {
+          R* dst = acc + y * S + 2 * m;
+          if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
+          else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
+          else {
+            *reinterpret_cast<C*>(a.rout[0] + p0) = C{dst[0], dst[1]};
+            *reinterpret_cast<C*>(a.rout[1] + p0) = C{x0, x1};
+          }
+        } else {
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{z_output<R>(a, p0, x0, f0), z_output<R>(a, p0 + 1, x1, f0)};
+        }
+      };
+      fft_lines<C, M, NL, true>(A, B, tw_m, +1, load, store);
+    }
+    // every read of `plane` is done before the next transfer overwrites it
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
+}
