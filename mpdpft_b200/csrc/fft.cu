@@ -937,8 +937,8 @@ int Ctx::fft_setup() {
     CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const bool f64 = rsize == sizeof(double);
     const bool inst = f64 ? plane_size_instantiated<double>(f.s) : plane_size_instantiated<float>(f.s);
-    const size_t need_smem = f64 ? plane_fwd_smem<double>(f.s, plane_nl<double>(f.s))
-                                 : plane_fwd_smem<float>(f.s, plane_nl<float>(f.s));
+    const size_t need_smem = f64 ? plane_inv_smem<double>(f.s, plane_nly<double>(f.s), plane_nlz<double>(f.s), true)
+                                 : plane_inv_smem<float>(f.s, plane_nly<float>(f.s), plane_nlz<float>(f.s), true);
     f.plane = f.dim == 3 && inst && need_smem + 1024 <= (size_t)optin;
   }
   // shared memory opt-in of the runtime-plan kernels (any grid size)
@@ -1098,24 +1098,26 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
 }
 
 // ---- plane passes (3D): instantiated (s, lines per tile) per precision ----
-template <typename R, int S, int NL>
+template <typename R, int S>
 static void plane_fwd_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
-  smem_optin(k_plane_fwd<R, S, NL>);
-  k_plane_fwd<R, S, NL><<<grid, kPlaneThreads, smem, st>>>(a);
+  constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
+  smem_optin(k_plane_fwd<R, S, NLY, NLZ>);
+  k_plane_fwd<R, S, NLY, NLZ><<<grid, kPlaneThreads, smem, st>>>(a);
 }
-template <typename R, int S, int NL>
+template <typename R, int S>
 static void plane_inv_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
-  smem_optin(k_plane_inv<R, S, NL>);
-  k_plane_inv<R, S, NL><<<grid, kPlaneThreads, smem, st>>>(a);
+  constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
+  smem_optin(k_plane_inv<R, S, NLY, NLZ>);
+  k_plane_inv<R, S, NLY, NLZ><<<grid, kPlaneThreads, smem, st>>>(a);
 }
 
 template <typename R>
 static void plane_dispatch(bool fwd, int s, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
   const unsigned grid = (unsigned)s;
-  if (s == 32) { fwd ? plane_fwd_ct<R, 32, 16>(grid, smem, st, a) : plane_inv_ct<R, 32, 16>(grid, smem, st, a); }
-  else if (s == 64) { fwd ? plane_fwd_ct<R, 64, 16>(grid, smem, st, a) : plane_inv_ct<R, 64, 16>(grid, smem, st, a); }
+  if (s == 32) { fwd ? plane_fwd_ct<R, 32>(grid, smem, st, a) : plane_inv_ct<R, 32>(grid, smem, st, a); }
+  else if (s == 64) { fwd ? plane_fwd_ct<R, 64>(grid, smem, st, a) : plane_inv_ct<R, 64>(grid, smem, st, a); }
   else if constexpr (sizeof(R) == sizeof(float)) {
-    if (s == 128) { fwd ? plane_fwd_ct<R, 128, 32>(grid, smem, st, a) : plane_inv_ct<R, 128, 32>(grid, smem, st, a); }
+    if (s == 128) { fwd ? plane_fwd_ct<R, 128>(grid, smem, st, a) : plane_inv_ct<R, 128>(grid, smem, st, a); }
   }
 }
 
@@ -1137,7 +1139,7 @@ static int launch_plane_fwd(Ctx& c, const R* in, int pro, void* out, bool sums) 
   a.err = &c.d_state->abort;
   if (sums) f.zparts = f.s;
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
-  plane_dispatch<R>(true, f.s, plane_fwd_smem<R>(f.s, plane_nl<R>(f.s)), c.stream, a);
+  plane_dispatch<R>(true, f.s, plane_fwd_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s)), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1160,7 +1162,7 @@ static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, 
   a.f0_blocks = f.zparts;
   a.err = &c.d_state->abort;
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
-  plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nl<R>(f.s), epi == EPI_GRAD), c.stream, a);
+  plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s), epi == EPI_GRAD), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }

@@ -76,48 +76,70 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Tile width (lines per fft_lines call) and the instantiated sizes.
+// Tile widths (lines per fft_lines call) and the instantiated sizes: the z
+// transforms (length s/2) take NLZ rows at a time, the y transforms NLY
+// columns.  The columns kz = 0 and kz = s/2 are transformed together as one
+// complex column (both are real before the forward y transform and after the
+// inverse one), so the y pass runs exactly s/2 columns.
 template <typename R>
-constexpr int plane_nl(int s) { return (sizeof(R) == sizeof(float) && s >= 128) ? 32 : 16; }
+constexpr int plane_nly(int s) { return (sizeof(R) == sizeof(float) && s >= 128) ? 32 : 16; }
+template <typename R>
+constexpr int plane_nlz(int s) { return 2 * plane_nly<R>(s); }
 
 template <typename R>
 inline bool plane_size_instantiated(int s) {
   return s == 32 || s == 64 || (sizeof(R) == sizeof(float) && s == 128);
 }
 
-// Shared-memory bytes of the plane kernels.
+// Shared-memory bytes: the spectrum plane (which first holds the real plane),
+// the two Stockham tiles, twiddles, and the |grad|^2 accumulator (inverse,
+// EPI_GRAD).
 template <typename R>
-__host__ __device__ constexpr size_t plane_fwd_smem(int S, int NL) {
-  return (size_t)S * S * sizeof(R) + ((size_t)S * (S / 2 + 1) + 2 * (size_t)S * (NL + 1) + (size_t)(S / 2) * (NL + 1) +
-                                       2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
+__host__ __device__ constexpr size_t plane_tile(int S, int NLY, int NLZ) {
+  return (size_t)S * (NLY + 1) > (size_t)(S / 2) * (NLZ + 1) ? (size_t)S * (NLY + 1) : (size_t)(S / 2) * (NLZ + 1);
 }
 template <typename R>
-__host__ __device__ constexpr size_t plane_inv_smem(int S, int NL, bool grad) {
-  return (grad ? (size_t)S * S * sizeof(R) : 0) +
-         ((size_t)S * (S / 2 + 1) + 2 * (size_t)S * (NL + 1) + 2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
+__host__ __device__ constexpr size_t plane_fwd_smem(int S, int NLY, int NLZ) {
+  return ((size_t)S * (S / 2 + 1) + 2 * plane_tile<R>(S, NLY, NLZ) + 2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
+}
+template <typename R>
+__host__ __device__ constexpr size_t plane_inv_smem(int S, int NLY, int NLZ, bool grad) {
+  return plane_fwd_smem<R>(S, NLY, NLZ) + (grad ? (size_t)S * S * sizeof(R) : 0);
+}
+
+// y transforms of columns 0 .. s/2 - 1 of the plane [y][kz], NLY at a time,
+// in place.
+template <typename C, int S, int NLY>
+__device__ __forceinline__ void plane_y_pass(C* plane, C* A, C* B, const C* tw, int dir) {
+  constexpr int H = S / 2 + 1;
+  for (int q0 = 0; q0 < S / 2; q0 += NLY) {
+    auto load = [&](int t, int l) -> C { return plane[t * H + q0 + l]; };
+    auto store = [&](int t, int l, C v) { plane[t * H + q0 + l] = v; };
+    fft_lines<C, S, NLY, false>(A, B, tw, dir, load, store);
+  }
 }
 
 // Forward: real plane -> half-spectrum plane, R2C along z and C2C along y.
 // a.in, a.out, a.pro (PRO_NONE or PRO_TAPER), a.part as for k_z_r2c; the
 // plane index is blockIdx.x.
-template <typename R, int S, int NL>
+template <typename R, int S, int NLY, int NLZ>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
   using C = typename Cx<R>::T;
   constexpr int M = S / 2, H = M + 1;
+  constexpr int TILE = (int)plane_tile<R>(S, NLY, NLZ);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  R* realP = reinterpret_cast<R*>(smem_raw);  // [y][z]
-  C* plane = reinterpret_cast<C*>(realP + S * S);  // [y][kz]
+  C* plane = reinterpret_cast<C*>(smem_raw);  // [y][kz]; first the real plane [y][z]
+  const R* realP = reinterpret_cast<const R*>(smem_raw);
   C* A = plane + S * H;
-  C* B = A + S * (NL + 1);
-  C* Z = B + S * (NL + 1);  // M x (NL + 1): z transforms before the R2C split
-  C* tw_s = Z + M * (NL + 1);
+  C* B = A + TILE;
+  C* tw_s = B + TILE;
   C* tw_n = tw_s + S;
   C* tw_m = tw_n + S;
   __shared__ unsigned long long bar;
   const int xi = blockIdx.x;
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
-  if (threadIdx.x == 0) tma_load_1d(realP, a.in + (long)xi * S * S, (unsigned)(S * S * sizeof(R)), &bar);
+  if (threadIdx.x == 0) tma_load_1d(plane, a.in + (long)xi * S * S, (unsigned)(S * S * sizeof(R)), &bar);
   for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
   double shift = 0.0;  // no shell points: no shift
@@ -125,8 +147,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
   const bool ok = __syncthreads_and(mbar_wait(&bar, 0, a.err)) != 0;
   if (!ok) return;
   double rowsum = 0.0;
-  // R2C along z, NL rows (y) at a time
-  for (int y0 = 0; y0 < S; y0 += NL) {
+  // R2C along z, NLZ rows at a time, in place: groups run from the last rows
+  // down, so a group's complex rows (H complex each) never reach the real
+  // rows (S reals each) of the groups still to come
+  for (int y0 = S - NLZ; y0 >= 0; y0 -= NLZ) {
     auto load = [&](int m, int l) -> C {
       const int y = y0 + l;
       R x0 = realP[y * S + 2 * m], x1 = realP[y * S + 2 * m + 1];
@@ -138,26 +162,45 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
       rowsum += (double)x0 + (double)x1;
       return C{x0, x1};
     };
-    auto store = [&](int m, int l, C v) { Z[m * (NL + 1) + l] = v; };
-    fft_lines<C, M, NL, true>(A, B, tw_m, -1, load, store);
-    for (int w = threadIdx.x; w < H * NL; w += blockDim.x) {
-      const int l = w / H, q = w % H;
-      const C zq = Z[(q % M) * (NL + 1) + l];
-      const C zc = cconj(Z[((M - q) % M) * (NL + 1) + l]);
-      const C E = cscale(cadd(zq, zc), R(0.5));
-      const C D = csub(zq, zc);  // 2 i O_q
-      const C O = {D.y * R(0.5), -D.x * R(0.5)};
-      plane[(y0 + l) * H + q] = cadd(E, cmul(tw_n[q], O));
+    auto store = [&](int m, int l, C v) { plane[(y0 + l) * H + m] = v; };
+    fft_lines<C, M, NLZ, true>(A, B, tw_m, -1, load, store);
+    // split Z_q -> X_q = E_q + e^{-2 pi i q/s} O_q, pairs (q, M - q) in place
+    for (int w = threadIdx.x; w < (M / 2 + 1) * NLZ; w += blockDim.x) {
+      const int l = w / (M / 2 + 1), q = w % (M / 2 + 1);
+      C* row = plane + (y0 + l) * H;
+      const C zq = row[q], zr = row[(M - q) % M];
+      auto split = [&](C za, C zb, int k) -> C {  // X_k from Z_k = za, Z_{M-k} = zb
+        const C zc = cconj(zb);
+        const C E = cscale(cadd(za, zc), R(0.5));
+        const C D = csub(za, zc);  // 2 i O_k
+        const C O = {D.y * R(0.5), -D.x * R(0.5)};
+        return cadd(E, cmul(tw_n[k], O));
+      };
+      if (q == 0) {
+        const C x0 = split(zq, zq, 0), xm = split(zq, zq, M);
+        row[0] = C{x0.x, xm.x};  // X_0 and X_M are real: packed as one column
+      } else {
+        const C xa = split(zq, zr, q), xb = split(zr, zq, M - q);
+        row[q] = xa;
+        row[M - q] = xb;
+      }
     }
     __syncthreads();
   }
-  // C2C along y, NL columns (kz) at a time, in place
-  for (int q0 = 0; q0 < H; q0 += NL) {
-    auto load = [&](int t, int l) -> C { return q0 + l < H ? plane[t * H + q0 + l] : C{R(0), R(0)}; };
-    auto store = [&](int t, int l, C v) {
-      if (q0 + l < H) plane[t * H + q0 + l] = v;
-    };
-    fft_lines<C, S, NL, false>(A, B, tw_s, -1, load, store);
+  plane_y_pass<C, S, NLY>(plane, A, B, tw_s, -1);
+  // unpack column 0: C(k) = Y_0(k) + i Y_M(k), Y_0 and Y_M Hermitian in k
+  for (int k = threadIdx.x; k <= S / 2; k += blockDim.x) {
+    const int kr = (S - k) % S;
+    const C c = plane[k * H], cr = plane[kr * H];
+    const C y0k = {R(0.5) * (c.x + cr.x), R(0.5) * (c.y - cr.y)};
+    const C ymk = {R(0.5) * (c.y + cr.y), R(0.5) * (cr.x - c.x)};
+    const C y0r = cconj(y0k), ymr = cconj(ymk);
+    plane[k * H] = y0k;
+    plane[k * H + M] = ymk;
+    if (kr != k) {
+      plane[kr * H] = y0r;
+      plane[kr * H + M] = ymr;
+    }
   }
   if (a.part) {
     double acc[1] = {rowsum};
@@ -171,15 +214,16 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
 // Inverse: a.nin half-spectrum planes -> real outputs with a.epi (as
 // k_z_c2r: EPI_GRAD sums the squares of fields 0 .. nin-2 into rout[0] and
 // writes field nin-1 to rout[1]; the others write rout[0]).
-template <typename R, int S, int NL>
+template <typename R, int S, int NLY, int NLZ>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
   using C = typename Cx<R>::T;
   constexpr int M = S / 2, H = M + 1;
+  constexpr int TILE = (int)plane_tile<R>(S, NLY, NLZ);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C* plane = reinterpret_cast<C*>(smem_raw);  // [y][kz]
   C* A = plane + S * H;
-  C* B = A + S * (NL + 1);
-  C* tw_s = B + S * (NL + 1);
+  C* B = A + TILE;
+  C* tw_s = B + TILE;
   C* tw_n = tw_s + S;
   C* tw_m = tw_n + S;
   R* acc = reinterpret_cast<R*>(tw_m + M);  // [y][z] (EPI_GRAD)
@@ -206,16 +250,22 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
     if (threadIdx.x == 0) tma_load_1d(plane, a.cin[f] + (long)xi * S * H, (unsigned)(S * H * sizeof(C)), &bar);
     const bool ok = __syncthreads_and(mbar_wait(&bar, (unsigned)(f & 1), a.err)) != 0;
     if (!ok) return;
-    // inverse C2C along y, in place
-    for (int q0 = 0; q0 < H; q0 += NL) {
-      auto load = [&](int t, int l) -> C { return q0 + l < H ? plane[t * H + q0 + l] : C{R(0), R(0)}; };
-      auto store = [&](int t, int l, C v) {
-        if (q0 + l < H) plane[t * H + q0 + l] = v;
-      };
-      fft_lines<C, S, NL, false>(A, B, tw_s, +1, load, store);
+    // pack columns 0 and M: C(k) = Y_0(k) + i Y_M(k)
+    for (int k = threadIdx.x; k < S; k += blockDim.x) {
+      const C y0 = plane[k * H], ym = plane[k * H + M];
+      plane[k * H] = C{y0.x - ym.y, y0.y + ym.x};
     }
-    // C2R along z, NL rows at a time, with the epilogue
-    for (int y0 = 0; y0 < S; y0 += NL) {
+    __syncthreads();
+    plane_y_pass<C, S, NLY>(plane, A, B, tw_s, +1);
+    // unpack: column 0 holds X_0(y) + i X_M(y), both real
+    for (int y = threadIdx.x; y < S; y += blockDim.x) {
+      const C c = plane[y * H];
+      plane[y * H] = C{c.x, R(0)};
+      plane[y * H + M] = C{c.y, R(0)};
+    }
+    __syncthreads();
+    // C2R along z, NLZ rows at a time, with the epilogue
+    for (int y0 = 0; y0 < S; y0 += NLZ) {
       auto load = [&](int q, int l) -> C {
         const C* X = plane + (y0 + l) * H;
         const C xq = X[q];
@@ -241,7 +291,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
           *reinterpret_cast<C*>(a.rout[0] + p0) = C{z_output<R>(a, p0, x0, f0), z_output<R>(a, p0 + 1, x1, f0)};
         }
       };
-      fft_lines<C, M, NL, true>(A, B, tw_m, +1, load, store);
+      fft_lines<C, M, NLZ, true>(A, B, tw_m, +1, load, store);
     }
     // every read of `plane` is done before the next transfer overwrites it
     fence_proxy_async_smem();
