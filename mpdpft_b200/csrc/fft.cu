@@ -102,7 +102,9 @@ __device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
 
 // ---------------------------------------------------------- prologues ----
 enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
-enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3, EPI_SCALE = 4 };
+// EPI_COULOMB_V: the Coulomb epilogue followed by the V assembly of one
+// species (k_assemble_v fused into the transform; plane kernels only)
+enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3, EPI_SCALE = 4, EPI_COULOMB_V = 5 };
 enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3 };
 
 template <typename R>
@@ -134,27 +136,60 @@ struct ZArgs {
   // plane kernels
   const typename Cx<R>::T* tw_s;  // length-s table for the y transforms
   int* err;                       // raised when a bulk copy does not complete
+  // EPI_COULOMB_V (one species): V = vext + min(1, inc_v) (vh + pointwise
+  // terms of ncur); |V_new - V_old|^2 block sums and the shell maximum of V
+  const ScState* st;
+  const R* vext;
+  const R* ncur;
+  R* vpot;
+  double beta, gamma_h;
+  int contact_self, dirac;
+  double shell_r, shell_w;
+  double* vres_part;              // [blocks][kMaxS]
+  unsigned long long* vmax_out;
+  int coul_reg;                   // 1: regularised kernel (erf term), 0: truncated (plain scale)
 };
 
 // R2C along the contiguous axis.  Block = zl rows; each row of s reals is
 // read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
 // into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
 // Input value of the R2C pass at element p (prologue: taper or charge sum).
-// DelField boundary taper (mpDPFT.cpp:7251-7264) of value x at point p.
+// DelField boundary taper (mpDPFT.cpp:7251-7264) of value x at (px, py, pz).
+template <typename R>
+__device__ __forceinline__ R taper_xyz(const ZArgs<R>& a, double px, double py, double pz, R x, double shift) {
+  if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the factor in FP32
+    const float r = sqrtf(float(px) * float(px) + float(py) * float(py) + float(pz) * float(pz));
+    float f = x - float(shift);
+    const float dr = r - float(a.taper_r0);
+    if (dr > 0.f) f *= expf(float(a.taper_a) * dr * dr);
+    return R(f);
+  } else {
+    const double r = sqrt(px * px + py * py + pz * pz);
+    double f = (double)x - shift;
+    if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
+    return R(f);
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ R taper_value(const ZArgs<R>& a, long p, R x, double shift) {
   double px, py, pz;
   point_coords(p, a.g, px, py, pz);
-  const double r = sqrt(px * px + py * py + pz * pz);
-  if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the factor in FP32
-    float f = x - float(shift);
-    const float dr = float(r - a.taper_r0);
-    if (r > a.taper_r0) f *= expf(float(a.taper_a) * dr * dr);
-    return R(f);
+  return taper_xyz<R>(a, px, py, pz, x, shift);
+}
+
+// Coulomb epilogue value at (x, y, z): coef (v + f0 pi erf(r/2)/r / (4 pi^2))
+// (mpDPFT.cpp:2704-2711).
+template <typename R>
+__device__ __forceinline__ R coulomb_xyz(const ZArgs<R>& a, double x, double y, double z, R v, double f0) {
+  if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the term in FP32
+    const float r = sqrtf(float(x) * float(x) + float(y) * float(y) + float(z) * float(z));
+    const float zf = r > 1.0e-10f ? float(kPi) * erff(0.5f * r) / r : float(1.7724538509055159);
+    return R(float(a.coul_coef) * (v + float(f0 / (4.0 * kPi * kPi)) * zf));
   } else {
-    double f = (double)x - shift;
-    if (r > a.taper_r0) f *= exp(a.taper_a * (r - a.taper_r0) * (r - a.taper_r0));
-    return R(f);
+    const double r = sqrt(x * x + y * y + z * z);
+    const double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
+    return R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
   }
 }
 
@@ -259,18 +294,10 @@ template <typename R>
 __device__ __forceinline__ R z_output(const ZArgs<R>& a, long p, R v, double f0) {
   if (a.epi == EPI_POS) return v > R(0) ? v : R(0);
   if (a.epi == EPI_SCALE) return R(a.coul_coef * (double)v);
-  if (a.epi == EPI_COULOMB) {  // mpDPFT.cpp:2704-2711
+  if (a.epi == EPI_COULOMB) {
     double x, y, z;
     point_coords(p, a.g, x, y, z);
-    if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the term in FP32
-      const float r = sqrtf(float(x * x + y * y + z * z));
-      const float zf = r > 1.0e-10f ? float(kPi) * erff(0.5f * r) / r : float(1.7724538509055159);
-      return R(float(a.coul_coef) * (v + float(f0 / (4.0 * kPi * kPi)) * zf));
-    } else {
-      const double r = sqrt(x * x + y * y + z * z);
-      const double zf = r > 1.0e-10 ? kPi * erf(0.5 * r) / r : sqrt(kPi);
-      return R(a.coul_coef * ((double)v + f0 * zf / (4.0 * kPi * kPi)));
-    }
+    return coulomb_xyz<R>(a, x, y, z, v, f0);
   }
   return v;
 }
@@ -1161,6 +1188,21 @@ static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, 
   a.f0_part = f.zpart;
   a.f0_blocks = f.zparts;
   a.err = &c.d_state->abort;
+  a.coul_reg = c.P.coulomb_kernel != MPDPFT_COULOMB_TRUNCATED;
+  if (epi == EPI_COULOMB_V) {  // V assembly of species 0 fused into the epilogue
+    a.st = c.d_state;
+    a.vext = (const R*)c.d_vext;
+    a.ncur = (const R*)c.d_cur;
+    a.vpot = (R*)c.d_V;
+    a.beta = c.P.beta;
+    a.gamma_h = c.P.gamma_h;
+    a.contact_self = c.has_interaction(MPDPFT_INT_CONTACT_SELF);
+    a.dirac = c.has_interaction(MPDPFT_INT_DIRAC);
+    a.shell_r = c.P.edge * c.P.regularization_threshold;
+    a.shell_w = 2.0 * c.geom.dx;
+    a.vres_part = f.vres_part;
+    a.vmax_out = f.vmax;
+  }
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s), epi == EPI_GRAD), c.stream, a);
   CU(cudaGetLastError());
@@ -1169,8 +1211,11 @@ static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, 
 
 // Coulomb potential of `src` (nsrc species combined with weights qcoef)
 // into out: out = coef * phi, phi = int rho(r')/|r - r'|.
+// fuse_v: also assemble V of species 0 in the final pass (plane path only;
+// the caller checked that this Coulomb term is species 0's whole vh).
 template <typename R>
-static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* out, double coef) {
+static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* out, double coef,
+                        bool fuse_v = false) {
   FftPlan& f = *c.fft;
   int st;
   const int pro = nsrc > 1 || (qcoef && qcoef[0] != 1.0) ? PRO_CHARGE : PRO_NONE;
@@ -1178,6 +1223,7 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
   if (f.plane && pro == PRO_NONE) {
     if ((st = launch_plane_fwd<R>(c, src, pro, f.spec[0], true))) return st;
     if ((st = launch_x<R>(c, f.spec[0], &f.spec[0], 1, mul, 0.0))) return st;
+    if (fuse_v) return launch_plane_inv<R>(c, &f.spec[0], 1, EPI_COULOMB_V, out, nullptr, 4.0 * kPi * coef);
     if (mul == MUL_COULOMB_REG)
       return launch_plane_inv<R>(c, &f.spec[0], 1, EPI_COULOMB, out, nullptr, 4.0 * kPi * coef);
     return launch_plane_inv<R>(c, &f.spec[0], 1, EPI_SCALE, out, nullptr, 4.0 * kPi * coef);
@@ -1305,20 +1351,33 @@ static int fft_terms_impl(Ctx& c) {
   // the device, so the kernels that write a new input density also store a
   // copy at the fixed address d_cur
   const R* dens = (const R*)c.d_cur;
-  if (c.has_coulomb) {
-    if ((st = coulomb_terms<R>(c, dens, (R*)c.d_vh))) return st;
-  }
+  // one species whose only Coulomb term is the Hartree potential: V is
+  // assembled in the epilogue of that transform
+  const bool fuse = F.plane && c.S == 1 && c.has_interaction(MPDPFT_INT_HARTREE) &&
+                    !c.has_interaction(MPDPFT_INT_HARTREE_INTER) && !c.has_interaction(MPDPFT_INT_COULOMB_CHARGED);
   CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+  if (fuse) {
+    if ((st = coulomb_into<R>(c, dens, 1, nullptr, (R*)c.d_vh, c.P.gamma_h, true))) return st;
+    c.assemble_in_step = 0;
+    c.vres_part_ext = F.vres_part;
+    c.vres_blocks_ext = F.s;
+  } else {
+    if (c.has_coulomb) {
+      if ((st = coulomb_terms<R>(c, dens, (R*)c.d_vh))) return st;
+    }
+  }
   KParams kp = c.kparams();
-  c.cnt[5]++;
-  k_assemble_v<R><<<F.vblocks, kThreads, 0, c.stream>>>(kp, c.d_state, (const R*)c.d_vext,
-                                                         c.has_coulomb ? (const R*)c.d_vh : nullptr,
-                                                         (const R*)c.d_nin, (R*)c.d_V, F.vres_part, F.vmax,
-                                                         shell_radius(c), shell_width(c));
-  CU(cudaGetLastError());
-  c.assemble_in_step = 0;
-  c.vres_part_ext = F.vres_part;
-  c.vres_blocks_ext = F.vblocks;
+  if (!fuse) {
+    c.cnt[5]++;
+    k_assemble_v<R><<<F.vblocks, kThreads, 0, c.stream>>>(kp, c.d_state, (const R*)c.d_vext,
+                                                           c.has_coulomb ? (const R*)c.d_vh : nullptr,
+                                                           (const R*)c.d_nin, (R*)c.d_V, F.vres_part, F.vmax,
+                                                           shell_radius(c), shell_width(c));
+    CU(cudaGetLastError());
+    c.assemble_in_step = 0;
+    c.vres_part_ext = F.vres_part;
+    c.vres_blocks_ext = F.vblocks;
+  }
   if (c.gradient) {
     for (int s = 0; s < c.S; ++s) {
       if (s > 0) {  // taper shift of species s

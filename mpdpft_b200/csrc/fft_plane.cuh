@@ -155,9 +155,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
       const int y = y0 + l;
       R x0 = realP[y * S + 2 * m], x1 = realP[y * S + 2 * m + 1];
       if (a.pro == PRO_TAPER) {
-        const long p0 = ((long)xi * S + y) * S + 2 * m;
-        x0 = taper_value<R>(a, p0, x0, shift);
-        x1 = taper_value<R>(a, p0 + 1, x1, shift);
+        const double h = -0.5 * a.g.L, dx = a.g.dx;
+        const double px = h + dx * xi, py = h + dx * y;
+        x0 = taper_xyz<R>(a, px, py, h + dx * (2 * m), x0, shift);
+        x1 = taper_xyz<R>(a, px, py, h + dx * (2 * m + 1), x1, shift);
       }
       rowsum += (double)x0 + (double)x1;
       return C{x0, x1};
@@ -233,15 +234,21 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
+  const bool coul = a.epi == EPI_COULOMB || a.epi == EPI_COULOMB_V;
+  const bool fusev = a.epi == EPI_COULOMB_V;
+  // V assembly: skipped once the SC loop has exited (V stays as it was)
+  const bool vwrite = fusev && !__ldcg(&a.st->exit_loop);
+  const double vfac = fusev ? fmin(1.0, __ldcg(&a.st->inc_v)) : 0.0;
+  double vacc = 0.0, vmx = -1.0e300;
   double f0 = 0.0;
-  if (a.epi == EPI_COULOMB) {  // f0 = dvol * sum of the forward pass's block sums
+  if (coul) {  // f0 = dvol * sum of the forward pass's block sums
     double t = 0.0;
     for (int b = threadIdx.x; b < a.f0_blocks; b += blockDim.x) t += a.f0_part[b];
     t = warp_sum(t);
     if ((threadIdx.x & 31) == 0) s_f0[threadIdx.x >> 5] = t;
   }
   __syncthreads();
-  if (a.epi == EPI_COULOMB) {
+  if (coul) {
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_f0[w];
     f0 = t * a.g.dvol;
@@ -287,6 +294,40 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
             *reinterpret_cast<C*>(a.rout[0] + p0) = C{dst[0], dst[1]};
             *reinterpret_cast<C*>(a.rout[1] + p0) = C{x0, x1};
           }
+        } else if (coul) {
+          const double h = -0.5 * a.g.L, dx = a.g.dx;
+          const double px = h + dx * xi, py = h + dx * y, pz0 = h + dx * (2 * m), pz1 = h + dx * (2 * m + 1);
+          R vh[2];
+          if (a.coul_reg) {
+            vh[0] = coulomb_xyz<R>(a, px, py, pz0, x0, f0);
+            vh[1] = coulomb_xyz<R>(a, px, py, pz1, x1, f0);
+          } else {
+            vh[0] = R(a.coul_coef * (double)x0);
+            vh[1] = R(a.coul_coef * (double)x1);
+          }
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{vh[0], vh[1]};
+          if (vwrite) {  // k_assemble_v for this point pair (mpDPFT.cpp:4815-4838)
+            const C ve = *reinterpret_cast<const C*>(a.vext + p0);
+            const C nc = *reinterpret_cast<const C*>(a.ncur + p0);
+            const C vo = *reinterpret_cast<const C*>(a.vpot + p0);
+            const R vev[2] = {ve.x, ve.y}, ncv[2] = {nc.x, nc.y}, vov[2] = {vo.x, vo.y};
+            R vn[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              R vi = vh[i];
+              if (a.contact_self) vi += R(2.0 * a.beta) * ncv[i];  // type 10 (:2261)
+              if (a.dirac) {                                       // type 11 (:2768)
+                R ns = ncv[i] > R(0) ? ncv[i] : R(0);
+                vi += R(-a.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+              }
+              vn[i] = vev[i] + R(vfac) * vi;
+              const double d = (double)vn[i] - (double)vov[i];
+              vacc += d * d;
+              const double pz = i ? pz1 : pz0;
+              if (in_shell(px * px + py * py + pz * pz, a.shell_r, a.shell_w)) vmx = fmax(vmx, (double)vn[i]);
+            }
+            *reinterpret_cast<C*>(a.vpot + p0) = C{vn[0], vn[1]};
+          }
         } else {
           *reinterpret_cast<C*>(a.rout[0] + p0) = C{z_output<R>(a, p0, x0, f0), z_output<R>(a, p0 + 1, x1, f0)};
         }
@@ -296,5 +337,19 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
     // every read of `plane` is done before the next transfer overwrites it
     fence_proxy_async_smem();
     __syncthreads();
+  }
+  if (fusev) {  // block sums of |V_new - V_old|^2 and the block's shell maximum
+    double accv[1] = {vacc};
+    block_reduce_store<1>(accv, a.vres_part + (long)blockIdx.x * kMaxS);
+    __shared__ double smx[kPlaneThreads / 32];
+    double t = vmx;
+    for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+    if ((threadIdx.x & 31) == 0) smx[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = smx[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, smx[w]);
+      if (b > -1.0e300) atomicMax(a.vmax_out, ordered_bits(b));
+    }
   }
 }
