@@ -210,13 +210,20 @@ def run_ours(args, world, rank, local):
     value = world * args.steps / (ms_max / 1000.0)
     launches = eng.iteration_kernels()
 
-    # roofline of the dominant stage (share = time per launch x launches per iteration)
-    stages = {abi.STAGE_SC_STEP: ("sc_step_kernel", 1)}
+    # roofline of the dominant kernel (share = time per launch x launches per
+    # iteration); each kernel timed alone with CUDA events on the engine stream
     per_iter = eng.stage_launch_counts()
-    stages.update({abi.STAGE_FFT_Z_R2C: ("k_z_r2c", per_iter.get("z_r2c", 0)),
-                   abi.STAGE_FFT_Y: ("k_axis_c2c", per_iter.get("y", 0)),
-                   abi.STAGE_FFT_X: ("k_x_roundtrip", per_iter.get("x", 0)),
-                   abi.STAGE_FFT_Z_C2R: ("k_z_c2r", per_iter.get("z_c2r", 0))})
+    stages = {abi.STAGE_SC_MU: ("sc_mu_kernel", 1),
+              abi.STAGE_SC_DENSITY: ("sc_density_kernel", 1),
+              abi.STAGE_SC_MIX: ("sc_mix_kernel", 1),
+              abi.STAGE_FFT_X: ("k_x_roundtrip", per_iter.get("x", 0))}
+    if per_iter.get("y", 0) == 0:  # 3D transforms by x-planes
+        stages.update({abi.STAGE_FFT_PLANE_FWD: ("k_plane_fwd", per_iter.get("z_r2c", 0)),
+                       abi.STAGE_FFT_PLANE_INV: ("k_plane_inv", per_iter.get("z_c2r", 0))})
+    else:
+        stages.update({abi.STAGE_FFT_Z_R2C: ("k_z_r2c", per_iter.get("z_r2c", 0)),
+                       abi.STAGE_FFT_Y: ("k_axis_c2c", per_iter.get("y", 0)),
+                       abi.STAGE_FFT_Z_C2R: ("k_z_c2r", per_iter.get("z_c2r", 0))})
     prof = {}
     for st, (name, cnt) in stages.items():
         mst, b = eng.profile_stage(st, reps=20)

@@ -284,20 +284,26 @@ int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result);
  * iterations on the current state (after mpdpft_sc_init); the FFT stages
  * transform a zeroed scratch spectrum. */
 enum {
-  MPDPFT_STAGE_SC_STEP = 0,   /* persistent SC-step kernel (mu search .. mix) */
+  MPDPFT_STAGE_SC_STEP = 0,   /* the SC kernels of one iteration (mu .. mix)  */
   MPDPFT_STAGE_FFT_Z_R2C = 1, /* R2C pass along the contiguous axis           */
   MPDPFT_STAGE_FFT_Y = 2,     /* C2C pass along y (3D)                        */
   MPDPFT_STAGE_FFT_X = 3,     /* x-axis round trip with one k-space multiplier */
   MPDPFT_STAGE_FFT_Z_C2R = 4, /* C2R pass along the contiguous axis           */
-  MPDPFT_STAGE_ITERATION = 5  /* one whole SC iteration (graph replay)        */
+  MPDPFT_STAGE_ITERATION = 5, /* one whole SC iteration (graph replay)        */
+  MPDPFT_STAGE_SC_MU = 6,     /* mu kernel: V update + mu search              */
+  MPDPFT_STAGE_SC_DENSITY = 7,/* density kernel: n_out, residual, sums, scalar step */
+  MPDPFT_STAGE_SC_MIX = 8,    /* mixing kernel                                */
+  MPDPFT_STAGE_FFT_PLANE_FWD = 9,  /* 3D: z R2C + y C2C by x-planes           */
+  MPDPFT_STAGE_FFT_PLANE_INV = 10  /* 3D: y C2C inverse + z C2R by x-planes   */
 };
 int mpdpft_profile_stage(mpdpft_ctx* ctx, int stage, int reps, double* ms_per_launch,
                          double* bytes_per_launch);
 
 /* Kernel launches in one SC iteration as captured in its CUDA graph:
- * counts[i] for i = MPDPFT_STAGE_SC_STEP .. MPDPFT_STAGE_FFT_Z_C2R, counts[5]
- * for the remaining (pointwise) kernels; *total = their sum.  Valid after
- * the first graph-mode mpdpft_sc_step. */
+ * counts[i] for i = MPDPFT_STAGE_SC_STEP .. MPDPFT_STAGE_FFT_Z_C2R (the plane
+ * kernels count as Z_R2C / Z_C2R), counts[5] for the remaining (pointwise)
+ * kernels; *total = their sum.  Valid after the first graph-mode
+ * mpdpft_sc_step. */
 int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
 
 /* Phase durations (microseconds, block 0 of the grid) of the last SC-step

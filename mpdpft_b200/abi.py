@@ -56,6 +56,11 @@ STAGE_FFT_Y = 2
 STAGE_FFT_X = 3
 STAGE_FFT_Z_C2R = 4
 STAGE_ITERATION = 5
+STAGE_SC_MU = 6
+STAGE_SC_DENSITY = 7
+STAGE_SC_MIX = 8
+STAGE_FFT_PLANE_FWD = 9
+STAGE_FFT_PLANE_INV = 10
 
 _D4 = C.c_double * MAX_SPECIES
 

@@ -420,11 +420,13 @@ StepArgs<R> Ctx::step_args(int mode) {
   return a;
 }
 
+// parts: bit 0 mu kernel, bit 1 density kernel, bit 2 mixing kernel (a
+// mode still runs only the kernels it has)
 template <typename R>
-static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk) {
+static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk, int parts = 7) {
   StepArgs<R> args = c.step_args<R>(mode);
   void* params[] = {&args};
-  if (mode != 2) {
+  if (mode != 2 && (parts & 1)) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3(c.step_blocks);
@@ -440,11 +442,14 @@ static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk) {
     cudaError_t e = cudaLaunchKernelExC(&cfg, sc_kernel_ptr<R>(0, fk), params);
     if (e != cudaSuccess) return e;
   }
-  c.cnt[MPDPFT_STAGE_SC_STEP]++;
-  cudaError_t e =
-      cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensThreads), params, 0, c.stream);
-  if (e != cudaSuccess) return e;
-  if (mode != 1) {
+  cudaError_t e = cudaSuccess;
+  if (parts & 2) {
+    c.cnt[MPDPFT_STAGE_SC_STEP]++;
+    e = cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensThreads), params, 0,
+                         c.stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (mode != 1 && (parts & 4)) {
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
     sc_mix_kernel<R><<<c.mix_blocks, kDensThreads, 0, c.stream>>>(args);
     e = cudaGetLastError();
@@ -455,9 +460,9 @@ static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk) {
 // One SC iteration's kernels (mode 0), the densities of the current V
 // (mode 1: mu kernel + density kernel) or the admix step alone (mode 2:
 // density kernel + mixing kernel).
-int Ctx::launch_step(int mode) {
-  cudaError_t e = rsize == sizeof(double) ? launch_sc_kernels<double>(*this, mode, fk)
-                                          : launch_sc_kernels<float>(*this, mode, fk);
+int Ctx::launch_step(int mode, int parts) {
+  cudaError_t e = rsize == sizeof(double) ? launch_sc_kernels<double>(*this, mode, fk, parts)
+                                          : launch_sc_kernels<float>(*this, mode, fk, parts);
   if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("SC kernel launch: ") + cudaGetErrorString(e));
   return MPDPFT_OK;
 }

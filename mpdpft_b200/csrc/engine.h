@@ -82,7 +82,7 @@ struct Ctx {
   int export_field(const void* src, double* dst, int layout, int mem);
   template <typename R>
   StepArgs<R> step_args(int mode);
-  int launch_step(int mode);
+  int launch_step(int mode, int parts = 7);  // parts: 1 mu, 2 density, 4 mixing kernel
   int issue_iteration();
   int sc_init(const double* const* v0, int layout, int mem);
   int sc_step(int use_graph);

@@ -1680,7 +1680,11 @@ static int profile_impl(Ctx& c, int stage, int reps, double* ms, double* bytes) 
   CU(cudaEventCreate(&e1));
   int st = MPDPFT_OK;
   double b = 0.0;
-  if (stage != MPDPFT_STAGE_SC_STEP && stage != MPDPFT_STAGE_ITERATION) {
+  const bool sc_stage = stage == MPDPFT_STAGE_SC_STEP || stage == MPDPFT_STAGE_ITERATION ||
+                        stage == MPDPFT_STAGE_SC_MU || stage == MPDPFT_STAGE_SC_DENSITY || stage == MPDPFT_STAGE_SC_MIX;
+  if ((stage == MPDPFT_STAGE_FFT_PLANE_FWD || stage == MPDPFT_STAGE_FFT_PLANE_INV) && !F.plane)
+    return set_error(MPDPFT_ERR_ARG, "this grid does not use the plane kernels");
+  if (!sc_stage) {
     if (!F.spec[0]) return set_error(MPDPFT_ERR_ARG, "context has no FFT buffers");
     CU(cudaMemsetAsync(F.spec[0], 0, (size_t)spec, c.stream));
     CU(cudaMemsetAsync(F.rtmp, 0, (size_t)field, c.stream));
@@ -1693,6 +1697,11 @@ static int profile_impl(Ctx& c, int stage, int reps, double* ms, double* bytes) 
       case MPDPFT_STAGE_FFT_X: return launch_x<R>(c, F.spec[0], &F.spec[0], 1, MUL_SMOOTH, -0.01);
       case MPDPFT_STAGE_FFT_Z_C2R: return launch_z_c2r<R>(c, &F.spec[0], 1, EPI_STORE, (R*)F.rtmp, nullptr, 0.0);
       case MPDPFT_STAGE_ITERATION: return c.sc_step(1);
+      case MPDPFT_STAGE_SC_MU: return c.launch_step(0, 1);
+      case MPDPFT_STAGE_SC_DENSITY: return c.launch_step(0, 2);
+      case MPDPFT_STAGE_SC_MIX: return c.launch_step(0, 4);
+      case MPDPFT_STAGE_FFT_PLANE_FWD: return launch_plane_fwd<R>(c, (const R*)F.rtmp, PRO_NONE, F.spec[0], false);
+      case MPDPFT_STAGE_FFT_PLANE_INV: return launch_plane_inv<R>(c, &F.spec[0], 1, EPI_STORE, (R*)F.rtmp, nullptr, 0.0);
       default: return set_error(MPDPFT_ERR_ARG, "unknown stage");
     }
   };
@@ -1716,6 +1725,17 @@ static int profile_impl(Ctx& c, int stage, int reps, double* ms, double* bytes) 
       b = field * S * ((c.gradient ? 3 : 1) + 1 + 1 + (I - 1) + 2 * I + 1);
       if (c.assemble_in_step) b += field * S * 3;
       break;
+    case MPDPFT_STAGE_SC_MU:  // V (+ Laplacian, |grad V|^2) read once
+      b = field * S * (c.gradient ? 3 : 1);
+      break;
+    case MPDPFT_STAGE_SC_DENSITY:  // V, n_in, I-1 older residuals read; residual written
+      b = field * S * (1 + 1 + (I - 1) + 1);
+      break;
+    case MPDPFT_STAGE_SC_MIX:  // I input densities and residuals read; mix and its copy written
+      b = field * S * (2 * I + 2);
+      break;
+    case MPDPFT_STAGE_FFT_PLANE_FWD: b = field + spec; break;
+    case MPDPFT_STAGE_FFT_PLANE_INV: b = spec + field; break;
     case MPDPFT_STAGE_FFT_Z_R2C: b = field + spec; break;
     case MPDPFT_STAGE_FFT_Y: b = 2.0 * spec; break;
     case MPDPFT_STAGE_FFT_X: b = 2.0 * spec; break;
