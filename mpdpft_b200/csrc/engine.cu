@@ -299,7 +299,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   if ((st = occupancy(f64 ? sc_kernel_ptr<double>(0, fk) : sc_kernel_ptr<float>(0, fk), kStepThreads, &occ_mu)))
     return st;
   dens_which = (P.mixer ? P.pulay_scope : 1) <= 5 ? 1 : 2;
-  if ((st = occupancy(f64 ? sc_kernel_ptr<double>(dens_which, fk) : sc_kernel_ptr<float>(dens_which, fk), kDensThreads,
+  if ((st = occupancy(f64 ? sc_kernel_ptr<double>(dens_which, fk) : sc_kernel_ptr<float>(dens_which, fk), kDensityThreads,
                       &occ_dens)))
     return st;
   if ((st = occupancy(f64 ? (const void*)sc_mix_kernel<double> : (const void*)sc_mix_kernel<float>, kDensThreads,
@@ -308,10 +308,9 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   step_blocks = num_sms * std::min(occ_mu, 2);
   long useful = (geom.n + kStepThreads - 1) / kStepThreads;
   if (step_blocks > useful) step_blocks = (int)std::max(1L, useful);
-  const long groups = (geom.n + 3) / 4;  // the density and mixing kernels take 4 points a thread
-  const long useful_dens = (groups + kDensThreads - 1) / kDensThreads;
-  dens_blocks = (int)std::max(1L, std::min((long)num_sms * occ_dens, useful_dens));
-  mix_blocks = (int)std::max(1L, std::min((long)num_sms * occ_mix, useful_dens));
+  const long groups = (geom.n + 3) / 4;  // the mixing kernel takes 4 points a thread
+  dens_blocks = (int)std::max(1L, std::min((long)num_sms * occ_dens, (geom.n + kDensityThreads - 1) / kDensityThreads));
+  mix_blocks = (int)std::max(1L, std::min((long)num_sms * occ_mix, (groups + kDensThreads - 1) / kDensThreads));
   // the mu kernel's list sweeps: a contiguous chunk of points per warp
   {
     const long warps = (long)step_blocks * kStepWarps;
@@ -445,7 +444,7 @@ static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk, int parts = 7) {
   cudaError_t e = cudaSuccess;
   if (parts & 2) {
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
-    e = cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensThreads), params, 0,
+    e = cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensityThreads), params, 0,
                          c.stream);
     if (e != cudaSuccess) return e;
   }

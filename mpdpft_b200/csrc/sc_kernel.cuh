@@ -101,6 +101,78 @@ __device__ inline bool warp_inverse(int n, const double* G, double* inv, double*
   return true;
 }
 
+// The same inverse on the first `nthr` threads of the block (whole warps),
+// synchronised with named barrier 1 so that the other warps can work
+// meanwhile: warp 0 finds each pivot, every thread updates elements of
+// [M | R].  Each pivot step costs a few barriers instead of a serial chain.
+__device__ __forceinline__ void group_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
+
+__device__ inline bool group_inverse(int n, const double* G, double* M, double* Rm, double* inv, int* colof,
+                                     double* s_pv, int* s_pi, int nthr) {
+  const int t = threadIdx.x, lane = t & 31;
+  const int nn = n * n;
+  for (int e = t; e < nn; e += nthr) {
+    M[e] = G[e];
+    Rm[e] = (e / n == e % n) ? 1.0 : 0.0;
+  }
+  if (t == 0) { s_pi[2] = 0; s_pi[3] = 0; s_pv[1] = 0.0; s_pv[2] = 1e300; }  // used rows, used cols, max, min pivot
+  group_bar(nthr);
+  for (int c = 0; c < n; ++c) {
+    if (t < 32) {  // first maximum |M| over unused rows and columns, row-major order
+      const unsigned ur = (unsigned)s_pi[2], uc = (unsigned)s_pi[3];
+      double best = -1.0;
+      int be = 0x7fffffff;
+      for (int e = lane; e < nn; e += 32) {
+        const int i = e / n, j = e % n;
+        if (((ur >> i) & 1u) || ((uc >> j) & 1u)) continue;
+        const double v = fabs(M[e]);
+        if (v > best) { best = v; be = e; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oe = __shfl_xor_sync(0xffffffffu, be, o);
+        if (ob > best || (ob == best && oe < be)) { best = ob; be = oe; }
+      }
+      if (lane == 0) {
+        const int pr = be / n, pc = be % n;
+        s_pi[0] = pr;
+        s_pi[1] = pc;
+        s_pv[0] = M[be];
+        s_pv[1] = fmax(s_pv[1], best);
+        s_pv[2] = fmin(s_pv[2], best);
+        s_pi[2] |= 1 << pr;
+        s_pi[3] |= 1 << pc;
+        colof[pr] = pc;
+      }
+    }
+    group_bar(nthr);
+    const int pr = s_pi[0], pc = s_pi[1];
+    const double piv = s_pv[0];
+    if (piv == 0.0) return false;  // same value for every thread
+    const double ip = 1.0 / piv;
+    // new values of this thread's (at most two) elements: 2 n^2 <= 288 <= 2 nthr
+    auto updated = [&](int e) -> double {
+      const bool right = e >= nn;
+      const int ee = right ? e - nn : e;
+      const int i = ee / n, j = ee % n;
+      const double* X = right ? Rm : M;
+      return (i == pr) ? X[ee] * ip : X[ee] - M[i * n + pc] * ip * X[pr * n + j];
+    };
+    const int e0 = t, e1 = t + nthr;
+    const double v0 = e0 < 2 * nn ? updated(e0) : 0.0;
+    const double v1 = e1 < 2 * nn ? updated(e1) : 0.0;
+    group_bar(nthr);
+    if (e0 < 2 * nn) { if (e0 >= nn) Rm[e0 - nn] = v0; else M[e0] = v0; }
+    if (e1 < 2 * nn) { if (e1 >= nn) Rm[e1 - nn] = v1; else M[e1] = v1; }
+    group_bar(nthr);
+  }
+  if (s_pv[2] <= 2.220446049250313e-16 * (double)n * s_pv[1]) return false;
+  for (int e = t; e < nn; e += nthr) inv[colof[e / n] * n + e % n] = Rm[e];
+  group_bar(nthr);
+  return true;
+}
+
 // sum_{i,j} ((inv G)_{ij} - delta_ij)^2 on one warp (the reference's
 // validation of the inverse, mpDPFT.cpp:5099-5107)
 __device__ inline double warp_inverse_defect(int n, const double* G, const double* inv) {
@@ -328,6 +400,50 @@ __device__ inline void block_rows_sum(const double* base, int nb, int stride, in
       for (int i = 0; i < nw; ++i) x += sh[i][threadIdx.x];
       const int v = c0 + threadIdx.x;
       out[(v / per) * pstride + v % per] = x;
+    }
+  }
+  __syncthreads();
+}
+
+// Two sources in one pass (all threads, CH2 values at a time): nv1 values of
+// nb1 rows as block_rows_sum, then nv2 values (v at base2[b * stride2 + v])
+// of nb2 rows into out2.
+__device__ inline void block_rows_sum2(const double* base1, int nb1, int stride1, int nv1, int per, int pstride,
+                                       double* out1, const double* base2, int nb2, int stride2, int nv2,
+                                       double* out2) {
+  constexpr int CH2 = 16;
+  __shared__ double sh[32][CH2];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int nv = nv1 + nv2;
+  const int nb = nb1 > nb2 ? nb1 : nb2;
+  for (int c0 = 0; c0 < nv; c0 += CH2) {
+    double t[CH2];
+#pragma unroll
+    for (int u = 0; u < CH2; ++u) t[u] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+      for (int u = 0; u < CH2; ++u) {
+        const int v = c0 + u;
+        if (v < nv1) {
+          if (b < nb1) t[u] += __ldcg(base1 + (long)b * stride1 + (v / per) * pstride + v % per);
+        } else if (v < nv) {
+          if (b < nb2) t[u] += __ldcg(base2 + (long)b * stride2 + (v - nv1));
+        }
+      }
+    }
+    __syncthreads();  // sh is free
+#pragma unroll
+    for (int u = 0; u < CH2; ++u) {
+      const double x = warp_sum(t[u]);
+      if (lane == 0) sh[w][u] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < CH2 && c0 + (int)threadIdx.x < nv) {
+      double x = 0.0;
+      for (int i = 0; i < nw; ++i) x += sh[i][threadIdx.x];
+      const int v = c0 + threadIdx.x;
+      if (v < nv1) out1[(v / per) * pstride + v % per] = x;
+      else out2[v - nv1] = x;
     }
   }
   __syncthreads();
@@ -572,15 +688,15 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
         if (lane == 0) red[v] = t;
       }
       __syncthreads();
+      for (int v = threadIdx.x; v < S * kMuAcc; v += blockDim.x) red[v] *= kp.geom.dvol;  // N(mu_c), dN/dmu
+      __syncthreads();
       if (threadIdx.x == 0) {
         double dmm = ls->dmm;
         int bits = 0;
         for (int s = 0; s < S; ++s) {
           if (s_ms[s].done) continue;
           MuState& ms = ls->ms[s];
-          double N[kMuCand];
-          for (int c = 0; c < ms.ncand; ++c) N[c] = red[s * kMuAcc + c] * kp.geom.dvol;
-          mu_decide(ms, N, red[s * kMuAcc + kMuCand] * kp.geom.dvol, kp.abundance[s], kp.rel_acc, dmm, bits);
+          mu_decide(ms, red + s * kMuAcc, red[s * kMuAcc + kMuCand], kp.abundance[s], kp.rel_acc, dmm, bits);
         }
         ls->dmm = dmm;
         ls->iter_bits |= bits;
@@ -607,14 +723,14 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
 // The last block to finish runs phase D: CheckConvergence, Intercept, the
 // Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
 template <typename R, int FK, int PW>
-__global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs<R> a) {
   // PW: the largest Pulay window this instantiation handles (<= kMaxP); a
   // small window keeps the per-thread sums in few registers
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
   const int S = kp.S;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int wib = threadIdx.x >> 5;
   __shared__ double red[kNPart];
   __shared__ double red_v[kMaxS];
   __shared__ double s_mu[kMaxS];      // mu of the final density
@@ -717,20 +833,21 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R>
   // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
   __shared__ ScState s_st;
   ScState* const ls = &s_st;
-  __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP];
-  __shared__ double s_prm[kMaxP], s_prr[kMaxP], s_pcol[kMaxP];
-  __shared__ int s_colof[kMaxP];
+  __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP], s_M[kMaxP * kMaxP], s_R[kMaxP * kMaxP];
+  __shared__ double s_prm[kMaxP], s_pv[4];
+  __shared__ int s_colof[kMaxP], s_pi[4];
   __shared__ double s_grow[kMaxP];
   __shared__ int s_pbits;
   state_load(ls, st);
   if (threadIdx.x == 0) s_pbits = 0;
   const int nv = 4 + I;  // per species: N, three dots, Gram row
   const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
-  block_rows_sum(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red);
-  if (vres) {
-    if (a.assemble_v) block_rows_sum(a.part + kVresOff, kp.mu_blocks, kNPart, S, S, 0, red_v);
-    else block_rows_sum(a.vres_part, a.vres_blocks, kMaxS, S, S, 0, red_v);
-  }
+  if (!vres) block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, nullptr, 0, 0, 0, red_v);
+  else if (a.assemble_v)
+    block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, a.part + kVresOff, kp.mu_blocks, kNPart, S,
+                    red_v);
+  else
+    block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, a.vres_part, a.vres_blocks, kMaxS, S, red_v);
   if (threadIdx.x < I) {  // Gram row summed over species
     double t = 0.0;
     for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
@@ -741,9 +858,10 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R>
   // matrix (last row/column new, the rest shifted from before), its inverse
   // (FullPivHouseholderQR + validation in the reference, :5089-5107) and the
   // coefficients c = G^{-1} 1 / (1^T G^{-1} 1) ...
-  if (a.mode != 1 && pulay_now && wib == 0) {
+  const int ngrp = blockDim.x - 32;  // warps 0 .. n-2 solve; the last warp does the bookkeeping
+  if (a.mode != 1 && pulay_now && (int)threadIdx.x < ngrp) {
     const int shift = (hist + 1 > kp.scope) ? 1 : 0;
-    for (int e = lane; e < I * I; e += 32) {
+    for (int e = threadIdx.x; e < I * I; e += ngrp) {
       const int i = e / I, j = e % I;
       double v;
       if (i == I - 1) v = s_grow[j];
@@ -751,18 +869,21 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R>
       else v = ls->gram[(i + shift) * kMaxP + (j + shift)];
       s_G[e] = v;
     }
-    __syncwarp();
-    for (int e = lane; e < I * I; e += 32) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
-    const bool inv_ok = warp_inverse(I, s_G, s_inv, s_prm, s_prr, s_pcol, s_colof);
-    const double test = inv_ok ? warp_inverse_defect(I, s_G, s_inv) : 0.0;
-    const bool used = inv_ok && test <= 1.0e-8;
-    if (used && lane < I) {  // row sums of the inverse
+    group_bar(ngrp);
+    for (int e = threadIdx.x; e < I * I; e += ngrp) ls->gram[(e / I) * kMaxP + (e % I)] = s_G[e];
+    const bool inv_ok = group_inverse(I, s_G, s_M, s_R, s_inv, s_colof, s_pv, s_pi, ngrp);
+    double test = 0.0;
+    if (inv_ok && wib == 0) test = warp_inverse_defect(I, s_G, s_inv);
+    if (threadIdx.x == 0) s_pv[3] = test;
+    group_bar(ngrp);
+    const bool used = inv_ok && s_pv[3] <= 1.0e-8;
+    if (used && (int)threadIdx.x < I) {  // row sums of the inverse
       double x = 0.0;
-      for (int k2 = 0; k2 < I; ++k2) x += s_inv[lane * I + k2];
-      s_prm[lane] = x;
+      for (int k2 = 0; k2 < I; ++k2) x += s_inv[threadIdx.x * I + k2];
+      s_prm[threadIdx.x] = x;
     }
-    __syncwarp();
-    if (lane == 0) {
+    group_bar(ngrp);
+    if (threadIdx.x == 0) {
       ls->hist = I;
       if (used) {
         double A = 0.0;
@@ -775,8 +896,8 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_density_kernel(StepArgs<R>
       ls->ncoeff = used ? I : 0;
     }
   }
-  // ... while warp 1 does CheckConvergence and Intercept
-  if (threadIdx.x == 32) {
+  // ... while the last warp does CheckConvergence and Intercept
+  if ((int)threadIdx.x == ngrp) {
     if (vres) {
       double w = 0.0;
       for (int s = 0; s < S; ++s) w = fmax(w, sqrt(red_v[s] / (double)n));

@@ -20,7 +20,8 @@ namespace mpdpft {
 constexpr int kStepThreads = 512;
 constexpr int kStepWarps = kStepThreads / 32;
 constexpr int kSegPts = 128;          // points of one warp step (4 per lane)
-constexpr int kDensThreads = 256;     // density and mixing kernels
+constexpr int kDensThreads = 256;     // mixing kernel
+constexpr int kDensityThreads = 256;  // density kernel
 constexpr int kMuAcc = kMuCand + 1;  // candidate sums + dN/dmu at candidate 0
 constexpr int kNF = 4 + kMaxP;        // per-species sums of the density/Gram pass
 // per-block partial sums: [0, kVresOff) the mu-pass or density-pass sums,
