@@ -118,5 +118,41 @@ def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **
     return p, [vext], [v0]
 
 
+def gaussian_landscape(steps, edge, count, seed):
+    """Smooth random potential: sum of `count` Gaussians with amplitudes
+    U[-2, 2], widths U[1, 4] and centres U[-12, 12]^3 (seeded)."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(-2.0, 2.0, count)
+    width = rng.uniform(1.0, 4.0, count)
+    centre = rng.uniform(-12.0, 12.0, (count, 3))
+    x = axis(steps, edge)
+    out = np.zeros((steps, steps, steps))
+    for a, w, c in zip(amp, width, centre):
+        gx = np.exp(-(x - c[0]) ** 2 / (2 * w * w))
+        gy = np.exp(-(x - c[1]) ** 2 / (2 * w * w))
+        gz = np.exp(-(x - c[2]) ** 2 / (2 * w * w))
+        out += a * gx[:, None, None] * gy[None, :, None] * gz[None, None, :]
+    return out.reshape(-1)
+
+
+def electron_hole(steps=256, edge=40.0, precision=abi.MIXED, seed=SEED_BASE + 5, **over):
+    """Two species of opposite charge (q = -1, +1), N = 20000 each, in the
+    box [-20, 20]^3 with a smooth random external potential (64 Gaussians),
+    gradient-corrected TF density (smoothing 0.3), Coulomb coupling of the
+    charge density (type 100: V_s = q_s V_H[sum q n]), Pulay history 8 with
+    the annealed damping of schedule 5; V_0 = V_ext + U(-1e-3, 1e-3)."""
+    kw = dict(dim=3, steps=steps, species=2, edge=edge, abundances=[20000.0, 20000.0],
+              rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
+              interactions=[abi.INT_COULOMB_CHARGED], gamma_h=1.0, charges=[-1.0, 1.0],
+              mu=[2.0, 2.0], mixer=1, pulay_scope=8, theta=[0.3, 0.3], schedule=5,
+              sc_criterion=1e-8, max_sc_count=300, smearing_extent=0.3, regularization_threshold=0.45,
+              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0, precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    vext = gaussian_landscape(steps, edge, 64, seed)
+    v0 = [vext + noise(vext.shape, 1e-3, seed + 100 * s) for s in range(2)]
+    return p, [vext, vext.copy()], v0
+
+
 def workload_names():
-    return ["harmonic_tf", "argon_atom"]
+    return ["harmonic_tf", "argon_atom", "electron_hole"]

@@ -156,7 +156,7 @@ struct State {
   int sc_count = 0, exit_count = 0, exit_loop = 0;
   bool trapped = false;
   long mu_trials = 0;
-  bool del_valid = false;  // DelField(V) cached for the current V
+  unsigned del_valid = 0;  // bit s: DelField(V[s]) cached for the current V[s]
   // Pulay
   std::vector<std::vector<std::vector<double>>> nin, nout, res;
   std::vector<std::vector<double>> gram;
@@ -401,9 +401,9 @@ void density(State& st, int s) {
       }
     }
   } else if (P.density_expression == MPDPFT_DENS_GRADIENT) {
-    if (!st.del_valid) {  // DelField(V) is independent of mu: computed once per V
+    if (!(st.del_valid >> s & 1u)) {  // DelField(V[s]) is independent of mu: computed once per V[s]
       delfield(st, V, st.Grad2[s], st.Lap[s]);
-      st.del_valid = true;
+      st.del_valid |= 1u << s;
     }
     const std::vector<double>& lap = st.Lap[s];
     const std::vector<double>& g2 = st.Grad2[s];
@@ -536,7 +536,7 @@ void update_v(State& st) {
   }
   if (st.sc_count > 0) st.incV += st.incV0;  // MD:4833
   st.incV = std::min(1., st.incV);
-  st.del_valid = false;
+  st.del_valid = 0;
 }
 
 // ------------------------------------ EnforceConstraints MD:4569-4743 --
@@ -1053,7 +1053,7 @@ int oracle_sc_run(const mpdpft_params* p, const double* vext, const double* v0,
       st.T[q] = std::max(std::fabs(st.mu[q] - vmin), std::fabs(st.mu[q] - vmax)) / 50.;
     }
   std::memset(result, 0, sizeof(*result));
-  st.del_valid = false;
+  st.del_valid = 0;
   get_densities(st);  // initial densities, MD:195
   long total_trials = st.mu_trials;
   int logged = 0;

@@ -273,3 +273,25 @@ def test_mu_bracket_failure_matches_reference(eng, oracle_lib, prec):
     assert res.mu[0] == res_r.mu[0] == -0.5
     assert abs(res.abundance[0] - res_r.abundance[0]) / res_r.abundance[0] < 1e-9 * (1 if prec == abi.FP64 else 1e4)
     assert rel(dens, dens_r[0]) < (1e-9 if prec == abi.FP64 else 1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,e_tol,n_tol", [(abi.FP64, 1e-6, 1e-5), (abi.MIXED, 1e-5, 1e-5)])
+def test_sc_electron_hole_converged(eng, oracle_lib, prec, e_tol, n_tol):
+    """Two species of opposite charge coupled through the charge density
+    (type 100), gradient-corrected density, Pulay 8 with schedule 5 (config
+    electron_hole at 32^3) against the converged FP64 oracle."""
+    p, vext, v0 = W.electron_hole(steps=32, precision=prec)
+    pr, _, _ = W.electron_hole(steps=32, precision=abi.FP64)
+    with eng.Engine(p) as e:
+        res, log, st = e.sc_run(vext, v0)
+        dens = [e.field(abi.FIELD_DENSITY, s) for s in range(2)]
+    res_r, log_r, dens_r, v_r = oracle_lib.sc_run(pr, vext, v0)
+    assert res.converged == 1 and res_r.converged == 1
+    de = abs(res.e_total - res_r.e_total) / abs(res_r.e_total)
+    dvol = (p.edge / p.steps) ** 3
+    l1 = [np.abs(dens[s] - dens_r[s]).sum() * dvol / p.abundances[s] for s in range(2)]
+    print("electron_hole 32^3 prec %d: iters %d/%d dE/E %.2e L1/N %s" %
+          (prec, res.iterations, res_r.iterations, de, ["%.2e" % x for x in l1]))
+    assert de < e_tol
+    assert max(l1) < n_tol

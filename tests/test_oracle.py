@@ -177,3 +177,16 @@ def test_delfield_of_gaussian(oracle_lib):
     g2_exact = 4 * a * a * r2 * f * f
     assert np.abs(lap - lap_exact).max() < 1e-6
     assert np.abs(g2 - g2_exact).max() < 1e-6
+
+
+def test_mu_search_two_species_gradient(oracle_lib):
+    """Two species with different potentials, gradient-corrected density: the
+    densities the mu search returns are n[V_s] of each species' own DelField
+    (GetnAiT recomputes DelField(V[s]) per species, mpDPFT.cpp:3455-3456)."""
+    p, vext, v0 = W.electron_hole(steps=16)
+    v = [v0[0], v0[1] + 0.05 * W.radius2(3, 16, p.edge).reshape(-1) / 400.0]
+    mu, ab, dens, trials, _ = oracle_lib.mu_search(p, v)
+    for s in range(2):
+        n, N = oracle_lib.density(p, s, v[s], mu[s])
+        assert np.abs(dens[s] - n).max() <= 1e-12 * np.abs(n).max()
+        assert abs(N - ab[s]) <= 1e-9 * ab[s]
