@@ -311,6 +311,31 @@ int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
  * [3] convergence test and Pulay solve, [4] grid barrier, [5] mix. */
 int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n);
 
+/* Batch: many independent SC solves advanced together on one GPU (a
+ * parameter sweep, the reference's TaskType 5/6/7 loops of GetData,
+ * mpDPFTmain.cpp:110-160, run as one job).  The solves share dimension 2,
+ * species count, precision, density functional (MPDPFT_DENS_GRADIENT),
+ * Pulay window and the interaction list (pointwise terms only); grid sizes,
+ * abundances, couplings, temperatures and potentials may differ.  Each
+ * iteration of all unfinished solves is one CUDA graph replay; a solve that
+ * has met its exit test does no further work.  Results equal those of
+ * mpdpft_sc_run on each solve alone.
+ *   params:  count parameter sets
+ *   v0:      count * species starting potentials, v0[i * species + s], or NULL
+ *   results: count records; status: count per-solve status codes (may be NULL) */
+int mpdpft_batch_create(const mpdpft_params* params, int count, int device, mpdpft_batch** out);
+int mpdpft_batch_destroy(mpdpft_batch* batch);
+int mpdpft_batch_set_external_potential(mpdpft_batch* batch, int i, int s, const double* v_ext,
+                                        int layout, int mem);
+int mpdpft_batch_sc_init(mpdpft_batch* batch, const double* const* v0, int layout, int mem);
+int mpdpft_batch_sc_step(mpdpft_batch* batch, int iterations);
+int mpdpft_batch_sc_run(mpdpft_batch* batch, const double* const* v0, int layout, int mem,
+                        mpdpft_result* results, int* status);
+int mpdpft_batch_get_field(mpdpft_batch* batch, int i, int which, int s, double* out, int layout,
+                           int mem);
+int mpdpft_batch_get_log(mpdpft_batch* batch, int i, mpdpft_iter_log* log, int log_cap, int* n_out);
+int mpdpft_batch_sync(mpdpft_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

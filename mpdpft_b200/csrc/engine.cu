@@ -82,7 +82,6 @@ __global__ void k_export(const R* __restrict__ src, double* __restrict__ dst, Ge
 // Energy integrands (GetEnergy, mpDPFT.cpp:5414-5436), one block partial per
 // accumulator: per species [0] int (mu-V)_+^{(D+2)/2}, [1] int Vext n,
 // [2] int n^2, [3] int n_+^{1+1/D}, [4] int n vh/2; pairs [16+...] int n_s n_s'.
-constexpr int kNEnergy = 5 * kMaxS + kMaxS * kMaxS;
 template <typename R>
 __global__ void k_energy(Geom g, int S, const R* V, const R* vext, const R* dens, const R* vh,
                          const double* mu, double* part) {
@@ -107,6 +106,18 @@ __global__ void k_energy(Geom g, int S, const R* V, const R* vext, const R* dens
   block_reduce_store<kNEnergy>(acc, part + (long)blockIdx.x * kNEnergy);
 }
 
+// out[v] = scale * sum over rows b < nb of part[b * nv + v], one block, in
+// a fixed order.
+__global__ void k_sum_rows(const double* part, int nb, int nv, double scale, double* out) {
+  const int lane = threadIdx.x & 31;
+  for (int v = threadIdx.x >> 5; v < nv; v += blockDim.x >> 5) {
+    double t = 0.0;
+    for (int b = lane; b < nb; b += 32) t += part[(long)b * nv + v];
+    t = warp_sum(t);
+    if (lane == 0) out[v] = t * scale;
+  }
+}
+
 template <typename R>
 __global__ void k_integrate(Geom g, const R* f, double* part) {
   double acc[1] = {0.0};
@@ -123,22 +134,20 @@ __global__ void k_density(Geom g, DensParams d, double mu, const R* V, const R* 
 }
 
 // The mu kernel (which 0) and the density kernel for Pulay windows <= 5
-// (which 1) or up to kMaxP (which 2), of functional kind fk.
+// (which 1), <= 8 (which 3) or up to kMaxP (which 2), of functional kind fk.
+template <typename R, int FK>
+static const void* sc_kernel_fk(int which) {
+  if (which == 0) return (const void*)sc_mu_kernel<R, FK>;
+  if (which == 1) return (const void*)sc_density_kernel<R, FK, 5>;
+  if (which == 3) return (const void*)sc_density_kernel<R, FK, 8>;
+  return (const void*)sc_density_kernel<R, FK, kMaxP>;
+}
+
 template <typename R>
 static const void* sc_kernel_ptr(int which, int fk) {
-  if (which == 0) {
-    if (fk == 1) return (const void*)sc_mu_kernel<R, 1>;
-    if (fk == 2) return (const void*)sc_mu_kernel<R, 2>;
-    return (const void*)sc_mu_kernel<R, 0>;
-  }
-  if (which == 1) {  // Pulay window <= 5
-    if (fk == 1) return (const void*)sc_density_kernel<R, 1, 5>;
-    if (fk == 2) return (const void*)sc_density_kernel<R, 2, 5>;
-    return (const void*)sc_density_kernel<R, 0, 5>;
-  }
-  if (fk == 1) return (const void*)sc_density_kernel<R, 1, kMaxP>;
-  if (fk == 2) return (const void*)sc_density_kernel<R, 2, kMaxP>;
-  return (const void*)sc_density_kernel<R, 0, kMaxP>;
+  if (fk == 1) return sc_kernel_fk<R, 1>(which);
+  if (fk == 2) return sc_kernel_fk<R, 2>(which);
+  return sc_kernel_fk<R, 0>(which);
 }
 
 // ---------------------------------------------------------- the context --
@@ -298,7 +307,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   fk = functional_kind(P.density_expression, P.dim);
   if ((st = occupancy(f64 ? sc_kernel_ptr<double>(0, fk) : sc_kernel_ptr<float>(0, fk), kStepThreads, &occ_mu)))
     return st;
-  dens_which = (P.mixer ? P.pulay_scope : 1) <= 5 ? 1 : 2;
+  dens_which = density_variant(P.mixer ? P.pulay_scope : 1);
   if ((st = occupancy(f64 ? sc_kernel_ptr<double>(dens_which, fk) : sc_kernel_ptr<float>(dens_which, fk), kDensityThreads,
                       &occ_dens)))
     return st;
@@ -418,6 +427,9 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.mode = mode;
   return a;
 }
+
+template StepArgs<double> Ctx::step_args<double>(int);
+template StepArgs<float> Ctx::step_args<float>(int);
 
 // parts: bit 0 mu kernel, bit 1 density kernel, bit 2 mixing kernel (a
 // mode still runs only the kernels it has)
@@ -579,7 +591,9 @@ int Ctx::fill_result(mpdpft_result* r, const ScState& h) {
 // Energies of the current state (GetEnergy, mpDPFT.cpp:5414-5436): the
 // densities are the mixed densities of the last iteration, V and mu those
 // of the last density evaluation, as in the reference's ExportData.
-int Ctx::energy(mpdpft_result* r, const ScState& h) {
+// energy_issue leaves the kNEnergy integrals (times dvol) at e_dev on the
+// stream; energy_finish forms the energies from them on the host.
+int Ctx::energy_issue(const ScState& h, double* e_dev) {
   int st;
   double* d_mu = d_io;  // scratch
   CU(cudaMemcpyAsync(d_mu, h.mu, sizeof(double) * kMaxS, cudaMemcpyHostToDevice, stream));
@@ -596,14 +610,23 @@ int Ctx::energy(mpdpft_result* r, const ScState& h) {
     k_energy<float><<<blocks, kThreads, 0, stream>>>(geom, S, (const float*)d_V, (const float*)d_vext,
                                                      (const float*)dens, has_coulomb ? (const float*)d_vh : nullptr,
                                                      d_mu, d_part);
+  k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, kNEnergy, geom.dvol, e_dev);
   CU(cudaGetLastError());
-  std::vector<double> hp((size_t)blocks * kNEnergy);
-  CU(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, stream));
+  return MPDPFT_OK;
+}
+
+int Ctx::energy(mpdpft_result* r, const ScState& h) {
+  int st;
+  double* e_dev = d_io + kMaxS;
+  if ((st = energy_issue(h, e_dev))) return st;
+  double E[kNEnergy];
+  CU(cudaMemcpyAsync(E, e_dev, sizeof(E), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
-  double E[kNEnergy] = {0};
-  for (int b = 0; b < blocks; ++b)
-    for (int j = 0; j < kNEnergy; ++j) E[j] += hp[(size_t)b * kNEnergy + j];
-  for (int j = 0; j < kNEnergy; ++j) E[j] *= geom.dvol;
+  energy_finish(r, E);
+  return MPDPFT_OK;
+}
+
+void Ctx::energy_finish(mpdpft_result* r, const double* E) {
   const double D = P.dim;
   double etot = 0.0;
   for (int a = 0; a < P.n_interactions; ++a) {
@@ -639,7 +662,6 @@ int Ctx::energy(mpdpft_result* r, const ScState& h) {
     etot += ekin + E[5 * s + 1];
   }
   r->e_total = etot;
-  return MPDPFT_OK;
 }
 
 // -------------------------------------------------- standalone operators --

@@ -16,6 +16,9 @@ extern thread_local std::string g_last_error;
 
 struct FftPlan;  // fft.cu
 
+// energy integrals per solve (k_energy)
+constexpr int kNEnergy = 5 * kMaxS + kMaxS * kMaxS;
+
 struct Ctx {
   mpdpft_params P;
   int device = 0;
@@ -50,7 +53,7 @@ struct Ctx {
   int log_cap = 0;
   int step_blocks = 0;
   int fk = 0;            // functional kind of the SC kernels (functional_kind)
-  int dens_which = 1;    // density kernel variant: 1 Pulay window <= 5, 2 up to kMaxP
+  int dens_which = 1;    // density kernel variant: 1 Pulay window <= 5, 3 <= 8, 2 up to kMaxP
   int dens_blocks = 0;   // grid of the density kernel
   int mix_blocks = 0;    // grid of the mixing kernel
   long chunk = kSegPts;  // points per warp in the mu kernel's list sweeps
@@ -89,6 +92,8 @@ struct Ctx {
   int sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph);
   int fill_result(mpdpft_result* r, const ScState& h);
   int energy(mpdpft_result* r, const ScState& h);
+  int energy_issue(const ScState& h, double* e_dev);  // kNEnergy integrals to e_dev (device)
+  void energy_finish(mpdpft_result* r, const double* E);
   int integrate_device(const void* f, double* out);
   // standalone operators
   int op_mu_search(int s, const double* v, double target, double* mu_io, double* ab_out, int* trials,

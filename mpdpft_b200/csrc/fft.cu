@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "engine.h"
 #include "fft.cuh"
 
@@ -148,6 +149,7 @@ struct ZArgs {
   double* vres_part;              // [blocks][kMaxS]
   unsigned long long* vmax_out;
   int coul_reg;                   // 1: regularised kernel (erf term), 0: truncated (plain scale)
+  const int* skip;                // batched launches: nonzero -> this solve has finished (no work)
 };
 
 // R2C along the contiguous axis.  Block = zl rows; each row of s reals is
@@ -211,13 +213,13 @@ __device__ __forceinline__ R z_input(const ZArgs<R>& a, long p, double shift) {
 // read as M complex z_m = x_2m + i x_2m+1, transformed (length M) and split
 // into the s/2 + 1 outputs X_q = E_q + e^{-2 pi i q/s} O_q.
 template <typename R, int NC, int NL>
-__global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
+__device__ __forceinline__ void z_r2c_body(const ZArgs<R>& a, const long blk) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   const int M = NC > 0 ? NC : a.M;
   const int zl = NC > 0 ? NL : a.zl;
   const int H = M + 1;
-  const long row0 = (long)blockIdx.x * zl;
+  const long row0 = blk * zl;
   const int s = a.g.s;
   double shift = 0.0;  // no shell points: no shift
   if (a.pro == PRO_TAPER && *a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
     fft_lines<C, NC, NL, true>(A, B, tws, -1, load, store);
     if (a.part) {
       double acc[1] = {rowsum};
-      block_reduce_store<1>(acc, a.part + blockIdx.x);
+      block_reduce_store<1>(acc, a.part + blk);
     }
   } else {
     C* A = reinterpret_cast<C*>(smem_raw);
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
     }
     if (a.part) {
       double acc[1] = {rowsum};
-      block_reduce_store<1>(acc, a.part + blockIdx.x);
+      block_reduce_store<1>(acc, a.part + blk);
     }
     __syncthreads();
     Z = tile_fft<C>(A, B, a.plan, zl, a.tw_m, -1);
@@ -289,6 +291,22 @@ __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
   }
 }
 
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
+  z_r2c_body<R, NC, NL>(a, blockIdx.x);
+}
+
+// Batched launch: blockIdx.y selects the transform's arguments (one solve
+// and species of a batch, all with the same grid size).
+__device__ __forceinline__ bool batch_skip(const int* skip) { return skip && __ldcg(skip) != 0; }
+
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_z_r2c_b(const ZArgs<R>* __restrict__ args) {
+  const ZArgs<R>& a = args[blockIdx.y];
+  if (batch_skip(a.skip)) return;
+  z_r2c_body<R, NC, NL>(a, blockIdx.x);
+}
+
 // Epilogue value of the C2R pass at element p (single-field epilogues).
 template <typename R>
 __device__ __forceinline__ R z_output(const ZArgs<R>& a, long p, R v, double f0) {
@@ -304,13 +322,13 @@ __device__ __forceinline__ R z_output(const ZArgs<R>& a, long p, R v, double f0)
 
 // C2R along the contiguous axis for nin half-spectrum rows, with epilogue.
 template <typename R, int NC, int NL>
-__global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
+__device__ __forceinline__ void z_c2r_body(const ZArgs<R>& a, const long blk) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   const int M = NC > 0 ? NC : a.M;
   const int zl = NC > 0 ? NL : a.zl;
   const int H = M + 1;
-  const long row0 = (long)blockIdx.x * zl;
+  const long row0 = blk * zl;
   const int s = a.g.s;
   double f0 = 0.0;
   if (a.epi == EPI_COULOMB) {  // f0 = dvol * sum of the R2C pass's block sums (same order in every block)
@@ -419,6 +437,18 @@ __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
   }
 }
 
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
+  z_c2r_body<R, NC, NL>(a, blockIdx.x);
+}
+
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_z_c2r_b(const ZArgs<R>* __restrict__ args) {
+  const ZArgs<R>& a = args[blockIdx.y];
+  if (batch_skip(a.skip)) return;
+  z_c2r_body<R, NC, NL>(a, blockIdx.x);
+}
+
 // Y or X pass arguments.  Lines run along an axis of stride `astride`
 // (complex elements); a line is identified by (outer, col) with base
 // outer * ostride + col, col in [0, H).  Blocks [0, nbulk) take tk adjacent
@@ -445,11 +475,11 @@ struct AxisArgs {
   double cutoff;        // truncated Coulomb radius
   const double* f0_part;  // Z-pass input sums (Coulomb, k = 0 mode)
   int f0_blocks;
+  const int* skip;        // batched launches: nonzero -> this solve has finished (no work)
 };
 
 template <typename R>
-__device__ __forceinline__ bool axis_line(const AxisArgs<R>& a, int l, long& base, long& outer, int& col) {
-  const long b = blockIdx.x;
+__device__ __forceinline__ bool axis_line(const AxisArgs<R>& a, long b, int l, long& base, long& outer, int& col) {
   if (b < a.nbulk) {
     outer = b / a.ntile;
     col = (int)(b % a.ntile) * a.tk + l;
@@ -467,6 +497,7 @@ template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
+  const long blk = blockIdx.x;
   C* data = a.data[blockIdx.y];
   const C* twg = a.dir < 0 ? a.twf : a.twb;
   if constexpr (NC > 0) {
@@ -479,7 +510,7 @@ __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
     if (threadIdx.x < NL) {
       long base, outer;
       int col;
-      s_ok[threadIdx.x] = axis_line(a, threadIdx.x, base, outer, col) ? 1 : 0;
+      s_ok[threadIdx.x] = axis_line(a, blk, threadIdx.x, base, outer, col) ? 1 : 0;
       s_base[threadIdx.x] = base;
     }
     __syncthreads();
@@ -501,7 +532,7 @@ __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
       long base, outer;
       int col;
       C v = {R(0), R(0)};
-      if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+      if (axis_line(a, blk, l, base, outer, col)) v = data[base + t * a.astride];
       A[t * tk + l] = v;
     }
     __syncthreads();
@@ -510,7 +541,7 @@ __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
       const int t = w / tk, l = w % tk;
       long base, outer;
       int col;
-      if (axis_line(a, l, base, outer, col)) data[base + t * a.astride] = res[t * tk + l];
+      if (axis_line(a, blk, l, base, outer, col)) data[base + t * a.astride] = res[t * tk + l];
     }
   }
 }
@@ -614,7 +645,7 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier_tab(const AxisArgs
 }
 
 template <typename R, int NC, int NL>
-__global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
+__device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const long blk) {
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double s_f0;
@@ -650,7 +681,7 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
       const int l = threadIdx.x;
       long base, outer;
       int col;
-      s_ok[l] = axis_line(a, l, base, outer, col) ? 1 : 0;
+      s_ok[l] = axis_line(a, blk, l, base, outer, col) ? 1 : 0;
       s_base[l] = base;
       s_outer[l] = outer;
       s_col[l] = col;
@@ -693,7 +724,7 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
       long base, outer;
       int col;
       C v = {R(0), R(0)};
-      if (axis_line(a, l, base, outer, col)) v = data[base + t * a.astride];
+      if (axis_line(a, blk, l, base, outer, col)) v = data[base + t * a.astride];
       A[t * tk + l] = v;
     }
     __syncthreads();
@@ -706,7 +737,7 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
         long base, outer;
         int col;
         C v = F[t * tk + l];
-        if (axis_line(a, l, base, outer, col)) v = apply_multiplier<R>(a, v, t, outer, col, o, f0);
+        if (axis_line(a, blk, l, base, outer, col)) v = apply_multiplier<R>(a, v, t, outer, col, o, f0);
         spare[t * tk + l] = v;
       }
       __syncthreads();
@@ -716,11 +747,23 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
         const int t = w / tk, l = w % tk;
         long base, outer;
         int col;
-        if (axis_line(a, l, base, outer, col)) dst[base + t * a.astride] = res[t * tk + l];
+        if (axis_line(a, blk, l, base, outer, col)) dst[base + t * a.astride] = res[t * tk + l];
       }
       __syncthreads();
     }
   }
+}
+
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
+  x_roundtrip_body<R, NC, NL>(a, blockIdx.x);
+}
+
+template <typename R, int NC, int NL>
+__global__ void __launch_bounds__(kFftThreads) k_x_roundtrip_b(const AxisArgs<R>* __restrict__ args) {
+  const AxisArgs<R>& a = args[blockIdx.y];
+  if (batch_skip(a.skip)) return;
+  x_roundtrip_body<R, NC, NL>(a, blockIdx.x);
 }
 
 // V assembly (UpdateV, mpDPFT.cpp:4815-4838) when Coulomb terms exist:
@@ -732,9 +775,14 @@ __device__ __forceinline__ bool in_shell(double r2, double r0, double w) {
   return r2 < hi * hi && (lo <= 0.0 || r2 > lo * lo);
 }
 
+// Body of the V assembly over blocks blk of nblk: species s < nmax also
+// update their taper-shell maximum vmax[s]; update = 0 only takes the
+// shell maxima of the current V (the DelField of the start potential).
 template <typename R>
-__global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const R* vh, const R* nin_ring, R* V,
-                             double* vres_part, unsigned long long* vmax, double shell_r, double shell_w) {
+__device__ __forceinline__ void assemble_v_body(const KParams& kp, const ScState* st, const R* vext, const R* vh,
+                                                const R* nin_ring, R* V, double* vres_part, unsigned long long* vmax,
+                                                double shell_r, double shell_w, int nmax, int update, long blk,
+                                                long nblk) {
   const long n = kp.geom.n;
   const int S = kp.S;
   if (__ldcg(&st->exit_loop)) return;
@@ -742,47 +790,62 @@ __global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const
   const double incv = __ldcg(&st->inc_v);
   const double fac = incv < 1.0 ? incv : 1.0;
   const R* nin = nin_ring + (long)cur * S * n;
-  double acc[kMaxS];
-  for (int s = 0; s < kMaxS; ++s) acc[s] = 0.0;
-  double vm = -1.0e300;
-  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+  double acc[kMaxS], vm[kMaxS];
+  for (int s = 0; s < kMaxS; ++s) { acc[s] = 0.0; vm[s] = -1.0e300; }
+  for (long p = blk * blockDim.x + threadIdx.x; p < n; p += nblk * blockDim.x) {
     double x, y, z;
     point_coords(p, kp.geom, x, y, z);
     const bool shell = in_shell(x * x + y * y + z * z, shell_r, shell_w);
     for (int s = 0; s < S; ++s) {
-      R vi = vh ? vh[(long)s * n + p] : R(0);
-      if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];
-      if (kp.contact_mutual) {
-        R t = R(0);
-        for (int q = 0; q < S; ++q)
-          if (q != s) t += nin[(long)q * n + p];
-        vi += R(kp.beta) * t;
+      R vnew;
+      if (update) {
+        R vi = vh ? vh[(long)s * n + p] : R(0);
+        if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];
+        if (kp.contact_mutual) {
+          R t = R(0);
+          for (int q = 0; q < S; ++q)
+            if (q != s) t += nin[(long)q * n + p];
+          vi += R(kp.beta) * t;
+        }
+        if (kp.dirac) {
+          R ns = nin[(long)s * n + p];
+          ns = ns > R(0) ? ns : R(0);
+          if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+          else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+        }
+        vnew = vext[(long)s * n + p] + R(fac) * vi;
+        double d = (double)vnew - (double)V[(long)s * n + p];
+        acc[s] += d * d;
+        V[(long)s * n + p] = vnew;
+      } else {
+        vnew = V[(long)s * n + p];
       }
-      if (kp.dirac) {
-        R ns = nin[(long)s * n + p];
-        ns = ns > R(0) ? ns : R(0);
-        if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
-        else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
-      }
-      R vnew = vext[(long)s * n + p] + R(fac) * vi;
-      double d = (double)vnew - (double)V[(long)s * n + p];
-      acc[s] += d * d;
-      V[(long)s * n + p] = vnew;
-      if (s == 0 && shell) vm = fmax(vm, (double)vnew);
+      if (s < nmax && shell) vm[s] = fmax(vm[s], (double)vnew);
     }
   }
-  block_reduce_store<kMaxS>(acc, vres_part + (long)blockIdx.x * kMaxS);
+  if (update) block_reduce_store<kMaxS>(acc, vres_part + blk * kMaxS);
   // block max -> global ordered max (order independent, so deterministic)
   __shared__ double sm[32];
-  double t = vm;
-  for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double b = sm[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, sm[w]);
-    if (b > -1.0e300) atomicMax(vmax, ordered_bits(b));
+  for (int s = 0; s < nmax; ++s) {
+    double t = vm[s];
+    for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = sm[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, sm[w]);
+      if (b > -1.0e300) atomicMax(vmax + s, ordered_bits(b));
+    }
   }
+}
+
+// V assembly of one solve; the taper shift of species 0 (the others take
+// k_shell_max before their DelField).
+template <typename R>
+__global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const R* vh, const R* nin_ring, R* V,
+                             double* vres_part, unsigned long long* vmax, double shell_r, double shell_w) {
+  assemble_v_body<R>(kp, st, vext, vh, nin_ring, V, vres_part, vmax, shell_r, shell_w, 1, 1, blockIdx.x, gridDim.x);
 }
 
 // Shell maximum of a standalone field (the DelField entry point).
@@ -906,6 +969,49 @@ static bool launch_x_ct(int n, unsigned grid, size_t smem, cudaStream_t st, cons
 template <typename R>
 constexpr int ct_width() { return sizeof(R) == sizeof(double) ? 8 : 16; }
 
+// Batched launches (grid.y = argument sets of one grid size).
+template <typename R, int NL>
+static bool launch_z_r2c_b_ct(int M, dim3 grid, size_t smem, cudaStream_t st, const ZArgs<R>* a) {
+  switch (M) {
+#define CASE(N)                                                   \
+  case N:                                                         \
+    smem_optin(k_z_r2c_b<R, N, NL>);                              \
+    k_z_r2c_b<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);      \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R, int NL>
+static bool launch_z_c2r_b_ct(int M, dim3 grid, size_t smem, cudaStream_t st, const ZArgs<R>* a) {
+  switch (M) {
+#define CASE(N)                                                   \
+  case N:                                                         \
+    smem_optin(k_z_c2r_b<R, N, NL>);                              \
+    k_z_c2r_b<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);      \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
+template <typename R, int NL>
+static bool launch_x_b_ct(int n, dim3 grid, size_t smem, cudaStream_t st, const AxisArgs<R>* a) {
+  switch (n) {
+#define CASE(N)                                                       \
+  case N:                                                             \
+    smem_optin(k_x_roundtrip_b<R, N, NL>);                            \
+    k_x_roundtrip_b<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);    \
+    return true;
+    MPDPFT_CT_LENGTHS(CASE)
+#undef CASE
+    default: return false;
+  }
+}
+
 // ------------------------------------------------------------ host side --
 template <typename R>
 static int make_twiddles(Ctx& c, FftPlan& f) {
@@ -1005,8 +1111,10 @@ static ZArgs<R> zargs(Ctx& c) {
   return a;
 }
 
+// Arguments of the R2C pass (vmax: the taper shift slot).
 template <typename R>
-static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qcoef, void* out, bool sums) {
+static ZArgs<R> r2c_args(Ctx& c, const R* in, int pro, int nsrc, const double* qcoef, void* out, bool sums,
+                         unsigned long long* vmax) {
   FftPlan& f = *c.fft;
   ZArgs<R> a = zargs<R>(c);
   a.tw_m = (const typename Cx<R>::T*)f.tw_m_f;
@@ -1014,13 +1122,25 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   a.pro = pro;
   a.nsrc = nsrc;
   for (int q = 0; q < nsrc && qcoef; ++q) a.qcoef[q] = qcoef[q];
-  a.vmax = f.vmax;
+  a.vmax = vmax;
   a.taper_r0 = c.P.regularization_threshold * c.P.edge;
   a.taper_a = -2500.0 / (c.P.edge * c.P.edge);
   a.out = (typename Cx<R>::T*)out;
   a.part = sums ? f.zpart : nullptr;
+  return a;
+}
+
+template <typename R>
+static size_t r2c_smem(const FftPlan& f) {
+  return (3 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T);
+}
+
+template <typename R>
+static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qcoef, void* out, bool sums) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = r2c_args<R>(c, in, pro, nsrc, qcoef, out, sums, f.vmax);
   if (sums) f.zparts = f.zblocks;
-  const size_t smem = (3 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T);
+  const size_t smem = r2c_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
   if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_r2c<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
@@ -1028,8 +1148,9 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   return MPDPFT_OK;
 }
 
+// Arguments of the C2R pass.
 template <typename R>
-static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* out1, double coul_coef) {
+static ZArgs<R> c2r_args(Ctx& c, void* const* in, int nin, int epi, R* out0, R* out1, double coul_coef) {
   FftPlan& f = *c.fft;
   ZArgs<R> a = zargs<R>(c);
   a.tw_m = (const typename Cx<R>::T*)f.tw_m_b;
@@ -1042,7 +1163,19 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   a.coul_coef = coul_coef;
   a.f0_part = f.zpart;
   a.f0_blocks = f.zparts;
-  const size_t smem = (2 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
+  return a;
+}
+
+template <typename R>
+static size_t c2r_smem(const FftPlan& f) {
+  return (2 * (size_t)f.M * (f.zl + 1) + f.M) * sizeof(typename Cx<R>::T) + sizeof(R) * (size_t)f.s * f.zl;
+}
+
+template <typename R>
+static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* out1, double coul_coef) {
+  FftPlan& f = *c.fft;
+  ZArgs<R> a = c2r_args<R>(c, in, nin, epi, out0, out1, coul_coef);
+  const size_t smem = c2r_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_c2r<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
@@ -1099,8 +1232,9 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   return MPDPFT_OK;
 }
 
+// Arguments of the X round trip.
 template <typename R>
-static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, double sigma_c) {
+static AxisArgs<R> x_args(Ctx& c, void* in, void* const* out, int nout, int mul, double sigma_c) {
   FftPlan& f = *c.fft;
   AxisArgs<R> a = axis_args<R>(c, 0);
   a.data[0] = (typename Cx<R>::T*)in;
@@ -1111,15 +1245,37 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   a.cutoff = c.P.coulomb_cutoff > 0.0 ? c.P.coulomb_cutoff : 0.5 * c.P.edge;
   a.f0_part = f.zpart;
   a.f0_blocks = f.zparts;
+  return a;
+}
+
+template <typename R>
+static unsigned x_grid(const AxisArgs<R>& a) {
   const long nyq_blocks = (a.nouter + a.tk - 1) / a.tk;
-  const size_t csz = sizeof(typename Cx<R>::T);
-  const size_t smem_ct = (3 * (size_t)f.s * (f.tk + 1) + 2 * f.s) * csz;
-  const size_t smem_rt = 3 * (size_t)f.s * f.tk * csz;
-  const unsigned grid = (unsigned)(a.nbulk + nyq_blocks);
+  return (unsigned)(a.nbulk + nyq_blocks);
+}
+
+// Compile-time tile of the X round trip: shared memory, and whether it fits.
+template <typename R>
+static size_t x_smem_ct(const FftPlan& f) {
+  return (3 * (size_t)f.s * (f.tk + 1) + 2 * f.s) * sizeof(typename Cx<R>::T);
+}
+template <typename R>
+static size_t x_smem_rt(const FftPlan& f) {
+  return 3 * (size_t)f.s * f.tk * sizeof(typename Cx<R>::T);
+}
+template <typename R>
+static bool x_ct_fits(const FftPlan& f) {
+  return x_smem_ct<R>(f) + sizeof(MulTables<R, 512, 16>) <= 227 * 1024;
+}
+
+template <typename R>
+static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, double sigma_c) {
+  FftPlan& f = *c.fft;
+  AxisArgs<R> a = x_args<R>(c, in, out, nout, mul, sigma_c);
+  const unsigned grid = x_grid<R>(a);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
-  const bool ct_fits = smem_ct + sizeof(MulTables<R, 512, 16>) <= 227 * 1024;
-  if (f.tk != ct_width<R>() || !ct_fits || !launch_x_ct<R, ct_width<R>()>(f.s, grid, smem_ct, c.stream, a))
-    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, smem_rt, c.stream>>>(a);
+  if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
+    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1754,6 +1910,258 @@ int Ctx::profile_stage(int stage, int reps, double* ms, double* bytes) {
 int Ctx::alloc_io(long doubles) {
   (void)doubles;  // d_io holds 2 * max(n_ref, n) doubles, enough for one complex field
   return MPDPFT_OK;
+}
+
+// ================================================================ batches ==
+// DelField of a 2D field as the six argument sets of delfield_into's row
+// and column passes: z[0] R2C (taper), x[0] derivatives + Laplacian, z[1]
+// C2R -> |grad f|^2 (raw) and Laplacian, z[2] R2C of |grad f|^2, x[1]
+// smoothing, z[3] C2R with the clamp at 0.
+template <typename R>
+struct Delfield2D {
+  ZArgs<R> z[4];
+  AxisArgs<R> x[2];
+};
+
+template <typename R>
+static Delfield2D<R> delfield2d_args(Ctx& c, const R* f, R* g2, R* lap, void* const* spec, void* rtmp,
+                                     unsigned long long* vmax) {
+  const double smear = c.P.smearing_extent > 0.0 ? c.P.smearing_extent : 6.0 * c.geom.dx;
+  const double sigma_c = -0.5 * smear * smear;
+  const int pro = c.P.taper_off ? PRO_TAPER : PRO_NONE;
+  void* outs[3] = {spec[1], spec[2], spec[3]};
+  Delfield2D<R> d;
+  d.z[0] = r2c_args<R>(c, f, pro, 1, nullptr, spec[0], false, vmax);
+  d.x[0] = x_args<R>(c, spec[0], outs, 3, MUL_DERIV, sigma_c);
+  d.z[1] = c2r_args<R>(c, outs, 3, EPI_GRAD, (R*)rtmp, lap, 0.0);
+  d.z[2] = r2c_args<R>(c, (const R*)rtmp, PRO_NONE, 1, nullptr, spec[0], false, vmax);
+  d.x[1] = x_args<R>(c, spec[0], &spec[0], 1, MUL_SMOOTH, sigma_c);
+  d.z[3] = c2r_args<R>(c, &spec[0], 1, EPI_POS, g2, nullptr, 0.0);
+  return d;
+}
+
+struct BatchFftClass {
+  size_t rsize = 8;
+  int count = 0;        // argument sets (members x species)
+  int M = 0, s = 0, zl = 0, tk = 0, zblocks = 0;
+  unsigned xgrid = 0;
+  size_t smem_r2c = 0, smem_c2r = 0, smem_xct = 0, smem_xrt = 0;
+  bool xct = false;
+  void* d_z[4] = {nullptr, nullptr, nullptr, nullptr};  // ZArgs<R>[count]
+  void* d_x[2] = {nullptr, nullptr};                    // AxisArgs<R>[count]
+};
+
+template <typename R>
+static int batch_fft_build(const std::vector<BatchMember>& members, unsigned long long* vmax_all, BatchFftClass* b) {
+  std::vector<ZArgs<R>> z[4];
+  std::vector<AxisArgs<R>> x[2];
+  for (const BatchMember& m : members) {
+    Ctx& c = *m.c;
+    FftPlan& f = *c.fft;
+    const long n = c.geom.n;
+    for (int s = 0; s < c.S; ++s) {
+      void* spec[4];
+      void* rtmp;
+      if (s == 0) {
+        for (int i = 0; i < 4; ++i) spec[i] = f.spec[i];
+        rtmp = f.rtmp;
+      } else {  // the species run concurrently: scratch of their own
+        int st;
+        for (int i = 0; i < 4; ++i)
+          if ((st = c.alloc(&spec[i], 2 * c.rsize * f.nspec))) return st;
+        if ((st = c.alloc(&rtmp, c.rsize * n))) return st;
+      }
+      Delfield2D<R> d = delfield2d_args<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
+                                           (R*)c.d_lap + (long)s * n, spec, rtmp,
+                                           vmax_all + (long)m.index * kMaxS + s);
+      const int* skip = &c.d_state->exit_loop;
+      for (int i = 0; i < 4; ++i) { d.z[i].skip = skip; z[i].push_back(d.z[i]); }
+      for (int i = 0; i < 2; ++i) { d.x[i].skip = skip; x[i].push_back(d.x[i]); }
+    }
+  }
+  Ctx& c0 = *members[0].c;
+  FftPlan& f = *c0.fft;
+  b->rsize = sizeof(R);
+  b->count = (int)z[0].size();
+  b->M = f.M;
+  b->s = f.s;
+  b->zl = f.zl;
+  b->tk = f.tk;
+  b->zblocks = f.zblocks;
+  b->xgrid = x_grid<R>(x[0][0]);
+  b->smem_r2c = r2c_smem<R>(f);
+  b->smem_c2r = c2r_smem<R>(f);
+  b->smem_xct = x_smem_ct<R>(f);
+  b->smem_xrt = x_smem_rt<R>(f);
+  b->xct = f.tk == ct_width<R>() && x_ct_fits<R>(f);
+  for (int i = 0; i < 4; ++i) {
+    CU(cudaMalloc(&b->d_z[i], sizeof(ZArgs<R>) * b->count));
+    CU(cudaMemcpy(b->d_z[i], z[i].data(), sizeof(ZArgs<R>) * b->count, cudaMemcpyHostToDevice));
+  }
+  for (int i = 0; i < 2; ++i) {
+    CU(cudaMalloc(&b->d_x[i], sizeof(AxisArgs<R>) * b->count));
+    CU(cudaMemcpy(b->d_x[i], x[i].data(), sizeof(AxisArgs<R>) * b->count, cudaMemcpyHostToDevice));
+  }
+  return MPDPFT_OK;
+}
+
+int batch_fft_create(const std::vector<BatchMember>& members, unsigned long long* vmax_all, BatchFftClass** out) {
+  *out = nullptr;
+  if (members.empty()) return set_error(MPDPFT_ERR_ARG, "empty batch class");
+  for (const BatchMember& m : members) {
+    const Ctx& c = *m.c;
+    if (c.P.dim != 2 || !c.gradient || !c.fft || c.fft->plane)
+      return set_error(MPDPFT_ERR_ARG, "batched DelField: 2D gradient-corrected solves only");
+    if (c.P.steps != members[0].c->P.steps || c.rsize != members[0].c->rsize)
+      return set_error(MPDPFT_ERR_ARG, "batched DelField: one grid size and precision per class");
+  }
+  BatchFftClass* b = new BatchFftClass;
+  const int st = members[0].c->rsize == sizeof(double) ? batch_fft_build<double>(members, vmax_all, b)
+                                                       : batch_fft_build<float>(members, vmax_all, b);
+  if (st) {
+    batch_fft_destroy(b);
+    return st;
+  }
+  *out = b;
+  return MPDPFT_OK;
+}
+
+template <typename R>
+static int batch_fft_issue_t(BatchFftClass* b, cudaStream_t st) {
+  const ZArgs<R>* z[4];
+  const AxisArgs<R>* x[2];
+  for (int i = 0; i < 4; ++i) z[i] = (const ZArgs<R>*)b->d_z[i];
+  for (int i = 0; i < 2; ++i) x[i] = (const AxisArgs<R>*)b->d_x[i];
+  const dim3 zg(b->zblocks, b->count), xg(b->xgrid, b->count);
+  auto r2c = [&](const ZArgs<R>* a) {
+    if (b->zl != 16 || !launch_z_r2c_b_ct<R, 16>(b->M, zg, b->smem_r2c, st, a))
+      k_z_r2c_b<R, 0, 0><<<zg, kFftThreads, b->smem_r2c, st>>>(a);
+  };
+  auto c2r = [&](const ZArgs<R>* a) {
+    if (b->zl != 16 || !launch_z_c2r_b_ct<R, 16>(b->M, zg, b->smem_c2r, st, a))
+      k_z_c2r_b<R, 0, 0><<<zg, kFftThreads, b->smem_c2r, st>>>(a);
+  };
+  auto xrt = [&](const AxisArgs<R>* a) {
+    if (!b->xct || !launch_x_b_ct<R, ct_width<R>()>(b->s, xg, b->smem_xct, st, a))
+      k_x_roundtrip_b<R, 0, 0><<<xg, kFftThreads, b->smem_xrt, st>>>(a);
+  };
+  r2c(z[0]);
+  xrt(x[0]);
+  c2r(z[1]);
+  r2c(z[2]);
+  xrt(x[1]);
+  c2r(z[3]);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+int batch_fft_issue(BatchFftClass* b, cudaStream_t st) {
+  return b->rsize == sizeof(double) ? batch_fft_issue_t<double>(b, st) : batch_fft_issue_t<float>(b, st);
+}
+
+void batch_fft_destroy(BatchFftClass* b) {
+  if (!b) return;
+  for (int i = 0; i < 4; ++i) cudaFree(b->d_z[i]);
+  for (int i = 0; i < 2; ++i) cudaFree(b->d_x[i]);
+  delete b;
+}
+
+double* batch_vres_part(const Ctx& c) { return c.fft ? c.fft->vres_part : nullptr; }
+
+// ---- batched V assembly: one launch over every member, block table ------
+template <typename R>
+struct AssembleArgs {
+  KParams kp;
+  const ScState* st;
+  const R* vext;
+  const R* nin;
+  R* V;
+  double* vres_part;
+  unsigned long long* vmax;  // [kMaxS]
+  double shell_r, shell_w;
+};
+
+template <typename R>
+__global__ void k_assemble_v_b(const AssembleArgs<R>* __restrict__ args, const int4* __restrict__ tab, int update) {
+  const int4 t = tab[blockIdx.x];  // (member, block, blocks)
+  const AssembleArgs<R>& a = args[t.x];
+  assemble_v_body<R>(a.kp, a.st, a.vext, nullptr, a.nin, a.V, a.vres_part, a.vmax, a.shell_r, a.shell_w, a.kp.S,
+                     update, t.y, t.z);
+}
+
+struct BatchAssemble {
+  size_t rsize = 8;
+  void* d_args = nullptr;
+  int4* d_tab = nullptr;
+  int blocks = 0;
+};
+
+template <typename R>
+static int batch_assemble_build(const std::vector<BatchMember>& members, unsigned long long* vmax_all,
+                                BatchAssemble* b, std::vector<int>* blocks_out) {
+  std::vector<AssembleArgs<R>> args;
+  std::vector<int4> tab;
+  blocks_out->clear();
+  for (size_t k = 0; k < members.size(); ++k) {
+    Ctx& c = *members[k].c;
+    AssembleArgs<R> a;
+    std::memset(&a, 0, sizeof(a));
+    a.kp = c.kparams();
+    a.st = c.d_state;
+    a.vext = (const R*)c.d_vext;
+    a.nin = (const R*)c.d_nin;
+    a.V = (R*)c.d_V;
+    a.vres_part = c.fft->vres_part;
+    a.vmax = vmax_all + (long)members[k].index * kMaxS;
+    a.shell_r = shell_radius(c);
+    a.shell_w = shell_width(c);
+    args.push_back(a);
+    // 8 points a thread, at most the rows of the residual partials
+    int nb = (int)std::min<long>((c.geom.n + 8L * kThreads - 1) / (8L * kThreads), c.fft->vblocks);
+    nb = std::max(nb, 1);
+    for (int i = 0; i < nb; ++i) tab.push_back(make_int4((int)k, i, nb, 0));
+    blocks_out->push_back(nb);
+  }
+  b->rsize = sizeof(R);
+  b->blocks = (int)tab.size();
+  CU(cudaMalloc(&b->d_args, sizeof(AssembleArgs<R>) * args.size()));
+  CU(cudaMemcpy(b->d_args, args.data(), sizeof(AssembleArgs<R>) * args.size(), cudaMemcpyHostToDevice));
+  CU(cudaMalloc((void**)&b->d_tab, sizeof(int4) * tab.size()));
+  CU(cudaMemcpy(b->d_tab, tab.data(), sizeof(int4) * tab.size(), cudaMemcpyHostToDevice));
+  return MPDPFT_OK;
+}
+
+int batch_assemble_create(const std::vector<BatchMember>& members, unsigned long long* vmax_all,
+                          BatchAssemble** out, std::vector<int>* blocks_out) {
+  *out = nullptr;
+  if (members.empty()) return set_error(MPDPFT_ERR_ARG, "empty batch");
+  for (const BatchMember& m : members)
+    if (m.c->has_coulomb || !m.c->fft) return set_error(MPDPFT_ERR_ARG, "batched V assembly: no Coulomb terms");
+  BatchAssemble* b = new BatchAssemble;
+  const int st = members[0].c->rsize == sizeof(double) ? batch_assemble_build<double>(members, vmax_all, b, blocks_out)
+                                                       : batch_assemble_build<float>(members, vmax_all, b, blocks_out);
+  if (st) {
+    batch_assemble_destroy(b);
+    return st;
+  }
+  *out = b;
+  return MPDPFT_OK;
+}
+
+int batch_assemble_issue(BatchAssemble* b, int update, cudaStream_t st) {
+  if (b->rsize == sizeof(double))
+    k_assemble_v_b<double><<<b->blocks, kThreads, 0, st>>>((const AssembleArgs<double>*)b->d_args, b->d_tab, update);
+  else
+    k_assemble_v_b<float><<<b->blocks, kThreads, 0, st>>>((const AssembleArgs<float>*)b->d_args, b->d_tab, update);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
+}
+
+void batch_assemble_destroy(BatchAssemble* b) {
+  if (!b) return;
+  cudaFree(b->d_args);
+  cudaFree(b->d_tab);
+  delete b;
 }
 
 }  // namespace mpdpft

@@ -322,6 +322,10 @@ inline int functional_kind(int expr, int dim) {
   return 0;
 }
 
+// Density kernel variant for a Pulay window (the PW template argument):
+// 1 -> 5, 3 -> 8, 2 -> kMaxP.
+inline int density_variant(int window) { return window <= 5 ? 1 : (window <= 8 ? 3 : 2); }
+
 // n at u = mu - V for one point.
 template <int FK>
 __device__ __forceinline__ double point_density(const DensParams& d, const EvalK& k, double u, double l, double g) {
@@ -468,15 +472,15 @@ __device__ __forceinline__ void block_sum2(int& x, int& y) {
 // current V (GetDensities for the initial densities, mpDPFT.cpp:195, and the
 // standalone mu-search entry point).  Not launched in mode 2 (admix only).
 template <typename R, int FK>
-__global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
+__device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, const int nblk) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
   const int S = kp.S;
-  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long nthreads = (long)gridDim.x * blockDim.x;
+  const long tid = (long)bid * blockDim.x + threadIdx.x;
+  const long nthreads = (long)nblk * blockDim.x;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const long gw = (long)blockIdx.x * kStepWarps + wib;
+  const long gw = (long)bid * kStepWarps + wib;
   __shared__ double red[kNPart];
   __shared__ MuState s_ms[kMaxS];
   // active-point lists as this block sees them (identical in every block)
@@ -486,20 +490,20 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
 
   if (a.mode == 0) {
     const int exited = ldcg(&st->exit_loop);
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->iter_active = exited ? 0 : 1;
+    if (bid == 0 && threadIdx.x == 0) st->iter_active = exited ? 0 : 1;
     if (exited) return;
   }
   // block 0 runs the scalar logic on a shared-memory copy of the state and
   // writes it back before every grid barrier after which others read it
   __shared__ ScState s_st;
   ScState* const ls = &s_st;
-  if (blockIdx.x == 0) {
+  if (bid == 0) {
     state_load(ls, st);
     __syncthreads();
   }
   const int cur = ldcg(&st->slot);
-  double* mypart = a.part + (long)blockIdx.x * kNPart;
-  MPDPFT_TSTAMP(0);
+  double* mypart = a.part + (long)bid * kNPart;
+  MPDPFT_TSTAMP_B(0);
 
   // ---- UpdateV (mpDPFT.cpp:4815-4838) -----------------------------------
   if (a.mode == 0 && a.assemble_v) {
@@ -554,16 +558,16 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
     s_llen[threadIdx.x] = 0;
   }
   __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) { ls->ms[s] = s_ms[s]; ls->prev_mu[s] = s_ms[s].start; }
     ls->mu_passes = 0;
     ls->iter_bits = 0;
   }
   // V written above is read at other points below
-  if (a.mode == 0 && a.assemble_v && !grid_barrier(st)) return;
+  if (a.mode == 0 && a.assemble_v && !grid_barrier(st, nblk)) return;
 
   const R* V = a.V;
-  MPDPFT_TSTAMP(1);
+  MPDPFT_TSTAMP_B(1);
   for (int pass = 0; pass < kMuMaxPasses; ++pass) {
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
@@ -608,16 +612,16 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
       if (threadIdx.x < S && s_need[threadIdx.x]) {
         int c = 0;
         for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
-        a.bcount[(long)threadIdx.x * gridDim.x + blockIdx.x] = c;
+        a.bcount[(long)threadIdx.x * nblk + bid] = c;
       }
-      if (!grid_barrier(st)) return;
+      if (!grid_barrier(st, nblk)) return;
       for (int s = 0; s < S; ++s) {
         if (!s_need[s]) continue;
         int before = 0, total = 0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-          const int c = __ldcg(a.bcount + (long)s * gridDim.x + b);
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+          const int c = __ldcg(a.bcount + (long)s * nblk + b);
           total += c;
-          if (b < (int)blockIdx.x) before += c;
+          if (b < (int)bid) before += c;
         }
         block_sum2(before, total);
         int off = before;
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
         s_lcap[threadIdx.x] = s_cap[threadIdx.x];
         s_need[threadIdx.x] = 0;
       }
-      if (!grid_barrier(st)) return;  // the lists are complete
+      if (!grid_barrier(st, nblk)) return;  // the lists are complete
     }
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
@@ -681,10 +685,10 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
       }
       block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
     }
-    if (!grid_barrier(st)) return;
-    if (blockIdx.x == 0) {
+    if (!grid_barrier(st, nblk)) return;
+    if (bid == 0) {
       for (int v = wib; v < S * kMuAcc; v += kStepWarps) {
-        const double t = warp_sum_rows(a.part + v, gridDim.x, kNPart);
+        const double t = warp_sum_rows(a.part + v, nblk, kNPart);
         if (lane == 0) red[v] = t;
       }
       __syncthreads();
@@ -705,13 +709,27 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
       __syncthreads();
       state_store(st, ls);
     }
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, nblk)) return;
   }
-  if (blockIdx.x == 0) {  // the pass-0 set-up when no pass ran
+  if (bid == 0) {  // the pass-0 set-up when no pass ran
     __syncthreads();
     state_store(st, ls);
   }
-  MPDPFT_TSTAMP(2);
+  MPDPFT_TSTAMP_B(2);
+}
+
+template <typename R, int FK>
+__global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
+  sc_mu_body<R, FK>(a, blockIdx.x, gridDim.x);
+}
+
+// Batched launches: entry b of the block table names the solve (x), the
+// block's index within that solve (y) and the solve's block count (z).
+template <typename R, int FK>
+__global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel_b(const StepArgs<R>* __restrict__ args,
+                                                                 const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  sc_mu_body<R, FK>(args[t.x], t.y, t.z);
 }
 
 // ------------------------------------------------------- density kernel --
@@ -723,7 +741,7 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
 // The last block to finish runs phase D: CheckConvergence, Intercept, the
 // Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
 template <typename R, int FK, int PW>
-__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs<R> a) {
+__device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int bid, const int nblk) {
   // PW: the largest Pulay window this instantiation handles (<= kMaxP); a
   // small window keeps the per-thread sums in few registers
   const KParams& kp = a.kp;
@@ -760,7 +778,7 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs
   __syncthreads();
   R* nin = a.nin + (long)cur * S * n;
   R* rcur = a.res + (long)cur * S * n;
-  const long gstride = (long)gridDim.x * blockDim.x;
+  const long gstride = (long)nblk * blockDim.x;
   for (int s = 0; s < S; ++s) {
     double acc[4 + PW];
 #pragma unroll
@@ -774,7 +792,7 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs
     const R* Gs = a.g2 ? a.g2 + so : nullptr;
     // one point per thread; every lane of a warp runs every trip (the vote
     // below needs them all)
-    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += gstride) {
+    for (long base = (long)bid * blockDim.x; base < n; base += gstride) {
       const long p = base + threadIdx.x;
       const bool valid = p < n;
       // issue the streaming loads first
@@ -819,12 +837,12 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs
         else if (j == I - 1) acc[4 + j] += wr * dr;
       }
     }
-    block_reduce_store<4 + PW>(acc, a.part2 + (long)blockIdx.x * kNPart + s * kNF);
+    block_reduce_store<4 + PW>(acc, a.part2 + (long)bid * kNPart + s * kNF);
   }
   // the last block to finish takes phase D
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(&st->k2_done, 1u) == gridDim.x - 1 ? 1 : 0;
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->k2_done, 1u) == nblk - 1 ? 1 : 0;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
@@ -842,12 +860,12 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs
   if (threadIdx.x == 0) s_pbits = 0;
   const int nv = 4 + I;  // per species: N, three dots, Gram row
   const int vres = (a.mode == 0 && (a.assemble_v || a.vres_part)) ? S : 0;
-  if (!vres) block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, nullptr, 0, 0, 0, red_v);
+  if (!vres) block_rows_sum2(a.part2, nblk, kNPart, S * nv, nv, kNF, red, nullptr, 0, 0, 0, red_v);
   else if (a.assemble_v)
-    block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, a.part + kVresOff, kp.mu_blocks, kNPart, S,
+    block_rows_sum2(a.part2, nblk, kNPart, S * nv, nv, kNF, red, a.part + kVresOff, kp.mu_blocks, kNPart, S,
                     red_v);
   else
-    block_rows_sum2(a.part2, gridDim.x, kNPart, S * nv, nv, kNF, red, a.vres_part, a.vres_blocks, kMaxS, S, red_v);
+    block_rows_sum2(a.part2, nblk, kNPart, S * nv, nv, kNF, red, a.vres_part, a.vres_blocks, kMaxS, S, red_v);
   if (threadIdx.x < I) {  // Gram row summed over species
     double t = 0.0;
     for (int s = 0; s < S; ++s) t += red[s * kNF + 4 + threadIdx.x];
@@ -1002,12 +1020,24 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs
   }
 }
 
+template <typename R, int FK, int PW>
+__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs<R> a) {
+  sc_density_body<R, FK, PW>(a, blockIdx.x, gridDim.x);
+}
+
+template <typename R, int FK, int PW>
+__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel_b(const StepArgs<R>* __restrict__ args,
+                                                                         const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  sc_density_body<R, FK, PW>(args[t.x], t.y, t.z);
+}
+
 // ---------------------------------------------------------- mix kernel --
 // The mixed density n = sum_j c_j (n_in,j + theta r_j) (Pulay) or
 // n_in + theta r (linear) into the next ring slot (AdmixDensities,
 // mpDPFT.cpp:4946-4955 / :4987).
 template <typename R>
-__global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) {
+__device__ __forceinline__ void sc_mix_body(const StepArgs<R>& a, const int bid, const int nblk) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
@@ -1016,7 +1046,7 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) 
   __shared__ double s_c[kMaxP];
   __shared__ int s_nc;
   if (a.mode == 0 && !ldcg(&st->iter_active)) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[5] = globaltimer();
+  if (bid == 0 && threadIdx.x == 0) st->tphase[5] = globaltimer();
   const int ring = kp.ring;
   const int cur = ldcg(&st->mix_src), next = ldcg(&st->slot);
   if (threadIdx.x == 0) {
@@ -1031,11 +1061,11 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) 
   }
   __syncthreads();
   const int nc = s_nc;
-  const long gstride = (long)gridDim.x * blockDim.x;
+  const long gstride = (long)nblk * blockDim.x;
   for (int s = 0; s < S; ++s) {
     const double th = ldcg(&st->theta_mix[s]);
     R* out = a.nin + (long)next * S * n + (long)s * n;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += gstride) {
+    for (long q = (long)bid * blockDim.x + threadIdx.x; 4 * q < n; q += gstride) {
       const long p0 = 4 * q;
       double v[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
@@ -1055,7 +1085,19 @@ __global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) 
       store4(a.cur_copy + (long)s * n, p0, n, kp.vec4, o4);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[6] = globaltimer();
+  if (bid == 0 && threadIdx.x == 0) st->tphase[6] = globaltimer();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) {
+  sc_mix_body<R>(a, blockIdx.x, gridDim.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel_b(const StepArgs<R>* __restrict__ args,
+                                                                  const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  sc_mix_body<R>(args[t.x], t.y, t.z);
 }
 
 }  // namespace mpdpft

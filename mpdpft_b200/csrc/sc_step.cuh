@@ -126,8 +126,9 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-#define MPDPFT_TSTAMP(k) \
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->tphase[k] = globaltimer()
+// phase timestamp from block 0 of a solve (bid: the block's index within it)
+#define MPDPFT_TSTAMP_B(k) \
+  if (bid == 0 && threadIdx.x == 0) st->tphase[k] = globaltimer()
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
@@ -148,7 +149,7 @@ __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
 // Bounded sense-free generation barrier over all blocks of a cooperative
 // launch.  Returns false (and raises the abort flag) if a block does not
 // arrive within the spin limit; every block then leaves its loop.
-__device__ inline bool grid_barrier(ScState* st) {
+__device__ inline bool grid_barrier(ScState* st, const int nblk) {
   __syncthreads();
   __shared__ int ok;
   if (threadIdx.x == 0) {
@@ -157,7 +158,7 @@ __device__ inline bool grid_barrier(ScState* st) {
     unsigned g = *gen;
     __threadfence();
     unsigned arrived = atomicAdd(&st->bar_count, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == (unsigned)nblk - 1u) {
       atomicExch(&st->bar_count, 0u);
       __threadfence();
       atomicAdd(&st->bar_gen, 1u);

@@ -29,6 +29,9 @@ EXPORTS = [
     "mpdpft_mu_search", "mpdpft_delfield", "mpdpft_fft", "mpdpft_integrate", "mpdpft_pulay_reset",
     "mpdpft_admix", "mpdpft_sc_run", "mpdpft_sc_step", "mpdpft_sc_init", "mpdpft_get_field",
     "mpdpft_energy", "mpdpft_profile_stage", "mpdpft_iteration_launches", "mpdpft_step_phase_times",
+    "mpdpft_batch_create", "mpdpft_batch_destroy", "mpdpft_batch_set_external_potential", "mpdpft_batch_sc_init",
+    "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
+    "mpdpft_batch_sync",
 ]
 
 
@@ -83,6 +86,15 @@ def load(path=LIB_PATH):
     L.mpdpft_profile_stage.argtypes = [vp, C.c_int, C.c_int, _dp, _dp]
     L.mpdpft_iteration_launches.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.mpdpft_step_phase_times.argtypes = [vp, _dp, C.c_int]
+    L.mpdpft_batch_create.argtypes = [P, C.c_int, C.c_int, C.POINTER(vp)]
+    L.mpdpft_batch_destroy.argtypes = [vp]
+    L.mpdpft_batch_set_external_potential.argtypes = [vp, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
+    L.mpdpft_batch_sc_init.argtypes = [vp, _dpp, C.c_int, C.c_int]
+    L.mpdpft_batch_sc_step.argtypes = [vp, C.c_int]
+    L.mpdpft_batch_sc_run.argtypes = [vp, _dpp, C.c_int, C.c_int, C.POINTER(abi.Result), C.POINTER(C.c_int)]
+    L.mpdpft_batch_get_field.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
+    L.mpdpft_batch_get_log.argtypes = [vp, C.c_int, C.POINTER(abi.IterLog), C.c_int, C.POINTER(C.c_int)]
+    L.mpdpft_batch_sync.argtypes = [vp]
     for name in EXPORTS:
         getattr(L, name)
     _lib = L
@@ -291,3 +303,86 @@ class Engine:
         r = abi.Result()
         self._check(self.lib.mpdpft_energy(self.h, C.byref(r)))
         return r
+
+
+class Batch:
+    """Many independent 2D SC solves advanced together (mpdpft_batch).
+
+    problems: list of (params, vext list, v0 list) as the workload builders
+    return them.  sc_run() returns (results, statuses)."""
+
+    def __init__(self, problems, device=0):
+        self.lib = load()
+        self.problems = problems
+        self.count = len(problems)
+        self.S = problems[0][0].species
+        params = (abi.Params * self.count)(*[p for p, _, _ in problems])
+        h = C.c_void_p()
+        st = self.lib.mpdpft_batch_create(params, self.count, device, C.byref(h))
+        if st != abi.OK:
+            raise MpdpftError(st, self.lib.mpdpft_last_error().decode())
+        self.h = h
+        for i, (p, vext, _) in enumerate(problems):
+            for s in range(self.S):
+                a = _arr(vext[s], p.grid_points(abi.LAYOUT_PERIODIC))
+                self._check(self.lib.mpdpft_batch_set_external_potential(self.h, i, s, _ptr(a),
+                                                                         abi.LAYOUT_PERIODIC, abi.MEM_HOST))
+
+    def _check(self, st):
+        if st != abi.OK:
+            raise MpdpftError(st, self.lib.mpdpft_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpdpft_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _v0(self):
+        arrs = []
+        for p, _, v0 in self.problems:
+            for s in range(self.S):
+                arrs.append(_arr(v0[s], p.grid_points(abi.LAYOUT_PERIODIC)))
+        self._keep = arrs
+        return _ptrs(arrs)
+
+    def sc_init(self):
+        self._check(self.lib.mpdpft_batch_sc_init(self.h, self._v0(), abi.LAYOUT_PERIODIC, abi.MEM_HOST))
+
+    def sc_step(self, iterations=1):
+        self._check(self.lib.mpdpft_batch_sc_step(self.h, iterations))
+
+    def sync(self):
+        self._check(self.lib.mpdpft_batch_sync(self.h))
+
+    def sc_run(self, check=True):
+        res = (abi.Result * self.count)()
+        status = (C.c_int * self.count)()
+        st = self.lib.mpdpft_batch_sc_run(self.h, self._v0(), abi.LAYOUT_PERIODIC, abi.MEM_HOST, res, status)
+        if check and st not in (abi.OK, abi.ERR_NOT_CONVERGED):
+            self._check(st)
+        return list(res), list(status)
+
+    def field(self, i, which, s, layout=abi.LAYOUT_PERIODIC):
+        p = self.problems[i][0]
+        out = np.empty(p.grid_points(layout))
+        self._check(self.lib.mpdpft_batch_get_field(self.h, i, which, s, _ptr(out), layout, abi.MEM_HOST))
+        return out
+
+    def log(self, i, cap=None):
+        cap = cap or (self.problems[i][0].max_sc_count + 2)
+        buf = (abi.IterLog * cap)()
+        n = C.c_int()
+        self._check(self.lib.mpdpft_batch_get_log(self.h, i, buf, cap, C.byref(n)))
+        return list(buf[:n.value])

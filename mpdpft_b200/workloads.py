@@ -11,8 +11,7 @@ Workloads (one SC solve each unless stated):
   argon_atom      Z=18 Gaussian nucleus, TF + gradient correction, Hartree,
                   Dirac exchange, 128^3
   sweep_2d        256 two-species 2D trapped gases, uneven grids (batched)
-  cluster_adjoint 13 Z=3 nuclei on an icosahedron, 192^3, adjoint loss
-  eh_plasma       two opposite-charge species on 256^3 in a random potential
+  electron_hole   two opposite-charge species on 256^3 in a random potential
 """
 import math
 
@@ -152,6 +151,48 @@ def electron_hole(steps=256, edge=40.0, precision=abi.MIXED, seed=SEED_BASE + 5,
     vext = gaussian_landscape(steps, edge, 64, seed)
     v0 = [vext + noise(vext.shape, 1e-3, seed + 100 * s) for s in range(2)]
     return p, [vext, vext.copy()], v0
+
+
+SWEEP_SIZES = (64, 128, 256, 512)
+
+
+def sweep_instance(i, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **over):
+    """Instance i of the batched 2D sweep: two species in the anisotropic
+    trap V = (x^2 + a^2 y^2)/2, a ~ U[1, 3]; grid s^2 with s drawn from
+    {64, 128, 256, 512}; N_s ~ U[100, 5000] per species; inter-species
+    contact coupling (type 1, V_s = beta n_s') with beta log-uniform in
+    [0.01, 2]; TF + gradient-corrected density (2D small-gradient form) at
+    the automatic temperature T = max|mu - V|/50; Pulay history 6 over both
+    species, theta 0.3.  The start mu is the Thomas-Fermi estimate
+    sqrt(2 a N (1 + beta/(2 pi)) / g) and the box edge is 3 sqrt(2 mu_max),
+    1.5 times the larger cloud radius; smoothing width 1.5 grid spacings.
+    V_0 = V_ext + U(-1e-3, 1e-3), seeded per instance and species."""
+    rng = np.random.default_rng(seed * 1000 + i)
+    s = int(rng.choice(SWEEP_SIZES))
+    if steps is not None:
+        s = steps
+    n_target = rng.uniform(100.0, 5000.0, 2)
+    beta = math.exp(rng.uniform(math.log(0.01), math.log(2.0)))
+    a = rng.uniform(1.0, 3.0)
+    g = 1.0
+    mu = [math.sqrt(2.0 * a * n_target[q] * (1.0 + beta / (2.0 * math.pi)) / g) for q in range(2)]
+    edge = 3.0 * math.sqrt(2.0 * max(mu))
+    x = axis(s, edge)
+    vext = (0.5 * (x[:, None] ** 2 + a * a * x[None, :] ** 2)).reshape(-1)
+    kw = dict(dim=2, steps=s, species=2, edge=edge, abundances=list(n_target), rel_acc=1e-10,
+              density_expression=abi.DENS_GRADIENT, degeneracy=g, interactions=[abi.INT_CONTACT_MUTUAL],
+              beta=beta, mu=mu, temperature=[-1.0, -1.0], mixer=1, pulay_scope=6, theta=[0.3, 0.3],
+              sc_criterion=1e-10, max_sc_count=300, smearing_extent=1.5 * edge / s,
+              regularization_threshold=0.45, precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    v0 = [vext + noise(vext.shape, 1e-3, seed * 1000 + i + 100 * q) for q in range(2)]
+    return p, [vext, vext.copy()], v0
+
+
+def sweep_2d(count=256, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **over):
+    """The batched sweep: `count` instances of sweep_instance."""
+    return [sweep_instance(i, seed, steps, precision, **over) for i in range(count)]
 
 
 def workload_names():

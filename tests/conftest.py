@@ -23,3 +23,11 @@ def oracle_lib():
 def engine_lib():
     from mpdpft_b200 import engine
     return engine.load()
+
+
+@pytest.fixture(scope="session")
+def eng():
+    """The engine module with its CUDA library loaded."""
+    from mpdpft_b200 import engine
+    engine.load()
+    return engine

@@ -14,13 +14,6 @@ from mpdpft_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def eng():
-    from mpdpft_b200 import engine
-    engine.load()
-    return engine
-
-
 def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
 
