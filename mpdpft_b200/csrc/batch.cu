@@ -56,6 +56,31 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_gangs(const StepArgs<R>
   }
 }
 
+// Minimum and maximum of field b (of counts[b] points) into out[2b], out[2b+1].
+template <typename R>
+__global__ void k_minmax_b(const R* const* fields, const long* counts, double* out) {
+  const R* f = fields[blockIdx.x];
+  const long n = counts[blockIdx.x];
+  double lo = 1.0e300, hi = -1.0e300;
+  for (long p = threadIdx.x; p < n; p += blockDim.x) {
+    const double v = (double)__ldcg(f + p);
+    lo = fmin(lo, v);
+    hi = fmax(hi, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  __shared__ double sl[32], sh[32];
+  if ((threadIdx.x & 31) == 0) { sl[threadIdx.x >> 5] = lo; sh[threadIdx.x >> 5] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { lo = fmin(lo, sl[w]); hi = fmax(hi, sh[w]); }
+    out[2 * blockIdx.x] = fmin(lo, sl[0]);
+    out[2 * blockIdx.x + 1] = fmax(hi, sh[0]);
+  }
+}
+
 // Solves that have not met their exit test.
 __global__ void k_count_active(ScState* const* states, int count, int* out) {
   __shared__ int sh;
@@ -90,6 +115,9 @@ struct Batch {
   int* d_active = nullptr;
   int* h_active = nullptr;  // pinned
   double* d_energy = nullptr;  // [count][kNEnergy]
+  void** d_vfields = nullptr;  // [count * S] potential of each species (automatic temperature)
+  long* d_vcounts = nullptr;
+  double* d_minmax = nullptr;  // [count * S][2]
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool initialised = false;
@@ -120,10 +148,12 @@ void Batch::release() {
     delete c;
   }
   members.clear();
-  void* bufs[] = {d_vmax, d_args[0], d_args[1], d_tab_mu, d_queue, d_tab_dens, d_tab_mix, d_states, d_active, d_energy};
+  void* bufs[] = {d_vmax, d_args[0], d_args[1], d_tab_mu, d_queue, d_tab_dens, d_tab_mix, d_states,
+                  d_active, d_energy, d_vfields, d_vcounts, d_minmax};
   for (void* p : bufs) if (p) cudaFree(p);
   d_vmax = nullptr; d_args[0] = d_args[1] = nullptr; d_tab_mu = nullptr; d_queue = nullptr;
   d_tab_dens = nullptr; d_tab_mix = nullptr; d_states = nullptr; d_active = nullptr; d_energy = nullptr;
+  d_vfields = nullptr; d_vcounts = nullptr; d_minmax = nullptr;
   if (h_active) { cudaFreeHost(h_active); h_active = nullptr; }
   for (cudaEvent_t e : events) cudaEventDestroy(e);
   events.clear();
@@ -141,11 +171,12 @@ static const void* density_b_ptr(int which) {
 
 template <typename R>
 static const void* batch_kernel(int which, int fk) {
-  // which: 0 mu gangs, 1/2/3 density (Pulay window variant), 4 mixing
+  // which: 0 mu gangs, 1/2/3 density (Pulay window variant), 4 mixing;
+  // batches are 2D gradient-corrected: functional kind 3
   if (which == 4) return (const void*)sc_mix_kernel_b<R>;
-  if (fk != 0) return nullptr;  // batches are 2D: the general functional kind
-  if (which == 0) return (const void*)sc_mu_gangs<R, 0>;
-  return density_b_ptr<R, 0>(which);
+  if (fk != 3) return nullptr;
+  if (which == 0) return (const void*)sc_mu_gangs<R, 3>;
+  return density_b_ptr<R, 3>(which);
 }
 
 int Batch::init(const mpdpft_params* params, int n, int dev) {
@@ -186,7 +217,7 @@ int Batch::init(const mpdpft_params* params, int n, int dev) {
   fk = members[0]->fk;
   dens_which = members[0]->dens_which;
   num_sms = members[0]->num_sms;
-  if (fk != 0) return set_error(MPDPFT_ERR_ARG, "batch: unsupported functional kind");
+  if (fk != 3) return set_error(MPDPFT_ERR_ARG, "batch: unsupported functional kind");
   CU(cudaMalloc((void**)&d_vmax, sizeof(unsigned long long) * kMaxS * count));
   // grid-size classes
   std::vector<int> sizes;
@@ -223,6 +254,20 @@ int Batch::init(const mpdpft_params* params, int n, int dev) {
   CU(cudaMalloc((void**)&d_active, sizeof(int)));
   CU(cudaMallocHost((void**)&h_active, sizeof(int)));
   CU(cudaMalloc((void**)&d_energy, sizeof(double) * kNEnergy * count));
+  {
+    std::vector<void*> f;
+    std::vector<long> nn;
+    for (Ctx* c : members)
+      for (int s = 0; s < S; ++s) {
+        f.push_back((char*)c->d_V + (size_t)s * c->geom.n * rsize);
+        nn.push_back(c->geom.n);
+      }
+    CU(cudaMalloc((void**)&d_vfields, sizeof(void*) * f.size()));
+    CU(cudaMemcpy(d_vfields, f.data(), sizeof(void*) * f.size(), cudaMemcpyHostToDevice));
+    CU(cudaMalloc((void**)&d_vcounts, sizeof(long) * nn.size()));
+    CU(cudaMemcpy(d_vcounts, nn.data(), sizeof(long) * nn.size(), cudaMemcpyHostToDevice));
+    CU(cudaMalloc((void**)&d_minmax, sizeof(double) * 2 * f.size()));
+  }
   CU(cudaMalloc((void**)&d_queue, sizeof(unsigned)));
   return build_tables();
 }
@@ -352,34 +397,38 @@ int Batch::sc_init(const double* const* v0, int layout, int mem) {
   CU(cudaStreamSynchronize(stream));
   for (int i = 0; i < count; ++i) {
     Ctx& c = *members[i];
-    if ((st = c.reset_state())) return st;
+    if ((st = c.reset_state(false))) return st;
     for (int s = 0; s < S; ++s) {
       void* dst = (char*)c.d_V + (size_t)s * c.geom.n * rsize;
       const double* src = v0 ? v0[(size_t)i * S + s] : nullptr;
-      if (src) {
-        if ((st = c.import_field(src, dst, layout, mem))) return st;
+      if (src) {  // host data staged in half s % 2 of the member's buffers
+        if ((st = c.import_field(src, dst, layout, mem, s & 1, S > 2 && (s & 1)))) return st;
       } else {
         CU(cudaMemcpyAsync(dst, (char*)c.d_vext + (size_t)s * c.geom.n * rsize, c.geom.n * rsize,
                            cudaMemcpyDeviceToDevice, stream));
       }
     }
-    // automatic temperature (PreparationsForSCdensity, mpDPFT.cpp:4523-4528)
+  }
+  // automatic temperature (PreparationsForSCdensity, mpDPFT.cpp:4523-4528)
+  // from the extremes of every start potential
+  bool need_t = false;
+  for (Ctx* c : members)
+    for (int s = 0; s < S; ++s) need_t |= c->P.temperature[s] < 0.0;
+  std::vector<double> mm(2 * (size_t)count * S);
+  if (need_t) {
+    if (rsize == sizeof(double))
+      k_minmax_b<double><<<count * S, 256, 0, stream>>>((const double* const*)d_vfields, d_vcounts, d_minmax);
+    else
+      k_minmax_b<float><<<count * S, 256, 0, stream>>>((const float* const*)d_vfields, d_vcounts, d_minmax);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(mm.data(), d_minmax, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, stream));
+  }
+  CU(cudaStreamSynchronize(stream));
+  for (int i = 0; i < count; ++i) {
+    Ctx& c = *members[i];
     for (int s = 0; s < S; ++s) {
       if (c.P.temperature[s] >= 0.0) { c.temperature[s] = c.P.temperature[s]; continue; }
-      double vmin, vmax;
-      const double* src = v0 ? v0[(size_t)i * S + s] : nullptr;
-      if (src && mem == MPDPFT_MEM_HOST) {
-        const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? c.n_ref : c.geom.n;
-        vmin = vmax = src[0];
-        for (long p = 1; p < cnt; ++p) { vmin = std::min(vmin, src[p]); vmax = std::max(vmax, src[p]); }
-      } else {
-        std::vector<double> h(c.geom.n);
-        if ((st = c.export_field((char*)c.d_V + (size_t)s * c.geom.n * rsize, h.data(), MPDPFT_LAYOUT_PERIODIC,
-                                 MPDPFT_MEM_HOST)))
-          return st;
-        vmin = vmax = h[0];
-        for (double x : h) { vmin = std::min(vmin, x); vmax = std::max(vmax, x); }
-      }
+      const double vmin = mm[2 * ((size_t)i * S + s)], vmax = mm[2 * ((size_t)i * S + s) + 1];
       c.temperature[s] = std::max(std::fabs(c.P.mu[s] - vmin), std::fabs(c.P.mu[s] - vmax)) / 50.0;
     }
   }

@@ -147,6 +147,7 @@ template <typename R>
 static const void* sc_kernel_ptr(int which, int fk) {
   if (fk == 1) return sc_kernel_fk<R, 1>(which);
   if (fk == 2) return sc_kernel_fk<R, 2>(which);
+  if (fk == 3) return sc_kernel_fk<R, 3>(which);
   return sc_kernel_fk<R, 0>(which);
 }
 
@@ -342,7 +343,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   return reset_state();
 }
 
-int Ctx::reset_state() {
+int Ctx::reset_state(bool sync) {
   ScState h;
   std::memset(&h, 0, sizeof(h));
   for (int s = 0; s < S; ++s) {
@@ -353,8 +354,9 @@ int Ctx::reset_state() {
   h.inc_v = P.incremental_v;
   h.cc = 0.0;
   h.old_cc = 0.0;  // the reference leaves data.CC indeterminate before iteration 0
+  // a pageable source: the copy has read h when the call returns
   CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
-  CU(cudaStreamSynchronize(stream));
+  if (sync) CU(cudaStreamSynchronize(stream));
   if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
   if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
   return MPDPFT_OK;
@@ -367,21 +369,26 @@ int Ctx::read_state(ScState* h) {
 }
 
 // Copy one grid (host or device double pointer, either layout) into the
-// compute-precision device array dst.
-int Ctx::import_field(const double* src, void* dst, int layout, int mem) {
+// compute-precision device array dst.  Host data is staged through half
+// `slot` (0 or 1) of the pinned buffer and of d_io; with sync = false the
+// caller synchronises the stream before that half is used again.
+int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slot, bool sync) {
   if (!src) return set_error(MPDPFT_ERR_ARG, "null input array");
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
   const double* dsrc = src;
   if (mem == MPDPFT_MEM_HOST) {
-    std::memcpy(pinned, src, sizeof(double) * cnt);
-    CU(cudaMemcpyAsync(d_io, pinned, sizeof(double) * cnt, cudaMemcpyHostToDevice, stream));
-    dsrc = d_io;
+    const long half = std::max(n_ref, geom.n);  // pinned and d_io hold two grids
+    double* stage = (double*)pinned + (slot ? half : 0);
+    double* dstage = d_io + (slot ? half : 0);
+    std::memcpy(stage, src, sizeof(double) * cnt);
+    CU(cudaMemcpyAsync(dstage, stage, sizeof(double) * cnt, cudaMemcpyHostToDevice, stream));
+    dsrc = dstage;
   }
   const int blocks = grid_blocks(geom.n);
   if (rsize == sizeof(double)) k_import<double><<<blocks, kThreads, 0, stream>>>(dsrc, (double*)dst, geom, layout);
   else k_import<float><<<blocks, kThreads, 0, stream>>>(dsrc, (float*)dst, geom, layout);
   CU(cudaGetLastError());
-  if (mem == MPDPFT_MEM_HOST) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
+  if (mem == MPDPFT_MEM_HOST && sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
   return MPDPFT_OK;
 }
 

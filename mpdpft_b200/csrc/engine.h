@@ -76,12 +76,12 @@ struct Ctx {
   void release();
   int alloc(void** p, size_t bytes);
   int init(const mpdpft_params& params, int dev);
-  int reset_state();
+  int reset_state(bool sync = true);
   int read_state(ScState* h);
   int status_from_state(const ScState& h);
   bool has_interaction(int t) const;
   KParams kparams() const;
-  int import_field(const double* src, void* dst, int layout, int mem);
+  int import_field(const double* src, void* dst, int layout, int mem, int slot = 0, bool sync = true);
   int export_field(const void* src, double* dst, int layout, int mem);
   template <typename R>
   StepArgs<R> step_args(int mode);

@@ -247,12 +247,14 @@ struct EvalK {
   double cg;      // gradient prefactor (times lap)
   double cg2;     // gradient prefactor times c2 / 4 (times |grad V|^2)
   double floor_u, c1, c3;  // below floor: u^{-1/2} -> u c1, u^{-3/2} -> u c3
+  double c2d, T, invT, lt;  // 2D finite-T form: g/(2 pi), T, 1/T, 1/(12 T)
 };
 
 __device__ __forceinline__ EvalK eval_constants(const DensParams& d) {
   EvalK k;
   k.fast = 0;
   k.ctf = k.cg = k.cg2 = k.floor_u = k.c1 = k.c3 = 0.0;
+  k.c2d = k.T = k.invT = k.lt = 0.0;
   if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 3) {
     k.fast = 1;
     k.ctf = 2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi);
@@ -264,6 +266,12 @@ __device__ __forceinline__ EvalK eval_constants(const DensParams& d) {
   } else if (d.expr == MPDPFT_DENS_TF && d.dim == 3) {
     k.fast = 2;
     k.ctf = 1.4142135623730951 * d.g / (3.0 * kPi * kPi);
+  } else if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 2) {
+    k.fast = 3;
+    k.c2d = d.g / (2.0 * kPi);
+    k.T = d.T;
+    k.invT = 1.0 / d.T;
+    k.lt = 1.0 / (12.0 * d.T);
   }
   return k;
 }
@@ -313,12 +321,45 @@ __device__ __forceinline__ double tf3_slope(const EvalK& k, double u) {
   return u > 0.0 ? 1.5 * k.ctf * u * r : 0.0;
 }
 
+// 2D gradient-corrected density at finite T (the small-gradient branch of
+// getDenEnAt, mpDPFT.cpp:3376-3384) in logistic form.  With a = (mu - V)/T
+// and s(a) = 1/(1 + e^{-a}):
+//   n      = g/(2 pi) [T softplus(a) - lap/(12 T) s (1 - s)],
+//   dn/dmu = g/(2 pi) [s - lap/(12 T^2) s (1 - s)(1 - 2 s)];
+// one exponential e = exp(-|a|) gives softplus(a) = max(a, 0) + log1p(e),
+// s = (a >= 0 ? 1 : e)/(1 + e) and s (1 - s) = e/(1 + e)^2 (the reference's
+// zeta = e^{-a}; its +-100 cut-offs are the two tails of the same forms).
+__device__ __forceinline__ double g2d_n(const EvalK& k, double u, double l) {
+  const double a = u * k.invT;
+  const double e = exp(-fabs(a));
+  const double ope = 1.0 + e;
+  const double r = k.c2d * (k.T * (fmax(a, 0.0) + log1p(e)) - l * k.lt * (e / (ope * ope)));
+  return r == r ? r : 0.0;
+}
+
+// n and dn/dmu together (one exponential).
+__device__ __forceinline__ void g2d_n_slope(const EvalK& k, double u, double l, double& n, double& slope) {
+  const double a = u * k.invT;
+  const double e = exp(-fabs(a));
+  const double ope = 1.0 + e;
+  const double rope = 1.0 / ope;
+  const double sg = (a >= 0.0 ? 1.0 : e) * rope;
+  const double q = e * rope * rope;
+  const double r = k.c2d * (k.T * (fmax(a, 0.0) + log1p(e)) - l * k.lt * q);
+  const double d = k.c2d * (sg - l * k.lt * k.invT * q * (1.0 - 2.0 * sg));
+  n = r == r ? r : 0.0;
+  slope = d == d ? d : 0.0;
+}
+
 // Functional kind, a template parameter of the kernels so that each
 // instantiation carries only its own evaluation code: 1 = 3D
-// gradient-corrected, 2 = 3D TF, 0 = any (density_at_d).
+// gradient-corrected, 2 = 3D TF, 3 = 2D gradient-corrected, 0 = any
+// (density_at_d).  The point values are FP64 in both precisions: the mu
+// search resolves N to RelAcc (1e-10), below the rounding of FP32 values.
 inline int functional_kind(int expr, int dim) {
   if (expr == MPDPFT_DENS_GRADIENT && dim == 3) return 1;
   if (expr == MPDPFT_DENS_TF && dim == 3) return 2;
+  if (expr == MPDPFT_DENS_GRADIENT && dim == 2) return 3;
   return 0;
 }
 
@@ -331,6 +372,7 @@ template <int FK>
 __device__ __forceinline__ double point_density(const DensParams& d, const EvalK& k, double u, double l, double g) {
   if constexpr (FK == 1) return grad3_n(k, u, k.cg * l, k.cg2 * g);
   else if constexpr (FK == 2) return tf3_n(k, u);
+  else if constexpr (FK == 3) return g2d_n(k, u, l);
   else return density_at_d(d, u, l, g);
 }
 
@@ -349,6 +391,16 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
     acc[kMuCand] += tf3_slope(k, cmu[0] - v);
 #pragma unroll
     for (int c = 0; c < kMuCand; ++c) acc[c] += tf3_n(k, cmu[c] - v);
+  } else if constexpr (FK == 3) {
+    double n0, sl0;
+    g2d_n_slope(k, cmu[0] - v, l, n0, sl0);
+    acc[0] += n0;
+    acc[kMuCand] += sl0;
+#pragma unroll
+    for (int c = 1; c < kMuCand; ++c) {
+      if (c >= nc) break;
+      acc[c] += g2d_n(k, cmu[c] - v, l);
+    }
   } else {
     acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
 #pragma unroll

@@ -366,10 +366,17 @@ class Batch:
     def sync(self):
         self._check(self.lib.mpdpft_batch_sync(self.h))
 
-    def sc_run(self, check=True):
+    def sc_run(self, check=True, device_v0=None):
+        """Initialise and solve all; device_v0: optional count * species
+        device addresses of float64 start potentials (periodic layout), in
+        place of the host arrays of the problems."""
         res = (abi.Result * self.count)()
         status = (C.c_int * self.count)()
-        st = self.lib.mpdpft_batch_sc_run(self.h, self._v0(), abi.LAYOUT_PERIODIC, abi.MEM_HOST, res, status)
+        if device_v0 is None:
+            v0, mem = self._v0(), abi.MEM_HOST
+        else:
+            v0, mem = (_dp * len(device_v0))(*[C.cast(C.c_void_p(a), _dp) for a in device_v0]), abi.MEM_DEVICE
+        st = self.lib.mpdpft_batch_sc_run(self.h, v0, abi.LAYOUT_PERIODIC, mem, res, status)
         if check and st not in (abi.OK, abi.ERR_NOT_CONVERGED):
             self._check(st)
         return list(res), list(status)

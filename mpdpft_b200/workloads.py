@@ -196,4 +196,4 @@ def sweep_2d(count=256, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **o
 
 
 def workload_names():
-    return ["harmonic_tf", "argon_atom", "electron_hole"]
+    return ["harmonic_tf", "argon_atom", "electron_hole", "sweep_2d"]

@@ -288,3 +288,26 @@ def test_sc_electron_hole_converged(eng, oracle_lib, prec, e_tol, n_tol):
           (prec, res.iterations, res_r.iterations, de, ["%.2e" % x for x in l1]))
     assert de < e_tol
     assert max(l1) < n_tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,e_tol,n_tol", [(abi.FP64, 1e-6, 1e-5), (abi.MIXED, 1e-5, 1e-5)])
+@pytest.mark.parametrize("i,steps", [(0, 64), (5, 96)])
+def test_sc_sweep_instance_converged(eng, oracle_lib, prec, e_tol, n_tol, i, steps):
+    """One solve of the 2D sweep (two species, contact coupling, finite-T
+    gradient-corrected density, Pulay 6) alone against the FP64 oracle."""
+    p, vext, v0 = W.sweep_instance(i, steps=steps, precision=prec)
+    pr, _, _ = W.sweep_instance(i, steps=steps, precision=abi.FP64)
+    with eng.Engine(p) as e:
+        res, log, st = e.sc_run(vext, v0)
+        dens = [e.field(abi.FIELD_DENSITY, s) for s in range(2)]
+    res_r, log_r, dens_r, v_r = oracle_lib.sc_run(pr, vext, v0)
+    assert res.converged == 1 and res_r.converged == 1
+    de = abs(res.e_total - res_r.e_total) / abs(res_r.e_total)
+    dvol = (p.edge / p.steps) ** 2
+    l1 = [np.abs(dens[s] - dens_r[s]).sum() * dvol / p.abundances[s] for s in range(2)]
+    print("sweep instance %d at %d^2 prec %d: iters %d/%d dE/E %.2e L1/N %s" %
+          (i, steps, prec, res.iterations, res_r.iterations, de, ["%.2e" % x for x in l1]))
+    assert abs(res.abundance[0] - p.abundances[0]) <= 2e-10 * p.abundances[0]
+    assert de < e_tol
+    assert max(l1) < n_tol
