@@ -11,6 +11,13 @@ synthetic and seeded (mpdpft_b200.workloads.argon_atom).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The batched half of the metric (extra.batched_sweep): 256 independent 2D
+two-species solves of uneven grid size (64^2 .. 512^2, sweep_2d) solved to
+convergence in one batch (mpdpft_batch, one CUDA graph replay per iteration
+of all solves), against the same 256 solved one after another through
+mpdpft_sc_run; solves/s by wall clock, start potentials resident on the GPU
+(and, separately, copied from host arrays).
+
 Under torchrun every rank runs an independent replica of the solve (a single
 SC solve does not shard); value = iterations of all ranks / max device time.
 `--impl reference` times the CPU oracle (the FP64 restatement of the
@@ -42,6 +49,8 @@ def parse():
     ap.add_argument("--steps-grid", type=int, default=128)
     ap.add_argument("--no-ttc", action="store_true", help="skip the time-to-converge runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched sweep")
+    ap.add_argument("--batch-count", type=int, default=256)
     return ap.parse_args()
 
 
@@ -57,8 +66,8 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d.get("hbm_gbs", 6650.0)), "measured"
-    return 6650.0, "fallback"
+        return float(d.get("hbm_gbs", 6650.0)), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (no MEASURED_PEAKS.json: the profiling recipe's 6.65 TB/s)"
 
 
 def traffic_from_profiles(stage):
@@ -232,7 +241,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = measured_peaks()
     ach = prof[dom]["bytes"] / (prof[dom]["ms"] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "frac": ach / peak, "peak_source": peak_kind,
                 "traffic": traffic_from_profiles(dom), "bytes_per_launch": prof[dom]["bytes"],
                 "ms_per_launch": prof[dom]["ms"],
                 "stages": {k: {"ms": v["ms"], "GBps": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] > 0 else None,
@@ -244,6 +253,8 @@ def run_ours(args, world, rank, local):
         extra = time_to_converge(sg, local)
 
     e2e = end_to_end(sg, local)
+    if not args.no_batch:
+        extra["batched_sweep"] = batched_sweep(args.batch_count, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -293,6 +304,68 @@ def time_to_converge(sg, device):
     out["energy_rel_err_mixed_vs_fp64"] = abs(out["energy_mixed"] - out["energy_fp64"]) / abs(out["energy_fp64"])
     dv = (20.0 / sg) ** 3
     out["density_l1_per_particle_mixed_vs_fp64"] = float(np.abs(dens["mixed"] - dens["fp64"]).sum() * dv / 18.0)
+    return out
+
+
+def batched_sweep(count, device, reps=3):
+    """Solves/s of the batched sweep against the same solves one at a time
+    (mpdpft_sc_run per solve, contexts created before the timing)."""
+    import torch
+    from mpdpft_b200 import abi, engine, workloads as W
+    probs = W.sweep_2d(count, precision=abi.MIXED)
+    out = {"count": count, "grids": {str(s): sum(1 for p, _, _ in probs if p.steps == s) for s in W.SWEEP_SIZES},
+           "precision": "mixed", "timing": "wall clock per full solve of all, best of %d" % reps}
+    dev = [torch.tensor(v, dtype=torch.float64, device="cuda:%d" % device) for _, _, v0 in probs for v in v0]
+    torch.cuda.synchronize(device)
+    with engine.Batch(probs, device=device) as b:
+        b.sc_run(device_v0=[x.data_ptr() for x in dev])  # warm-up: graph instantiation
+        best = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            res, status = b.sc_run(device_v0=[x.data_ptr() for x in dev])
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        best_host = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            b.sc_run()
+            dt = time.perf_counter() - t0
+            best_host = dt if best_host is None else min(best_host, dt)
+    out["batched_solves_per_s"] = count / best
+    out["batched_s"] = best
+    out["batched_host_inputs_solves_per_s"] = count / best_host
+    out["converged"] = sum(r.converged for r in res)
+    out["status_ok"] = sum(1 for st in status if st == abi.OK)
+    out["iterations_mean"] = float(np.mean([r.iterations for r in res]))
+    out["iterations_max"] = int(max(r.iterations for r in res))
+    engines = []
+    for p, vext, v0 in probs:
+        e = engine.Engine(p, device=device)
+        for s in range(p.species):
+            e.set_external_potential(s, vext[s])
+        engines.append(e)
+    S = probs[0][0].species
+    engines[0].sc_run(None, device_v0=[x.data_ptr() for x in dev[:S]])  # warm-up
+    seq_best, seq_host = None, None
+    for _ in range(2):
+        t0 = time.perf_counter()
+        seq = [e.sc_run(None, device_v0=[x.data_ptr() for x in dev[i * S:(i + 1) * S]])[0]
+               for i, e in enumerate(engines)]
+        dt = time.perf_counter() - t0
+        seq_best = dt if seq_best is None else min(seq_best, dt)
+    t0 = time.perf_counter()
+    for e, (p, vext, v0) in zip(engines, probs):
+        e.sc_run(None, v0)
+    seq_host = time.perf_counter() - t0
+    for e in engines:
+        e.close()
+    out["sequential_solves_per_s"] = count / seq_best
+    out["sequential_s"] = seq_best
+    out["sequential_host_inputs_solves_per_s"] = count / seq_host
+    out["speedup_batched_vs_sequential"] = seq_best / best
+    out["speedup_host_inputs"] = seq_host / best_host
+    out["max_energy_rel_diff_vs_sequential"] = float(max(abs(a.e_total - c.e_total) / abs(c.e_total)
+                                                         for a, c in zip(res, seq)))
     return out
 
 

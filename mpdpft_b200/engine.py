@@ -229,18 +229,24 @@ class Engine:
         return outs, coeffs[:nc.value].copy(), st
 
     # --- SC loop ----------------------------------------------------------
-    def sc_run(self, vext, v0=None, layout=abi.LAYOUT_PERIODIC, log_cap=None, check=True):
-        for s in range(self.S):
-            self.set_external_potential(s, vext[s], layout)
-        v0p = None
-        if v0 is not None:
+    def sc_run(self, vext, v0=None, layout=abi.LAYOUT_PERIODIC, log_cap=None, check=True, device_v0=None):
+        """Full solve.  vext (None: keep the potentials already set);
+        device_v0: optional device addresses of float64 start potentials
+        (periodic layout) in place of the host arrays v0."""
+        if vext is not None:
+            for s in range(self.S):
+                self.set_external_potential(s, vext[s], layout)
+        v0p, mem = None, abi.MEM_HOST
+        if device_v0 is not None:
+            v0p, mem = (_dp * len(device_v0))(*[C.cast(C.c_void_p(a), _dp) for a in device_v0]), abi.MEM_DEVICE
+        elif v0 is not None:
             arrs = [_arr(x, self._count(layout)) for x in v0]
             self._keep = arrs
             v0p = _ptrs(arrs)
         cap = log_cap or (self.params.max_sc_count + 2)
         res = abi.Result()
         log = (abi.IterLog * cap)()
-        st = self.lib.mpdpft_sc_run(self.h, v0p, layout, abi.MEM_HOST, C.byref(res), log, cap)
+        st = self.lib.mpdpft_sc_run(self.h, v0p, layout, mem, C.byref(res), log, cap)
         if check and st not in (abi.OK, abi.ERR_NOT_CONVERGED):
             self._check(st)
         return res, list(log[:min(res.iterations, cap)]), st
