@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
@@ -395,14 +396,33 @@ int Batch::sc_init(const double* const* v0, int layout, int mem) {
   int st;
   CU(cudaSetDevice(device));
   CU(cudaStreamSynchronize(stream));
+  // host arrays: copied into the members' pinned staging halves (one per
+  // species) by several host threads, then sent by one stream
+  const bool staged = v0 && mem == MPDPFT_MEM_HOST && S <= 2;
+  if (staged) {
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+      pool.emplace_back([&, t]() {
+        for (int i = t; i < count; i += nt) {
+          Ctx& c = *members[i];
+          const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? c.n_ref : c.geom.n;
+          for (int s = 0; s < S; ++s)
+            if (v0[(size_t)i * S + s]) std::memcpy(c.host_stage(s), v0[(size_t)i * S + s], sizeof(double) * cnt);
+        }
+      });
+    for (std::thread& th : pool) th.join();
+  }
   for (int i = 0; i < count; ++i) {
     Ctx& c = *members[i];
     if ((st = c.reset_state(false))) return st;
     for (int s = 0; s < S; ++s) {
       void* dst = (char*)c.d_V + (size_t)s * c.geom.n * rsize;
       const double* src = v0 ? v0[(size_t)i * S + s] : nullptr;
-      if (src) {  // host data staged in half s % 2 of the member's buffers
-        if ((st = c.import_field(src, dst, layout, mem, s & 1, S > 2 && (s & 1)))) return st;
+      if (src && staged) {
+        if ((st = c.import_staged(nullptr, dst, layout, s, false))) return st;
+      } else if (src) {  // device arrays, or host data staged in half s % 2
+        if ((st = c.import_field(src, dst, layout, mem, s & 1, mem == MPDPFT_MEM_HOST && (s & 1)))) return st;
       } else {
         CU(cudaMemcpyAsync(dst, (char*)c.d_vext + (size_t)s * c.geom.n * rsize, c.geom.n * rsize,
                            cudaMemcpyDeviceToDevice, stream));

@@ -372,23 +372,31 @@ int Ctx::read_state(ScState* h) {
 // compute-precision device array dst.  Host data is staged through half
 // `slot` (0 or 1) of the pinned buffer and of d_io; with sync = false the
 // caller synchronises the stream before that half is used again.
+double* Ctx::host_stage(int slot) { return (double*)pinned + (slot ? std::max(n_ref, geom.n) : 0); }
+
 int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slot, bool sync) {
   if (!src) return set_error(MPDPFT_ERR_ARG, "null input array");
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
+  if (mem == MPDPFT_MEM_HOST) std::memcpy(host_stage(slot), src, sizeof(double) * cnt);
+  return import_staged(mem == MPDPFT_MEM_HOST ? nullptr : src, dst, layout, slot, sync);
+}
+
+// The device half of import_field: src (device) or, when src is null, the
+// grid already copied into host_stage(slot).
+int Ctx::import_staged(const double* src, void* dst, int layout, int slot, bool sync) {
+  const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
   const double* dsrc = src;
-  if (mem == MPDPFT_MEM_HOST) {
-    const long half = std::max(n_ref, geom.n);  // pinned and d_io hold two grids
-    double* stage = (double*)pinned + (slot ? half : 0);
-    double* dstage = d_io + (slot ? half : 0);
-    std::memcpy(stage, src, sizeof(double) * cnt);
-    CU(cudaMemcpyAsync(dstage, stage, sizeof(double) * cnt, cudaMemcpyHostToDevice, stream));
+  const bool staged = src == nullptr;
+  if (staged) {
+    double* dstage = d_io + (slot ? std::max(n_ref, geom.n) : 0);  // d_io holds two grids
+    CU(cudaMemcpyAsync(dstage, host_stage(slot), sizeof(double) * cnt, cudaMemcpyHostToDevice, stream));
     dsrc = dstage;
   }
   const int blocks = grid_blocks(geom.n);
   if (rsize == sizeof(double)) k_import<double><<<blocks, kThreads, 0, stream>>>(dsrc, (double*)dst, geom, layout);
   else k_import<float><<<blocks, kThreads, 0, stream>>>(dsrc, (float*)dst, geom, layout);
   CU(cudaGetLastError());
-  if (mem == MPDPFT_MEM_HOST && sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
+  if (staged && sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
   return MPDPFT_OK;
 }
 

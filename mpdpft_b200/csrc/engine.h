@@ -82,6 +82,8 @@ struct Ctx {
   bool has_interaction(int t) const;
   KParams kparams() const;
   int import_field(const double* src, void* dst, int layout, int mem, int slot = 0, bool sync = true);
+  int import_staged(const double* src, void* dst, int layout, int slot, bool sync);
+  double* host_stage(int slot);  // half slot of the pinned staging buffer
   int export_field(const void* src, double* dst, int layout, int mem);
   template <typename R>
   StepArgs<R> step_args(int mode);
