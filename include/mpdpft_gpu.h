@@ -311,6 +311,28 @@ int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
  * [3] convergence test and Pulay solve, [4] grid barrier, [5] mix. */
 int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n);
 
+/* Adjoint of the converged SC fixed point (no counterpart in the reference,
+ * whose optimisation drivers take finite differences of whole solves,
+ * mpDPFT.cpp:8448).  After mpdpft_sc_run on a one-species context, dl_dn
+ * holds the gradient of a scalar loss L with respect to the converged
+ * density at the grid points (periodic layout, host or device doubles);
+ * dl_dvext receives dL/dV_ext at the grid points.  The adjoint linear system
+ * lambda = dl_dn + J_W^T J_N^T lambda (J_N: density map with the particle-
+ * number constraint, DelField and taper; J_W: Hartree, Dirac, contact) is
+ * solved by the context's device Pulay mixer until
+ * |T(lambda) - lambda| / |T(lambda)| <= tol or max_iter iterations
+ * (MPDPFT_ERR_NOT_CONVERGED).  The converged state is kept (its Pulay
+ * history restarts).  Functionals: 3D gradient-corrected, 3D TF, 2D
+ * gradient-corrected; interactions 8, 10, 11. */
+int mpdpft_adjoint(mpdpft_ctx* ctx, const double* dl_dn, double* dl_dvext, int layout, int mem, double tol,
+                   int max_iter, int* iterations, double* residual);
+/* dL/dR (3 per nucleus) of Gaussian nuclei V_ext = sum_a -Z_a
+ * erf(|r - R_a| / (sqrt(2) sigma)) / |r - R_a| from dL/dV_ext (periodic
+ * layout, 3D). */
+int mpdpft_adjoint_nuclei(mpdpft_ctx* ctx, const double* dl_dvext, int mem, int n_nuclei,
+                          const double* charges, const double* positions, double sigma,
+                          double* dl_dpositions);
+
 /* Batch: many independent SC solves advanced together on one GPU (a
  * parameter sweep, the reference's TaskType 5/6/7 loops of GetData,
  * mpDPFTmain.cpp:110-160, run as one job).  The solves share dimension 2,

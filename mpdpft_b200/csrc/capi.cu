@@ -262,6 +262,20 @@ int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total) {
   return MPDPFT_OK;
 }
 
+int mpdpft_adjoint(mpdpft_ctx* ctx, const double* dl_dn, double* dl_dvext, int layout, int mem, double tol,
+                   int max_iter, int* iterations, double* residual) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.adjoint(dl_dn, dl_dvext, layout, mem, tol, max_iter, iterations, residual);
+}
+
+int mpdpft_adjoint_nuclei(mpdpft_ctx* ctx, const double* dl_dvext, int mem, int n_nuclei, const double* charges,
+                          const double* positions, double sigma, double* dl_dpositions) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.adjoint_nuclei(dl_dvext, mem, n_nuclei, charges, positions, sigma, dl_dpositions);
+}
+
 int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n) {
   CHECK_CTX(ctx);
   if (!us || n < 1) return set_error(MPDPFT_ERR_ARG, "bad arguments");

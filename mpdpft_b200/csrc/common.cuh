@@ -63,6 +63,22 @@ __device__ __forceinline__ void point_coords(long p, const Geom& g, double& x, d
   }
 }
 
+// Order-preserving 64-bit image of a double (atomicMax of doubles).
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
+  b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+  return __longlong_as_double((long long)b);
+}
+
+// |r - r0| < w from r^2, without the square root (the DelField taper shell).
+__device__ __forceinline__ bool in_shell(double r2, double r0, double w) {
+  const double lo = r0 - w, hi = r0 + w;
+  return r2 < hi * hi && (lo <= 0.0 || r2 > lo * lo);
+}
+
 // ---------------------------------------------------------- reductions --
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -155,6 +155,7 @@ static const void* sc_kernel_ptr(int which, int fk) {
 Ctx::~Ctx() { release(); }
 
 void Ctx::release() {
+  adjoint_release();
   if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
   if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
   for (void* p : allocations) cudaFree(p);

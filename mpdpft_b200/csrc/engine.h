@@ -15,6 +15,10 @@ int set_error(int status, const std::string& msg);
 extern thread_local std::string g_last_error;
 
 struct FftPlan;  // fft.cu
+struct Adjoint;  // adjoint.cu
+
+// kinds of Ctx::spectral
+enum { SPEC_DERIV = 0, SPEC_SMOOTH = 1, SPEC_COULOMB = 2 };
 
 // energy integrals per solve (k_energy)
 constexpr int kNEnergy = 5 * kMaxS + kMaxS * kMaxS;
@@ -69,6 +73,7 @@ struct Ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   FftPlan* fft = nullptr;
+  Adjoint* adj = nullptr;  // adjoint work fields (allocated on first use)
   int cnt[6] = {0, 0, 0, 0, 0, 0};       // launches issued, by stage
   int iter_cnt[6] = {0, 0, 0, 0, 0, 0};  // launches in the captured iteration
 
@@ -122,6 +127,15 @@ struct Ctx {
   int full_c2c(void* buf, int sign);
   int alloc_io(long doubles);
   int profile_stage(int stage, int reps, double* ms, double* bytes);
+  // linear spectral operators and the Hartree operator of one field (fft.cu)
+  int spectral(const void* in, int kind, int j, void* out, double coef);
+  int coulomb_field(const void* in, void* out);
+  // adjoint of the converged fixed point (adjoint.cu)
+  int adjoint(const double* dl_dn, double* dl_dvext, int layout, int mem, double tol, int max_iter, int* iters,
+              double* resid);
+  int adjoint_nuclei(const double* dl_dvext, int mem, int nn, const double* z, const double* pos, double sigma,
+                     double* dl_dpos);
+  void adjoint_release();
 };
 
 }  // namespace mpdpft

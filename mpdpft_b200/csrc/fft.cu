@@ -91,15 +91,6 @@ struct FftPlan {
   bool plane = false;      // 3D transforms by x-planes (k_plane_fwd / k_plane_inv)
 };
 
-// --------------------------------------------------- ordered max of doubles --
-__device__ __forceinline__ unsigned long long ordered_bits(double v) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(v);
-  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
-}
-__device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
-  b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
-  return __longlong_as_double((long long)b);
-}
 
 // ---------------------------------------------------------- prologues ----
 enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
@@ -476,6 +467,7 @@ struct AxisArgs {
   const double* f0_part;  // Z-pass input sums (Coulomb, k = 0 mode)
   int f0_blocks;
   const int* skip;        // batched launches: nonzero -> this solve has finished (no work)
+  int o0;                 // output o uses multiplier o0 + o (one derivative or the Laplacian alone)
 };
 
 template <typename R>
@@ -708,7 +700,7 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
       C* dst = a.out[o];
       auto mload = [&](int t, int l) -> C {
         C v = F[t * (NL + 1) + l];
-        return s_ok[l] ? apply_multiplier_tab<R, NC, NL>(a, T, v, t, l, o, f0, s_outer[l], s_col[l]) : v;
+        return s_ok[l] ? apply_multiplier_tab<R, NC, NL>(a, T, v, t, l, a.o0 + o, f0, s_outer[l], s_col[l]) : v;
       };
       auto gstore = [&](int t, int l, C v) { if (s_ok[l]) dst[s_base[l] + t * as] = v; };
       fft_lines<C, NC, NL, false>(A, B, twb, +1, mload, gstore);
@@ -737,7 +729,7 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
         long base, outer;
         int col;
         C v = F[t * tk + l];
-        if (axis_line(a, blk, l, base, outer, col)) v = apply_multiplier<R>(a, v, t, outer, col, o, f0);
+        if (axis_line(a, blk, l, base, outer, col)) v = apply_multiplier<R>(a, v, t, outer, col, a.o0 + o, f0);
         spare[t * tk + l] = v;
       }
       __syncthreads();
@@ -769,11 +761,6 @@ __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip_b(const AxisArgs<R>
 // V assembly (UpdateV, mpDPFT.cpp:4815-4838) when Coulomb terms exist:
 // V_s = Vext_s + incV (vh_s + contact + Dirac); partial sums of |dV|^2 and
 // the maximum of V over the taper shell (DelField, mpDPFT.cpp:7253-7259).
-// |r - r0| < w from r^2, without the square root.
-__device__ __forceinline__ bool in_shell(double r2, double r0, double w) {
-  const double lo = r0 - w, hi = r0 + w;
-  return r2 < hi * hi && (lo <= 0.0 || r2 > lo * lo);
-}
 
 // Body of the V assembly over blocks blk of nblk: species s < nmax also
 // update their taper-shell maximum vmax[s]; update = 0 only takes the
@@ -1266,6 +1253,17 @@ static size_t x_smem_rt(const FftPlan& f) {
 template <typename R>
 static bool x_ct_fits(const FftPlan& f) {
   return x_smem_ct<R>(f) + sizeof(MulTables<R, 512, 16>) <= 227 * 1024;
+}
+
+template <typename R>
+static int launch_x_args(Ctx& c, const AxisArgs<R>& a) {
+  FftPlan& f = *c.fft;
+  const unsigned grid = x_grid<R>(a);
+  c.cnt[MPDPFT_STAGE_FFT_X]++;
+  if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
+    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
+  CU(cudaGetLastError());
+  return MPDPFT_OK;
 }
 
 template <typename R>
@@ -2064,6 +2062,51 @@ void batch_fft_destroy(BatchFftClass* b) {
   for (int i = 0; i < 4; ++i) cudaFree(b->d_z[i]);
   for (int i = 0; i < 2; ++i) cudaFree(b->d_x[i]);
   delete b;
+}
+
+// ============================================================ adjoint ops ==
+// out = IFFT(m(k) FFT(in)) on the pass kernels, one output:
+//   SPEC_DERIV   j < dim: d/dx_j with the DelField smoothing e^{sigma k^2} and
+//                the Nyquist index of axis j dropped; j = dim: the Laplacian
+//                smoothed twice (the multipliers of DelField's outputs);
+//   SPEC_SMOOTH  e^{sigma k^2};
+//   SPEC_COULOMB the Coulomb multiplier of the context's kernel times
+//                4 pi coef, with the regularised kernel's terms in the total
+//                charge left out (k = 0 mode, Gaussian subtraction,
+//                compensation term): a translation-invariant symmetric part.
+template <typename R>
+static int spectral_impl(Ctx& c, const R* in, int kind, int j, R* out, double coef) {
+  FftPlan& f = *c.fft;
+  int st;
+  const double smear = c.P.smearing_extent > 0.0 ? c.P.smearing_extent : 6.0 * c.geom.dx;
+  const double sigma_c = -0.5 * smear * smear;
+  int mul = MUL_SMOOTH;
+  if (kind == SPEC_DERIV) mul = MUL_DERIV;
+  else if (kind == SPEC_COULOMB) mul = c.P.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED ? MUL_COULOMB_TRUNC : MUL_COULOMB_REG;
+  if ((st = launch_z_r2c<R>(c, in, PRO_NONE, 1, nullptr, f.spec[0], false))) return st;
+  if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, -1))) return st;
+  AxisArgs<R> a = x_args<R>(c, f.spec[0], &f.spec[0], 1, mul, sigma_c);
+  a.f0_blocks = 0;  // no k = 0 / total-charge terms
+  a.o0 = kind == SPEC_DERIV ? j : 0;
+  if ((st = launch_x_args<R>(c, a))) return st;
+  if (f.dim == 3 && (st = launch_y<R>(c, &f.spec[0], 1, +1))) return st;
+  if (kind == SPEC_COULOMB) return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_SCALE, out, nullptr, 4.0 * kPi * coef);
+  return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_STORE, out, nullptr, 0.0);
+}
+
+int Ctx::spectral(const void* in, int kind, int j, void* out, double coef) {
+  if (!fft) return set_error(MPDPFT_ERR_ARG, "no FFT plan");
+  return rsize == sizeof(double) ? spectral_impl<double>(*this, (const double*)in, kind, j, (double*)out, coef)
+                                 : spectral_impl<float>(*this, (const float*)in, kind, j, (float*)out, coef);
+}
+
+// The forward Hartree operator (coefficient gammaH, the context's kernel) on
+// one field.
+int Ctx::coulomb_field(const void* in, void* out) {
+  double one = 1.0;
+  return rsize == sizeof(double)
+             ? coulomb_into<double>(*this, (const double*)in, 1, &one, (double*)out, P.gamma_h)
+             : coulomb_into<float>(*this, (const float*)in, 1, &one, (float*)out, P.gamma_h);
 }
 
 double* batch_vres_part(const Ctx& c) { return c.fft ? c.fft->vres_part : nullptr; }

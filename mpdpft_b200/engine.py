@@ -31,7 +31,7 @@ EXPORTS = [
     "mpdpft_energy", "mpdpft_profile_stage", "mpdpft_iteration_launches", "mpdpft_step_phase_times",
     "mpdpft_batch_create", "mpdpft_batch_destroy", "mpdpft_batch_set_external_potential", "mpdpft_batch_sc_init",
     "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
-    "mpdpft_batch_sync",
+    "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei",
 ]
 
 
@@ -95,6 +95,8 @@ def load(path=LIB_PATH):
     L.mpdpft_batch_get_field.argtypes = [vp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
     L.mpdpft_batch_get_log.argtypes = [vp, C.c_int, C.POINTER(abi.IterLog), C.c_int, C.POINTER(C.c_int)]
     L.mpdpft_batch_sync.argtypes = [vp]
+    L.mpdpft_adjoint.argtypes = [vp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), _dp]
+    L.mpdpft_adjoint_nuclei.argtypes = [vp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_double, _dp]
     for name in EXPORTS:
         getattr(L, name)
     _lib = L
@@ -304,6 +306,29 @@ class Engine:
         us = np.zeros(6)
         self._check(self.lib.mpdpft_step_phase_times(self.h, _ptr(us), 6))
         return us
+
+    def adjoint(self, dl_dn, tol=1e-10, max_iter=300, check=True):
+        """dL/dV_ext of the converged solve for dL/dn (periodic layout):
+        (gradient, iterations, residual, status)."""
+        g = _arr(dl_dn, self.n)
+        out = np.empty(self.n)
+        it = C.c_int()
+        res = C.c_double()
+        st = self.lib.mpdpft_adjoint(self.h, _ptr(g), _ptr(out), abi.LAYOUT_PERIODIC, abi.MEM_HOST, tol, max_iter,
+                                     C.byref(it), C.byref(res))
+        if check and st != abi.OK:
+            self._check(st)
+        return out, it.value, res.value, st
+
+    def adjoint_nuclei(self, dl_dvext, z, pos, sigma):
+        """dL/dR (n_nuclei x 3) of Gaussian nuclei from dL/dV_ext."""
+        g = _arr(dl_dvext, self.n)
+        zz = _arr(z)
+        pp = _arr(pos)
+        out = np.empty(pp.size)
+        self._check(self.lib.mpdpft_adjoint_nuclei(self.h, _ptr(g), abi.MEM_HOST, zz.size, _ptr(zz), _ptr(pp),
+                                                   sigma, _ptr(out)))
+        return out.reshape(-1, 3)
 
     def energy(self):
         r = abi.Result()

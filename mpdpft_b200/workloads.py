@@ -11,6 +11,7 @@ Workloads (one SC solve each unless stated):
   argon_atom      Z=18 Gaussian nucleus, TF + gradient correction, Hartree,
                   Dirac exchange, 128^3
   sweep_2d        256 two-species 2D trapped gases, uneven grids (batched)
+  cluster_adjoint 13 Z=3 nuclei on an icosahedron, 192^3 (adjoint gradients)
   electron_hole   two opposite-charge species on 256^3 in a random potential
 """
 import math
@@ -117,6 +118,52 @@ def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **
     return p, [vext], [v0]
 
 
+def icosahedral_cluster(sites=13, spacing=5.5, jitter=0.05, seed=SEED_BASE + 4):
+    """Centre plus the 12 vertices of an icosahedron at distance `spacing`
+    (the first `sites` of that list), each coordinate jittered by
+    N(0, jitter^2) (seeded)."""
+    phi = 0.5 * (1.0 + math.sqrt(5.0))
+    verts = [(0.0, 0.0, 0.0)]
+    for a in (-1.0, 1.0):
+        for b in (-phi, phi):
+            verts += [(0.0, a, b), (a, b, 0.0), (b, 0.0, a)]
+    v = np.array(verts)
+    v[1:] *= spacing / math.sqrt(1.0 + phi * phi)
+    rng = np.random.default_rng(seed)
+    return v[:sites] + rng.normal(0.0, jitter, (sites, 3)) if jitter > 0 else v[:sites].copy()
+
+
+def nuclei_potential(steps, edge, pos, z, sigma):
+    """Sum of Gaussian-nucleus potentials at the rows of pos."""
+    out = np.zeros(steps ** 3)
+    for c in pos:
+        out += gaussian_nucleus(3, steps, edge, z, sigma, centre=tuple(c))
+    return out
+
+
+def cluster_adjoint(steps=192, edge=32.0, precision=abi.MIXED, sites=13, spacing=5.5, jitter=0.05,
+                    seed=SEED_BASE + 4, **over):
+    """Icosahedral cluster of Gaussian Z = 3 nuclei (sigma 0.1 bohr; centre
+    plus 12 vertices at 5.5 bohr, positions jittered by N(0, 0.05^2)) on
+    [-16, 16]^3, the functional of argon_atom (TF + gradient correction,
+    smoothing 0.2, Hartree, Dirac, g = 2), N = 3 per nucleus.  Returns
+    (params, [V_ext], [V_0], nuclei) with nuclei = dict(z, pos, sigma)."""
+    z, sigma = 3.0, 0.1
+    pos = icosahedral_cluster(sites, spacing, jitter, seed)
+    kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z * sites],
+              rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
+              interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
+              mu=[-5.0], mixer=1, pulay_scope=5, theta=[0.5], sc_criterion=1e-8,
+              max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
+              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0,
+              precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    vext = nuclei_potential(steps, edge, pos, z, sigma)
+    v0 = vext + noise(vext.shape, 1e-3, seed)
+    return p, [vext], [v0], {"z": np.full(sites, z), "pos": pos, "sigma": sigma}
+
+
 def gaussian_landscape(steps, edge, count, seed):
     """Smooth random potential: sum of `count` Gaussians with amplitudes
     U[-2, 2], widths U[1, 4] and centres U[-12, 12]^3 (seeded)."""
@@ -196,4 +243,4 @@ def sweep_2d(count=256, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **o
 
 
 def workload_names():
-    return ["harmonic_tf", "argon_atom", "electron_hole", "sweep_2d"]
+    return ["harmonic_tf", "argon_atom", "electron_hole", "sweep_2d", "cluster_adjoint"]
