@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched sweep")
     ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint run")
     return ap.parse_args()
 
 
@@ -255,6 +256,8 @@ def run_ours(args, world, rank, local):
     e2e = end_to_end(sg, local)
     if not args.no_batch:
         extra["batched_sweep"] = batched_sweep(args.batch_count, local)
+    if not args.no_adjoint:
+        extra["adjoint_cluster"] = adjoint_cluster(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -366,6 +369,43 @@ def batched_sweep(count, device, reps=3):
     out["speedup_host_inputs"] = seq_host / best_host
     out["max_energy_rel_diff_vs_sequential"] = float(max(abs(a.e_total - c.e_total) / abs(c.e_total)
                                                          for a, c in zip(res, seq)))
+    return out
+
+
+def adjoint_cluster(device, max_iter=60):
+    """The 192^3 icosahedral cluster (13 Z = 3 nuclei): converged mixed and
+    FP64 solves, L = dvol sum (n - n_target)^2 against the unjittered
+    cluster, dL/dV_ext by the adjoint and dL/dR of the 39 coordinates; wall
+    times of the solve and of the adjoint."""
+    from mpdpft_b200 import abi, engine, workloads as W
+    out = {"grid": "192^3", "nuclei": 13, "adjoint_max_iter": max_iter}
+    dR = {}
+    for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
+        pt, vt, v0t, _ = W.cluster_adjoint(precision=prec, jitter=0.0)
+        with engine.Engine(pt, device=device) as et:
+            et.sc_run(vt, v0t, check=False)
+            nt = et.field(abi.FIELD_DENSITY, 0)
+        p, vext, v0, nuc = W.cluster_adjoint(precision=prec)
+        with engine.Engine(p, device=device) as e:
+            e.sc_run(vext, v0, check=False)  # warm-up (graph)
+            t0 = time.perf_counter()
+            res, log, st = e.sc_run(vext, v0, check=False)
+            t1 = time.perf_counter()
+            n = e.field(abi.FIELD_DENSITY, 0)
+            dvol = (p.edge / p.steps) ** 3
+            g = 2.0 * dvol * (n - nt)
+            t2 = time.perf_counter()
+            grad, it, resid, ast = e.adjoint(g, max_iter=max_iter, check=False)
+            t3 = time.perf_counter()
+            dR[name] = e.adjoint_nuclei(grad, nuc["z"], nuc["pos"], nuc["sigma"])
+        out["solve_s_%s" % name] = t1 - t0
+        out["solve_iters_%s" % name] = res.iterations
+        out["adjoint_s_%s" % name] = t3 - t2
+        out["adjoint_iters_%s" % name] = it
+        out["adjoint_residual_%s" % name] = resid
+        out["loss_%s" % name] = float(dvol * ((n - nt) ** 2).sum())
+    out["max_abs_dL_dR_fp64"] = float(np.abs(dR["fp64"]).max())
+    out["dL_dR_rel_diff_mixed_vs_fp64"] = float(np.abs(dR["mixed"] - dR["fp64"]).max() / np.abs(dR["fp64"]).max())
     return out
 
 

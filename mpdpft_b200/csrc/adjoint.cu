@@ -24,6 +24,10 @@
 // J_W^T: Hartree = gammaH (K_sym + q 1^T) with K_sym the translation-invariant
 // part and q the field of the regularised kernel's total-charge terms
 // (q = K e_0 - K_sym e_0 from a unit impulse), Dirac and contact pointwise.
+// The iteration is preconditioned by the pointwise part of the map: near the
+// density edge the Dirac term's d V / d n ~ n^{-2/3} makes the local gain
+// -dx A exceed 1; at points where it exceeds 2, lambda is mixed with
+// lambda + (T(lambda) - lambda)/(1 + dx A) (the same fixed point).
 // The fixed-point adjoint needs only the converged state, not the forward
 // iteration history.
 #include <cuda_runtime.h>
@@ -58,7 +62,7 @@ struct Adjoint {
   unsigned long long* vmax = nullptr;
   long long* pstar = nullptr;
 };
-enum { F_VSAVE, F_NSTAR, F_G, F_A, F_B, F_C, F_W, F_D0, F_D1, F_D2, F_DX, F_Q, F_LAM, F_ETA, F_OUT, F_T1, F_T2,
+enum { F_VSAVE, F_NSTAR, F_G, F_A, F_B, F_C, F_W, F_D0, F_D1, F_D2, F_DX, F_Q, F_M, F_ETA, F_OUT, F_T1, F_T2,
        F_T3, F_H, F_NF };
 
 // ------------------------------------------------------------ kernels ----
@@ -240,6 +244,27 @@ __global__ void k_adj_finish_w(long n, const R* g, const R* kc, const R* dx, con
     double v = (double)g[p] + (double)dx[p] * (double)eta[p];
     if (coulomb) v += (double)kc[p] + qe;
     out[p] = R(v);
+  }
+}
+
+// Diagonal preconditioner of the adjoint iteration: the pointwise part of
+// J_W^T J_N^T is D = -dx A (the local feedback of the Dirac and contact
+// terms through the density).  Where that gain exceeds 2 the point is
+// unstable under the plain iteration and M = 1 - D; elsewhere M = 1.
+template <typename R>
+__global__ void k_adj_precond(long n, const R* A, const R* dx, R* M) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const double d = -(double)dx[p] * (double)A[p];
+    M[p] = R(d > 2.0 ? 1.0 - d : 1.0);
+  }
+}
+
+// Mixer input: lambda + (T(lambda) - lambda) / M (same fixed point as T).
+template <typename R>
+__global__ void k_adj_step(long n, const R* lam, const R* out, const R* M, R* next) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const double l = (double)lam[p];
+    next[p] = R(l + ((double)out[p] - l) / (double)M[p]);
   }
 }
 
@@ -459,6 +484,8 @@ static int adjoint_impl(Ctx& c, const double* dl_dn, double* dl_dvext, int mem, 
 #undef PREP
   CU(cudaGetLastError());
   if ((st = adj_dot<R>(c, F[F_A], nullptr, SC_SUM_A))) return st;
+  k_adj_precond<R><<<nb, kThreads, 0, c.stream>>>(n, F[F_A], F[F_DX], F[F_M]);
+  CU(cudaGetLastError());
   // Hartree: the total-charge field q = K e_0 - K_sym e_0
   if (c.has_interaction(MPDPFT_INT_HARTREE)) {
     k_adj_unit<R><<<nb, kThreads, 0, c.stream>>>(n, 0, F[F_T1]);
@@ -487,8 +514,10 @@ static int adjoint_impl(Ctx& c, const double* dl_dn, double* dl_dvext, int mem, 
     resid = scal2[1] > 0.0 ? std::sqrt(scal2[0] / scal2[1]) : 0.0;
     if (!(resid == resid)) return set_error(MPDPFT_ERR_NONFINITE, "adjoint: non-finite residual");
     if (resid <= tol) break;
-    // output of the map in V (species 0), the admix step mixes into the next slot
-    CU(cudaMemcpyAsync(c.d_V, F[F_OUT], sizeof(R) * n, cudaMemcpyDeviceToDevice, c.stream));
+    // the (preconditioned) map's output in V (species 0); the admix step
+    // mixes it with lambda into the next slot
+    k_adj_step<R><<<nb, kThreads, 0, c.stream>>>(n, lam, F[F_OUT], F[F_M], (R*)c.d_V);
+    CU(cudaGetLastError());
     if ((st = c.launch_step(2))) return st;
     if ((st = c.read_state(&hs))) return st;
     lam = (R*)c.d_nin + (long)hs.slot * n;
