@@ -311,6 +311,14 @@ int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
  * [3] convergence test and Pulay solve, [4] grid barrier, [5] mix. */
 int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n);
 
+/* FFT path of the context (no counterpart in the reference, which plans
+ * FFTW once, mpDPFT.cpp:6313-6335): *path 1 = x-plane kernels, 0 = one pass
+ * per axis; the autotuner's timings of one iteration's transforms both ways
+ * (ms; 0 when not measured); *how 0 = one path only, 1 = measured by this
+ * context, 2 = taken from an earlier context of the same kind, 3 = forced by
+ * MPDPFT_FFT_PATH. */
+int mpdpft_fft_config(mpdpft_ctx* ctx, int* path, double* ms_plane, double* ms_pass, int* how);
+
 /* Adjoint of the converged SC fixed point (no counterpart in the reference,
  * whose optimisation drivers take finite differences of whole solves,
  * mpDPFT.cpp:8448).  After mpdpft_sc_run on a one-species context, dl_dn

@@ -262,6 +262,11 @@ int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total) {
   return MPDPFT_OK;
 }
 
+int mpdpft_fft_config(mpdpft_ctx* ctx, int* path, double* ms_plane, double* ms_pass, int* how) {
+  CHECK_CTX(ctx);
+  return ctx->impl.fft_config(path, ms_plane, ms_pass, how);
+}
+
 int mpdpft_adjoint(mpdpft_ctx* ctx, const double* dl_dn, double* dl_dvext, int layout, int mem, double tol,
                    int max_iter, int* iterations, double* residual) {
   CHECK_CTX(ctx);

@@ -111,6 +111,8 @@ struct Ctx {
                double* coeffs, int* ncoeff, int layout, int mem);
   // FFT-based terms (fft.cu)
   int fft_setup();
+  int fft_autotune();  // plane or pass path for 3D transforms (timed, cached per kind)
+  int fft_config(int* path, double* ms_plane, double* ms_pass, int* how);
   void fft_release();
   int issue_fft_terms();                      // Coulomb terms + V assembly + DelField(V)
   int issue_coulomb(const void* dens, void* out, int for_energy);

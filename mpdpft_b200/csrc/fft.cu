@@ -16,9 +16,12 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -89,6 +92,8 @@ struct FftPlan {
   void* cbuf = nullptr;    // complex s^D field for the fftParallel op
   int zparts = 0;          // block sums in zpart written by the last forward pass
   bool plane = false;      // 3D transforms by x-planes (k_plane_fwd / k_plane_inv)
+  double tune_ms[2] = {0.0, 0.0};  // autotuner: transforms of one iteration, plane / pass path
+  int tuned = 0;                   // 0: one path only, 1: measured now, 2: from the cache, 3: forced
 };
 
 
@@ -1073,7 +1078,7 @@ int Ctx::fft_setup() {
     CU(smem_optin(k_axis_c2c<float, 0, 0>));
     CU(smem_optin(k_x_roundtrip<float, 0, 0>));
   }
-  return MPDPFT_OK;
+  return fft_autotune();
 }
 
 void Ctx::fft_release() {
@@ -2107,6 +2112,98 @@ int Ctx::coulomb_field(const void* in, void* out) {
   return rsize == sizeof(double)
              ? coulomb_into<double>(*this, (const double*)in, 1, &one, (double*)out, P.gamma_h)
              : coulomb_into<float>(*this, (const float*)in, 1, &one, (float*)out, P.gamma_h);
+}
+
+// ============================================================ autotuner ==
+// 3D grids whose x-plane kernels are instantiated have two complete
+// transform paths: x-plane kernels (z and y passes fused per plane, TMA bulk
+// copies) and one pass per axis.  Which is faster depends on the grid size,
+// precision and the mix of transforms an iteration runs, so the first
+// context of each (grid, precision, functional, Coulomb) kind times the
+// transforms of one SC iteration (DelField of every species and the Coulomb
+// terms) both ways on its own buffers and keeps the faster; later contexts
+// of the same kind reuse the choice.  MPDPFT_FFT_PATH=plane|pass forces a path.
+template <typename R>
+static int tune_transforms(Ctx& c) {
+  int st;
+  FftPlan& F = *c.fft;
+  const long n = c.geom.n;
+  if (c.has_coulomb) {
+    double one = 1.0;
+    if ((st = coulomb_into<R>(c, (const R*)c.d_V, 1, &one, (R*)c.d_tmp, c.P.gamma_h))) return st;
+  }
+  if (c.gradient)
+    for (int s = 0; s < c.S; ++s) {
+      CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+      if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
+                                 (R*)c.d_lap + (long)s * n)))
+        return st;
+    }
+  return MPDPFT_OK;
+}
+
+int Ctx::fft_autotune() {
+  FftPlan& F = *fft;
+  F.tuned = 0;
+  if (F.dim != 3 || !F.plane || !(gradient || has_coulomb)) return MPDPFT_OK;  // one path only
+  const char* env = std::getenv("MPDPFT_FFT_PATH");
+  if (env && (!std::strcmp(env, "pass") || !std::strcmp(env, "plane"))) {
+    F.plane = !std::strcmp(env, "plane");
+    F.tuned = 3;
+    return MPDPFT_OK;
+  }
+  using Key = std::tuple<int, size_t, int, int, int>;
+  static std::mutex mu;
+  static std::map<Key, std::pair<double, double>> cache;
+  const Key key{F.s, rsize, gradient ? 1 : 0, has_coulomb, S};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      F.tune_ms[0] = it->second.first;
+      F.tune_ms[1] = it->second.second;
+      F.plane = F.tune_ms[0] <= F.tune_ms[1];
+      F.tuned = 2;
+      return MPDPFT_OK;
+    }
+  }
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  int st = MPDPFT_OK;
+  for (int path = 0; path < 2 && !st; ++path) {
+    F.plane = path == 0;
+    for (int rep = 0; rep < 2 && !st; ++rep)  // warm-up
+      st = rsize == sizeof(double) ? tune_transforms<double>(*this) : tune_transforms<float>(*this);
+    if (st) break;
+    const int reps = 5;
+    cudaEventRecord(e0, stream);
+    for (int rep = 0; rep < reps && !st; ++rep)
+      st = rsize == sizeof(double) ? tune_transforms<double>(*this) : tune_transforms<float>(*this);
+    cudaEventRecord(e1, stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) st = set_error(MPDPFT_ERR_CUDA, "autotuner timing");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    F.tune_ms[path] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int i = 0; i < 6; ++i) cnt[i] = 0;
+  if (st) return st;
+  F.plane = F.tune_ms[0] <= F.tune_ms[1];
+  F.tuned = 1;
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = {F.tune_ms[0], F.tune_ms[1]};
+  return MPDPFT_OK;
+}
+
+int Ctx::fft_config(int* path, double* ms_plane, double* ms_pass, int* how) {
+  if (!fft) return set_error(MPDPFT_ERR_ARG, "no FFT plan");
+  if (path) *path = fft->plane ? 1 : 0;
+  if (ms_plane) *ms_plane = fft->tune_ms[0];
+  if (ms_pass) *ms_pass = fft->tune_ms[1];
+  if (how) *how = fft->tuned;
+  return MPDPFT_OK;
 }
 
 double* batch_vres_part(const Ctx& c) { return c.fft ? c.fft->vres_part : nullptr; }

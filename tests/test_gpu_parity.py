@@ -311,3 +311,26 @@ def test_sc_sweep_instance_converged(eng, oracle_lib, prec, e_tol, n_tol, i, ste
     assert abs(res.abundance[0] - p.abundances[0]) <= 2e-10 * p.abundances[0]
     assert de < e_tol
     assert max(l1) < n_tol
+
+
+@pytest.mark.gpu
+def test_fft_autotuner_paths_agree(eng, monkeypatch):
+    """The autotuner picks the faster of the x-plane and per-axis transform
+    paths for a 3D grid; both paths give the same solve."""
+    p, vext, v0 = W.argon_atom(steps=64, precision=abi.FP64)
+    res = {}
+    for path in ("plane", "pass"):
+        monkeypatch.setenv("MPDPFT_FFT_PATH", path)
+        with eng.Engine(p) as e:
+            got, a, b, how = e.fft_config()
+            assert how == 3 and got == (1 if path == "plane" else 0)
+            res[path], _, _ = e.sc_run(vext, v0)
+    monkeypatch.delenv("MPDPFT_FFT_PATH")
+    with eng.Engine(p) as e:
+        got, ms_plane, ms_pass, how = e.fft_config()
+    print("autotuner 64^3 FP64: plane %.3f ms, pass %.3f ms -> %s (how %d)" %
+          (ms_plane, ms_pass, "plane" if got else "pass", how))
+    assert how in (1, 2) and ms_plane > 0 and ms_pass > 0
+    assert got == (1 if ms_plane <= ms_pass else 0)
+    assert res["plane"].iterations == res["pass"].iterations
+    assert abs(res["plane"].e_total - res["pass"].e_total) <= 1e-10 * abs(res["pass"].e_total)
