@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched sweep")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint run")
+    ap.add_argument("--no-eh", action="store_true", help="skip the 256^3 electron-hole solves")
     return ap.parse_args()
 
 
@@ -258,6 +259,8 @@ def run_ours(args, world, rank, local):
         extra["batched_sweep"] = batched_sweep(args.batch_count, local)
     if not args.no_adjoint:
         extra["adjoint_cluster"] = adjoint_cluster(local)
+    if not args.no_eh:
+        extra["electron_hole_256"] = electron_hole_256(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -369,6 +372,31 @@ def batched_sweep(count, device, reps=3):
     out["speedup_host_inputs"] = seq_host / best_host
     out["max_energy_rel_diff_vs_sequential"] = float(max(abs(a.e_total - c.e_total) / abs(c.e_total)
                                                          for a, c in zip(res, seq)))
+    return out
+
+
+def electron_hole_256(device):
+    """Two charged species on 256^3 (electron_hole): time-to-converge in
+    mixed precision and in FP64 on the same GPU (device time of the solve
+    loop from the engine), their energy and density differences."""
+    from mpdpft_b200 import abi, engine, workloads as W
+    out = {"grid": "256^3", "species": 2}
+    dens = {}
+    for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
+        p, vext, v0 = W.electron_hole(steps=256, precision=prec)
+        with engine.Engine(p, device=device) as e:
+            e.sc_run(vext, v0)  # warm-up (graph instantiation)
+            res, log, st = e.sc_run(vext, v0)
+            dens[name] = [e.field(abi.FIELD_DENSITY, s) for s in range(2)]
+        out["ttc_%s_s" % name] = res.seconds
+        out["iters_%s" % name] = res.iterations
+        out["converged_%s" % name] = res.converged
+        out["energy_%s" % name] = res.e_total
+    out["ttc_speedup_mixed_vs_fp64"] = out["ttc_fp64_s"] / out["ttc_mixed_s"]
+    out["energy_rel_err_mixed_vs_fp64"] = abs(out["energy_mixed"] - out["energy_fp64"]) / abs(out["energy_fp64"])
+    dv = (40.0 / 256) ** 3
+    out["density_l1_per_particle_mixed_vs_fp64"] = float(max(np.abs(dens["mixed"][s] - dens["fp64"][s]).sum() * dv / 20000.0
+                                                             for s in range(2)))
     return out
 
 
