@@ -534,7 +534,8 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const long gw = (long)bid * kStepWarps + wib;
   __shared__ double red[kNPart];
-  __shared__ MuState s_ms[kMaxS];
+  __shared__ MuState s_ms[kMaxS];  // every block runs the same search on its own copy
+  __shared__ double s_dmm;
   // active-point lists as this block sees them (identical in every block)
   __shared__ int s_wcnt[kMaxS][kStepWarps];
   __shared__ int s_need[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
@@ -595,6 +596,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
   if (threadIdx.x == 0) {  // every block derives the pass-0 candidates itself
     double dmm = ldcg(&st->dmm);
+    s_dmm = dmm;
     double pn = 0.0;
     for (int s = 0; s < S; ++s) { double pm = ldcg(&st->mu[s]); pn += pm * pm; }
     for (int s = 0; s < S; ++s) {
@@ -623,9 +625,6 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   for (int pass = 0; pass < kMuMaxPasses; ++pass) {
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
-      s_ms[s].done = ldcg(&st->ms[s].done);
-      s_ms[s].ncand = ldcg(&st->ms[s].ncand);
-      for (int c = 0; c < s_ms[s].ncand; ++c) s_ms[s].cand[c] = ldcg(&st->ms[s].cand[c]);
       for (int c = s_ms[s].ncand; c < kMuCand; ++c) s_ms[s].cand[c] = s_ms[s].cand[0];
     }
     __syncthreads();
@@ -735,33 +734,40 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
         mu_point<FK>(d, k, cmu, nc, v, l, g, acc);
       }
-      block_reduce_store<kMuAcc>(acc, mypart + s * kMuAcc);
+      // partial sums double-buffered by pass: a block that has decided may
+      // write the next pass's row while others still read this one
+      block_reduce_store<kMuAcc>(acc, a.part + ((long)(pass & 1) * nblk + bid) * kNPart + s * kMuAcc);
     }
     if (!grid_barrier(st, nblk)) return;
-    if (bid == 0) {
+    // every block sums the partials in the same order and runs the same
+    // decision on its own copy of the search state (no broadcast, no second
+    // barrier); block 0 keeps the state copy that is written back
+    {
+      const double* pbase = a.part + (long)(pass & 1) * nblk * kNPart;
       for (int v = wib; v < S * kMuAcc; v += kStepWarps) {
-        const double t = warp_sum_rows(a.part + v, nblk, kNPart);
+        const double t = warp_sum_rows(pbase + v, nblk, kNPart);
         if (lane == 0) red[v] = t;
       }
       __syncthreads();
       for (int v = threadIdx.x; v < S * kMuAcc; v += blockDim.x) red[v] *= kp.geom.dvol;  // N(mu_c), dN/dmu
       __syncthreads();
       if (threadIdx.x == 0) {
-        double dmm = ls->dmm;
+        double dmm = s_dmm;
         int bits = 0;
         for (int s = 0; s < S; ++s) {
           if (s_ms[s].done) continue;
-          MuState& ms = ls->ms[s];
-          mu_decide(ms, red + s * kMuAcc, red[s * kMuAcc + kMuCand], kp.abundance[s], kp.rel_acc, dmm, bits);
+          mu_decide(s_ms[s], red + s * kMuAcc, red[s * kMuAcc + kMuCand], kp.abundance[s], kp.rel_acc, dmm, bits);
         }
-        ls->dmm = dmm;
-        ls->iter_bits |= bits;
-        ls->mu_passes++;
+        s_dmm = dmm;
+        if (bid == 0) {
+          for (int s = 0; s < S; ++s) ls->ms[s] = s_ms[s];
+          ls->dmm = dmm;
+          ls->iter_bits |= bits;
+          ls->mu_passes++;
+        }
       }
       __syncthreads();
-      state_store(st, ls);
     }
-    if (!grid_barrier(st, nblk)) return;
   }
   if (bid == 0) {  // the pass-0 set-up when no pass ran
     __syncthreads();
