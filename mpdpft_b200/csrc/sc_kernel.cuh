@@ -376,9 +376,8 @@ __device__ __forceinline__ double point_density(const DensParams& d, const EvalK
   else return density_at_d(d, u, l, g);
 }
 
-// N(mu_c) contributions of one point for all candidates, and dN/dmu at
-// candidate 0.  Candidate slots at or beyond nc hold copies of candidate 0
-// in the fast forms (evaluated, never read).
+// N(mu_c) contributions of one point for the nc candidates, and dN/dmu at
+// candidate 0.
 template <int FK>
 __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, const double* cmu, int nc, double v,
                                          double l, double g, double (&acc)[kMuAcc]) {
@@ -386,11 +385,17 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
     const double A = k.cg * l, B = k.cg2 * g;
     acc[kMuCand] += grad3_slope(k, cmu[0] - v, A, B);
 #pragma unroll
-    for (int c = 0; c < kMuCand; ++c) acc[c] += grad3_n(k, cmu[c] - v, A, B);
+    for (int c = 0; c < kMuCand; ++c) {
+      if (c >= nc) break;
+      acc[c] += grad3_n(k, cmu[c] - v, A, B);
+    }
   } else if constexpr (FK == 2) {
     acc[kMuCand] += tf3_slope(k, cmu[0] - v);
 #pragma unroll
-    for (int c = 0; c < kMuCand; ++c) acc[c] += tf3_n(k, cmu[c] - v);
+    for (int c = 0; c < kMuCand; ++c) {
+      if (c >= nc) break;
+      acc[c] += tf3_n(k, cmu[c] - v);
+    }
   } else if constexpr (FK == 3) {
     double n0, sl0;
     g2d_n_slope(k, cmu[0] - v, l, n0, sl0);
