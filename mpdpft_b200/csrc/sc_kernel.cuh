@@ -337,6 +337,13 @@ __device__ __forceinline__ double g2d_n(const EvalK& k, double u, double l) {
   return r == r ? r : 0.0;
 }
 
+// n from a = u/T and e = exp(-|a|) given.
+__device__ __forceinline__ double g2d_n_e(const EvalK& k, double a, double e, double l) {
+  const double ope = 1.0 + e;
+  const double r = k.c2d * (k.T * (fmax(a, 0.0) + log1p(e)) - l * k.lt * (e / (ope * ope)));
+  return r == r ? r : 0.0;
+}
+
 // n and dn/dmu together (one exponential).
 __device__ __forceinline__ void g2d_n_slope(const EvalK& k, double u, double l, double& n, double& slope) {
   const double a = u * k.invT;
@@ -378,9 +385,12 @@ __device__ __forceinline__ double point_density(const DensParams& d, const EvalK
 
 // N(mu_c) contributions of one point for the nc candidates, and dN/dmu at
 // candidate 0.
+// kx (2D form only): per candidate exp(-(mu_c - mu_0)/T) at [c] and its
+// inverse at [kMuCand + c], 0 where the step is too large to share the
+// exponential of candidate 0 (then exp(-|a_c|) is taken directly).
 template <int FK>
 __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, const double* cmu, int nc, double v,
-                                         double l, double g, double (&acc)[kMuAcc]) {
+                                         double l, double g, double (&acc)[kMuAcc], const double* kx = nullptr) {
   if constexpr (FK == 1) {
     const double A = k.cg * l, B = k.cg2 * g;
     acc[kMuCand] += grad3_slope(k, cmu[0] - v, A, B);
@@ -397,14 +407,26 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
       acc[c] += tf3_n(k, cmu[c] - v);
     }
   } else if constexpr (FK == 3) {
-    double n0, sl0;
-    g2d_n_slope(k, cmu[0] - v, l, n0, sl0);
-    acc[0] += n0;
-    acc[kMuCand] += sl0;
+    const double a0 = (cmu[0] - v) * k.invT;
+    const double e0 = exp(-fabs(a0));
+    {
+      const double ope = 1.0 + e0, rope = 1.0 / ope;
+      const double sg = (a0 >= 0.0 ? 1.0 : e0) * rope;
+      const double q = e0 * rope * rope;
+      const double r = k.c2d * (k.T * (fmax(a0, 0.0) + log1p(e0)) - l * k.lt * q);
+      const double dd = k.c2d * (sg - l * k.lt * k.invT * q * (1.0 - 2.0 * sg));
+      acc[0] += r == r ? r : 0.0;
+      acc[kMuCand] += dd == dd ? dd : 0.0;
+    }
+    // e_c = e_0 exp(-+(a_c - a_0)) while a_c keeps the sign of a_0
+    const int side = a0 >= 0.0 ? 0 : kMuCand;
 #pragma unroll
     for (int c = 1; c < kMuCand; ++c) {
       if (c >= nc) break;
-      acc[c] += g2d_n(k, cmu[c] - v, l);
+      const double a = (cmu[c] - v) * k.invT;
+      const double kk = kx[side + c];
+      const double e = ((a >= 0.0) == (a0 >= 0.0) && kk > 0.0) ? e0 * kk : exp(-fabs(a));
+      acc[c] += g2d_n_e(k, a, e, l);
     }
   } else {
     acc[kMuCand] += density_slope_d(d, cmu[0] - v, l, g);
@@ -541,6 +563,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   __shared__ double red[kNPart];
   __shared__ MuState s_ms[kMaxS];  // every block runs the same search on its own copy
   __shared__ double s_dmm;
+  __shared__ double s_kx[kMaxS][2 * kMuCand];  // 2D form: shared exponentials of the candidates
   // active-point lists as this block sees them (identical in every block)
   __shared__ int s_wcnt[kMaxS][kStepWarps];
   __shared__ int s_need[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
@@ -631,6 +654,18 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
       for (int c = s_ms[s].ncand; c < kMuCand; ++c) s_ms[s].cand[c] = s_ms[s].cand[0];
+    }
+    if constexpr (FK == 3) {
+      if (threadIdx.x < S) {
+        const int s = threadIdx.x;
+        const double invT = 1.0 / kp.dens[s].T;
+        for (int c = 0; c < kMuCand; ++c) {
+          const double dlt = (s_ms[s].cand[c] - s_ms[s].cand[0]) * invT;
+          const bool ok = fabs(dlt) < 50.0;
+          s_kx[s][c] = ok ? exp(-dlt) : 0.0;
+          s_kx[s][kMuCand + c] = ok ? exp(dlt) : 0.0;
+        }
+      }
     }
     __syncthreads();
     if (threadIdx.x < S) {
@@ -737,7 +772,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         const double v = (double)__ldcg(Vs + p);
         const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
         const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
-        mu_point<FK>(d, k, cmu, nc, v, l, g, acc);
+        mu_point<FK>(d, k, cmu, nc, v, l, g, acc, s_kx[s]);
       }
       // partial sums double-buffered by pass: a block that has decided may
       // write the next pass's row while others still read this one
