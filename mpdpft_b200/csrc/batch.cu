@@ -337,6 +337,7 @@ int Batch::upload_args() {
       c.vres_part_ext = batch_vres_part(c);
       c.vres_blocks_ext = asm_blocks[i];
       a[i] = c.step_args<R>(mode);
+      a[i].split_d = 0;  // the last block of each solve runs its phase D
     }
     CU(cudaMemcpyAsync(d_args[mode], a.data(), sizeof(StepArgs<R>) * count, cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));

@@ -441,6 +441,7 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.log_cap = log_cap;
   a.assemble_v = assemble_in_step;
   a.mode = mode;
+  a.split_d = 1;
   return a;
 }
 
@@ -474,6 +475,12 @@ static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk, int parts = 7) {
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
     e = cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensityThreads), params, 0,
                          c.stream);
+    if (e != cudaSuccess) return e;
+    c.cnt[MPDPFT_STAGE_SC_STEP]++;
+    if (c.dens_which == 1) sc_phase_d_kernel<R, 5><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
+    else if (c.dens_which == 3) sc_phase_d_kernel<R, 8><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
+    else sc_phase_d_kernel<R, kMaxP><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   if (mode != 1 && (parts & 4)) {

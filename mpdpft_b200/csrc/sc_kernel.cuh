@@ -830,18 +830,12 @@ __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel_b(const StepArgs
   sc_mu_body<R, FK>(args[t.x], t.y, t.z);
 }
 
-// ------------------------------------------------------- density kernel --
-// Final densities n_out = n[V] at the mu the search chose, residual
-// r = n_out - n_in into the ring, and per species [0] N, [1] <n_out, n_in>_w,
-// [2] <n_out, n_out>_w, [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram
-// row), w = multiplicity in the reference storage.  mode 1 writes n_out
-// into the current ring slot instead; mode 2 (admix only) takes n_out from V.
-// The last block to finish runs phase D: CheckConvergence, Intercept, the
-// Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
-template <typename R, int FK, int PW>
-__device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int bid, const int nblk) {
-  // PW: the largest Pulay window this instantiation handles (<= kMaxP); a
-  // small window keeps the per-thread sums in few registers
+// ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
+// over the nblk rows of density-kernel partial sums; cur/next: ring slots,
+// I: Pulay window of this step, mu_rep: the mu reported per species.
+template <typename R, int PW>
+__device__ __forceinline__ void sc_phase_d(const StepArgs<R>& a, const int nblk, const int cur, const int next,
+                                           const int I, const int hist, const int pulay_now, const double* s_mu_rep) {
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const long n = kp.geom.n;
@@ -849,104 +843,7 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
   const int wib = threadIdx.x >> 5;
   __shared__ double red[kNPart];
   __shared__ double red_v[kMaxS];
-  __shared__ double s_mu[kMaxS];      // mu of the final density
-  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
-  __shared__ int s_flag, s_last;
-  __shared__ long s_roff[kMaxP];
-
-  if (a.mode == 0 && !ldcg(&st->iter_active)) return;
-  const int cur = ldcg(&st->slot);
-  const int ring = kp.ring;
-  const int next = (cur + 1) % ring;
-  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
-  if (threadIdx.x < S) {
-    const int s = threadIdx.x;
-    s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
-    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
-  }
-  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
-  __syncthreads();
-  const int pulay_now = s_flag;
-  const int hist = ldcg(&st->hist);
-  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
-  if (threadIdx.x < I) {
-    const int j = threadIdx.x;
-    s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
-  }
-  __syncthreads();
-  R* nin = a.nin + (long)cur * S * n;
-  R* rcur = a.res + (long)cur * S * n;
-  const long gstride = (long)nblk * blockDim.x;
-  for (int s = 0; s < S; ++s) {
-    double acc[4 + PW];
-#pragma unroll
-    for (int j = 0; j < 4 + PW; ++j) acc[j] = 0.0;
-    const DensParams d = kp.dens[s];
-    const EvalK k = eval_constants(d);
-    const double mus = s_mu[s];
-    const long so = (long)s * n;
-    const R* Vs = a.V + so;
-    const R* Ls = a.lap ? a.lap + so : nullptr;
-    const R* Gs = a.g2 ? a.g2 + so : nullptr;
-    // one point per thread; every lane of a warp runs every trip (the vote
-    // below needs them all)
-    for (long base = (long)bid * blockDim.x; base < n; base += gstride) {
-      const long p = base + threadIdx.x;
-      const bool valid = p < n;
-      // issue the streaming loads first
-      const double v = valid ? (double)__ldcg(Vs + p) : 0.0;
-      R ni = R(0);
-      R rj[PW];
-      if (a.mode == 0 || a.mode == 2) {
-        ni = valid ? __ldcg(nin + so + p) : R(0);
-#pragma unroll
-        for (int j = 0; j < PW; ++j)
-          rj[j] = (j < I - 1 && valid) ? __ldcg(a.res + s_roff[j] + so + p) : R(0);
-      }
-      double nod = 0.0;
-      if (a.mode == 2) {  // admix only: V holds the output densities
-        nod = v;
-      } else {
-        const bool mine = valid && (!d.cut || mus - v > 0.0);
-        if (__any_sync(0xffffffffu, mine) && mine) {
-          const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
-          const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
-          nod = point_density<FK>(d, k, mus - v, l, g);
-        }
-      }
-      if (!valid) continue;
-      const R no = R(nod);
-      acc[0] += nod;
-      if (a.mode == 1) {
-        nin[so + p] = no;
-        a.cur_copy[so + p] = no;
-        continue;
-      }
-      const R r = no - ni;
-      rcur[so + p] = r;
-      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
-      const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
-      acc[1] += w * dno * dni;
-      acc[2] += w * dno * dno;
-      acc[3] += w * dni * dni;
-#pragma unroll
-      for (int j = 0; j < PW; ++j) {
-        if (j < I - 1) acc[4 + j] += wr * (double)rj[j];
-        else if (j == I - 1) acc[4 + j] += wr * dr;
-      }
-    }
-    block_reduce_store<4 + PW>(acc, a.part2 + (long)bid * kNPart + s * kNF);
-  }
-  // the last block to finish takes phase D
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(&st->k2_done, 1u) == nblk - 1 ? 1 : 0;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
   if (threadIdx.x == 0) st->tphase[3] = globaltimer();
-
-  // ---- phase D: CheckConvergence, Intercept, PulayMixer, InjectSchedule --
   __shared__ ScState s_st;
   ScState* const ls = &s_st;
   __shared__ double s_G[kMaxP * kMaxP], s_inv[kMaxP * kMaxP], s_M[kMaxP * kMaxP], s_R[kMaxP * kMaxP];
@@ -1118,6 +1015,122 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
   }
 }
 
+// ------------------------------------------------------- density kernel --
+// Final densities n_out = n[V] at the mu the search chose, residual
+// r = n_out - n_in into the ring, and per species [0] N, [1] <n_out, n_in>_w,
+// [2] <n_out, n_out>_w, [3] <n_in, n_in>_w, [4 + j] <r_new, r_j>_w (Gram
+// row), w = multiplicity in the reference storage.  mode 1 writes n_out
+// into the current ring slot instead; mode 2 (admix only) takes n_out from V.
+// The last block to finish runs phase D: CheckConvergence, Intercept, the
+// Pulay solve (AdmixDensities / PulayMixer) and InjectSchedule.
+template <typename R, int FK, int PW>
+__device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int bid, const int nblk) {
+  // PW: the largest Pulay window this instantiation handles (<= kMaxP); a
+  // small window keeps the per-thread sums in few registers
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const long n = kp.geom.n;
+  const int S = kp.S;
+  const int wib = threadIdx.x >> 5;
+  __shared__ double s_mu[kMaxS];      // mu of the final density
+  __shared__ double s_mu_rep[kMaxS];  // mu reported (the start value after a bracket failure)
+  __shared__ int s_flag, s_last;
+  __shared__ long s_roff[kMaxP];
+
+  if (a.mode == 0 && !ldcg(&st->iter_active)) return;
+  const int cur = ldcg(&st->slot);
+  const int ring = kp.ring;
+  const int next = (cur + 1) % ring;
+  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
+  if (threadIdx.x < S) {
+    const int s = threadIdx.x;
+    s_mu[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].dens_mu) : ldcg(&st->mu[s]);
+    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
+  }
+  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
+  __syncthreads();
+  const int pulay_now = s_flag;
+  const int hist = ldcg(&st->hist);
+  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
+  if (threadIdx.x < I) {
+    const int j = threadIdx.x;
+    s_roff[j] = (long)((cur - (I - 1) + j + ring) % ring) * S * n;
+  }
+  __syncthreads();
+  R* nin = a.nin + (long)cur * S * n;
+  R* rcur = a.res + (long)cur * S * n;
+  const long gstride = (long)nblk * blockDim.x;
+  for (int s = 0; s < S; ++s) {
+    double acc[4 + PW];
+#pragma unroll
+    for (int j = 0; j < 4 + PW; ++j) acc[j] = 0.0;
+    const DensParams d = kp.dens[s];
+    const EvalK k = eval_constants(d);
+    const double mus = s_mu[s];
+    const long so = (long)s * n;
+    const R* Vs = a.V + so;
+    const R* Ls = a.lap ? a.lap + so : nullptr;
+    const R* Gs = a.g2 ? a.g2 + so : nullptr;
+    // one point per thread; every lane of a warp runs every trip (the vote
+    // below needs them all)
+    for (long base = (long)bid * blockDim.x; base < n; base += gstride) {
+      const long p = base + threadIdx.x;
+      const bool valid = p < n;
+      // issue the streaming loads first
+      const double v = valid ? (double)__ldcg(Vs + p) : 0.0;
+      R ni = R(0);
+      R rj[PW];
+      if (a.mode == 0 || a.mode == 2) {
+        ni = valid ? __ldcg(nin + so + p) : R(0);
+#pragma unroll
+        for (int j = 0; j < PW; ++j)
+          rj[j] = (j < I - 1 && valid) ? __ldcg(a.res + s_roff[j] + so + p) : R(0);
+      }
+      double nod = 0.0;
+      if (a.mode == 2) {  // admix only: V holds the output densities
+        nod = v;
+      } else {
+        const bool mine = valid && (!d.cut || mus - v > 0.0);
+        if (__any_sync(0xffffffffu, mine) && mine) {
+          const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
+          const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
+          nod = point_density<FK>(d, k, mus - v, l, g);
+        }
+      }
+      if (!valid) continue;
+      const R no = R(nod);
+      acc[0] += nod;
+      if (a.mode == 1) {
+        nin[so + p] = no;
+        a.cur_copy[so + p] = no;
+        continue;
+      }
+      const R r = no - ni;
+      rcur[so + p] = r;
+      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
+      const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
+      acc[1] += w * dno * dni;
+      acc[2] += w * dno * dno;
+      acc[3] += w * dni * dni;
+#pragma unroll
+      for (int j = 0; j < PW; ++j) {
+        if (j < I - 1) acc[4 + j] += wr * (double)rj[j];
+        else if (j == I - 1) acc[4 + j] += wr * dr;
+      }
+    }
+    block_reduce_store<4 + PW>(acc, a.part2 + (long)bid * kNPart + s * kNF);
+  }
+  if (a.split_d) return;  // phase D runs as its own launch
+  // the last block to finish takes phase D
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->k2_done, 1u) == nblk - 1 ? 1 : 0;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  sc_phase_d<R, PW>(a, nblk, cur, next, I, hist, pulay_now, s_mu_rep);
+}
+
 template <typename R, int FK, int PW>
 __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs<R> a) {
   sc_density_body<R, FK, PW>(a, blockIdx.x, gridDim.x);
@@ -1128,6 +1141,31 @@ __global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel_b(const 
                                                                          const int4* __restrict__ tab) {
   const int4 t = tab[blockIdx.x];
   sc_density_body<R, FK, PW>(args[t.x], t.y, t.z);
+}
+
+// Phase D as its own launch: one block, no register cap from the streaming
+// kernel's occupancy.
+template <typename R, int PW>
+__global__ void __launch_bounds__(kDensityThreads, 1) sc_phase_d_kernel(StepArgs<R> a, int nblk) {
+  const KParams& kp = a.kp;
+  ScState* st = a.st;
+  const int S = kp.S;
+  __shared__ double s_mu_rep[kMaxS];
+  __shared__ int s_flag;
+  if (a.mode == 0 && !ldcg(&st->iter_active)) return;
+  const int cur = ldcg(&st->slot);
+  const int next = (cur + 1) % kp.ring;
+  const int active = kp.rel_acc > 1.0e-12 ? 1 : 0;
+  if (threadIdx.x < S) {
+    const int s = threadIdx.x;
+    s_mu_rep[s] = (active && a.mode != 2) ? ldcg(&st->ms[s].best_mu) : ldcg(&st->mu[s]);
+  }
+  if (threadIdx.x == 0) s_flag = (a.mode != 1 && kp.mixer > 0 && ldcg(&st->sc_count) > 0) ? 1 : 0;
+  __syncthreads();
+  const int pulay_now = s_flag;
+  const int hist = ldcg(&st->hist);
+  const int I = pulay_now ? (hist + 1 < kp.scope ? hist + 1 : kp.scope) : 0;
+  sc_phase_d<R, PW>(a, nblk, cur, next, I, hist, pulay_now, s_mu_rep);
 }
 
 // ---------------------------------------------------------- mix kernel --

@@ -119,6 +119,8 @@ struct StepArgs {
   int assemble_v;  // 1: phase A assembles V from vext, n_in and vh
   int mode;        // 0: SC iteration; 1: densities of the current V only;
                    // 2: admix only (V holds the output densities)
+  int split_d;     // 1: phase D runs as its own one-block launch after the
+                   // density kernel; 0: the density kernel's last block runs it
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
