@@ -256,7 +256,7 @@ def run_ours(args, world, rank, local):
 
     e2e = end_to_end(sg, local)
     if not args.no_batch:
-        extra["batched_sweep"] = batched_sweep(args.batch_count, local)
+        extra["batched_sweep"] = batched_sweep(args.batch_count, local, rank=rank, world=world, pg=pg)
     if not args.no_adjoint:
         extra["adjoint_cluster"] = adjoint_cluster(local)
     if not args.no_eh:
@@ -313,35 +313,61 @@ def time_to_converge(sg, device):
     return out
 
 
-def batched_sweep(count, device, reps=3):
+def batched_sweep(count, device, reps=3, rank=0, world=1, pg=None):
     """Solves/s of the batched sweep against the same solves one at a time
-    (mpdpft_sc_run per solve, contexts created before the timing)."""
+    (mpdpft_sc_run per solve, contexts created before the timing).  With
+    several ranks every rank solves its shard of the solves
+    (workloads.sweep_shard, no exchange) and the time is the maximum over
+    ranks."""
     import torch
     from mpdpft_b200 import abi, engine, workloads as W
-    probs = W.sweep_2d(count, precision=abi.MIXED)
-    out = {"count": count, "grids": {str(s): sum(1 for p, _, _ in probs if p.steps == s) for s in W.SWEEP_SIZES},
-           "precision": "mixed", "timing": "wall clock per full solve of all, best of %d" % reps}
+    idx = W.sweep_shard(count, rank, world)
+    probs = W.sweep_2d(count, precision=abi.MIXED, indices=idx)
+
+    def tmax(t):  # wall time of the slowest rank
+        if pg is None:
+            return t
+        x = torch.tensor([t], dtype=torch.float64, device="cuda:%d" % device)
+        pg.all_reduce(x, op=pg.ReduceOp.MAX)
+        return float(x.item())
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    out = {"count": count, "ranks": world, "solves_this_rank": len(idx),
+           "grids": {str(s): sum(1 for i in range(count) if W.sweep_steps(i) == s) for s in W.SWEEP_SIZES},
+           "precision": "mixed", "timing": "wall clock per full solve of all (max over ranks), best of %d" % reps}
     dev = [torch.tensor(v, dtype=torch.float64, device="cuda:%d" % device) for _, _, v0 in probs for v in v0]
     torch.cuda.synchronize(device)
     with engine.Batch(probs, device=device) as b:
         b.sc_run(device_v0=[x.data_ptr() for x in dev])  # warm-up: graph instantiation
         best = None
         for _ in range(reps):
+            barrier()
             t0 = time.perf_counter()
             res, status = b.sc_run(device_v0=[x.data_ptr() for x in dev])
-            dt = time.perf_counter() - t0
+            dt = tmax(time.perf_counter() - t0)
             best = dt if best is None else min(best, dt)
         best_host = None
         for _ in range(reps):
+            barrier()
             t0 = time.perf_counter()
             b.sc_run()
-            dt = time.perf_counter() - t0
+            dt = tmax(time.perf_counter() - t0)
             best_host = dt if best_host is None else min(best_host, dt)
     out["batched_solves_per_s"] = count / best
     out["batched_s"] = best
     out["batched_host_inputs_solves_per_s"] = count / best_host
-    out["converged"] = sum(r.converged for r in res)
-    out["status_ok"] = sum(1 for st in status if st == abi.OK)
+    def tsum(v):  # over ranks
+        if pg is None:
+            return v
+        x = torch.tensor([float(v)], dtype=torch.float64, device="cuda:%d" % device)
+        pg.all_reduce(x, op=pg.ReduceOp.SUM)
+        return int(round(x.item()))
+
+    out["converged"] = tsum(sum(r.converged for r in res))
+    out["status_ok"] = tsum(sum(1 for st in status if st == abi.OK))
     out["iterations_mean"] = float(np.mean([r.iterations for r in res]))
     out["iterations_max"] = int(max(r.iterations for r in res))
     engines = []
@@ -354,15 +380,17 @@ def batched_sweep(count, device, reps=3):
     engines[0].sc_run(None, device_v0=[x.data_ptr() for x in dev[:S]])  # warm-up
     seq_best, seq_host = None, None
     for _ in range(2):
+        barrier()
         t0 = time.perf_counter()
         seq = [e.sc_run(None, device_v0=[x.data_ptr() for x in dev[i * S:(i + 1) * S]])[0]
                for i, e in enumerate(engines)]
-        dt = time.perf_counter() - t0
+        dt = tmax(time.perf_counter() - t0)
         seq_best = dt if seq_best is None else min(seq_best, dt)
+    barrier()
     t0 = time.perf_counter()
     for e, (p, vext, v0) in zip(engines, probs):
         e.sc_run(None, v0)
-    seq_host = time.perf_counter() - t0
+    seq_host = tmax(time.perf_counter() - t0)
     for e in engines:
         e.close()
     out["sequential_solves_per_s"] = count / seq_best
@@ -371,7 +399,7 @@ def batched_sweep(count, device, reps=3):
     out["speedup_batched_vs_sequential"] = seq_best / best
     out["speedup_host_inputs"] = seq_host / best_host
     out["max_energy_rel_diff_vs_sequential"] = float(max(abs(a.e_total - c.e_total) / abs(c.e_total)
-                                                         for a, c in zip(res, seq)))
+                                                         for a, c in zip(res, seq)))  # this rank's solves
     return out
 
 

@@ -237,9 +237,31 @@ def sweep_instance(i, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **ove
     return p, [vext, vext.copy()], v0
 
 
-def sweep_2d(count=256, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, **over):
-    """The batched sweep: `count` instances of sweep_instance."""
-    return [sweep_instance(i, seed, steps, precision, **over) for i in range(count)]
+def sweep_2d(count=256, seed=SEED_BASE + 3, steps=None, precision=abi.MIXED, indices=None, **over):
+    """The batched sweep: `count` instances of sweep_instance (or those of
+    `indices`)."""
+    idx = range(count) if indices is None else indices
+    return [sweep_instance(i, seed, steps, precision, **over) for i in idx]
+
+
+def sweep_steps(i, seed=SEED_BASE + 3):
+    """Grid size of instance i of the sweep (its first seeded draw)."""
+    return int(np.random.default_rng(seed * 1000 + i).choice(SWEEP_SIZES))
+
+
+def sweep_shard(count, rank, world, seed=SEED_BASE + 3):
+    """Instances of the sweep that rank `rank` of `world` solves: greedy
+    longest-processing-time assignment by grid points (largest first, each to
+    the least loaded rank, ties to the lower rank), the same on every rank."""
+    order = sorted(range(count), key=lambda i: (-sweep_steps(i, seed) ** 2, i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += sweep_steps(i, seed) ** 2
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
 
 
 def workload_names():
