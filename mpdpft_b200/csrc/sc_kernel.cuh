@@ -24,87 +24,15 @@ namespace mpdpft {
 
 // ---------------------------------------------------------- small solve --
 // Inverse of the Pulay Gram matrix (n <= kMaxP) by Gauss-Jordan elimination
-// with full pivoting on one warp; rank test as Eigen's
-// FullPivHouseholderQR::isInvertible (threshold eps * n * max|pivot|), which
-// the reference uses (mpDPFT.cpp:5089).  Each pivot is the first maximum, in
-// row-major order, among the rows and columns not used yet.  Rows are never
-// swapped: lane l holds elements l, l + 32, ... of [M | R] in registers, the
-// pivot row and column pass through shared memory, and at the end row pc_k
-// of the inverse is row pr_k of R.
-constexpr int kInvQ = (kMaxP * kMaxP + 31) / 32;
-
-__device__ inline bool warp_inverse(int n, const double* G, double* inv, double* prow_m, double* prow_r,
-                                    double* pcol, int* colof) {
-  const int lane = threadIdx.x & 31;
-  const int nn = n * n;
-  double m[kInvQ], r[kInvQ];
-  int ei[kInvQ], ej[kInvQ];
-#pragma unroll
-  for (int q = 0; q < kInvQ; ++q) {
-    const int e = lane + 32 * q;
-    ei[q] = e < nn ? e / n : -1;  // -1: this slot holds no element
-    ej[q] = e < nn ? e % n : 0;
-    m[q] = e < nn ? G[e] : 0.0;
-    r[q] = (e < nn && ei[q] == ej[q]) ? 1.0 : 0.0;
-  }
-  unsigned used_r = 0u, used_c = 0u;
-  double maxpiv = 0.0, minpiv = 1e300;
-  for (int c = 0; c < n; ++c) {
-    double best = -1.0;
-    int be = 0x7fffffff;
-#pragma unroll
-    for (int q = 0; q < kInvQ; ++q) {
-      if (ei[q] < 0 || ((used_r >> ei[q]) & 1u) || ((used_c >> ej[q]) & 1u)) continue;
-      const double v = fabs(m[q]);
-      if (v > best) { best = v; be = lane + 32 * q; }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oe = __shfl_xor_sync(0xffffffffu, be, o);
-      if (ob > best || (ob == best && oe < be)) { best = ob; be = oe; }
-    }
-    const int pr = be / n, pc = be % n;
-#pragma unroll
-    for (int q = 0; q < kInvQ; ++q) {
-      if (ei[q] == pr) { prow_m[ej[q]] = m[q]; prow_r[ej[q]] = r[q]; }
-      if (ei[q] >= 0 && ej[q] == pc) pcol[ei[q]] = m[q];
-    }
-    if (lane == 0) colof[pr] = pc;
-    __syncwarp();
-    const double piv = pcol[pr];
-    maxpiv = fmax(maxpiv, fabs(piv));
-    minpiv = fmin(minpiv, fabs(piv));
-    if (piv == 0.0) return false;  // same value on every lane
-    const double ip = 1.0 / piv;
-#pragma unroll
-    for (int q = 0; q < kInvQ; ++q) {
-      if (ei[q] < 0) continue;
-      if (ei[q] == pr) {
-        m[q] *= ip;
-        r[q] *= ip;
-      } else {
-        const double f = pcol[ei[q]] * ip;
-        m[q] -= f * prow_m[ej[q]];
-        r[q] -= f * prow_r[ej[q]];
-      }
-    }
-    used_r |= 1u << pr;
-    used_c |= 1u << pc;
-    __syncwarp();
-  }
-  if (minpiv <= 2.220446049250313e-16 * (double)n * maxpiv) return false;
-#pragma unroll
-  for (int q = 0; q < kInvQ; ++q)
-    if (ei[q] >= 0) inv[colof[ei[q]] * n + ej[q]] = r[q];
-  __syncwarp();
-  return true;
-}
-
-// The same inverse on the first `nthr` threads of the block (whole warps),
-// synchronised with named barrier 1 so that the other warps can work
-// meanwhile: warp 0 finds each pivot, every thread updates elements of
-// [M | R].  Each pivot step costs a few barriers instead of a serial chain.
+// with full pivoting; rank test as Eigen's FullPivHouseholderQR::isInvertible
+// (threshold eps * n * max|pivot|), which the reference uses
+// (mpDPFT.cpp:5089).  Each pivot is the first maximum, in row-major order,
+// among the rows and columns not used yet; rows are never swapped (row pc_k
+// of the inverse is row pr_k of R).  Runs on the first `nthr` threads of the
+// block (whole warps), synchronised with named barrier 1 so that the other
+// warps can work meanwhile: warp 0 finds each pivot, every thread updates
+// elements of [M | R].  A matrix with no finite pivot left (NaN or Inf
+// entries) is reported singular.
 __device__ __forceinline__ void group_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
 
 __device__ inline bool group_inverse(int n, const double* G, double* M, double* Rm, double* inv, int* colof,
@@ -135,15 +63,21 @@ __device__ inline bool group_inverse(int n, const double* G, double* M, double* 
         if (ob > best || (ob == best && oe < be)) { best = ob; be = oe; }
       }
       if (lane == 0) {
-        const int pr = be / n, pc = be % n;
-        s_pi[0] = pr;
-        s_pi[1] = pc;
-        s_pv[0] = M[be];
-        s_pv[1] = fmax(s_pv[1], best);
-        s_pv[2] = fmin(s_pv[2], best);
-        s_pi[2] |= 1 << pr;
-        s_pi[3] |= 1 << pc;
-        colof[pr] = pc;
+        if (be >= nn || !(best <= 1.0e300)) {  // no finite pivot: singular
+          s_pi[0] = 0;
+          s_pi[1] = 0;
+          s_pv[0] = 0.0;
+        } else {
+          const int pr = be / n, pc = be % n;
+          s_pi[0] = pr;
+          s_pi[1] = pc;
+          s_pv[0] = M[be];
+          s_pv[1] = fmax(s_pv[1], best);
+          s_pv[2] = fmin(s_pv[2], best);
+          s_pi[2] |= 1 << pr;
+          s_pi[3] |= 1 << pc;
+          colof[pr] = pc;
+        }
       }
     }
     group_bar(nthr);
@@ -981,7 +915,7 @@ __device__ __forceinline__ void sc_phase_d(const StepArgs<R>& a, const int nblk,
           if (ls->theta[s] < 0.2)
             ls->theta[s] = ls->theta0[s] + (0.2 - ls->theta0[s]) * (double)sc / (double)kp.max_sc;
       }
-      if (a.log && sc < a.log_cap) {
+      if (a.log && sc >= 0 && sc < a.log_cap) {
         mpdpft_iter_log& L = a.log[sc];
         L.sc_count = sc;
         L.mu_trials = ls->mu_passes;

@@ -334,3 +334,26 @@ def test_fft_autotuner_paths_agree(eng, monkeypatch):
     assert got == (1 if ms_plane <= ms_pass else 0)
     assert res["plane"].iterations == res["pass"].iterations
     assert abs(res["plane"].e_total - res["pass"].e_total) <= 1e-10 * abs(res["pass"].e_total)
+
+
+@pytest.mark.gpu
+def test_admix_nonfinite_history_is_singular(eng):
+    """A Pulay history with NaN / Inf residuals has no finite pivot: the
+    device solve reports it singular and falls back to linear mixing (the
+    context stays usable) instead of reading past the Gram matrix."""
+    s = 16
+    p = abi.make_params(dim=3, steps=s, edge=8.0, mixer=1, pulay_scope=5, precision=abi.FP64)
+    rng = np.random.default_rng(5)
+    with eng.Engine(p) as e:
+        n_in = [rng.uniform(0.5, 1.0, s ** 3)]
+        for k in range(3):
+            n_out = [n_in[0] + rng.uniform(-0.1, 0.1, s ** 3)]
+            if k == 2:
+                n_out[0][::7] = np.nan
+                n_out[0][1::11] = np.inf
+            mixed, coeffs, st = e.AdmixDensities(n_in, n_out, check=False)
+            n_in = [np.nan_to_num(mixed[0], nan=0.7, posinf=0.7, neginf=0.7)]
+        assert st in (abi.OK, abi.ERR_PULAY_SINGULAR, abi.ERR_NONFINITE)
+        # the context still works
+        r = e.Integrate(np.ones(s ** 3))
+        assert abs(r - 8.0 ** 3) < 1e-9 * 8.0 ** 3
