@@ -166,9 +166,19 @@ __device__ __forceinline__ void reg_dft(C (&a)[8], int dir) {
   }
 }
 
+// Element (t, l) of an NL-line tile: rows padded to NL + 1, and the line
+// index XOR-ed with (t / 8) mod NL.  The element-fastest first stage writes
+// the radix-8 outputs of consecutive threads 8 rows apart, which padding
+// alone maps onto two banks (8-way conflicts); the swizzle spreads them over
+// all banks while line-fastest accesses stay conflict-free (NL a power of 2).
+template <int NL>
+__device__ __forceinline__ int tile_at(int t, int l) {
+  static_assert((NL & (NL - 1)) == 0, "tile width must be a power of two");
+  return t * (NL + 1) + (l ^ ((t >> 3) & (NL - 1)));
+}
+
 // Stockham stages STAGE .. END-1 of a length-N transform of an NL-line tile
-// stored as element (t, l) at t * (NL + 1) + l: the padded row keeps both
-// line-fastest and element-fastest accesses free of bank conflicts.
+// (element (t, l) at tile_at<NL>(t, l)).
 template <typename C, int N, int NL, int STAGE, int STRIDE, int END = ct_num_stages(N)>
 __device__ __forceinline__ void ct_stages(C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw,
                                           int dir) {
@@ -183,13 +193,13 @@ __device__ __forceinline__ void ct_stages(C* __restrict__ src, C* __restrict__ d
       const int q = b / STRIDE, k = b % STRIDE;
       C a[8];
 #pragma unroll
-      for (int t = 0; t < R; ++t) a[t] = src[(k + STRIDE * (q + t * M)) * (NL + 1) + l];
+      for (int t = 0; t < R; ++t) a[t] = src[tile_at<NL>(k + STRIDE * (q + t * M), l)];
       reg_dft<R>(a, dir);
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         C v = a[u];
         if (u > 0) v = cmul(v, tw[q * u * STRIDE]);
-        dst[(k + STRIDE * (R * q + u)) * (NL + 1) + l] = v;
+        dst[tile_at<NL>(k + STRIDE * (R * q + u), l)] = v;
       }
     }
     __syncthreads();
@@ -206,7 +216,7 @@ __host__ __device__ constexpr int ct_stride_before(int n, int stage) {
 // Length-N transforms of NL lines with the first stage reading its inputs
 // from `load(t, l)` straight into registers and the last stage handing its
 // outputs to `store(t, l, v)`; only the middle stages exchange through the
-// shared-memory tile A/B (layout t * (NL + 1) + l).  ELEM_FAST maps consecutive
+// shared-memory tile A/B (layout tile_at<NL>).  ELEM_FAST maps consecutive
 // threads to consecutive elements of a line in the first and last stages
 // (contiguous rows); otherwise to consecutive lines (strided columns).
 // The twiddle table tw (length N) holds e^{dir 2 pi i t/N}.  Ends with
@@ -242,7 +252,7 @@ __device__ __forceinline__ void fft_lines(C* __restrict__ A, C* __restrict__ B, 
       for (int u = 0; u < R0; ++u) {
         C v = a[u];
         if (u > 0) v = cmul(v, tw[q * u]);
-        A[(R0 * q + u) * (NL + 1) + l] = v;
+        A[tile_at<NL>(R0 * q + u, l)] = v;
       }
     }
     __syncthreads();
@@ -257,7 +267,7 @@ __device__ __forceinline__ void fft_lines(C* __restrict__ A, C* __restrict__ B, 
       const int k = ELEM_FAST ? w % SL : w / NL;
       C a[8];
 #pragma unroll
-      for (int t = 0; t < RL; ++t) a[t] = src[(k + SL * t) * (NL + 1) + l];
+      for (int t = 0; t < RL; ++t) a[t] = src[tile_at<NL>(k + SL * t, l)];
       reg_dft<RL>(a, dir);
 #pragma unroll
       for (int u = 0; u < RL; ++u) store(k + SL * u, l, a[u]);
