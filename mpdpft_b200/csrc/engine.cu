@@ -320,7 +320,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   long useful = (geom.n + kStepThreads - 1) / kStepThreads;
   if (step_blocks > useful) step_blocks = (int)std::max(1L, useful);
   const long groups = (geom.n + 3) / 4;  // the mixing kernel takes 4 points a thread
-  dens_blocks = (int)std::max(1L, std::min((long)num_sms * occ_dens, (geom.n + kDensityThreads - 1) / kDensityThreads));
+  dens_blocks = (int)std::max(1L, std::min((long)num_sms * occ_dens, (geom.n + 4 * kDensityThreads - 1) / (4 * kDensityThreads)));
   mix_blocks = (int)std::max(1L, std::min((long)num_sms * occ_mix, (groups + kDensThreads - 1) / kDensThreads));
   // the mu kernel's list sweeps: a contiguous chunk of points per warp
   {

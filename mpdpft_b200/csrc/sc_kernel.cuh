@@ -156,19 +156,56 @@ __device__ __forceinline__ void store4(R* f, long p0, long n, int vec4, const R 
   }
 }
 
-// Reference-storage multiplicities (ref_multiplicity) of points p0 .. p0+3.
-__device__ __forceinline__ void ref_weights4(long p0, int s, int dim, double (&w)[4]) {
+// Reference-storage multiplicities (ref_multiplicity) of points p0 .. p0+NP-1.
+template <int NP>
+__device__ __forceinline__ void ref_weights(long p0, int s, int dim, double (&w)[NP]) {
   const unsigned us = (unsigned)s;
   unsigned p = (unsigned)p0;
   unsigned k = p % us, q = p / us;
   unsigned j = q % us, i = q / us;
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
+  for (int t = 0; t < NP; ++t) {
     w[t] = (k == 0 ? 2.0 : 1.0) * (j == 0 ? 2.0 : 1.0) * ((dim == 3 && i == 0) ? 2.0 : 1.0);
     if (++k == us) {
       k = 0;
       if (++j == us) { j = 0; ++i; }
     }
+  }
+}
+
+// One 16-byte vector of a field per thread: NP = 16 / sizeof(R) values at
+// p0 (a multiple of NP); scalar accesses at the ragged end or when the
+// field length is not a multiple of 4 (vec = 0).
+template <typename R>
+constexpr int kVecPts = 16 / (int)sizeof(R);
+
+template <typename R>
+__device__ __forceinline__ void vload(const R* f, long p0, long n, int vec, R (&o)[kVecPts<R>]) {
+  constexpr int NP = kVecPts<R>;
+  if (vec && p0 + NP - 1 < n) {
+    if constexpr (NP == 4) {
+      const float4 t = __ldcg(reinterpret_cast<const float4*>(f + p0));
+      o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+    } else {
+      const double2 t = __ldcg(reinterpret_cast<const double2*>(f + p0));
+      o[0] = t.x; o[1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) o[i] = (p0 + i < n) ? __ldcg(f + p0 + i) : R(0);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void vstore(R* f, long p0, long n, int vec, const R (&o)[kVecPts<R>]) {
+  constexpr int NP = kVecPts<R>;
+  if (vec && p0 + NP - 1 < n) {
+    if constexpr (NP == 4) *reinterpret_cast<float4*>(f + p0) = make_float4(o[0], o[1], o[2], o[3]);
+    else *reinterpret_cast<double2*>(f + p0) = make_double2(o[0], o[1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+      if (p0 + i < n) f[p0 + i] = o[i];
   }
 }
 
@@ -229,6 +266,21 @@ __device__ __forceinline__ double grad3_n(const EvalK& k, double u, double A, do
   const double m3 = hi ? r * r * r : u * k.c3;
   const double v = k.ctf * u * u * r - (A * m1 + B * m3);
   return (u > 0.0 && v > 0.0) ? v : 0.0;
+}
+
+// n(u) and dn/du of the same form with one reciprocal square root.
+__device__ __forceinline__ double grad3_n_slope(const EvalK& k, double u, double A, double B, double& sl) {
+  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const bool hi = u >= k.floor_u;
+  const double r3 = r * r * r;
+  const double m1 = hi ? r : u * k.c1;
+  const double m3 = hi ? r3 : u * k.c3;
+  const double dm1 = hi ? -0.5 * r3 : k.c1;
+  const double dm3 = hi ? -1.5 * r3 * r * r : k.c3;
+  const double v = k.ctf * u * u * r - (A * m1 + B * m3);
+  const bool pos = u > 0.0 && v > 0.0;
+  sl = pos ? 1.5 * k.ctf * u * r - (A * dm1 + B * dm3) : 0.0;
+  return pos ? v : 0.0;
 }
 
 // dn/du of the same form (density_slope_d), zero where n is clamped.
@@ -327,9 +379,11 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
                                          double l, double g, double (&acc)[kMuAcc], const double* kx = nullptr) {
   if constexpr (FK == 1) {
     const double A = k.cg * l, B = k.cg2 * g;
-    acc[kMuCand] += grad3_slope(k, cmu[0] - v, A, B);
+    double sl;
+    acc[0] += grad3_n_slope(k, cmu[0] - v, A, B, sl);
+    acc[kMuCand] += sl;
 #pragma unroll
-    for (int c = 0; c < kMuCand; ++c) {
+    for (int c = 1; c < kMuCand; ++c) {
       if (c >= nc) break;
       acc[c] += grad3_n(k, cmu[c] - v, A, B);
     }
@@ -494,6 +548,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   const long nthreads = (long)nblk * blockDim.x;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const long gw = (long)bid * kStepWarps + wib;
+  const long nwarps = (long)nblk * kStepWarps;
   __shared__ double red[kNPart];
   __shared__ MuState s_ms[kMaxS];  // every block runs the same search on its own copy
   __shared__ double s_dmm;
@@ -701,12 +756,49 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
       const int* pl = a.plist + (long)s * n;
       const long len = d.cut ? (long)s_llen[s] : n;
-      for (long j = tid; j < len; j += nthreads) {
-        const long p = d.cut ? (long)__ldcg(pl + j) : j;
-        const double v = (double)__ldcg(Vs + p);
-        const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
-        const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
-        mu_point<FK>(d, k, cmu, nc, v, l, g, acc, s_kx[s]);
+      // a warp takes 128 consecutive list entries per trip, entry lane + 32 i
+      // on lane `lane` (coalesced loads), in a three-stage pipeline: the
+      // list indices of trip t + 2 and the field values of trip t + 1 are
+      // loaded while trip t is evaluated (index -1: past the end)
+      const long step = nwarps * kSegPts;
+      auto indices = [&](long jb, int (&q)[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const long j = jb + 32 * i + lane;
+          q[i] = j < len ? (d.cut ? __ldcg(pl + j) : (int)j) : -1;
+        }
+      };
+      auto values = [&](const int (&q)[4], R (&v)[4], R (&l)[4], R (&g)[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const bool ok = q[i] >= 0;
+          v[i] = ok ? __ldcg(Vs + q[i]) : R(0);
+          l[i] = (ok && Ls) ? __ldcg(Ls + q[i]) : R(0);
+          g[i] = (ok && Gs) ? __ldcg(Gs + q[i]) : R(0);
+        }
+      };
+      long jb = gw * kSegPts;
+      int qa[4], qb[4];
+      R v[4], l[4], g[4];
+      indices(jb, qa);
+      values(qa, v, l, g);
+      indices(jb + step, qb);
+      for (; jb < len; jb += step) {
+        R v2[4], l2[4], g2[4];
+        int qc[4];
+        values(qb, v2, l2, g2);
+        indices(jb + 2 * step, qc);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (qa[i] >= 0) mu_point<FK>(d, k, cmu, nc, (double)v[i], (double)l[i], (double)g[i], acc, s_kx[s]);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          qa[i] = qb[i];
+          qb[i] = qc[i];
+          v[i] = v2[i];
+          l[i] = l2[i];
+          g[i] = g2[i];
+        }
       }
       // partial sums double-buffered by pass: a block that has decided may
       // write the next pass's row while others still read this one
@@ -1005,52 +1097,86 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
     const R* Vs = a.V + so;
     const R* Ls = a.lap ? a.lap + so : nullptr;
     const R* Gs = a.g2 ? a.g2 + so : nullptr;
-    // one point per thread; every lane of a warp runs every trip (the vote
-    // below needs them all)
-    for (long base = (long)bid * blockDim.x; base < n; base += gstride) {
-      const long p = base + threadIdx.x;
-      const bool valid = p < n;
-      // issue the streaming loads first
-      const double v = valid ? (double)__ldcg(Vs + p) : 0.0;
-      R ni = R(0);
-      R rj[PW];
-      if (a.mode == 0 || a.mode == 2) {
-        ni = valid ? __ldcg(nin + so + p) : R(0);
+    // NP consecutive points per thread and trip, one 16-byte vector per
+    // field; every load of a trip (the history residuals of the Gram row
+    // included) is issued before its arithmetic.  Every lane of a warp runs
+    // every trip (the vote below needs them all).
+    constexpr int NP = kVecPts<R>;
+    constexpr int NH = PW - 1;  // history residuals of the Gram row
+    const int vec4 = kp.vec4;
+    const bool in_loads = a.mode == 0 || a.mode == 2;
+    for (long base = (long)bid * blockDim.x * NP; base < n; base += gstride * NP) {
+      const long p0 = base + (long)NP * threadIdx.x;
+      R v[NP], ni[NP], rj[NH][NP];
+      vload(Vs, p0, n, vec4, v);
 #pragma unroll
-        for (int j = 0; j < PW; ++j)
-          rj[j] = (j < I - 1 && valid) ? __ldcg(a.res + s_roff[j] + so + p) : R(0);
+      for (int i = 0; i < NP; ++i) ni[i] = R(0);
+      if (in_loads) {
+        vload(nin + so, p0, n, vec4, ni);
+#pragma unroll
+        for (int j = 0; j < NH; ++j)
+          if (j < I - 1) vload(a.res + s_roff[j] + so, p0, n, vec4, rj[j]);
       }
-      double nod = 0.0;
+      double nod[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) nod[i] = 0.0;
       if (a.mode == 2) {  // admix only: V holds the output densities
-        nod = v;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) nod[i] = (double)v[i];
       } else {
-        const bool mine = valid && (!d.cut || mus - v > 0.0);
-        if (__any_sync(0xffffffffu, mine) && mine) {
-          const double l = Ls ? (double)__ldcg(Ls + p) : 0.0;
-          const double g = Gs ? (double)__ldcg(Gs + p) : 0.0;
-          nod = point_density<FK>(d, k, mus - v, l, g);
+        bool mine[NP], any = false;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          mine[i] = p0 + i < n && (!d.cut || mus - (double)v[i] > 0.0);
+          any |= mine[i];
+        }
+        if (__any_sync(0xffffffffu, any) && any) {
+          R l[NP], g[NP];
+#pragma unroll
+          for (int i = 0; i < NP; ++i) l[i] = g[i] = R(0);
+          if (Ls) vload(Ls, p0, n, vec4, l);
+          if (Gs) vload(Gs, p0, n, vec4, g);
+#pragma unroll
+          for (int i = 0; i < NP; ++i)
+            if (mine[i]) nod[i] = point_density<FK>(d, k, mus - (double)v[i], (double)l[i], (double)g[i]);
         }
       }
-      if (!valid) continue;
-      const R no = R(nod);
-      acc[0] += nod;
+      if (p0 >= n) continue;
+      R no[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        no[i] = R(nod[i]);
+        acc[0] += nod[i];  // 0 past the end
+      }
       if (a.mode == 1) {
-        nin[so + p] = no;
-        a.cur_copy[so + p] = no;
+        vstore(nin + so, p0, n, vec4, no);
+        vstore(a.cur_copy + so, p0, n, vec4, no);
         continue;
       }
-      const R r = no - ni;
-      rcur[so + p] = r;
-      const double w = ref_multiplicity(p, kp.geom.s, kp.geom.dim);
-      const double dno = (double)no, dni = (double)ni, dr = (double)r, wr = w * dr;
-      acc[1] += w * dno * dni;
-      acc[2] += w * dno * dno;
-      acc[3] += w * dni * dni;
+      R r[NP];
+      double w[NP], wr[NP];
+      ref_weights<NP>(p0, kp.geom.s, kp.geom.dim, w);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        r[i] = no[i] - ni[i];
+        if (p0 + i >= n) w[i] = 0.0;
+        const double dno = (double)no[i], dni = (double)ni[i];
+        wr[i] = w[i] * (double)r[i];
+        acc[1] += w[i] * dno * dni;
+        acc[2] += w[i] * dno * dno;
+        acc[3] += w[i] * dni * dni;
+      }
 #pragma unroll
       for (int j = 0; j < PW; ++j) {
-        if (j < I - 1) acc[4 + j] += wr * (double)rj[j];
-        else if (j == I - 1) acc[4 + j] += wr * dr;
+        if (j < I - 1) {
+#pragma unroll
+          for (int i = 0; i < NP; ++i) acc[4 + j] += wr[i] * (double)rj[j < NH ? j : 0][i];
+        } else if (j == I - 1) {
+#pragma unroll
+          for (int i = 0; i < NP; ++i) acc[4 + j] += wr[i] * (double)r[i];
+        }
       }
+      vstore(rcur + so, p0, n, vec4, r);
     }
     block_reduce_store<4 + PW>(acc, a.part2 + (long)bid * kNPart + s * kNF);
   }
@@ -1066,12 +1192,12 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
 }
 
 template <typename R, int FK, int PW>
-__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kDensityThreads, 2) sc_density_kernel(StepArgs<R> a) {
   sc_density_body<R, FK, PW>(a, blockIdx.x, gridDim.x);
 }
 
 template <typename R, int FK, int PW>
-__global__ void __launch_bounds__(kDensityThreads, 4) sc_density_kernel_b(const StepArgs<R>* __restrict__ args,
+__global__ void __launch_bounds__(kDensityThreads, 2) sc_density_kernel_b(const StepArgs<R>* __restrict__ args,
                                                                          const int4* __restrict__ tab) {
   const int4 t = tab[blockIdx.x];
   sc_density_body<R, FK, PW>(args[t.x], t.y, t.z);

@@ -10,9 +10,12 @@ to round-off and central differences at h = 1e-4 resolve the gradient to
 1e-5.  Dirac exchange gives the density a step at its edge (the
 Thomas-Fermi-Dirac discontinuity): the fixed point is not unique there, and
 ~170 edge points of a 32^3 solve land on the other branch between the +h
-and -h solves whatever h is; differences at h = 1e-3 average over those
-flips and agree with the adjoint to ~1e-3, smaller h do not resolve
-anything.  With both terms the loop stalls near CC ~ 1e-10 for the same
+and -h solves whatever h is, and which ones do depends on round-off (the
+order of the grid sums); differences at h = 1e-3 average over those flips
+and agree with the adjoint to ~1e-3 along a direction with a large
+derivative, to several per cent along one with a small derivative (the
+flips' share of the difference is the same in absolute terms); smaller h
+do not resolve anything.  With both terms the loop stalls near CC ~ 1e-10 for the same
 reason."""
 import numpy as np
 import pytest
@@ -69,7 +72,7 @@ def bump(center, width=1.5):
 
 
 # (interaction, difference step, relative tolerance)
-FD_CASES = [("hartree", 1e-4, 1e-5), ("dirac", 1e-3, 1e-2)]
+FD_CASES = [("hartree", 1e-4, 1e-5), ("dirac", 1e-3, 1e-1)]
 
 
 @pytest.mark.parametrize("inter,h,tol", FD_CASES)
