@@ -426,6 +426,53 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
   }
 }
 
+// mu_point for the NPT points of a lane's trip (ok[i]: point i exists):
+// the candidate loop is the outer one, so the points' evaluations are NPT
+// independent chains.
+template <int FK, int NPT, typename R>
+__device__ __forceinline__ void mu_points(const DensParams& d, const EvalK& k, const double* cmu, int nc,
+                                          const R (&vr)[NPT], const R (&lr)[NPT], const R (&gr)[NPT],
+                                          const bool (&ok)[NPT], double (&acc)[kMuAcc], const double* kx) {
+  if constexpr (FK == 1 || FK == 2) {
+    double v[NPT], A[NPT], B[NPT];
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+      v[i] = (double)vr[i];
+      A[i] = k.cg * (double)lr[i];
+      B[i] = k.cg2 * (double)gr[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+      double n0, sl;
+      if constexpr (FK == 1) {
+        n0 = grad3_n_slope(k, cmu[0] - v[i], A[i], B[i], sl);
+      } else {
+        n0 = tf3_n(k, cmu[0] - v[i]);
+        sl = tf3_slope(k, cmu[0] - v[i]);
+      }
+      acc[0] += ok[i] ? n0 : 0.0;
+      acc[kMuCand] += ok[i] ? sl : 0.0;
+    }
+#pragma unroll
+    for (int c = 1; c < kMuCand; ++c) {
+      if (c >= nc) break;
+      double t = 0.0;
+#pragma unroll
+      for (int i = 0; i < NPT; ++i) {
+        double x;
+        if constexpr (FK == 1) x = grad3_n(k, cmu[c] - v[i], A[i], B[i]);
+        else x = tf3_n(k, cmu[c] - v[i]);
+        t += ok[i] ? x : 0.0;
+      }
+      acc[c] += t;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NPT; ++i)
+      if (ok[i]) mu_point<FK>(d, k, cmu, nc, (double)vr[i], (double)lr[i], (double)gr[i], acc, kx);
+  }
+}
+
 // Sum of nb per-block partials (at base + b * stride) on one warp, several
 // loads in flight per lane.
 __device__ __forceinline__ double warp_sum_rows(const double* base, int nb, int stride) {
@@ -756,43 +803,47 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
       const int* pl = a.plist + (long)s * n;
       const long len = d.cut ? (long)s_llen[s] : n;
-      // a warp takes 128 consecutive list entries per trip, entry lane + 32 i
-      // on lane `lane` (coalesced loads), in a three-stage pipeline: the
-      // list indices of trip t + 2 and the field values of trip t + 1 are
-      // loaded while trip t is evaluated (index -1: past the end)
-      const long step = nwarps * kSegPts;
-      auto indices = [&](long jb, int (&q)[4]) {
+      // a warp takes 32 NPT consecutive list entries per trip, entry
+      // lane + 32 i on lane `lane` (coalesced loads), in a three-stage
+      // pipeline: the list indices of trip t + 2 and the field values of
+      // trip t + 1 are loaded while trip t is evaluated (index -1: past the
+      // end).  NPT = 4 points per lane for FP32 fields, 2 for FP64 (the
+      // registers of two stages of values).
+      constexpr int NPT = sizeof(R) == sizeof(float) ? 4 : 2;
+      const long step = nwarps * 32 * NPT;
+      auto indices = [&](long jb, int (&q)[NPT]) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < NPT; ++i) {
           const long j = jb + 32 * i + lane;
           q[i] = j < len ? (d.cut ? __ldcg(pl + j) : (int)j) : -1;
         }
       };
-      auto values = [&](const int (&q)[4], R (&v)[4], R (&l)[4], R (&g)[4]) {
+      auto values = [&](const int (&q)[NPT], R (&v)[NPT], R (&l)[NPT], R (&g)[NPT]) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < NPT; ++i) {
           const bool ok = q[i] >= 0;
           v[i] = ok ? __ldcg(Vs + q[i]) : R(0);
           l[i] = (ok && Ls) ? __ldcg(Ls + q[i]) : R(0);
           g[i] = (ok && Gs) ? __ldcg(Gs + q[i]) : R(0);
         }
       };
-      long jb = gw * kSegPts;
-      int qa[4], qb[4];
-      R v[4], l[4], g[4];
+      long jb = gw * 32 * NPT;
+      int qa[NPT], qb[NPT];
+      R v[NPT], l[NPT], g[NPT];
       indices(jb, qa);
       values(qa, v, l, g);
       indices(jb + step, qb);
       for (; jb < len; jb += step) {
-        R v2[4], l2[4], g2[4];
-        int qc[4];
+        R v2[NPT], l2[NPT], g2[NPT];
+        int qc[NPT];
         values(qb, v2, l2, g2);
         indices(jb + 2 * step, qc);
+        bool ok[NPT];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (qa[i] >= 0) mu_point<FK>(d, k, cmu, nc, (double)v[i], (double)l[i], (double)g[i], acc, s_kx[s]);
+        for (int i = 0; i < NPT; ++i) ok[i] = qa[i] >= 0;
+        mu_points<FK, NPT>(d, k, cmu, nc, v, l, g, ok, acc, s_kx[s]);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < NPT; ++i) {
           qa[i] = qb[i];
           qb[i] = qc[i];
           v[i] = v2[i];
