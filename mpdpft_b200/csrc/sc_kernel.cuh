@@ -751,6 +751,10 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
           if (b < (int)bid) before += c;
         }
         block_sum2(before, total);
+        if (2L * total > n) {  // most points active: the pass sweeps the whole grid
+          if (threadIdx.x == 0) s_llen[s] = -1;
+          continue;
+        }
         int off = before;
         for (int w = 0; w < wib; ++w) off += s_wcnt[s][w];
         const R* Vs = V + (long)s * n;
@@ -779,12 +783,17 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         if (threadIdx.x == 0) s_llen[s] = total;
       }
       __syncthreads();
+      // (the same decisions in every block: `total` sums the same counts)
+      int written = 0;
+      for (int s = 0; s < S; ++s) written |= s_need[s] && s_llen[s] >= 0;
+      __syncthreads();
       if (threadIdx.x < S && s_need[threadIdx.x]) {
-        s_lok[threadIdx.x] = 1;
-        s_lcap[threadIdx.x] = s_cap[threadIdx.x];
-        s_need[threadIdx.x] = 0;
+        const int s = threadIdx.x;
+        s_lok[s] = 1;
+        s_lcap[s] = s_llen[s] >= 0 ? s_cap[s] : 1e300;  // no rebuild after a whole-grid decision
+        s_need[s] = 0;
       }
-      if (!grid_barrier(st, nblk)) return;  // the lists are complete
+      if (written && !grid_barrier(st, nblk)) return;  // the lists are complete
     }
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
@@ -802,7 +811,8 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
       const int* pl = a.plist + (long)s * n;
-      const long len = d.cut ? (long)s_llen[s] : n;
+      const bool listed = d.cut && s_llen[s] >= 0;  // s_llen < 0: the whole grid
+      const long len = listed ? (long)s_llen[s] : n;
       // a warp takes 32 NPT consecutive list entries per trip, entry
       // lane + 32 i on lane `lane` (coalesced loads), in a three-stage
       // pipeline: the list indices of trip t + 2 and the field values of
@@ -815,7 +825,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
 #pragma unroll
         for (int i = 0; i < NPT; ++i) {
           const long j = jb + 32 * i + lane;
-          q[i] = j < len ? (d.cut ? __ldcg(pl + j) : (int)j) : -1;
+          q[i] = j < len ? (listed ? __ldcg(pl + j) : (int)j) : -1;
         }
       };
       auto values = [&](const int (&q)[NPT], R (&v)[NPT], R (&l)[NPT], R (&g)[NPT]) {
