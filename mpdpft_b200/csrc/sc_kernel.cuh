@@ -1168,10 +1168,14 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
     const bool in_loads = a.mode == 0 || a.mode == 2;
     for (long base = (long)bid * blockDim.x * NP; base < n; base += gstride * NP) {
       const long p0 = base + (long)NP * threadIdx.x;
-      R v[NP], ni[NP], rj[NH][NP];
+      R v[NP], ni[NP], rj[NH][NP], l[NP], g[NP];
       vload(Vs, p0, n, vec4, v);
 #pragma unroll
-      for (int i = 0; i < NP; ++i) ni[i] = R(0);
+      for (int i = 0; i < NP; ++i) ni[i] = l[i] = g[i] = R(0);
+      if (a.mode != 2) {
+        if (Ls) vload(Ls, p0, n, vec4, l);
+        if (Gs) vload(Gs, p0, n, vec4, g);
+      }
       if (in_loads) {
         vload(nin + so, p0, n, vec4, ni);
 #pragma unroll
@@ -1192,14 +1196,17 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
           any |= mine[i];
         }
         if (__any_sync(0xffffffffu, any) && any) {
-          R l[NP], g[NP];
+          if constexpr (FK != 0) {  // branch-free forms: the points are independent chains
 #pragma unroll
-          for (int i = 0; i < NP; ++i) l[i] = g[i] = R(0);
-          if (Ls) vload(Ls, p0, n, vec4, l);
-          if (Gs) vload(Gs, p0, n, vec4, g);
+            for (int i = 0; i < NP; ++i) {
+              const double x = point_density<FK>(d, k, mus - (double)v[i], (double)l[i], (double)g[i]);
+              nod[i] = mine[i] ? x : 0.0;
+            }
+          } else {
 #pragma unroll
-          for (int i = 0; i < NP; ++i)
-            if (mine[i]) nod[i] = point_density<FK>(d, k, mus - (double)v[i], (double)l[i], (double)g[i]);
+            for (int i = 0; i < NP; ++i)
+              if (mine[i]) nod[i] = point_density<FK>(d, k, mus - (double)v[i], (double)l[i], (double)g[i]);
+          }
         }
       }
       if (p0 >= n) continue;
