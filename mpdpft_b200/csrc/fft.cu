@@ -784,35 +784,72 @@ __device__ __forceinline__ void assemble_v_body(const KParams& kp, const ScState
   const R* nin = nin_ring + (long)cur * S * n;
   double acc[kMaxS], vm[kMaxS];
   for (int s = 0; s < kMaxS; ++s) { acc[s] = 0.0; vm[s] = -1.0e300; }
-  for (long p = blk * blockDim.x + threadIdx.x; p < n; p += nblk * blockDim.x) {
-    double x, y, z;
-    point_coords(p, kp.geom, x, y, z);
-    const bool shell = in_shell(x * x + y * y + z * z, shell_r, shell_w);
+  // one 16-byte vector per field and thread per trip (NP points), every
+  // load of a species issued before its arithmetic
+  constexpr int NP = kVecPts<R>;
+  const int vec = kp.vec4;
+  for (long p0 = (blk * blockDim.x + threadIdx.x) * NP; p0 < n; p0 += nblk * blockDim.x * NP) {
+    bool shell[NP];
+#pragma unroll
+    for (int t = 0; t < NP; ++t) {
+      double x, y, z;
+      point_coords(p0 + t, kp.geom, x, y, z);
+      shell[t] = p0 + t < n && in_shell(x * x + y * y + z * z, shell_r, shell_w);
+    }
     for (int s = 0; s < S; ++s) {
-      R vnew;
+      R vnew[NP];
       if (update) {
-        R vi = vh ? vh[(long)s * n + p] : R(0);
-        if (kp.contact_self) vi += R(2.0 * kp.beta) * nin[p];
-        if (kp.contact_mutual) {
-          R t = R(0);
-          for (int q = 0; q < S; ++q)
-            if (q != s) t += nin[(long)q * n + p];
-          vi += R(kp.beta) * t;
+        R vi[NP], ve[NP], vo[NP];
+#pragma unroll
+        for (int t = 0; t < NP; ++t) vi[t] = R(0);
+        if (vh) vload(vh + (long)s * n, p0, n, vec, vi);
+        vload(vext + (long)s * n, p0, n, vec, ve);
+        vload(V + (long)s * n, p0, n, vec, vo);
+        if (kp.contact_self) {  // type 10 (:2261)
+          R a[NP];
+          vload(nin, p0, n, vec, a);
+#pragma unroll
+          for (int t = 0; t < NP; ++t) vi[t] += R(2.0 * kp.beta) * a[t];
         }
-        if (kp.dirac) {
-          R ns = nin[(long)s * n + p];
-          ns = ns > R(0) ? ns : R(0);
-          if (kp.geom.dim == 3) vi += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
-          else vi += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+        if (kp.contact_mutual) {  // type 1 (:2247)
+          R tsum[NP];
+#pragma unroll
+          for (int t = 0; t < NP; ++t) tsum[t] = R(0);
+          for (int q = 0; q < S; ++q) {
+            if (q == s) continue;
+            R a[NP];
+            vload(nin + (long)q * n, p0, n, vec, a);
+#pragma unroll
+            for (int t = 0; t < NP; ++t) tsum[t] += a[t];
+          }
+#pragma unroll
+          for (int t = 0; t < NP; ++t) vi[t] += R(kp.beta) * tsum[t];
         }
-        vnew = vext[(long)s * n + p] + R(fac) * vi;
-        double d = (double)vnew - (double)V[(long)s * n + p];
-        acc[s] += d * d;
-        V[(long)s * n + p] = vnew;
+        if (kp.dirac) {  // type 11 (:2768)
+          R a[NP];
+          vload(nin + (long)s * n, p0, n, vec, a);
+#pragma unroll
+          for (int t = 0; t < NP; ++t) {
+            const R ns = a[t] > R(0) ? a[t] : R(0);
+            if (kp.geom.dim == 3) vi[t] += R(-kp.gamma_h) * cbrt(R(3.0 / kPi) * ns);
+            else vi[t] += R(-2.0 * kp.gamma_h) * sqrt(R(2.0 / kPi) * ns);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < NP; ++t) {
+          vnew[t] = ve[t] + R(fac) * vi[t];
+          const double d = (double)vnew[t] - (double)vo[t];
+          acc[s] += p0 + t < n ? d * d : 0.0;
+        }
+        vstore(V + (long)s * n, p0, n, vec, vnew);
       } else {
-        vnew = V[(long)s * n + p];
+        vload(V + (long)s * n, p0, n, vec, vnew);
       }
-      if (s < nmax && shell) vm[s] = fmax(vm[s], (double)vnew);
+      if (s < nmax) {
+#pragma unroll
+        for (int t = 0; t < NP; ++t)
+          if (shell[t]) vm[s] = fmax(vm[s], (double)vnew[t]);
+      }
     }
   }
   if (update) block_reduce_store<kMaxS>(acc, vres_part + blk * kMaxS);

@@ -173,42 +173,6 @@ __device__ __forceinline__ void ref_weights(long p0, int s, int dim, double (&w)
   }
 }
 
-// One 16-byte vector of a field per thread: NP = 16 / sizeof(R) values at
-// p0 (a multiple of NP); scalar accesses at the ragged end or when the
-// field length is not a multiple of 4 (vec = 0).
-template <typename R>
-constexpr int kVecPts = 16 / (int)sizeof(R);
-
-template <typename R>
-__device__ __forceinline__ void vload(const R* f, long p0, long n, int vec, R (&o)[kVecPts<R>]) {
-  constexpr int NP = kVecPts<R>;
-  if (vec && p0 + NP - 1 < n) {
-    if constexpr (NP == 4) {
-      const float4 t = __ldcg(reinterpret_cast<const float4*>(f + p0));
-      o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-    } else {
-      const double2 t = __ldcg(reinterpret_cast<const double2*>(f + p0));
-      o[0] = t.x; o[1] = t.y;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < NP; ++i) o[i] = (p0 + i < n) ? __ldcg(f + p0 + i) : R(0);
-  }
-}
-
-template <typename R>
-__device__ __forceinline__ void vstore(R* f, long p0, long n, int vec, const R (&o)[kVecPts<R>]) {
-  constexpr int NP = kVecPts<R>;
-  if (vec && p0 + NP - 1 < n) {
-    if constexpr (NP == 4) *reinterpret_cast<float4*>(f + p0) = make_float4(o[0], o[1], o[2], o[3]);
-    else *reinterpret_cast<double2*>(f + p0) = make_double2(o[0], o[1]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < NP; ++i)
-      if (p0 + i < n) f[p0 + i] = o[i];
-  }
-}
-
 // ------------------------------------------------------- point evaluation --
 // Constants of the branch-free forms (fast = 1: 3D gradient-corrected,
 // fast = 2: 3D TF, 0: the general density_at_d / density_slope_d).
