@@ -881,10 +881,15 @@ __global__ void k_assemble_v(KParams kp, const ScState* st, const R* vext, const
 template <typename R>
 __global__ void k_shell_max(Geom g, const R* f, unsigned long long* vmax, double shell_r, double shell_w) {
   double vm = -1.0e300;
-  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += (long)gridDim.x * blockDim.x) {
-    double x, y, z;
-    point_coords(p, g, x, y, z);
-    if (in_shell(x * x + y * y + z * z, shell_r, shell_w)) vm = fmax(vm, (double)f[p]);
+  // four points per thread and trip; a value is read only inside the shell
+  for (long p0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4; p0 < g.n; p0 += (long)gridDim.x * blockDim.x * 4) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const long p = p0 + t;
+      double x, y, z;
+      point_coords(p, g, x, y, z);
+      if (p < g.n && in_shell(x * x + y * y + z * z, shell_r, shell_w)) vm = fmax(vm, (double)f[p]);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
   if ((threadIdx.x & 31) == 0 && vm > -1.0e300) atomicMax(vmax, ordered_bits(vm));
@@ -926,8 +931,17 @@ __global__ void k_scale_copy(const R* src, R* dst, long n, double a) {
 
 template <typename R>
 __global__ void k_axpy(const R* x, R* y, long n, double a, int accumulate) {
-  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x)
-    y[p] = accumulate ? R((double)y[p] + a * (double)x[p]) : R(a * (double)x[p]);
+  constexpr int NP = kVecPts<R>;
+  const int vec = (n % 4) == 0;
+  for (long p0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * NP; p0 < n; p0 += (long)gridDim.x * blockDim.x * NP) {
+    R xv[NP], yv[NP];
+    vload(x, p0, n, vec, xv);
+    if (accumulate) vload(y, p0, n, vec, yv);
+#pragma unroll
+    for (int t = 0; t < NP; ++t)
+      yv[t] = accumulate ? R((double)yv[t] + a * (double)xv[t]) : R(a * (double)xv[t]);
+    vstore(y, p0, n, vec, yv);
+  }
 }
 
 #include "fft_plane.cuh"
