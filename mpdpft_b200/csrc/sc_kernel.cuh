@@ -635,14 +635,9 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
     }
   }
   if (threadIdx.x < kMaxS) {
-    // a species whose earlier list build found most of the grid active
-    // sweeps the whole grid without counting again
-    const int t = threadIdx.x;
-    const int dense = t < S && kp.dens[t].cut && ldcg(&st->dense[t]);
-    s_need[t] = 0;
-    s_lok[t] = dense;
-    s_llen[t] = dense ? -1 : 0;
-    s_lcap[t] = 1e300;
+    s_need[threadIdx.x] = 0;
+    s_lok[threadIdx.x] = 0;
+    s_llen[threadIdx.x] = 0;
   }
   __syncthreads();
   if (bid == 0 && threadIdx.x == 0) {
@@ -721,10 +716,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         }
         block_sum2(before, total);
         if (2L * total > n) {  // most points active: the pass sweeps the whole grid
-          if (threadIdx.x == 0) {
-            s_llen[s] = -1;
-            if (bid == 0) ls->dense[s] = 1;  // and so do the later iterations
-          }
+          if (threadIdx.x == 0) s_llen[s] = -1;
           continue;
         }
         int off = before;

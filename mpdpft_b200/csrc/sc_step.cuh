@@ -84,7 +84,6 @@ struct ScState {
   int mu_passes;
   int mu_passes_total;
   MuState ms[kMaxS];
-  int dense[kMaxS];  // 1: an earlier list build of species s found most of the grid active
   unsigned bar_count, bar_gen;
   int abort;
   // not part of the state copies (written by one kernel, read by the next)
