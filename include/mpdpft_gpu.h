@@ -182,6 +182,17 @@ int mpdpft_ctx_sync(mpdpft_ctx* ctx);
 /* The context's cudaStream_t, as an opaque pointer. */
 void* mpdpft_ctx_stream(mpdpft_ctx* ctx);
 
+/* Limits of the device loops of this context (the reference bounds its mu
+ * search by 20 bracket steps and DeltamuModifier, mpDPFT.cpp:4584-4711, and
+ * has no device waits): mu_max_passes caps the evaluation passes of one mu
+ * search (1 .. 24, default 24; reaching it raises MPDPFT_ERR_TIMEOUT with
+ * the best mu found), barrier_spin_limit bounds each wait of the mu
+ * kernel's grid barriers (polls with a 64 ns back-off, default 2e7; running
+ * out aborts the kernel and raises MPDPFT_ERR_TIMEOUT).  Negative values
+ * restore the defaults.  The context stays usable after a timeout: the
+ * next mpdpft_sc_init, mpdpft_mu_search or mpdpft_pulay_reset clears it. */
+int mpdpft_set_limits(mpdpft_ctx* ctx, int mu_max_passes, long long barrier_spin_limit);
+
 /* External potential V_ext of species s.  Replaces GetEnv (mpDPFT.cpp:1385). */
 int mpdpft_set_external_potential(mpdpft_ctx* ctx, int s, const double* v_ext,
                                   int layout, int mem);
@@ -226,7 +237,9 @@ int mpdpft_delfield(mpdpft_ctx* ctx, const double* f, double* grad2_out,
 int mpdpft_fft(mpdpft_ctx* ctx, int sign, const double* in, double* out, int mem);
 
 /* Trapezoid integral over the box.  Replaces Integrate(method 1)
- * (Riemann, mpDPFT.cpp:7981-8026). */
+ * (Riemann, mpDPFT.cpp:7981-8026).  In the reference layout every stored
+ * point counts with Riemann's end weights (1/2 on the first and last plane
+ * of each axis); in the periodic layout every point has weight 1. */
 int mpdpft_integrate(mpdpft_ctx* ctx, const double* f, double* out, int layout, int mem);
 
 /* The same trapezoid integral without a context and without allocating any
@@ -234,16 +247,21 @@ int mpdpft_integrate(mpdpft_ctx* ctx, const double* f, double* out, int layout, 
  * callers that cannot call cudaMalloc, e.g. a plug-in whose host application
  * owns all device memory, or a loop that must not pay cudaMalloc's implicit
  * device synchronisation.
- *   f      device pointer, double, periodic s^D or reference (s+1)^D layout;
+ *   f      device pointer, double, periodic s^D or reference (s+1)^D layout
+ *          (reference layout: every stored point with the trapezoid end
+ *          weights 1/2, as Riemann does; the duplicate planes need not
+ *          repeat plane 0);
  *   out    device pointer to one double, written with the integral;
  *   stream cudaStream_t (NULL: the default stream) on the current device.
- * Grids of more than MPDPFT_NOALLOC_MAX_POINTS points (s > 256 in 3D,
- * s > 4096 in 2D) are rejected with MPDPFT_ERR_ARG.  The partial sums live in
- * one fixed 32 KiB array per GPU, kept from library load to process exit and
- * shared by all calls: calls whose kernels overlap on one GPU (other streams,
- * other host threads) race on it and must be serialised by the caller.  The
- * first call on each device looks up that array's device address, so make it
- * before any stream capture.  Returns once the work is queued on stream. */
+ * Grids of more than MPDPFT_NOALLOC_MAX_POINTS periodic points (s > 256 in
+ * 3D, s > 4096 in 2D) are rejected with MPDPFT_ERR_ARG.  The partial sums
+ * live in one fixed array of 33160 bytes that every GPU loading this library
+ * holds until the process exits, shared by all calls: calls whose kernels
+ * overlap on one GPU (other streams, other host threads) race on it and must
+ * be serialised by the caller.  The array's device address belongs to the
+ * CUDA context: the first call in each context (and the first after a
+ * device reset) looks it up, so make that call before any stream capture.
+ * Returns once the work is queued on stream. */
 int mpdpft_integrate_noalloc(int dim, int steps, double edge, const double* f, double* out, int layout,
                              void* stream);
 

@@ -109,6 +109,11 @@ int mpdpft_ctx_sync(mpdpft_ctx* ctx) {
 
 void* mpdpft_ctx_stream(mpdpft_ctx* ctx) { return ctx ? (void*)ctx->impl.stream : nullptr; }
 
+int mpdpft_set_limits(mpdpft_ctx* ctx, int mu_max_passes, long long barrier_spin_limit) {
+  CHECK_CTX(ctx);
+  return ctx->impl.set_limits(mu_max_passes, barrier_spin_limit);
+}
+
 int mpdpft_set_external_potential(mpdpft_ctx* ctx, int s, const double* v_ext, int layout, int mem) {
   CHECK_CTX(ctx);
   Ctx& c = ctx->impl;

@@ -88,6 +88,22 @@ __device__ __forceinline__ void vstore(R* f, long p0, long n, int vec, const R (
   }
 }
 
+// Trapezoid weight of point q of the reference's (s+1)^D storage (el = s + 1
+// points per axis): 1/2 on the first and the last plane of every axis, as in
+// Riemann (mpDPFT.cpp:7981-8026).  Indices fit 32 bits (el <= 1025 in 3D).
+__device__ __forceinline__ double riemann_weight(unsigned q, unsigned el, int dim) {
+  const unsigned t = q / el, k = q - t * el;
+  double w = (k == 0 || k == el - 1) ? 0.5 : 1.0;
+  if (dim == 3) {
+    const unsigned i = t / el, j = t - i * el;
+    w *= (j == 0 || j == el - 1) ? 0.5 : 1.0;
+    w *= (i == 0 || i == el - 1) ? 0.5 : 1.0;
+  } else {
+    w *= (t == 0 || t == el - 1) ? 0.5 : 1.0;
+  }
+  return w;
+}
+
 __device__ __forceinline__ void point_coords(long p, const Geom& g, double& x, double& y, double& z) {
   const unsigned us = (unsigned)g.s, pp = (unsigned)p;
   const unsigned q = pp / us, k = pp - q * us;

@@ -126,6 +126,18 @@ __global__ void k_integrate(Geom g, const R* f, double* part) {
   block_reduce_store<1>(acc, part + blockIdx.x);
 }
 
+// Trapezoid sum over the reference's (s+1)^D storage with its end weights
+// (Riemann, mpDPFT.cpp:7981-8026); the duplicate planes need not repeat
+// plane 0.
+__global__ void k_integrate_ref(Geom g, const double* f, double* part) {
+  const unsigned el = (unsigned)g.s + 1;
+  const unsigned total = g.dim == 3 ? el * el * el : el * el;
+  double acc[1] = {0.0};
+  for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
+    acc[0] += riemann_weight(q, el, g.dim) * f[q];
+  block_reduce_store<1>(acc, part + blockIdx.x);
+}
+
 // n[V] at a fixed mu (GetDensity), no reduction.
 template <typename R>
 __global__ void k_density(Geom g, DensParams d, double mu, const R* V, const R* lap, const R* g2, R* out) {
@@ -242,7 +254,22 @@ KParams Ctx::kparams() const {
   k.chunk = chunk;
   k.mu_blocks = step_blocks;
   k.vec4 = (geom.n % 4) == 0;
+  k.mu_max_passes = mu_max_passes;
+  k.spin_limit = spin_limit;
   return k;
+}
+
+// Device loop limits of this context: the mu-search pass cap and the grid
+// barrier's spin limit (negative: the defaults).  The captured iteration
+// carries the old values, so it is rebuilt on the next graph step.
+int Ctx::set_limits(int mu_passes, long long spins) {
+  if (mu_passes > kMuMaxPasses) return set_error(MPDPFT_ERR_ARG, "mu pass cap above the device maximum");
+  if (mu_passes == 0) return set_error(MPDPFT_ERR_ARG, "mu pass cap must be at least 1");
+  mu_max_passes = mu_passes < 0 ? kMuMaxPasses : mu_passes;
+  spin_limit = spins < 0 ? kBarrierSpinLimit : (long)spins;
+  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  return MPDPFT_OK;
 }
 
 int Ctx::init(const mpdpft_params& params, int dev) {
@@ -757,6 +784,26 @@ int Ctx::integrate_device(const void* f, double* out) {
 
 int Ctx::op_integrate(const double* f, double* out, int layout, int mem) {
   int st;
+  if (!f) return set_error(MPDPFT_ERR_ARG, "null input array");
+  if (layout == MPDPFT_LAYOUT_REFERENCE) {
+    // every stored point with the reference's weights, duplicate planes included
+    const double* src = f;
+    if (mem == MPDPFT_MEM_HOST) {
+      std::memcpy(host_stage(0), f, sizeof(double) * n_ref);
+      CU(cudaMemcpyAsync(d_io, host_stage(0), sizeof(double) * n_ref, cudaMemcpyHostToDevice, stream));
+      src = d_io;
+    }
+    const int blocks = grid_blocks(n_ref);
+    k_integrate_ref<<<blocks, kThreads, 0, stream>>>(geom, src, d_part);
+    CU(cudaGetLastError());
+    std::vector<double> hp(blocks);
+    CU(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * blocks, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    double t = 0.0;
+    for (double x : hp) t += x;
+    *out = t * geom.dvol;
+    return MPDPFT_OK;
+  }
   if ((st = import_field(f, d_tmp, layout, mem))) return st;
   return integrate_device(d_tmp, out);
 }

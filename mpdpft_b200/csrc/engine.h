@@ -74,6 +74,8 @@ struct Ctx {
   cudaGraphExec_t graph_exec = nullptr;
   FftPlan* fft = nullptr;
   Adjoint* adj = nullptr;  // adjoint work fields (allocated on first use)
+  int mu_max_passes = kMuMaxPasses;     // device loop limits (mpdpft_set_limits)
+  long spin_limit = kBarrierSpinLimit;
   int cnt[6] = {0, 0, 0, 0, 0, 0};       // launches issued, by stage
   int iter_cnt[6] = {0, 0, 0, 0, 0, 0};  // launches in the captured iteration
 
@@ -84,6 +86,7 @@ struct Ctx {
   int reset_state(bool sync = true);
   int read_state(ScState* h);
   int status_from_state(const ScState& h);
+  int set_limits(int mu_passes, long long spins);
   bool has_interaction(int t) const;
   KParams kparams() const;
   int import_field(const double* src, void* dst, int layout, int mem, int slot = 0, bool sync = true);
@@ -127,7 +130,6 @@ struct Ctx {
   int copy_current_density();
   int pointwise_vint(int type, int s, void* out);
   int full_c2c(void* buf, int sign);
-  int alloc_io(long doubles);
   int profile_stage(int stage, int reps, double* ms, double* bytes);
   // linear spectral operators and the Hartree operator of one field (fft.cu)
   int spectral(const void* in, int kind, int j, void* out, double coef);

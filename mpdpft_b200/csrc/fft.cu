@@ -1777,8 +1777,7 @@ int Ctx::op_fft(int sign, const double* in, double* out, int mem) {
   double* din = d_io;
   double* dout = d_io;
   std::vector<double> stage;
-  if (mem == MPDPFT_MEM_HOST) {
-    if ((st = alloc_io(2 * n))) return st;
+  if (mem == MPDPFT_MEM_HOST) {  // d_io holds 2 * max(n_ref, n) doubles: one complex field
     CU(cudaMemcpyAsync(d_io, in, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, stream));
   } else {
     din = (double*)in;
@@ -1959,11 +1958,6 @@ static int profile_impl(Ctx& c, int stage, int reps, double* ms, double* bytes) 
 int Ctx::profile_stage(int stage, int reps, double* ms, double* bytes) {
   return rsize == sizeof(double) ? profile_impl<double>(*this, stage, reps, ms, bytes)
                                  : profile_impl<float>(*this, stage, reps, ms, bytes);
-}
-
-int Ctx::alloc_io(long doubles) {
-  (void)doubles;  // d_io holds 2 * max(n_ref, n) doubles, enough for one complex field
-  return MPDPFT_OK;
 }
 
 // ================================================================ batches ==

@@ -8,7 +8,9 @@
 // passes the field and the result slot (both device memory), and the per-tile
 // partial sums live in the file-scope array below, which every GPU that loads
 // this library holds until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <mutex>
 #include <string>
@@ -20,35 +22,32 @@ namespace mpdpft {
 
 int set_error(int status, const std::string& msg);
 
-// One block sums one tile of kTile consecutive grid points; the tile count
+// One block sums one tile of kTile consecutive stored points; the tile count
 // (and so the summation order) depends only on the grid, never on the GPU.
 constexpr int kNoAllocThreads = 256;
 constexpr int kNoAllocTile = kNoAllocThreads * 16;  // 4096 points per tile
-constexpr int kNoAllocMaxTiles = MPDPFT_NOALLOC_MAX_POINTS / kNoAllocTile;
-static_assert(MPDPFT_NOALLOC_MAX_POINTS % kNoAllocTile == 0, "whole tiles");
+// The largest accepted grids are s = 256 in 3D and s = 4096 in 2D; in the
+// reference layout they store (s+1)^D points, 257^3 = 16974593 at most.
+constexpr long kNoAllocMaxStored = 257L * 257L * 257L;
+constexpr int kNoAllocMaxTiles = (int)((kNoAllocMaxStored + kNoAllocTile - 1) / kNoAllocTile);  // 4145
+static_assert(4097L * 4097L <= kNoAllocMaxStored, "2D reference grids fit the scratch");
 
-// The scratch: one partial sum per tile (32 KiB).  Every call writes the
+// The scratch: one partial sum per tile (33160 bytes).  Every call writes the
 // partials it later reads, so nothing has to be cleared between calls.
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxTiles];
 
-// Periodic point p -> its index in the caller's layout.
-__device__ __forceinline__ long noalloc_index(long p, int dim, int s, int layout) {
-  if (layout != MPDPFT_LAYOUT_REFERENCE) return p;
-  const long el = s + 1;
-  const int k = (int)(p % s);
-  const long t = p / s;
-  if (dim == 3) return ((t / s) * el + (t % s)) * el + k;
-  return t * el + k;
-}
-
-__global__ void __launch_bounds__(kNoAllocThreads) k_noalloc_tiles(const double* __restrict__ f, long n, int dim,
-                                                                    int s, int layout, double* partials) {
+// Sum of tile blockIdx.x: periodic layout, every point weight 1; reference
+// layout, the trapezoid end weights 1/2 per axis (Riemann,
+// mpDPFT.cpp:7981-8026), so the duplicate planes count as stored.
+__global__ void __launch_bounds__(kNoAllocThreads) k_noalloc_tiles(const double* __restrict__ f, unsigned total,
+                                                                    int dim, unsigned el, int layout,
+                                                                    double* partials) {
   __shared__ double sh[kNoAllocThreads];
-  const long base = (long)blockIdx.x * kNoAllocTile;
+  const unsigned base = blockIdx.x * (unsigned)kNoAllocTile;
   double t = 0.0;
   for (int i = threadIdx.x; i < kNoAllocTile; i += kNoAllocThreads) {
-    const long p = base + i;
-    if (p < n) t += f[noalloc_index(p, dim, s, layout)];
+    const unsigned q = base + i;
+    if (q < total) t += (layout == MPDPFT_LAYOUT_REFERENCE ? riemann_weight(q, el, dim) : 1.0) * f[q];
   }
   sh[threadIdx.x] = t;
   __syncthreads();
@@ -73,24 +72,73 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_noalloc_finish(const double
   if (threadIdx.x == 0) *out = sh[0] * dvol;
 }
 
-// Device address of the scratch, looked up once per device (the symbol's
-// name in host code is only a stand-in, not a device pointer).
+// Device address of the scratch.  The symbol's name in host code is only a
+// stand-in, and its device address belongs to a CUDA context, not to a
+// device ordinal: a caller may make its own driver context current, and a
+// device reset replaces the primary context.  So the address is looked up
+// once per context, keyed by the context's process-unique id (cuCtxGetId,
+// reached through the runtime's driver entry points so that the library
+// does not link the driver).
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
+constexpr int kNoAllocCache = 32;
 std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct NoAllocEntry {
+  unsigned long long ctx_id;
+  double* ptr;
+};
+NoAllocEntry g_noalloc_cache[kNoAllocCache] = {};
+int g_noalloc_next = 0;
+PFN_cuCtxGetCurrent_v4000 g_ctx_get_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_get_id = nullptr;
 
-int noalloc_scratch(int dev, double** out) {
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(MPDPFT_ERR_ARG, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (e != cudaSuccess)
-      return set_error(MPDPFT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
+int current_context_id(unsigned long long* id, bool* have) {
+  *have = false;
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return set_error(MPDPFT_ERR_CUDA, "cuCtxGetCurrent/cuCtxGetId not available from the driver");
+    g_ctx_get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    g_ctx_get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
   }
-  *out = g_noalloc_ptr[dev];
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS)
+    return set_error(MPDPFT_ERR_CUDA, "cuCtxGetCurrent failed");
+  if (!ctx) return MPDPFT_OK;  // no context yet: the runtime creates one below
+  if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return set_error(MPDPFT_ERR_CUDA, "cuCtxGetId failed");
+  *have = true;
+  return MPDPFT_OK;
+}
+
+int noalloc_scratch(double** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  unsigned long long id = 0;
+  bool have = false;
+  int st = current_context_id(&id, &have);
+  if (st) return st;
+  if (have)
+    for (const NoAllocEntry& e : g_noalloc_cache)
+      if (e.ptr && e.ctx_id == id) {
+        *out = e.ptr;
+        return MPDPFT_OK;
+      }
+  // first call in this context: cudaGetSymbolAddress also initialises the
+  // runtime's context when none is current yet
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+  if (e != cudaSuccess)
+    return set_error(MPDPFT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  if (!have) {
+    if ((st = current_context_id(&id, &have))) return st;
+    if (!have) return set_error(MPDPFT_ERR_CUDA, "no current CUDA context after cudaGetSymbolAddress");
+  }
+  g_noalloc_cache[g_noalloc_next] = NoAllocEntry{id, static_cast<double*>(p)};
+  g_noalloc_next = (g_noalloc_next + 1) % kNoAllocCache;
+  *out = static_cast<double*>(p);
   return MPDPFT_OK;
 }
 }  // namespace
@@ -106,24 +154,37 @@ extern "C" int mpdpft_integrate_noalloc(int dim, int steps, double edge, const d
   if (layout != MPDPFT_LAYOUT_PERIODIC && layout != MPDPFT_LAYOUT_REFERENCE)
     return set_error(MPDPFT_ERR_ARG, "bad layout");
   if (!f || !out) return set_error(MPDPFT_ERR_ARG, "null field or result pointer");
-  // 2^24 points: s <= 256 in 3D, s <= 4096 in 2D
+  // 2^24 periodic points: s <= 256 in 3D, s <= 4096 in 2D
   if ((dim == 3 && steps > 256) || (dim == 2 && steps > 4096))
     return set_error(MPDPFT_ERR_ARG, "grid larger than MPDPFT_NOALLOC_MAX_POINTS (16777216 points, 256^3): "
                                      "use mpdpft_integrate with a context");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(MPDPFT_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  const long n = dim == 3 ? (long)steps * steps * steps : (long)steps * steps;
+  const unsigned el = layout == MPDPFT_LAYOUT_REFERENCE ? (unsigned)steps + 1 : (unsigned)steps;
+  const unsigned total = dim == 3 ? el * el * el : el * el;
   double* scratch = nullptr;
-  int st = noalloc_scratch(dev, &scratch);
+  int st = noalloc_scratch(&scratch);
   if (st) return st;
-  const int ntiles = (int)((n + kNoAllocTile - 1) / kNoAllocTile);
+  const int ntiles = (int)((total + kNoAllocTile - 1) / kNoAllocTile);
   const double dx = edge / steps;
   const double dvol = dim == 3 ? dx * dx * dx : dx * dx;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_noalloc_tiles<<<ntiles, kNoAllocThreads, 0, s>>>(f, n, dim, steps, layout, scratch);
-  k_noalloc_finish<<<1, kNoAllocThreads, 0, s>>>(scratch, ntiles, dvol, out);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("integrate_noalloc launch: ") + cudaGetErrorString(e));
+  // each launch's own return code: an error the caller left pending is
+  // neither reported as ours nor cleared
+  {
+    void* args[] = {(void*)&f, (void*)&total, (void*)&dim, (void*)&el, (void*)&layout, (void*)&scratch};
+    cudaError_t e = cudaLaunchKernel((const void*)k_noalloc_tiles, dim3(ntiles), dim3(kNoAllocThreads), args, 0, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(MPDPFT_ERR_CUDA, std::string("k_noalloc_tiles launch: ") + cudaGetErrorString(e));
+    }
+  }
+  {
+    const double* cp = scratch;
+    void* args[] = {(void*)&cp, (void*)&ntiles, (void*)&dvol, (void*)&out};
+    cudaError_t e = cudaLaunchKernel((const void*)k_noalloc_finish, dim3(1), dim3(kNoAllocThreads), args, 0, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(MPDPFT_ERR_CUDA, std::string("k_noalloc_finish launch: ") + cudaGetErrorString(e));
+    }
+  }
   return MPDPFT_OK;
 }

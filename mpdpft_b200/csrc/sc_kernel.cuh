@@ -646,11 +646,11 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
     ls->iter_bits = 0;
   }
   // V written above is read at other points below
-  if (a.mode == 0 && a.assemble_v && !grid_barrier(st, nblk)) return;
+  if (a.mode == 0 && a.assemble_v && !grid_barrier(st, nblk, kp.spin_limit)) return;
 
   const R* V = a.V;
   MPDPFT_TSTAMP_B(1);
-  for (int pass = 0; pass < kMuMaxPasses; ++pass) {
+  for (int pass = 0; pass < kp.mu_max_passes; ++pass) {
     if (pass > 0 && threadIdx.x < S) {
       const int s = threadIdx.x;
       for (int c = s_ms[s].ncand; c < kMuCand; ++c) s_ms[s].cand[c] = s_ms[s].cand[0];
@@ -705,7 +705,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
         a.bcount[(long)threadIdx.x * nblk + bid] = c;
       }
-      if (!grid_barrier(st, nblk)) return;
+      if (!grid_barrier(st, nblk, kp.spin_limit)) return;
       for (int s = 0; s < S; ++s) {
         if (!s_need[s]) continue;
         int before = 0, total = 0;
@@ -757,7 +757,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         s_lcap[s] = s_llen[s] >= 0 ? s_cap[s] : 1e300;  // no rebuild after a whole-grid decision
         s_need[s] = 0;
       }
-      if (written && !grid_barrier(st, nblk)) return;  // the lists are complete
+      if (written && !grid_barrier(st, nblk, kp.spin_limit)) return;  // the lists are complete
     }
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
@@ -829,7 +829,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
       // write the next pass's row while others still read this one
       block_reduce_store<kMuAcc>(acc, a.part + ((long)(pass & 1) * nblk + bid) * kNPart + s * kMuAcc);
     }
-    if (!grid_barrier(st, nblk)) return;
+    if (!grid_barrier(st, nblk, kp.spin_limit)) return;
     // every block sums the partials in the same order and runs the same
     // decision on its own copy of the search state (no broadcast, no second
     // barrier); block 0 keeps the state copy that is written back
@@ -847,7 +847,8 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
         int bits = 0;
         for (int s = 0; s < S; ++s) {
           if (s_ms[s].done) continue;
-          mu_decide(s_ms[s], red + s * kMuAcc, red[s * kMuAcc + kMuCand], kp.abundance[s], kp.rel_acc, dmm, bits);
+          mu_decide(s_ms[s], red + s * kMuAcc, red[s * kMuAcc + kMuCand], kp.abundance[s], kp.rel_acc, dmm, bits,
+                    kp.mu_max_passes);
         }
         s_dmm = dmm;
         if (bid == 0) {

@@ -50,6 +50,8 @@ struct KParams {
   long chunk;     // points per warp in the mu kernel's sweeps (multiple of kSegPts)
   int mu_blocks;  // grid of the mu kernel (rows of its partial sums)
   int vec4;       // n % 4 == 0: a lane loads 4 points as one vector
+  int mu_max_passes;  // mu-search pass cap (1 .. kMuMaxPasses)
+  long spin_limit;    // grid-barrier spin limit
 };
 
 struct MuState {
@@ -150,8 +152,8 @@ __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
 
 // Bounded sense-free generation barrier over all blocks of a cooperative
 // launch.  Returns false (and raises the abort flag) if a block does not
-// arrive within the spin limit; every block then leaves its loop.
-__device__ inline bool grid_barrier(ScState* st, const int nblk) {
+// arrive within `limit` spins; every block then leaves its loop.
+__device__ inline bool grid_barrier(ScState* st, const int nblk, const long limit) {
   __syncthreads();
   __shared__ int ok;
   if (threadIdx.x == 0) {
@@ -168,7 +170,7 @@ __device__ inline bool grid_barrier(ScState* st, const int nblk) {
       long spins = 0;
       while (*gen == g) {
         if (*(volatile int*)&st->abort) { ok = 0; break; }
-        if (++spins > kBarrierSpinLimit) {
+        if (++spins > limit) {
           atomicExch(&st->abort, 1);
           atomicOr(&st->status_bits, kBitTimeout);
           ok = 0;
@@ -241,7 +243,7 @@ __device__ inline void set_bracket(MuState& m, double a, double Na, double b, do
 // dN/dmu at candidate 0.  Finds the bracket, tightens it with every
 // candidate inside, and places the next candidates or finishes.
 __device__ inline void mu_decide(MuState& m, const double* N, double slope, double target, double rel_acc,
-                                 double& dmm, int& bits) {
+                                 double& dmm, int& bits, int max_passes) {
   const double denom = fabs(2.0 * target);
   for (int c = 0; c < m.ncand; ++c)
     if (!isfinite(N[c])) bits |= kBitNonfinite;
@@ -285,7 +287,7 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
   m.pass++;
   m.dens_mu = m.best_mu;
   if (m.best_err <= rel_acc) { m.done = 1; return; }
-  if (m.pass >= kMuMaxPasses) { m.done = 1; bits |= kBitTimeout; return; }
+  if (m.pass >= max_passes) { m.done = 1; bits |= kBitTimeout; return; }
   m.ncand = 0;
   if (!(m.have_lo && m.have_hi)) {
     if (m.next_c > 20) {

@@ -32,6 +32,7 @@ EXPORTS = [
     "mpdpft_batch_create", "mpdpft_batch_destroy", "mpdpft_batch_set_external_potential", "mpdpft_batch_sc_init",
     "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
     "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei", "mpdpft_fft_config",
+    "mpdpft_set_limits", "mpdpft_integrate_noalloc",
 ]
 
 
@@ -67,6 +68,7 @@ def load(path=LIB_PATH):
     L.mpdpft_ctx_sync.argtypes = [vp]
     L.mpdpft_ctx_stream.argtypes = [vp]
     L.mpdpft_ctx_stream.restype = vp
+    L.mpdpft_set_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.mpdpft_set_external_potential.argtypes = [vp, C.c_int, _dp, C.c_int, C.c_int]
     L.mpdpft_density.argtypes = [vp, C.c_int, _dp, C.c_double, _dp, _dp, C.c_int, C.c_int]
     L.mpdpft_vint.argtypes = [vp, C.c_int, C.c_int, _dpp, _dp, C.c_int, C.c_int]
@@ -271,6 +273,10 @@ class Engine:
 
     def sync(self):
         self._check(self.lib.mpdpft_ctx_sync(self.h))
+
+    def set_limits(self, mu_max_passes=-1, barrier_spin_limit=-1):
+        """Device loop limits (negative: defaults)."""
+        self._check(self.lib.mpdpft_set_limits(self.h, mu_max_passes, barrier_spin_limit))
 
     def stream(self):
         return self.lib.mpdpft_ctx_stream(self.h)

@@ -4,7 +4,10 @@ allocation, or a loop that must not pay cudaMalloc's implicit device
 synchronisation).  It takes device pointers only and keeps its partial sums
 in a fixed array inside the library, so the checks here run it through the
 C ABI twice in a row on the same buffers and compare each result with the
-context-based mpdpft_integrate on the same field.
+context-based mpdpft_integrate on the same field and with the oracle's
+trapezoid rule (a plain sum in the periodic layout, Riemann's end weights in
+the reference layout, whose test fields do not repeat plane 0 in their last
+plane).  The 256^3 cases fill the whole scratch array.
 
 This file is collected last on purpose: a failure here leaves every other
 test already run.
@@ -47,11 +50,45 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     assert f(3, 64, 10.0, None, fake, abi.LAYOUT_PERIODIC, None) == abi.ERR_ARG
 
 
+def _riemann(dim, s, edge, layout, host):
+    """Trapezoid rule on the stored values (Riemann, mpDPFT.cpp:7981-8026):
+    end weights 1/2 per axis in the reference layout, weight 1 on the
+    periodic grid."""
+    dvol = (edge / s) ** dim
+    if layout != abi.LAYOUT_REFERENCE:
+        return float(host.sum()) * dvol
+    m = s + 1
+    w = np.ones(m)
+    w[0] = w[-1] = 0.5
+    f = host.reshape((m,) * dim)
+    if dim == 3:
+        return float(np.einsum("k,ijk->ij", w, f).dot(w).dot(w)) * dvol
+    return float(w.dot(f).dot(w)) * dvol
+
+
+def test_noalloc_riemann_matches_oracle_reference_layout():
+    """The test's trapezoid rule equals the oracle's on fields whose last
+    planes differ from plane 0 (the case the reference layout must not
+    shortcut), and differs from the periodic-only sum there."""
+    from oracle import oracle
+    for dim, s, edge in ((3, 6, 3.0), (2, 10, 4.0)):
+        host = _field(dim, s, abi.LAYOUT_REFERENCE, seed=s)
+        p = abi.make_params(dim=dim, steps=s, edge=edge, precision=abi.FP64)
+        expect = oracle.integrate_reference_layout(p, host)
+        got = _riemann(dim, s, edge, abi.LAYOUT_REFERENCE, host)
+        assert abs(got - expect) <= 1e-13 * abs(expect), (got, expect)
+        periodic_only = float(host.reshape((s + 1,) * dim)[(slice(0, s),) * dim].sum()) * (edge / s) ** dim
+        assert abs(periodic_only - expect) > 1e-6 * abs(expect)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("dim,s,layout", [
     (3, 64, abi.LAYOUT_PERIODIC),
     (3, 48, abi.LAYOUT_REFERENCE),
     (2, 256, abi.LAYOUT_PERIODIC),
+    (2, 200, abi.LAYOUT_REFERENCE),
+    (3, 256, abi.LAYOUT_PERIODIC),
+    (3, 256, abi.LAYOUT_REFERENCE),
 ])
 def test_noalloc_integral_matches_context_integral_twice(dim, s, layout):
     import torch
@@ -78,7 +115,10 @@ def test_noalloc_integral_matches_context_integral_twice(dim, s, layout):
         assert st == abi.OK, lib.mpdpft_last_error()
         torch.cuda.synchronize()
         results.append(float(out.item()))
+    expect = _riemann(dim, s, edge, layout, host)
+    assert abs(ref - expect) <= REL_TOL * max(1.0, abs(expect)), (ref, expect)
     for v in results:
         assert np.isfinite(v)
         assert abs(v - ref) <= REL_TOL * max(1.0, abs(ref)), (v, ref)
+        assert abs(v - expect) <= REL_TOL * max(1.0, abs(expect)), (v, expect)
     assert results[0] == results[1]  # fixed tiling: the same summation order every call
