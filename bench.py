@@ -3,11 +3,15 @@
 
 Workload (the headline configuration): neutral atom Z = 18 on 128^3, box
 [-10, 10]^3 bohr, Gaussian nucleus (sigma 0.1), TF + gradient-corrected
-density (spectral grad V and Laplacian smoothed with width 0.2), Hartree by
-FFT Poisson, Dirac exchange; mixed precision (FP32 fields and FFTs, FP64
-particle-number integral, mu search, Pulay Gram/solve and energy), one SC
-iteration replayed as a CUDA graph.  A step is one SC iteration.  Inputs are
-synthetic and seeded (mpdpft_b200.workloads.argon_atom).
+density (the reference's small-gradient branch in its T -> 0 form; spectral
+Laplacian smoothed with width 0.2), Hartree by FFT Poisson, Dirac exchange;
+mixed precision (FP32 fields and FFTs, FP64 particle-number integral, mu
+search, Pulay Gram/solve and energy), one SC iteration replayed as a CUDA
+graph.  A step is one SC iteration.  Inputs are synthetic and seeded
+(mpdpft_b200.workloads.argon_atom).  The same replay on an all-FP64 context
+is extra.fp64_arm; time-to-converge of both (extra.ttc_*) includes the
+initial densities.  roofline: the iteration replayed launch by launch from
+its graph (CUDA events per launch), the kernel with the largest share of it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -138,16 +142,55 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(steps_grid, iters=3):
-    """The oracle (FP64 C++ restatement of the reference loop, OpenMP) on a
-    bounded sample: `iters` SC iterations of the same workload."""
+def host_cpu():
+    """(nproc, CPU model) of this host."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return os.cpu_count(), model
+
+
+def oracle_atom_rate(steps_grid, iters, threads):
+    """SC iterations/s of the oracle on `iters` iterations of the atom (after
+    its initial density) with `threads` OpenMP threads (0: all)."""
     from oracle import oracle as O
     from mpdpft_b200 import abi, workloads as W
+    O.set_threads(threads)
     p, vext, v0 = W.argon_atom(steps=steps_grid, precision=abi.FP64, max_sc_count=iters - 1, sc_criterion=-1.0)
     res, log, dens, v = O.sc_run(p, vext, v0)
     ms = [l.ms for l in log]
-    return {"value": 1000.0 * len(ms) / sum(ms), "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-            "sample": "%d SC iterations of the %d^3 atom (after its initial density), FP64 oracle" % (len(ms), steps_grid)}
+    return 1000.0 * len(ms) / sum(ms), len(ms), O.num_threads()
+
+
+def cpu_baseline(steps_grid, iters=3):
+    """The oracle (FP64 C++ restatement of the reference loop, OpenMP) on
+    bounded samples: `iters` SC iterations of the headline atom on all host
+    threads (the reported value) and on one thread, and a full C1 solve
+    (harmonic_tf at 64^3, FP64) on all threads."""
+    from oracle import oracle as O
+    from mpdpft_b200 import abi, workloads as W
+    nproc, model = host_cpu()
+    rate, k, threads = oracle_atom_rate(steps_grid, iters, 0)
+    rate1, k1, _ = oracle_atom_rate(steps_grid, 1, 1)
+    O.set_threads(0)
+    p, vext, v0 = W.harmonic_tf(steps=64, precision=abi.FP64)
+    t0 = time.perf_counter()
+    res, log, dens, v = O.sc_run(p, vext, v0)
+    c1_s = time.perf_counter() - t0
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d SC iterations of the %d^3 atom (after its initial density), FP64 oracle" % (k, steps_grid),
+            "host": {"nproc": nproc, "cpu_model": model},
+            "one_core": {"value": rate1, "unit": UNIT, "cores": 1,
+                         "sample": "%d SC iterations of the %d^3 atom on one thread" % (k1, steps_grid)},
+            "c1_harmonic_64": {"ttc_s": c1_s, "iterations": res.iterations, "converged": res.converged,
+                               "iter_per_s": res.iterations / c1_s, "cores": threads,
+                               "sample": "full C1 solve (harmonic_tf 64^3, CC < 1e-12, r_V <= 1e-8)"}}
 
 
 def run_reference(args, world, rank):
@@ -156,6 +199,7 @@ def run_reference(args, world, rank):
     from oracle import oracle as O
     from mpdpft_b200 import abi, workloads as W
     O.lib()
+    O.set_threads(0)
     # each step is one SC iteration of the oracle on the same workload; the
     # sample is capped so the run ends within a few minutes
     per_iter = 3.5 * 8.0 / max(1, O.num_threads()) * (args.steps_grid / 128.0) ** 3
@@ -165,20 +209,85 @@ def run_reference(args, world, rank):
     res, log, dens, v = O.sc_run(p, vext, v0)
     ms = [l.ms for l in log[w:w + k]]
     value = 1000.0 * len(ms) / sum(ms)
+    nproc, model = host_cpu()
     sample = "%d timed SC iterations (after %d warm-up) of the %d^3 atom, FP64" % (len(ms), w, args.steps_grid)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": len(ms), "warmup": w, "ms_per_step": float(np.mean(ms)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "argon_atom", "grid": "%d^3" % args.steps_grid, "precision": "fp64",
                        "implementation": "CPU oracle (C++ restatement of the reference loop, OpenMP)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port", "sample": sample,
+                             "host": {"nproc": nproc, "cpu_model": model}},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def graph_replay(prec, sg, steps, warmup, device, barrier, stream_of):
+    """K SC iterations of the atom replayed from one CUDA graph, timed with
+    CUDA events on the engine stream after W warm-up iterations.  Returns
+    (ms, kernels per iteration, the engine)."""
+    import torch
+    from mpdpft_b200 import engine, workloads as W
+    total = warmup + steps + 16
+    p, vext, v0 = W.argon_atom(steps=sg, precision=prec, sc_criterion=-1.0, max_sc_count=total + 8)
+    eng = engine.Engine(p, device=device)
+    eng.sc_init(vext, v0)
+    stream = stream_of(eng)
+    for _ in range(warmup):
+        eng.sc_step(graph=True)
+    eng.sync()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        eng.sc_step(graph=True)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    return e0.elapsed_time(e1), eng.iteration_kernels(), eng
+
+
+def loop_roofline(eng, ms_per_step, iters=5):
+    """Per-kernel device time inside the SC loop: `iters` iterations replayed
+    launch by launch from the captured graph (mpdpft_iteration_profile, CUDA
+    events on the engine stream), aggregated by kernel.  The dominant kernel
+    is the one with the largest share of the iteration; achieved = its
+    algorithmic bytes per launch / its mean launch time."""
+    per = {}
+    total = 0.0
+    for _ in range(iters):
+        for name, ms, b in eng.iteration_profile():
+            d = per.setdefault(name, {"ms": 0.0, "launches": 0, "bytes": 0.0})
+            d["ms"] += ms
+            d["launches"] += 1
+            d["bytes"] += b
+            total += ms
+    peak, peak_kind = measured_peaks()
+    kernels = {}
+    for name, d in per.items():
+        ms_launch = d["ms"] / d["launches"]
+        b_launch = d["bytes"] / d["launches"]
+        kernels[name] = {"share": d["ms"] / total, "launches_per_iter": d["launches"] // iters,
+                         "ms_per_iter": d["ms"] / iters, "ms_per_launch": ms_launch,
+                         "bytes_per_launch": b_launch,
+                         "GBps": b_launch / (ms_launch / 1000.0) / 1e9 if ms_launch > 0 else None}
+    dom = max((k for k in kernels if k != "memset"), key=lambda k: kernels[k]["share"])
+    d = kernels[dom]
+    ach = d["GBps"]
+    return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_source": peak_kind, "traffic": traffic_from_profiles(dom),
+            "bytes_per_launch": d["bytes_per_launch"], "ms_per_launch": d["ms_per_launch"],
+            "share_of_iteration": d["share"],
+            "iteration_sum_ms": total / iters, "graph_ms_per_step": ms_per_step,
+            "method": "iteration replayed launch by launch from its CUDA graph, CUDA events per launch, "
+                      "mean of %d iterations; bytes: each launch's own input and output fields once" % iters,
+            "kernels": kernels}
+
+
 def run_ours(args, world, rank, local):
     import torch
-    from mpdpft_b200 import abi, engine, workloads as W
+    from mpdpft_b200 import abi
 
     torch.cuda.set_device(local)
     pg = None
@@ -193,68 +302,39 @@ def run_ours(args, world, rank, local):
             pg.barrier()
         torch.cuda.synchronize()
 
+    def stream_of(e):
+        return torch.cuda.ExternalStream(e.stream(), device=local)
+
+    def max_over_ranks(ms):
+        t = torch.tensor([ms], device="cuda")
+        if pg:
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
     sg = args.steps_grid
-    total_iters = args.warmup + args.steps + 16
-    p, vext, v0 = W.argon_atom(steps=sg, precision=abi.MIXED, sc_criterion=-1.0, max_sc_count=total_iters + 8)
-    eng = engine.Engine(p, device=local)
-    eng.sc_init(vext, v0)
-    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
     clocks = ClockSampler(local)
     with clocks:
-        for _ in range(args.warmup):
-            eng.sc_step(graph=True)
-        eng.sync()
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            eng.sc_step(graph=True)
-        e1.record(stream)
-        e1.synchronize()
-        barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    ms_max = float(t.item())
+        ms, launches, eng = graph_replay(abi.MIXED, sg, args.steps, args.warmup, local, barrier, stream_of)
+    ms_max = max_over_ranks(ms)
     value = world * args.steps / (ms_max / 1000.0)
-    launches = eng.iteration_kernels()
-
-    # roofline of the dominant kernel (share = time per launch x launches per
-    # iteration); each kernel timed alone with CUDA events on the engine stream
-    per_iter = eng.stage_launch_counts()
-    stages = {abi.STAGE_SC_MU: ("sc_mu_kernel", 1),
-              abi.STAGE_SC_DENSITY: ("sc_density_kernel", 1),
-              abi.STAGE_SC_MIX: ("sc_mix_kernel", 1),
-              abi.STAGE_FFT_X: ("k_x_roundtrip", per_iter.get("x", 0))}
-    if per_iter.get("y", 0) == 0:  # 3D transforms by x-planes
-        stages.update({abi.STAGE_FFT_PLANE_FWD: ("k_plane_fwd", per_iter.get("z_r2c", 0)),
-                       abi.STAGE_FFT_PLANE_INV: ("k_plane_inv", per_iter.get("z_c2r", 0))})
-    else:
-        stages.update({abi.STAGE_FFT_Z_R2C: ("k_z_r2c", per_iter.get("z_r2c", 0)),
-                       abi.STAGE_FFT_Y: ("k_axis_c2c", per_iter.get("y", 0)),
-                       abi.STAGE_FFT_Z_C2R: ("k_z_c2r", per_iter.get("z_c2r", 0))})
-    prof = {}
-    for st, (name, cnt) in stages.items():
-        mst, b = eng.profile_stage(st, reps=20)
-        prof[name] = {"ms": mst, "bytes": b, "per_iter": cnt, "share_ms": mst * cnt}
-    dom = max(prof, key=lambda k: prof[k]["share_ms"])
-    peak, peak_kind = measured_peaks()
-    ach = prof[dom]["bytes"] / (prof[dom]["ms"] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "peak_source": peak_kind,
-                "traffic": traffic_from_profiles(dom), "bytes_per_launch": prof[dom]["bytes"],
-                "ms_per_launch": prof[dom]["ms"],
-                "stages": {k: {"ms": v["ms"], "GBps": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] > 0 else None,
-                               "launches_per_iter": v["per_iter"]} for k, v in prof.items()}}
+    roofline = loop_roofline(eng, ms_max / args.steps)
     eng.close()
 
-    extra = {}
-    if not args.no_ttc:
-        extra = time_to_converge(sg, local)
+    # the all-FP64 arm: the same graph replay on an FP64 context
+    ms64, launches64, eng64 = graph_replay(abi.FP64, sg, args.steps, args.warmup, local, barrier, stream_of)
+    ms64 = max_over_ranks(ms64)
+    roof64 = loop_roofline(eng64, ms64 / args.steps, iters=2)
+    eng64.close()
+    fp64_arm = {"value": world * args.steps / (ms64 / 1000.0), "unit": UNIT, "ms_per_step": ms64 / args.steps,
+                "gpu_launches": launches64 * args.steps, "dominant_kernel": roof64["kernel"],
+                "dominant_share": roof64["share_of_iteration"], "dominant_frac": roof64["frac"],
+                "speedup_mixed_vs_fp64_per_iteration": ms64 / ms_max}
 
-    e2e = end_to_end(sg, local)
+    extra = {"fp64_arm": fp64_arm}
+    if not args.no_ttc:
+        extra.update(time_to_converge(sg, local))
+    e2e = end_to_end(sg, local, abi.MIXED)
+    fp64_arm["e2e"] = end_to_end(sg, local, abi.FP64)
     if not args.no_batch:
         extra["batched_sweep"] = batched_sweep(args.batch_count, local, rank=rank, world=world, pg=pg)
     if not args.no_adjoint:
@@ -274,12 +354,14 @@ def run_ours(args, world, rank, local):
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": "argon_atom", "grid": "%d^3" % sg, "box": "[-10,10]^3 bohr", "Z": 18,
-                           "functional": "TF + gradient correction (spectral grad V, Laplacian; smoothing 0.2)",
+                           "functional": "TF + gradient correction: the reference's small-gradient branch, T -> 0 "
+                                         "form, no |grad V|^2 term (spectral Laplacian smoothed with width 0.2)",
                            "interactions": "Hartree (FFT Poisson, regularised kernel) + Dirac exchange",
                            "precision": "mixed: FP32 fields/FFTs, FP64 N(mu), mu search, Pulay, energy",
                            "graph": "one SC iteration per CUDA graph replay",
                            "parallelism": "replicas x%d" % world,
-                           "l2": "inputs larger than L2: an iteration touches ~180 MB (126 MB L2)"},
+                           "l2": "no flush; an iteration touches ~150 MB (L2 126 MB), the 2M-point fields of "
+                                 "one kernel partly stay in L2 for the next"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
                 "gpu_launches": launches * args.steps, "extra": extra}
         print(json.dumps(line), flush=True)
@@ -288,28 +370,62 @@ def run_ours(args, world, rank, local):
         pg.destroy_process_group()
 
 
+def fixture(name):
+    p = os.path.join(ROOT, "tests", "golden", "config_%s.npz" % name)
+    return dict(np.load(p)) if os.path.exists(p) else None
+
+
+def against_fixture(name, p, res, dens, pot):
+    """Errors of a converged GPU solve against the oracle fixture of its
+    configuration (energy, mu, and the density / potential on 16^3 coarse
+    blocks)."""
+    fx = fixture(name)
+    if fx is None:
+        return None
+    S, dvol, b = p.species, (p.edge / p.steps) ** p.dim, p.steps // 16
+
+    def blocks(f):
+        g = np.asarray(f).reshape((16, b) * p.dim)
+        return g.sum(axis=tuple(range(1, 2 * p.dim, 2))).reshape(-1)
+
+    return {"dE_over_E": abs(res.e_total - float(fx["e_total"])) / abs(float(fx["e_total"])),
+            "coarse_L1_per_particle": max(float(np.abs(blocks(dens[s]) * dvol - fx["dens_blocks"][s]).sum())
+                                          / p.abundances[s] for s in range(S)),
+            "coarse_potential_max_err": max(float(np.abs(blocks(pot[s]) / b ** p.dim - fx["pot_blocks"][s]).max())
+                                            for s in range(S)),
+            "mu_abs_err": max(abs(res.mu[s] - float(fx["mu"][s])) for s in range(S)),
+            "oracle_iterations": int(fx["iterations"]), "iterations": res.iterations}
+
+
 def time_to_converge(sg, device):
-    """Full solves to the SC criterion (CC < 1e-8 three times) in mixed and
-    in all-FP64 precision on the same GPU; device time from the engine."""
+    """Full solves through mpdpft_sc_run to the SC criterion (CC < 1e-8 three
+    times) in mixed and in all-FP64 precision on the same GPU; wall time of
+    the whole solve from the initial densities on (start potential already
+    on the host side of the ABI), errors against the FP64 oracle fixture."""
     from mpdpft_b200 import abi, engine, workloads as W
     out = {}
-    dens = {}
+    acc = {}
     for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
         p, vext, v0 = W.argon_atom(steps=sg, precision=prec)
         with engine.Engine(p, device=device) as e:
             e.sc_run(vext, v0)  # warm-up solve (graph instantiation, clocks)
-            res, log, st = e.sc_run(vext, v0)
-            dens[name] = e.field(abi.FIELD_DENSITY, 0)
-            out["ttc_%s_s" % name] = res.seconds
-            out["iters_%s" % name] = res.iterations
-            out["converged_%s" % name] = res.converged
-            out["energy_%s" % name] = res.e_total
-            out["mu_%s" % name] = res.mu[0]
-            out["iter_per_s_%s" % name] = res.iterations / res.seconds
+            best = None
+            for _ in range(3):
+                res, log, st = e.sc_run(vext, v0)
+                best = res if best is None or res.seconds < best.seconds else best
+            res = best
+            dens = [e.field(abi.FIELD_DENSITY, 0)]
+            pot = [e.field(abi.FIELD_POTENTIAL, 0)]
+        out["ttc_%s_s" % name] = res.seconds
+        out["iters_%s" % name] = res.iterations
+        out["converged_%s" % name] = res.converged
+        out["energy_%s" % name] = res.e_total
+        out["mu_%s" % name] = res.mu[0]
+        out["iter_per_s_%s" % name] = res.iterations / res.seconds
+        acc[name] = against_fixture("argon_atom_%d" % sg, p, res, dens, pot)
     out["ttc_speedup_mixed_vs_fp64"] = out["ttc_fp64_s"] / out["ttc_mixed_s"]
-    out["energy_rel_err_mixed_vs_fp64"] = abs(out["energy_mixed"] - out["energy_fp64"]) / abs(out["energy_fp64"])
-    dv = (20.0 / sg) ** 3
-    out["density_l1_per_particle_mixed_vs_fp64"] = float(np.abs(dens["mixed"] - dens["fp64"]).sum() * dv / 18.0)
+    out["ttc_note"] = "wall time of mpdpft_sc_run, best of 3: initial densities, SC loop and energies"
+    out["accuracy_vs_fp64_oracle"] = acc
     return out
 
 
@@ -410,12 +526,15 @@ def electron_hole_256(device):
     from mpdpft_b200 import abi, engine, workloads as W
     out = {"grid": "256^3", "species": 2}
     dens = {}
+    acc = {}
     for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
         p, vext, v0 = W.electron_hole(steps=256, precision=prec)
         with engine.Engine(p, device=device) as e:
             e.sc_run(vext, v0)  # warm-up (graph instantiation)
             res, log, st = e.sc_run(vext, v0)
             dens[name] = [e.field(abi.FIELD_DENSITY, s) for s in range(2)]
+            pot = [e.field(abi.FIELD_POTENTIAL, s) for s in range(2)]
+        acc[name] = against_fixture("electron_hole_256", p, res, dens[name], pot)
         out["ttc_%s_s" % name] = res.seconds
         out["iters_%s" % name] = res.iterations
         out["converged_%s" % name] = res.converged
@@ -425,6 +544,7 @@ def electron_hole_256(device):
     dv = (40.0 / 256) ** 3
     out["density_l1_per_particle_mixed_vs_fp64"] = float(max(np.abs(dens["mixed"][s] - dens["fp64"][s]).sum() * dv / 20000.0
                                                              for s in range(2)))
+    out["accuracy_vs_fp64_oracle"] = acc
     return out
 
 
@@ -436,6 +556,7 @@ def adjoint_cluster(device, max_iter=60):
     from mpdpft_b200 import abi, engine, workloads as W
     out = {"grid": "192^3", "nuclei": 13, "adjoint_max_iter": max_iter}
     dR = {}
+    acc = {}
     for name, prec in (("mixed", abi.MIXED), ("fp64", abi.FP64)):
         pt, vt, v0t, _ = W.cluster_adjoint(precision=prec, jitter=0.0)
         with engine.Engine(pt, device=device) as et:
@@ -448,6 +569,7 @@ def adjoint_cluster(device, max_iter=60):
             res, log, st = e.sc_run(vext, v0, check=False)
             t1 = time.perf_counter()
             n = e.field(abi.FIELD_DENSITY, 0)
+            acc[name] = against_fixture("cluster_adjoint_192", p, res, [n], [e.field(abi.FIELD_POTENTIAL, 0)])
             dvol = (p.edge / p.steps) ** 3
             g = 2.0 * dvol * (n - nt)
             t2 = time.perf_counter()
@@ -462,14 +584,15 @@ def adjoint_cluster(device, max_iter=60):
         out["loss_%s" % name] = float(dvol * ((n - nt) ** 2).sum())
     out["max_abs_dL_dR_fp64"] = float(np.abs(dR["fp64"]).max())
     out["dL_dR_rel_diff_mixed_vs_fp64"] = float(np.abs(dR["mixed"] - dR["fp64"]).max() / np.abs(dR["fp64"]).max())
+    out["accuracy_vs_fp64_oracle"] = acc
     return out
 
 
-def end_to_end(sg, device, solves=2):
+def end_to_end(sg, device, prec, solves=2):
     """Full solves through the C ABI with host arrays: V_ext and V_0 copied
     in, the density copied out; iterations / wall time."""
-    from mpdpft_b200 import abi, engine, workloads as W
-    p, vext, v0 = W.argon_atom(steps=sg, precision=abi.MIXED)
+    from mpdpft_b200 import engine, workloads as W
+    p, vext, v0 = W.argon_atom(steps=sg, precision=prec)
     with engine.Engine(p, device=device) as e:
         e.sc_run(vext, v0)
         iters = 0

@@ -155,7 +155,8 @@ typedef struct {
   double e_kinetic[MPDPFT_MAX_SPECIES];
   double e_external[MPDPFT_MAX_SPECIES];
   double e_interaction[MPDPFT_MAX_INTERACTIONS];
-  double seconds;           /* wall time of the solve                              */
+  double seconds;           /* wall time of the solve (mpdpft_sc_run: from the
+                               initial densities to the energies of the result) */
 } mpdpft_result;
 
 typedef struct mpdpft_ctx mpdpft_ctx;
@@ -323,6 +324,21 @@ int mpdpft_profile_stage(mpdpft_ctx* ctx, int stage, int reps, double* ms_per_la
  * kernels; *total = their sum.  Valid after the first graph-mode
  * mpdpft_sc_step. */
 int mpdpft_iteration_launches(mpdpft_ctx* ctx, int* counts, int* total);
+
+/* Per-launch device time of one SC iteration as the captured graph runs it
+ * (the reference's per-routine timers, mpDPFT.cpp:11997-12003, at kernel
+ * granularity).  The nodes of the captured iteration are replayed one at a
+ * time, in order, each bracketed by CUDA events on the context stream, so
+ * the replay is one real SC iteration on the current state.  Each record
+ * names the kernel (or "memset"), its device time and the algorithmic bytes
+ * of that launch (its own input and output fields, each counted once).
+ * Valid after the first graph-mode mpdpft_sc_step; *n_out = launches. */
+typedef struct {
+  char name[32];
+  double ms;
+  double bytes;
+} mpdpft_launch_record;
+int mpdpft_iteration_profile(mpdpft_ctx* ctx, int cap, mpdpft_launch_record* records, int* n_out);
 
 /* Phase durations (microseconds, block 0 of the grid) of the last SC-step
  * kernel: [0] V update, [1] mu search, [2] densities/residual/Gram row,

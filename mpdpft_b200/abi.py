@@ -144,6 +144,14 @@ class Result(C.Structure):
     ]
 
 
+class LaunchRecord(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 32),
+        ("ms", C.c_double),
+        ("bytes", C.c_double),
+    ]
+
+
 def make_params(**kw):
     """Params with the reference defaults, overridden by keyword arguments.
 

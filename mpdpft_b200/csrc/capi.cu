@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points of include/mpdpft_gpu.h.
+#include <chrono>
 #include <cstring>
 #include <new>
 
@@ -207,9 +208,14 @@ int mpdpft_sc_run(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem,
                   mpdpft_iter_log* log, int log_cap) {
   CHECK_CTX(ctx);
   cudaSetDevice(ctx->impl.device);
+  // result->seconds: the whole solve, the initial densities (sc_init: V_0
+  // import, DelField, the first mu search) included
+  const auto t0 = std::chrono::steady_clock::now();
   int st = ctx->impl.sc_init(v0, layout, mem);
   if (st) return st;
-  return ctx->impl.sc_run(result, log, log_cap, /*use_graph=*/1);
+  st = ctx->impl.sc_run(result, log, log_cap, /*use_graph=*/1);
+  if (result) result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return st;
 }
 
 int mpdpft_get_field(mpdpft_ctx* ctx, int which, int s, double* out, int layout, int mem) {
@@ -284,6 +290,13 @@ int mpdpft_adjoint_nuclei(mpdpft_ctx* ctx, const double* dl_dvext, int mem, int 
   CHECK_CTX(ctx);
   cudaSetDevice(ctx->impl.device);
   return ctx->impl.adjoint_nuclei(dl_dvext, mem, n_nuclei, charges, positions, sigma, dl_dpositions);
+}
+
+int mpdpft_iteration_profile(mpdpft_ctx* ctx, int cap, mpdpft_launch_record* records, int* n_out) {
+  CHECK_CTX(ctx);
+  if (cap < 0) return set_error(MPDPFT_ERR_ARG, "negative capacity");
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.iteration_profile(cap, records, n_out);
 }
 
 int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n) {

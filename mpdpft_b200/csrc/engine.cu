@@ -301,6 +301,10 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   S = P.species;
   ring = (P.mixer ? P.pulay_scope : 1) + 1;
   gradient = P.density_expression == MPDPFT_DENS_GRADIENT;
+  // |grad V|^2 enters only the 3D form with a |grad V|^2 coefficient; the
+  // reference's small-gradient branch (and the 2D form) use the Laplacian
+  // alone, so the SC loop's DelField then skips the gradients
+  need_g2 = gradient && P.dim == 3 && P.gradient_grad2 != 0.0;
   has_coulomb = has_interaction(MPDPFT_INT_HARTREE) || has_interaction(MPDPFT_INT_HARTREE_INTER) ||
                 has_interaction(MPDPFT_INT_COULOMB_CHARGED);
   for (int s = 0; s < S; ++s) temperature[s] = P.temperature[s];
@@ -368,6 +372,10 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   CU(cudaMemsetAsync(d_cur, 0, field * S, stream));
   CU(cudaMemsetAsync(d_res, 0, field * S * ring, stream));
   CU(cudaMemsetAsync(d_log, 0, sizeof(mpdpft_iter_log) * log_cap, stream));
+  if (gradient) {
+    CU(cudaMemsetAsync(d_g2, 0, field * S, stream));
+    CU(cudaMemsetAsync(d_lap, 0, field * S, stream));
+  }
   return reset_state();
 }
 
@@ -453,7 +461,7 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.vext = (const R*)d_vext;
   a.V = (R*)d_V;
   a.lap = gradient ? (const R*)d_lap : nullptr;
-  a.g2 = gradient ? (const R*)d_g2 : nullptr;
+  a.g2 = need_g2 ? (const R*)d_g2 : nullptr;
   a.vh = has_coulomb ? (const R*)d_vh : nullptr;
   a.nin = (R*)d_nin;
   a.res = (R*)d_res;
@@ -481,6 +489,22 @@ template <typename R>
 static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk, int parts = 7) {
   StepArgs<R> args = c.step_args<R>(mode);
   void* params[] = {&args};
+  // algorithmic bytes per species: the fields each kernel reads and writes,
+  // once (the mu search counts one sweep whatever its passes)
+  const double fb = c.field_bytes() * c.S;
+  const double deriv = (args.lap ? 1.0 : 0.0) + (args.g2 ? 1.0 : 0.0);
+  const double m = c.P.mixer ? c.P.pulay_scope : 1;
+  if (c.noting) {
+    if (mode != 2 && (parts & 1))
+      c.note("sc_mu_kernel", ((mode == 0 && args.assemble_v) ? 4.0 * fb : 0.0) + (1.0 + deriv) * fb);
+    if (parts & 2) {
+      // V, derivatives, n_in, m - 1 history residuals in; the residual out
+      c.note("sc_density_kernel", (2.0 + deriv + m) * fb);
+      c.note("sc_phase_d_kernel", (double)c.dens_blocks * kNPart * sizeof(double));
+    }
+    // m input densities and residuals in; the next density and its copy out
+    if (mode != 1 && (parts & 4)) c.note("sc_mix_kernel", (2.0 * m + 2.0) * fb);
+  }
   if (mode != 2 && (parts & 1)) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
@@ -586,7 +610,10 @@ int Ctx::sc_step(int use_graph) {
   if (!graph_exec) {
     CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < 6; ++i) cnt[i] = 0;
+    notes.clear();
+    noting = true;
     st = issue_iteration();
+    noting = false;
     for (int i = 0; i < 6; ++i) iter_cnt[i] = cnt[i];
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(stream, &g);
@@ -597,6 +624,103 @@ int Ctx::sc_step(int use_graph) {
   }
   CU(cudaGraphLaunch(graph_exec, stream));
   return MPDPFT_OK;
+}
+
+void Ctx::note(const char* name, double bytes) {
+  if (!noting) return;
+  LaunchNote r;
+  std::memset(&r, 0, sizeof(r));
+  std::strncpy(r.name, name, sizeof(r.name) - 1);
+  r.bytes = bytes;
+  notes.push_back(r);
+}
+
+// One SC iteration replayed node by node from the captured graph (dependency
+// order; a stream capture is a chain), each node as a one-node graph with the
+// kernel's launch attributes (the mu kernel stays cooperative), timed with
+// CUDA events on the context stream.
+int Ctx::iteration_profile(int cap, mpdpft_launch_record* out, int* n_out) {
+  if (!graph) return set_error(MPDPFT_ERR_ARG, "no captured iteration (run one graph-mode mpdpft_sc_step first)");
+  size_t nn = 0;
+  CU(cudaGraphGetNodes(graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CU(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  // topological order: repeatedly take the nodes whose dependencies are taken
+  std::vector<cudaGraphNode_t> order;
+  std::vector<char> done(nn, 0);
+  while (order.size() < nn) {
+    bool progress = false;
+    for (size_t i = 0; i < nn; ++i) {
+      if (done[i]) continue;
+      size_t nd = 0;
+      CU(cudaGraphNodeGetDependencies(nodes[i], nullptr, &nd));
+      std::vector<cudaGraphNode_t> deps(nd);
+      if (nd) CU(cudaGraphNodeGetDependencies(nodes[i], deps.data(), &nd));
+      bool ready = true;
+      for (cudaGraphNode_t d : deps) {
+        size_t j = 0;
+        while (j < nn && nodes[j] != d) ++j;
+        if (j < nn && !done[j]) ready = false;
+      }
+      if (!ready) continue;
+      done[i] = 1;
+      order.push_back(nodes[i]);
+      progress = true;
+    }
+    if (!progress) return set_error(MPDPFT_ERR_CUDA, "captured iteration has a dependency cycle");
+  }
+  if (order.size() != notes.size())
+    return set_error(MPDPFT_ERR_CUDA, "captured iteration: " + std::to_string(order.size()) + " nodes, " +
+                                          std::to_string(notes.size()) + " recorded launches");
+  cudaEvent_t ev0, ev1;
+  CU(cudaEventCreate(&ev0));
+  CU(cudaEventCreate(&ev1));
+  int st = MPDPFT_OK;
+  int k = 0;
+  for (size_t i = 0; i < order.size() && st == MPDPFT_OK; ++i) {
+    cudaGraphNodeType type;
+    if (cudaGraphNodeGetType(order[i], &type) != cudaSuccess) { st = set_error(MPDPFT_ERR_CUDA, "node type"); break; }
+    cudaGraph_t g1 = nullptr;
+    cudaGraphExec_t x1 = nullptr;
+    cudaGraphNode_t n1 = nullptr;
+    cudaError_t e = cudaGraphCreate(&g1, 0);
+    if (e == cudaSuccess && type == cudaGraphNodeTypeKernel) {
+      cudaKernelNodeParams kp;
+      e = cudaGraphKernelNodeGetParams(order[i], &kp);
+      if (e == cudaSuccess) e = cudaGraphAddKernelNode(&n1, g1, nullptr, 0, &kp);
+      if (e == cudaSuccess) e = cudaGraphKernelNodeCopyAttributes(n1, order[i]);
+    } else if (e == cudaSuccess && type == cudaGraphNodeTypeMemset) {
+      cudaMemsetParams mp;
+      e = cudaGraphMemsetNodeGetParams(order[i], &mp);
+      if (e == cudaSuccess) e = cudaGraphAddMemsetNode(&n1, g1, nullptr, 0, &mp);
+    } else if (e == cudaSuccess) {
+      e = cudaErrorNotSupported;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x1, g1, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(ev0, stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(x1, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev1, stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev0, ev1);
+    if (x1) cudaGraphExecDestroy(x1);
+    if (g1) cudaGraphDestroy(g1);
+    if (e != cudaSuccess) { st = set_error(MPDPFT_ERR_CUDA, std::string("iteration profile: ") + cudaGetErrorString(e)); break; }
+    if (k < cap && out) {
+      std::memset(&out[k], 0, sizeof(out[k]));
+      std::strncpy(out[k].name, notes[i].name, sizeof(out[k].name) - 1);
+      out[k].ms = ms;
+      out[k].bytes = notes[i].bytes;
+    }
+    ++k;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (n_out) *n_out = k;
+  if (st) return st;
+  ScState h;
+  if ((st = read_state(&h))) return st;
+  return status_from_state(h);
 }
 
 int Ctx::sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph) {

@@ -34,6 +34,7 @@ struct Ctx {
   int S = 1;
   int ring = 2;
   bool gradient = false;
+  bool need_g2 = false;  // the SC loop's functional reads |grad V|^2
   int has_coulomb = 0;
   double temperature[kMaxS];
   bool initialised = false;
@@ -74,6 +75,18 @@ struct Ctx {
   cudaGraphExec_t graph_exec = nullptr;
   FftPlan* fft = nullptr;
   Adjoint* adj = nullptr;  // adjoint work fields (allocated on first use)
+  // launches of the iteration being captured, in issue order: kernel name
+  // and algorithmic bytes (each input and output field counted once)
+  struct LaunchNote {
+    char name[32];
+    double bytes;
+  };
+  std::vector<LaunchNote> notes;
+  bool noting = false;
+  void note(const char* name, double bytes);
+  double field_bytes() const { return (double)geom.n * (double)rsize; }
+  double spec_bytes() const { return (double)geom.n * (double)rsize * (geom.s + 2) / geom.s; }
+  int iteration_profile(int cap, mpdpft_launch_record* out, int* n_out);
   int mu_max_passes = kMuMaxPasses;     // device loop limits (mpdpft_set_limits)
   long spin_limit = kBarrierSpinLimit;
   int cnt[6] = {0, 0, 0, 0, 0, 0};       // launches issued, by stage

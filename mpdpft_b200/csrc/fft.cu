@@ -102,7 +102,8 @@ enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
 // EPI_COULOMB_V: the Coulomb epilogue followed by the V assembly of one
 // species (k_assemble_v fused into the transform; plane kernels only)
 enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3, EPI_SCALE = 4, EPI_COULOMB_V = 5 };
-enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3 };
+// MUL_LAP: the Laplacian output of MUL_DERIV alone (one output)
+enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3, MUL_LAP = 4 };
 
 template <typename R>
 struct ZArgs {
@@ -578,9 +579,9 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier(const AxisArgs<R>&
     fr = k2 > 0.0 ? (1.0 - cos(sqrt(k2) * a.cutoff)) / k2 : 0.5 * a.cutoff * a.cutoff;
   } else if (a.mul == MUL_SMOOTH) {
     fr = exp(a.sigma_c * k2);
-  } else {  // MUL_DERIV: outputs d/dx, d/dy (, d/dz), Laplacian
+  } else {  // MUL_DERIV: outputs d/dx, d/dy (, d/dz), Laplacian; MUL_LAP: Laplacian
     const double sm = exp(a.sigma_c * k2);
-    if (o < a.dim) {
+    if (a.mul == MUL_DERIV && o < a.dim) {
       // i k_j: the reference takes Im of IFT(-k f~), which drops the
       // Nyquist index of axis j (mpDPFT.cpp:7442-7444)
       double kj;
@@ -628,8 +629,8 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier_tab(const AxisArgs
   const R e = T.ex[t] * T.eyz[l];  // e^{sigma k^2}
   if (a.mul == MUL_SMOOTH) return C{v.x * e * sc, v.y * e * sc};
   // MUL_DERIV: i k_j e^{sigma k^2} (Nyquist of axis j dropped), Laplacian
-  // -k^2 e^{2 sigma k^2}
-  if (o < a.dim) {
+  // -k^2 e^{2 sigma k^2}; MUL_LAP: the Laplacian alone
+  if (a.mul == MUL_DERIV && o < a.dim) {
     R kj;
     if (o == 0) kj = (t == a.s / 2) ? R(0) : kx;
     else if (o == 1 && a.dim == 3) kj = T.ky[l];
@@ -1185,6 +1186,7 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   if (sums) f.zparts = f.zblocks;
   const size_t smem = r2c_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
+  c.note("k_z_r2c", nsrc * c.field_bytes() + c.spec_bytes());
   if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_r2c<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
@@ -1220,6 +1222,7 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   ZArgs<R> a = c2r_args<R>(c, in, nin, epi, out0, out1, coul_coef);
   const size_t smem = c2r_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
+  c.note("k_z_c2r", nin * c.spec_bytes() + ((out0 ? 1 : 0) + (out1 ? 1 : 0)) * c.field_bytes());
   if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
     k_z_c2r<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
@@ -1269,6 +1272,7 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   dim3 grid((unsigned)(a.nbulk + nyq_blocks), nfield);
   const size_t smem = (2 * (size_t)f.s * (f.tk + 1) + f.s) * sizeof(typename Cx<R>::T);
   c.cnt[MPDPFT_STAGE_FFT_Y]++;
+  c.note("k_axis_c2c", 2.0 * nfield * c.spec_bytes());
   if (f.tk != ct_width<R>() || !launch_axis_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
     k_axis_c2c<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
   CU(cudaGetLastError());
@@ -1316,6 +1320,7 @@ static int launch_x_args(Ctx& c, const AxisArgs<R>& a) {
   FftPlan& f = *c.fft;
   const unsigned grid = x_grid<R>(a);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
+  c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
   if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
     k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
   CU(cudaGetLastError());
@@ -1328,6 +1333,7 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   AxisArgs<R> a = x_args<R>(c, in, out, nout, mul, sigma_c);
   const unsigned grid = x_grid<R>(a);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
+  c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
   if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
     k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
   CU(cudaGetLastError());
@@ -1376,6 +1382,7 @@ static int launch_plane_fwd(Ctx& c, const R* in, int pro, void* out, bool sums) 
   a.err = &c.d_state->abort;
   if (sums) f.zparts = f.s;
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
+  c.note("k_plane_fwd", c.field_bytes() + c.spec_bytes());
   plane_dispatch<R>(true, f.s, plane_fwd_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s)), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1414,6 +1421,13 @@ static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, 
     a.vmax_out = f.vmax;
   }
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
+  {
+    // spectra in, outputs out; the fused V assembly also reads V_ext, the
+    // density and the old V and writes V
+    double b = nin * c.spec_bytes() + ((out0 ? 1 : 0) + (out1 ? 1 : 0)) * c.field_bytes();
+    if (epi == EPI_COULOMB_V) b += (3.0 + ((a.contact_self || a.dirac) ? 1.0 : 0.0)) * c.field_bytes();
+    c.note("k_plane_inv", b);
+  }
   plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s), epi == EPI_GRAD), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1453,6 +1467,7 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
 int Ctx::scale_copy(const void* src, void* dst, double a) {
   const int blocks = grid_blocks(geom.n);
   cnt[5]++;
+  note("k_scale_copy", 2.0 * field_bytes());
   if (rsize == sizeof(double)) k_scale_copy<double><<<blocks, kThreads, 0, stream>>>((const double*)src, (double*)dst, geom.n, a);
   else k_scale_copy<float><<<blocks, kThreads, 0, stream>>>((const float*)src, (float*)dst, geom.n, a);
   CU(cudaGetLastError());
@@ -1498,7 +1513,10 @@ static int coulomb_terms(Ctx& c, const R* dens, R* out) {
     }
   }
   for (int s = 0; s < S; ++s)
-    if (!touched[s]) CU(cudaMemsetAsync(out + (long)s * n, 0, sizeof(R) * n, c.stream));
+    if (!touched[s]) {
+      CU(cudaMemsetAsync(out + (long)s * n, 0, sizeof(R) * n, c.stream));
+      c.note("memset", c.field_bytes());
+    }
   return MPDPFT_OK;
 }
 
@@ -1506,6 +1524,7 @@ static int coulomb_terms(Ctx& c, const R* dens, R* out) {
 int Ctx::axpy(const void* x, void* y, double a, int accumulate) {
   const int blocks = grid_blocks(geom.n);
   cnt[5]++;
+  note("k_axpy", (accumulate ? 3.0 : 2.0) * field_bytes());
   if (rsize == sizeof(double)) k_axpy<double><<<blocks, kThreads, 0, stream>>>((const double*)x, (double*)y, geom.n, a, accumulate);
   else k_axpy<float><<<blocks, kThreads, 0, stream>>>((const float*)x, (float*)y, geom.n, a, accumulate);
   CU(cudaGetLastError());
@@ -1513,13 +1532,28 @@ int Ctx::axpy(const void* x, void* y, double a, int accumulate) {
 }
 
 // DelField of species-0 field f (already in compute precision): g2 and lap.
+// want_g2 = false: the Laplacian alone (a density functional without a
+// |grad V|^2 term needs no gradients; g2 is left as it is).
 template <typename R>
-static int delfield_into(Ctx& c, const R* f, R* g2, R* lap) {
+static int delfield_into(Ctx& c, const R* f, R* g2, R* lap, bool want_g2 = true) {
   FftPlan& F = *c.fft;
   int st;
   const double smear = c.P.smearing_extent > 0.0 ? c.P.smearing_extent : 6.0 * c.geom.dx;
   const double sigma_c = -0.5 * smear * smear;  // ConvolutionSigma (mpDPFT.cpp:1106)
   const int pro = c.P.taper_off ? PRO_TAPER : PRO_NONE;
+  if (!want_g2) {  // in place, as the smoothing pass below
+    void* out = F.spec[0];
+    if (F.plane) {
+      if ((st = launch_plane_fwd<R>(c, f, pro, F.spec[0], false))) return st;
+      if ((st = launch_x<R>(c, F.spec[0], &out, 1, MUL_LAP, sigma_c))) return st;
+      return launch_plane_inv<R>(c, &out, 1, EPI_STORE, lap, nullptr, 0.0);
+    }
+    if ((st = launch_z_r2c<R>(c, f, pro, 1, nullptr, F.spec[0], false))) return st;
+    if (F.dim == 3 && (st = launch_y<R>(c, &F.spec[0], 1, -1))) return st;
+    if ((st = launch_x<R>(c, F.spec[0], &out, 1, MUL_LAP, sigma_c))) return st;
+    if (F.dim == 3 && (st = launch_y<R>(c, &out, 1, +1))) return st;
+    return launch_z_c2r<R>(c, &out, 1, EPI_STORE, lap, nullptr, 0.0);
+  }
   if (F.plane) {
     void* outs[4] = {F.spec[0], F.spec[1], F.spec[2], F.spec[3]};
     if ((st = launch_plane_fwd<R>(c, f, pro, F.spec[0], false))) return st;
@@ -1566,6 +1600,7 @@ static int fft_terms_impl(Ctx& c) {
   const bool fuse = F.plane && c.S == 1 && c.has_interaction(MPDPFT_INT_HARTREE) &&
                     !c.has_interaction(MPDPFT_INT_HARTREE_INTER) && !c.has_interaction(MPDPFT_INT_COULOMB_CHARGED);
   CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+  c.note("memset", sizeof(unsigned long long));
   if (fuse) {
     if ((st = coulomb_into<R>(c, dens, 1, nullptr, (R*)c.d_vh, c.P.gamma_h, true))) return st;
     c.assemble_in_step = 0;
@@ -1579,6 +1614,9 @@ static int fft_terms_impl(Ctx& c) {
   KParams kp = c.kparams();
   if (!fuse) {
     c.cnt[5]++;
+    // per species V_ext, the density, the Coulomb term and the old V in,
+    // the new V out
+    c.note("k_assemble_v", c.S * (4.0 + (c.has_coulomb ? 1.0 : 0.0)) * c.field_bytes());
     k_assemble_v<R><<<F.vblocks, kThreads, 0, c.stream>>>(kp, c.d_state, (const R*)c.d_vext,
                                                            c.has_coulomb ? (const R*)c.d_vh : nullptr,
                                                            (const R*)c.d_nin, (R*)c.d_V, F.vres_part, F.vmax,
@@ -1592,13 +1630,15 @@ static int fft_terms_impl(Ctx& c) {
     for (int s = 0; s < c.S; ++s) {
       if (s > 0) {  // taper shift of species s
         CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
+        c.note("memset", sizeof(unsigned long long));
         c.cnt[5]++;
+        c.note("k_shell_max", c.field_bytes());
         k_shell_max<R><<<grid_blocks(n), kThreads, 0, c.stream>>>(c.geom, (const R*)c.d_V + (long)s * n, F.vmax,
                                                                   shell_radius(c), shell_width(c));
         CU(cudaGetLastError());
       }
       if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
-                                 (R*)c.d_lap + (long)s * n)))
+                                 (R*)c.d_lap + (long)s * n, c.need_g2)))
         return st;
     }
   }
@@ -1646,7 +1686,8 @@ static int delfield_of_v_impl(Ctx& c) {
     k_shell_max<R><<<grid_blocks(n), kThreads, 0, c.stream>>>(c.geom, (const R*)c.d_V + (long)s * n, F.vmax,
                                                               shell_radius(c), shell_width(c));
     CU(cudaGetLastError());
-    if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n, (R*)c.d_lap + (long)s * n)))
+    if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n, (R*)c.d_lap + (long)s * n,
+                               c.need_g2)))
       return st;
   }
   return MPDPFT_OK;
@@ -1663,9 +1704,12 @@ int Ctx::op_delfield(const double* f, double* grad2, double* lap, int layout, in
   void* V0 = d_V;  // species 0 slot is used as staging
   if ((st = import_field(f, V0, layout, mem))) return st;
   const int S_save = S;
+  const bool g2_save = need_g2;
   S = 1;
+  need_g2 = true;  // the caller asks for |grad f|^2 as well
   st = issue_delfield_of_V();
   S = S_save;
+  need_g2 = g2_save;
   if (st) return st;
   if (grad2 && (st = export_field(d_g2, grad2, layout, mem))) return st;
   if (lap && (st = export_field(d_lap, lap, layout, mem))) return st;
@@ -2181,7 +2225,7 @@ static int tune_transforms(Ctx& c) {
     for (int s = 0; s < c.S; ++s) {
       CU(cudaMemsetAsync(F.vmax, 0, sizeof(unsigned long long), c.stream));
       if ((st = delfield_into<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
-                                 (R*)c.d_lap + (long)s * n)))
+                                 (R*)c.d_lap + (long)s * n, c.need_g2)))
         return st;
     }
   return MPDPFT_OK;

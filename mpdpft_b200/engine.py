@@ -32,7 +32,7 @@ EXPORTS = [
     "mpdpft_batch_create", "mpdpft_batch_destroy", "mpdpft_batch_set_external_potential", "mpdpft_batch_sc_init",
     "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
     "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei", "mpdpft_fft_config",
-    "mpdpft_set_limits", "mpdpft_integrate_noalloc",
+    "mpdpft_set_limits", "mpdpft_integrate_noalloc", "mpdpft_iteration_profile",
 ]
 
 
@@ -69,6 +69,7 @@ def load(path=LIB_PATH):
     L.mpdpft_ctx_stream.argtypes = [vp]
     L.mpdpft_ctx_stream.restype = vp
     L.mpdpft_set_limits.argtypes = [vp, C.c_int, C.c_longlong]
+    L.mpdpft_iteration_profile.argtypes = [vp, C.c_int, C.POINTER(abi.LaunchRecord), C.POINTER(C.c_int)]
     L.mpdpft_set_external_potential.argtypes = [vp, C.c_int, _dp, C.c_int, C.c_int]
     L.mpdpft_density.argtypes = [vp, C.c_int, _dp, C.c_double, _dp, _dp, C.c_int, C.c_int]
     L.mpdpft_vint.argtypes = [vp, C.c_int, C.c_int, _dpp, _dp, C.c_int, C.c_int]
@@ -306,6 +307,14 @@ class Engine:
     def stage_launch_counts(self):
         c, _ = self._launches()
         return {"sc_step": c[0], "z_r2c": c[1], "y": c[2], "x": c[3], "z_c2r": c[4], "other": c[5]}
+
+    def iteration_profile(self, cap=256):
+        """One SC iteration replayed launch by launch from its CUDA graph:
+        [(kernel name, ms, algorithmic bytes)] in issue order."""
+        recs = (abi.LaunchRecord * cap)()
+        n = C.c_int()
+        self._check(self.lib.mpdpft_iteration_profile(self.h, cap, recs, C.byref(n)))
+        return [(r.name.decode(), r.ms, r.bytes) for r in recs[:min(n.value, cap)]]
 
     def step_phase_times(self):
         """Phase durations (us) of the last SC-step kernel: V update, mu

@@ -22,6 +22,12 @@ from . import abi
 
 SEED_BASE = 20261203
 
+# The 3D gradient-corrected density with a second-order |grad V|^2 term and
+# its singular factors floored at mu - V = 0.5 hartree: a regularised form of
+# the reference's small-gradient branch (which has neither), kept for the
+# workloads whose SC loop does not converge without it on their grids.
+REGULARISED_GRADIENT = dict(gradient_floor=0.5, gradient_grad2=1.0)
+
 
 def axis(steps, edge):
     """Periodic-grid coordinates along one axis (rGrid, mpDPFT.cpp:7130)."""
@@ -97,19 +103,22 @@ def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **
     """Neutral atom Z = 18: Gaussian nucleus (sigma 0.1 bohr) at the centre of
     [-10, 10]^3, TF + gradient correction (spectral grad V and Laplacian,
     each smoothed by a Gaussian of width 0.2 bohr), Hartree by FFT Poisson,
-    Dirac exchange, g = 2, atomic units (gammaH = 1).  The gradient
-    terms' singular factors are floored at mu - V = 0.5 hartree, the order of the
-    Airy energy 1/2 |grad V|^{2/3} below which the small-gradient expansion
-    fails (the reference switches to its Airy branch there).  The start mu = -30
-    lies within the reference's 20 bracket steps of the bare-nucleus root
-    (the first density is computed in V_ext alone)."""
+    Dirac exchange, g = 2, atomic units (gammaH = 1).  The density is the
+    reference's small-gradient branch (mpDPFT.cpp:3376-3388) in its T -> 0
+    form, n = g (2u)^{3/2}/(6 pi^2) - g lap V (2u)^{-1/2}/(24 pi^2),
+    u = mu - V, clamped at 0, with no |grad V|^2 term; the factor u^{-1/2}
+    is continued linearly below u = 1e-3 hartree (a floor for the singular
+    point at the classical turning surface).  Converges from 40^3 up (24 SC
+    iterations at 128^3).  The start mu = -30 lies within the reference's 20
+    bracket steps of the bare-nucleus root (the first density is computed
+    in V_ext alone)."""
     z = 18.0
     kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z],
               rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
               interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
               mu=[-30.0], mixer=1, pulay_scope=5, theta=[0.5], sc_criterion=1e-8,
               max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
-              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0,
+              gradient_floor=1e-3, gradient_grad2=0.0, potential_tol=0.0,
               precision=precision)
     kw.update(over)
     p = abi.make_params(**kw)
@@ -145,9 +154,12 @@ def cluster_adjoint(steps=192, edge=32.0, precision=abi.MIXED, sites=13, spacing
                     seed=SEED_BASE + 4, **over):
     """Icosahedral cluster of Gaussian Z = 3 nuclei (sigma 0.1 bohr; centre
     plus 12 vertices at 5.5 bohr, positions jittered by N(0, 0.05^2)) on
-    [-16, 16]^3, the functional of argon_atom (TF + gradient correction,
-    smoothing 0.2, Hartree, Dirac, g = 2), N = 3 per nucleus.  Returns
-    (params, [V_ext], [V_0], nuclei) with nuclei = dict(z, pos, sigma)."""
+    [-16, 16]^3, TF + gradient correction (smoothing 0.2), Hartree, Dirac,
+    g = 2, N = 3 per nucleus.  The gradient form is REGULARISED_GRADIENT:
+    with the reference's small-gradient branch (as argon_atom) the 192^3
+    loop needs 111 SC iterations instead of 50, and the adjoint tests were
+    calibrated on this form.  Returns (params, [V_ext], [V_0], nuclei) with
+    nuclei = dict(z, pos, sigma)."""
     z, sigma = 3.0, 0.1
     pos = icosahedral_cluster(sites, spacing, jitter, seed)
     kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z * sites],
@@ -155,7 +167,7 @@ def cluster_adjoint(steps=192, edge=32.0, precision=abi.MIXED, sites=13, spacing
               interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
               mu=[-5.0], mixer=1, pulay_scope=5, theta=[0.5], sc_criterion=1e-8,
               max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
-              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0,
+              potential_tol=0.0, **REGULARISED_GRADIENT,
               precision=precision)
     kw.update(over)
     p = abi.make_params(**kw)
@@ -186,13 +198,16 @@ def electron_hole(steps=256, edge=40.0, precision=abi.MIXED, seed=SEED_BASE + 5,
     box [-20, 20]^3 with a smooth random external potential (64 Gaussians),
     gradient-corrected TF density (smoothing 0.3), Coulomb coupling of the
     charge density (type 100: V_s = q_s V_H[sum q n]), Pulay history 8 with
-    the annealed damping of schedule 5; V_0 = V_ext + U(-1e-3, 1e-3)."""
+    the annealed damping of schedule 5; V_0 = V_ext + U(-1e-3, 1e-3).  The
+    gradient form is REGULARISED_GRADIENT: with the reference's
+    small-gradient branch the 256^3 loop needs 142 (FP64) and 252 (mixed) SC
+    iterations instead of 19."""
     kw = dict(dim=3, steps=steps, species=2, edge=edge, abundances=[20000.0, 20000.0],
               rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
               interactions=[abi.INT_COULOMB_CHARGED], gamma_h=1.0, charges=[-1.0, 1.0],
               mu=[2.0, 2.0], mixer=1, pulay_scope=8, theta=[0.3, 0.3], schedule=5,
               sc_criterion=1e-8, max_sc_count=300, smearing_extent=0.3, regularization_threshold=0.45,
-              gradient_floor=0.5, gradient_grad2=1.0, potential_tol=0.0, precision=precision)
+              potential_tol=0.0, precision=precision, **REGULARISED_GRADIENT)
     kw.update(over)
     p = abi.make_params(**kw)
     vext = gaussian_landscape(steps, edge, 64, seed)

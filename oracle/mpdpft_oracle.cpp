@@ -1144,4 +1144,13 @@ int oracle_num_threads(void) {
 #endif
 }
 
+// OpenMP threads of later oracle calls (<= 0: all host threads).
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+#else
+  (void)n;
+#endif
+}
+
 }  // extern "C"

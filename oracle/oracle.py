@@ -50,6 +50,8 @@ def lib():
         L.oracle_pulay_sequence.argtypes = [P, C.c_int, _dp, _dp, _dp, _dp,
                                             C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.oracle_num_threads.restype = C.c_int
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_set_threads.restype = None
         _lib = L
     return _lib
 
@@ -68,6 +70,11 @@ def _per(p, f):
 
 def num_threads():
     return lib().oracle_num_threads()
+
+
+def set_threads(n):
+    """OpenMP threads of later oracle calls (0: all host threads)."""
+    lib().oracle_set_threads(int(n))
 
 
 def fft(p, field, sign):
@@ -175,3 +182,11 @@ def pulay_sequence(p, nin_seq, nout_seq):
                                 C.byref(nc), used)
     out = [[_per(p, mixed[(t * S + q) * G:(t * S + q + 1) * G]) for q in range(S)] for t in range(T)]
     return out, coeffs[:nc.value].copy(), list(used)
+
+
+def block_sums(f, steps, dim, blocks=16):
+    """Sums of a periodic s^D field over blocks^D equal coarse blocks
+    (steps divisible by blocks), flattened in x-major order."""
+    b = steps // blocks
+    g = np.asarray(f, dtype=np.float64).reshape((blocks, b) * dim)
+    return g.sum(axis=tuple(range(1, 2 * dim, 2))).reshape(-1)

@@ -1,0 +1,146 @@
+"""Parity at the configurations' own sizes: converged GPU solves against the
+converged FP64 oracle, with the errors each configuration states.
+
+  C1  harmonic_tf at 64^3: TF + contact, CC < 1e-12 three times and
+      potential residual <= 1e-8 (FP64; mixed to CC < 1e-10)
+  C2  argon_atom at 128^3: the reference's small-gradient density branch,
+      Hartree, Dirac exchange (FP64 and mixed)
+  C4  cluster_adjoint at 192^3 and C5 electron_hole at 256^3: against
+      committed oracle fixtures (tests/golden/make_config_fixtures.py runs
+      the oracle once; the fixtures hold the energy, mu, N, the iteration
+      count and the density and potential integrated over 16^3 coarse
+      blocks, so the coarse L1 error below is a lower bound of the full one)
+
+Targets (stated per precision): relative energy <= 1e-6 (FP64) and <= 1e-5
+(mixed), L1 density error <= 1e-5 per particle.  Each test prints its
+errors, the potential's max and rms error among them.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mpdpft_b200 import abi
+from mpdpft_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TARGET = {abi.FP64: (1e-6, 1e-5), abi.MIXED: (1e-5, 1e-5)}
+NAME = {abi.FP64: "fp64", abi.MIXED: "mixed"}
+
+
+def errors(p, res, dens, pot, res_r, dens_r, pot_r):
+    """dE/E, L1/N per species (max), potential max and rms error (max over
+    species), |dmu|."""
+    dvol = (p.edge / p.steps) ** p.dim
+    l1 = max(np.abs(dens[s] - dens_r[s]).sum() * dvol / p.abundances[s] for s in range(p.species))
+    vmax = max(np.abs(pot[s] - pot_r[s]).max() for s in range(p.species))
+    vrms = max(np.sqrt(np.mean((pot[s] - pot_r[s]) ** 2)) for s in range(p.species))
+    de = abs(res.e_total - res_r.e_total) / abs(res_r.e_total)
+    dmu = max(abs(res.mu[s] - res_r.mu[s]) for s in range(p.species))
+    return de, l1, vmax, vrms, dmu
+
+
+def gpu_solve(eng, p, vext, v0):
+    with eng.Engine(p) as e:
+        res, log, st = e.sc_run(vext, v0)
+        dens = [e.field(abi.FIELD_DENSITY, s) for s in range(p.species)]
+        pot = [e.field(abi.FIELD_POTENTIAL, s) for s in range(p.species)]
+    return res, dens, pot
+
+
+_oracle_cache = {}
+
+
+def oracle_solve(oracle_lib, key, p, vext, v0):
+    if key not in _oracle_cache:
+        res_r, log_r, dens_r, pot_r = oracle_lib.sc_run(p, vext, v0)
+        _oracle_cache[key] = (res_r, dens_r, pot_r)
+    return _oracle_cache[key]
+
+
+@pytest.mark.parametrize("prec", [abi.FP64, abi.MIXED])
+def test_c1_harmonic_64(eng, oracle_lib, prec):
+    over = dict(potential_tol=1e-8, sc_criterion=1e-12) if prec == abi.FP64 else \
+        dict(potential_tol=0.0, sc_criterion=1e-10)
+    p, vext, v0 = W.harmonic_tf(steps=64, precision=prec, **over)
+    pr, _, _ = W.harmonic_tf(steps=64, precision=abi.FP64)
+    res, dens, pot = gpu_solve(eng, p, vext, v0)
+    res_r, dens_r, pot_r = oracle_solve(oracle_lib, "c1", pr, vext, v0)
+    de, l1, vmax, vrms, dmu = errors(p, res, dens, pot, res_r, dens_r, pot_r)
+    print("C1 harmonic_tf 64^3 %s: iterations %d (oracle %d), dE/E %.2e, L1/N %.2e, |dV| max %.2e rms %.2e, "
+          "|dmu| %.2e, CC %.1e, r_V %.1e" % (NAME[prec], res.iterations, res_r.iterations, de, l1, vmax, vrms, dmu,
+                                             res.cc, res.v_residual))
+    assert res.converged == 1 and res_r.converged == 1
+    if prec == abi.FP64:
+        assert res.v_residual <= 1e-8 and res_r.v_residual <= 1e-8
+        assert abs(res.iterations - res_r.iterations) <= 3
+    e_tol, n_tol = TARGET[prec]
+    assert de <= e_tol
+    assert l1 <= n_tol
+    assert abs(res.abundance[0] - 1000.0) <= 2e-10 * 1000.0 * (1 if prec == abi.FP64 else 10)
+
+
+@pytest.mark.parametrize("prec", [abi.FP64, abi.MIXED])
+def test_c2_argon_128(eng, oracle_lib, prec):
+    p, vext, v0 = W.argon_atom(steps=128, precision=prec)
+    pr, _, _ = W.argon_atom(steps=128, precision=abi.FP64)
+    res, dens, pot = gpu_solve(eng, p, vext, v0)
+    res_r, dens_r, pot_r = oracle_solve(oracle_lib, "c2", pr, vext, v0)
+    de, l1, vmax, vrms, dmu = errors(p, res, dens, pot, res_r, dens_r, pot_r)
+    print("C2 argon_atom 128^3 %s: iterations %d (oracle %d), dE/E %.2e, L1/N %.2e, |dV| max %.2e rms %.2e, "
+          "|dmu| %.2e" % (NAME[prec], res.iterations, res_r.iterations, de, l1, vmax, vrms, dmu))
+    assert res.converged == 1 and res_r.converged == 1
+    e_tol, n_tol = TARGET[prec]
+    assert de <= e_tol
+    assert l1 <= n_tol
+    assert abs(res.abundance[0] - 18.0) <= 2e-9 * 18.0
+
+
+def _fixture(name):
+    path = os.path.join(GOLDEN, "config_%s.npz" % name)
+    if not os.path.exists(path):
+        pytest.skip("fixture %s not generated" % path)
+    return dict(np.load(path))
+
+
+def block_integrals(f, steps, dim, dvol, blocks=16):
+    from oracle import oracle
+    return oracle.block_sums(f, steps, dim, blocks) * dvol
+
+
+def block_means(f, steps, dim, blocks=16):
+    from oracle import oracle
+    b = steps // blocks
+    return oracle.block_sums(f, steps, dim, blocks) / float(b ** dim)
+
+
+def check_against_fixture(eng, name, p, vext, v0, prec, fx):
+    res, dens, pot = gpu_solve(eng, p, vext, v0)
+    dvol = (p.edge / p.steps) ** p.dim
+    de = abs(res.e_total - float(fx["e_total"])) / abs(float(fx["e_total"]))
+    l1 = max(np.abs(block_integrals(dens[s], p.steps, p.dim, dvol) - fx["dens_blocks"][s]).sum() / p.abundances[s]
+             for s in range(p.species))
+    dv = max(np.abs(block_means(pot[s], p.steps, p.dim) - fx["pot_blocks"][s]).max() for s in range(p.species))
+    dmu = max(abs(res.mu[s] - float(fx["mu"][s])) for s in range(p.species))
+    print("%s %s: iterations %d (oracle %d), dE/E %.2e, coarse L1/N %.2e, coarse |dV| max %.2e, |dmu| %.2e" %
+          (name, NAME[prec], res.iterations, int(fx["iterations"]), de, l1, dv, dmu))
+    assert res.converged == 1 and int(fx["converged"]) == 1
+    e_tol, n_tol = TARGET[prec]
+    assert de <= e_tol
+    assert l1 <= n_tol
+
+
+@pytest.mark.parametrize("prec", [abi.FP64, abi.MIXED])
+def test_c4_cluster_192_against_oracle_fixture(eng, prec):
+    fx = _fixture("cluster_adjoint_192")
+    p, vext, v0, nuc = W.cluster_adjoint(steps=192, precision=prec)
+    check_against_fixture(eng, "C4 cluster_adjoint 192^3", p, vext, v0, prec, fx)
+
+
+@pytest.mark.parametrize("prec", [abi.FP64, abi.MIXED])
+def test_c5_electron_hole_256_against_oracle_fixture(eng, prec):
+    fx = _fixture("electron_hole_256")
+    p, vext, v0 = W.electron_hole(steps=256, precision=prec)
+    check_against_fixture(eng, "C5 electron_hole 256^3", p, vext, v0, prec, fx)

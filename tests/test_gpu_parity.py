@@ -199,9 +199,11 @@ TRAJ_TOL = {abi.FP64: {0: 1e-9, 1: 1e-9, 6: 1e-7, 20: 1e-5},
 @pytest.mark.parametrize("prec", [abi.FP64, abi.MIXED])
 def test_sc_argon_trajectory(eng, oracle_lib, prec, iters):
     """SC loop with Hartree, Dirac and the gradient-corrected density
-    (config argon_atom at 32^3) against the oracle after a fixed number of
+    (argon_atom at 32^3 with the regularised gradient form, on which these
+    drift bounds were measured) against the oracle after a fixed number of
     iterations (maxSCcount exit)."""
-    p, vext, v0 = W.argon_atom(steps=32, precision=prec, max_sc_count=iters, sc_criterion=-1.0)
+    p, vext, v0 = W.argon_atom(steps=32, precision=prec, max_sc_count=iters, sc_criterion=-1.0,
+                               **W.REGULARISED_GRADIENT)
     with eng.Engine(p) as e:
         res, log, st = e.sc_run(vext, v0)
         dens = e.field(abi.FIELD_DENSITY, 0)

@@ -86,7 +86,7 @@ def test_noalloc_riemann_matches_oracle_reference_layout():
     (3, 64, abi.LAYOUT_PERIODIC),
     (3, 48, abi.LAYOUT_REFERENCE),
     (2, 256, abi.LAYOUT_PERIODIC),
-    (2, 200, abi.LAYOUT_REFERENCE),
+    (2, 192, abi.LAYOUT_REFERENCE),
     (3, 256, abi.LAYOUT_PERIODIC),
     (3, 256, abi.LAYOUT_REFERENCE),
 ])
