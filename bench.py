@@ -591,7 +591,7 @@ def adjoint_cluster(device, max_iter=60):
 def end_to_end(sg, device, prec, solves=2):
     """Full solves through the C ABI with host arrays: V_ext and V_0 copied
     in, the density copied out; iterations / wall time."""
-    from mpdpft_b200 import engine, workloads as W
+    from mpdpft_b200 import abi, engine, workloads as W
     p, vext, v0 = W.argon_atom(steps=sg, precision=prec)
     with engine.Engine(p, device=device) as e:
         e.sc_run(vext, v0)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MPDPFT_ABI_VERSION 1
+#define MPDPFT_ABI_VERSION 2
 #define MPDPFT_MAX_SPECIES 4
 #define MPDPFT_MAX_INTERACTIONS 8
 #define MPDPFT_MAX_PULAY 12
@@ -126,7 +126,23 @@ typedef struct {
                                Wigner-Kirkwood)                                    */
   double potential_tol;     /* extra exit test: rms(V_new - V_old) <= tol (0: off)  */
   int precision;            /* MPDPFT_FP64 or MPDPFT_MIXED                          */
+  /* MPDPFT_DENS_GRADIENT in 3D (ABI version 2) */
+  int gradient_form;        /* MPDPFT_GRADIENT_T0 or MPDPFT_GRADIENT_FINITE_T       */
+  double airy_threshold;    /* line 17 Mpp[2]: Airy-averaged branch where
+                               ar = |grad V|^{2/3}/2 >= threshold (finite-T form
+                               only; <= 0: never)                                    */
+  int boole_pairs;          /* line 17 Mpp[0]: Boole pairs per half interval       */
+  int boole_max_iter;       /* line 17 Mpp[1]: bisection depth of the Airy integral */
+  double internal_acc;      /* line 12 InternalAcc: relative accuracy of the Airy
+                               integral (RTPNA)                                     */
 } mpdpft_params;
+
+/* 3D forms of MPDPFT_DENS_GRADIENT. */
+enum {
+  MPDPFT_GRADIENT_T0 = 0,       /* closed T -> 0 form (gradient_floor, gradient_grad2) */
+  MPDPFT_GRADIENT_FINITE_T = 1  /* the reference's finite-T Fermi-Dirac form with the
+                                   Airy-averaged branch, mpDPFT.cpp:3363-3453       */
+};
 
 /* Per-iteration record of mpdpft_sc_run (the reference prints SCcount, CC,
  * mu and abundances per iteration, mpDPFT.cpp:4862). */
@@ -167,8 +183,9 @@ typedef struct mpdpft_batch mpdpft_batch;
 void mpdpft_params_default(mpdpft_params* p);
 
 int mpdpft_abi_version(void);
-/* sizeof(mpdpft_params), sizeof(mpdpft_result), sizeof(mpdpft_iter_log) for
- * which = 0, 1, 2 (binding checks); 0 for any other value. */
+/* sizeof(mpdpft_params), sizeof(mpdpft_result), sizeof(mpdpft_iter_log),
+ * sizeof(mpdpft_input), sizeof(mpdpft_launch_record) for which = 0 .. 4
+ * (binding checks); 0 for any other value. */
 size_t mpdpft_struct_size(int which);
 const char* mpdpft_last_error(void);
 const char* mpdpft_status_string(int status);
@@ -374,6 +391,106 @@ int mpdpft_adjoint(mpdpft_ctx* ctx, const double* dl_dn, double* dl_dvext, int l
 int mpdpft_adjoint_nuclei(mpdpft_ctx* ctx, const double* dl_dvext, int mem, int n_nuclei,
                           const double* charges, const double* positions, double sigma,
                           double* dl_dpositions);
+
+/* ---------------------------------------------------------------------
+ * The reference's files.
+ *
+ * mpDPFT.input: 47 lines, one parameter (or vector) per line in a fixed
+ * order, anything after the values ignored (GetInputParameters,
+ * mpDPFT.cpp:633-690).  Lines are numbered from 0, as the parser's cases
+ * (and the line numbers of mpdpft_params) are.  mpdpft_read_input parses it into mpdpft_input,
+ * field by field and in the file's units; mpdpft_params_from_input maps it
+ * onto the engine's parameters and rejects (MPDPFT_ERR_ARG, naming the line)
+ * options the engine does not implement.  The input's Symmetry is accepted
+ * whatever its value: the engine always computes the whole grid.
+ */
+#define MPDPFT_INPUT_MAX_VEC 16
+typedef struct {
+  int system;                    /* line 0  System                               */
+  int symmetry;                  /* line 1  Symmetry                             */
+  int task_type;                 /* line 2  TaskType                             */
+  int task_parameter_count;      /* line 3  TaskParameterCount                   */
+  int n_task_hyperbox;           /* line 4  TaskHyperBox (values read)           */
+  double task_hyperbox[MPDPFT_INPUT_MAX_VEC];
+  int dim;                       /* line 5  DIM                                  */
+  int units;                     /* line 6  Units: 1 HO / atomic, 2 eV-Angstrom  */
+  double edge;                   /* line 7  edge                                 */
+  int steps;                     /* line 8  steps                                */
+  int species;                   /* line 9 S                                    */
+  double abundances[MPDPFT_MAX_SPECIES]; /* line 10                              */
+  double rel_acc;                /* line 11 RelAcc                               */
+  double internal_acc;           /* line 12 InternalAcc                          */
+  int k_resources;               /* line 13 K                                    */
+  int density_expression;        /* line 15 DensityExpression                    */
+  int n_mpp;                     /* line 16 mpp (environment parameters)         */
+  double mpp[MPDPFT_INPUT_MAX_VEC];
+  int n_Mpp;                     /* line 17 Mpp (density parameters)             */
+  double Mpp[MPDPFT_INPUT_MAX_VEC];
+  double tau[MPDPFT_MAX_SPECIES];          /* line 18 tauVec                     */
+  double territory[MPDPFT_MAX_SPECIES];    /* line 19 tVec                       */
+  double temperature[MPDPFT_MAX_SPECIES];  /* line 20 TVec                       */
+  int environments[MPDPFT_MAX_SPECIES];    /* line 21 Environments               */
+  double stretchfactor;          /* line 22                                      */
+  double wall;                   /* line 23 Wall                                 */
+  double noise;                  /* line 24 Noise                                */
+  int interpol_vq;               /* line 25 InterpolVQ                           */
+  int n_interactions;            /* line 26 Interactions                         */
+  int interactions[MPDPFT_INPUT_MAX_VEC];
+  double incremental_v;          /* line 27 incrementalV                         */
+  double mu[MPDPFT_MAX_SPECIES]; /* line 28 muVec                                */
+  double deltamu_modifier;       /* line 29 DeltamuModifier                      */
+  double mixer[3];               /* line 30 Mixer: mode, scope, metric weight    */
+  double theta[MPDPFT_MAX_SPECIES]; /* line 31 thetaVec                          */
+  double sc_criterion;           /* line 32 SCcriterion                          */
+  int max_sc_count;              /* line 33 maxSCcount                           */
+  int method;                    /* line 34 integration method                   */
+  int delfield_method;           /* line 35 DelFieldMethod                       */
+  int movie;                     /* line 36 MovieQ                               */
+  int n_schedule;                /* line 37 Schedule                             */
+  int schedule[MPDPFT_INPUT_MAX_VEC];
+  int n_ekin_types;              /* line 38 EkinTypes                            */
+  int ekin_types[MPDPFT_INPUT_MAX_VEC];
+  double alpha, beta, gamma, gamma_h; /* lines 39-42                             */
+  double degeneracy;             /* line 43                                      */
+  int n_regularize;              /* line 44 regularize                           */
+  int regularize[MPDPFT_INPUT_MAX_VEC];
+  double regularization_threshold; /* line 45                                    */
+  int print;                     /* line 46 Print                                */
+  int lines;                     /* lines read                                   */
+} mpdpft_input;
+
+/* Parse an mpDPFT.input file (the reference's line order; lines 0-46
+ * above).  MPDPFT_ERR_ARG names the file or the first line that does not
+ * parse. */
+int mpdpft_read_input(const char* path, mpdpft_input* out);
+/* Engine parameters of a parsed input: reference defaults
+ * (mpdpft_params_default) overridden by every line the engine uses.
+ * Rejected with MPDPFT_ERR_ARG (the message names the line): Units other
+ * than 1, DensityExpression other than 1, 2, 5, 7, interaction types the
+ * engine lacks, Mixer mode 2, integration method other than 1 (Riemann),
+ * DelFieldMethod other than 5 with DensityExpression 5, more than one
+ * Schedule entry or one other than 0, 5, 9, and S above
+ * MPDPFT_MAX_SPECIES.  DensityExpression 5 in 3D maps to the finite-T form
+ * with the Airy branch (Mpp = BoolePairs, maxIter, threshold). */
+int mpdpft_params_from_input(const mpdpft_input* in, mpdpft_params* out);
+
+/* Write the context's current potentials and densities in the reference's
+ * text formats (ExportData, mpDPFT.cpp:12492-12519): mpDPFT_V.dat has one
+ * line per point of the (s+1)^D storage, x-major, with the D coordinates
+ * and then V of every species; mpDPFT_Den.dat one line per point with the
+ * densities of every species.  16 significant digits.  Either path may be
+ * NULL (not written). */
+int mpdpft_write_field_files(mpdpft_ctx* ctx, const char* v_path, const char* den_path);
+
+/* Start potentials from an mpDPFT_V.dat of any grid (the InterpolVQ = 1
+ * restart, LoadV mpDPFT.cpp:6445-6499): the file's n^D points (x-major,
+ * D coordinates then S values per line) are interpolated trilinearly (2D:
+ * bilinearly) onto this context's grid on the GPU, the outermost cells
+ * continued linearly beyond the file's box, and written to v_out[s] (the
+ * caller passes them to mpdpft_sc_run as v0).  *n_file receives n.  The
+ * file's species count must equal the context's. */
+int mpdpft_interpolate_v_file(mpdpft_ctx* ctx, const char* path, double* const* v_out, int layout, int mem,
+                              int* n_file);
 
 /* Batch: many independent SC solves advanced together on one GPU (a
  * parameter sweep, the reference's TaskType 5/6/7 loops of GetData,

@@ -1,4 +1,4 @@
-"""ctypes mirror of include/mpdpft_gpu.h (ABI version 1).
+"""ctypes mirror of include/mpdpft_gpu.h (ABI version 2).
 
 Only declarations live here: the parameter, result and log structs, the
 status codes and the enum values.  ``mpdpft_b200.engine`` binds the CUDA
@@ -6,7 +6,7 @@ library against these declarations.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_SPECIES = 4
 MAX_INTERACTIONS = 8
 MAX_PULAY = 12
@@ -43,6 +43,9 @@ INT_COULOMB_CHARGED = 100
 
 COULOMB_REGULARISED = 0
 COULOMB_TRUNCATED = 1
+
+GRADIENT_T0 = 0
+GRADIENT_FINITE_T = 1
 
 FIELD_DENSITY = 0
 FIELD_POTENTIAL = 1
@@ -100,6 +103,11 @@ class Params(C.Structure):
         ("gradient_grad2", C.c_double),
         ("potential_tol", C.c_double),
         ("precision", C.c_int),
+        ("gradient_form", C.c_int),
+        ("airy_threshold", C.c_double),
+        ("boole_pairs", C.c_int),
+        ("boole_max_iter", C.c_int),
+        ("internal_acc", C.c_double),
     ]
 
     def grid_points(self, layout=LAYOUT_PERIODIC):
@@ -141,6 +149,33 @@ class Result(C.Structure):
         ("e_external", _D4),
         ("e_interaction", C.c_double * MAX_INTERACTIONS),
         ("seconds", C.c_double),
+    ]
+
+
+INPUT_MAX_VEC = 16
+_DV = C.c_double * INPUT_MAX_VEC
+_IV = C.c_int * INPUT_MAX_VEC
+
+
+class Input(C.Structure):
+    """mpdpft_input: the 47 lines of mpDPFT.input (numbered from 0)."""
+    _fields_ = [
+        ("system", C.c_int), ("symmetry", C.c_int), ("task_type", C.c_int), ("task_parameter_count", C.c_int),
+        ("n_task_hyperbox", C.c_int), ("task_hyperbox", _DV),
+        ("dim", C.c_int), ("units", C.c_int), ("edge", C.c_double), ("steps", C.c_int), ("species", C.c_int),
+        ("abundances", _D4), ("rel_acc", C.c_double), ("internal_acc", C.c_double), ("k_resources", C.c_int),
+        ("density_expression", C.c_int),
+        ("n_mpp", C.c_int), ("mpp", _DV), ("n_Mpp", C.c_int), ("Mpp", _DV),
+        ("tau", _D4), ("territory", _D4), ("temperature", _D4), ("environments", C.c_int * MAX_SPECIES),
+        ("stretchfactor", C.c_double), ("wall", C.c_double), ("noise", C.c_double), ("interpol_vq", C.c_int),
+        ("n_interactions", C.c_int), ("interactions", _IV),
+        ("incremental_v", C.c_double), ("mu", _D4), ("deltamu_modifier", C.c_double), ("mixer", C.c_double * 3),
+        ("theta", _D4), ("sc_criterion", C.c_double), ("max_sc_count", C.c_int), ("method", C.c_int),
+        ("delfield_method", C.c_int), ("movie", C.c_int),
+        ("n_schedule", C.c_int), ("schedule", _IV), ("n_ekin_types", C.c_int), ("ekin_types", _IV),
+        ("alpha", C.c_double), ("beta", C.c_double), ("gamma", C.c_double), ("gamma_h", C.c_double),
+        ("degeneracy", C.c_double), ("n_regularize", C.c_int), ("regularize", _IV),
+        ("regularization_threshold", C.c_double), ("print", C.c_int), ("lines", C.c_int),
     ]
 
 
@@ -193,6 +228,11 @@ def make_params(**kw):
     p.gradient_grad2 = 0.0
     p.potential_tol = 0.0
     p.precision = FP64
+    p.gradient_form = GRADIENT_T0
+    p.airy_threshold = 1.0e-6
+    p.boole_pairs = 1
+    p.boole_max_iter = 1
+    p.internal_acc = 0.01
     for key, val in kw.items():
         if key == "interactions":
             p.n_interactions = len(val)

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmpdpft_b200.so")
-SOURCES = ["engine.cu", "fft.cu", "capi.cu", "noalloc.cu", "batch.cu", "adjoint.cu"]
+SOURCES = ["engine.cu", "fft.cu", "capi.cu", "noalloc.cu", "batch.cu", "adjoint.cu", "refio.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

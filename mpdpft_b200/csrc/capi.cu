@@ -47,6 +47,12 @@ void mpdpft_params_default(mpdpft_params* p) {
   p->coulomb_kernel = MPDPFT_COULOMB_REGULARISED;
   p->gradient_floor = 1.0e-3;
   p->precision = MPDPFT_FP64;
+  // mpDPFT.input sample: Mpp 1 1 1e-6, InternalAcc 0.01
+  p->gradient_form = MPDPFT_GRADIENT_T0;
+  p->airy_threshold = 1.0e-6;
+  p->boole_pairs = 1;
+  p->boole_max_iter = 1;
+  p->internal_acc = 0.01;
 }
 
 int mpdpft_abi_version(void) { return MPDPFT_ABI_VERSION; }
@@ -56,6 +62,8 @@ size_t mpdpft_struct_size(int which) {
     case 0: return sizeof(mpdpft_params);
     case 1: return sizeof(mpdpft_result);
     case 2: return sizeof(mpdpft_iter_log);
+    case 3: return sizeof(mpdpft_input);
+    case 4: return sizeof(mpdpft_launch_record);
     default: return 0;
   }
 }
@@ -220,28 +228,21 @@ int mpdpft_sc_run(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem,
 
 int mpdpft_get_field(mpdpft_ctx* ctx, int which, int s, double* out, int layout, int mem) {
   CHECK_CTX(ctx);
-  Ctx& c = ctx->impl;
-  if (s < 0 || s >= c.S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
-  cudaSetDevice(c.device);
-  const size_t off = (size_t)s * c.geom.n * c.rsize;
-  const void* src = nullptr;
-  if (which == MPDPFT_FIELD_DENSITY) {
-    mpdpft::ScState h;
-    int st = c.read_state(&h);
-    if (st) return st;
-    src = (char*)c.d_nin + (size_t)h.slot * c.S * c.geom.n * c.rsize + off;
-  } else if (which == MPDPFT_FIELD_POTENTIAL) {
-    src = (char*)c.d_V + off;
-  } else if (which == MPDPFT_FIELD_EXTERNAL) {
-    src = (char*)c.d_vext + off;
-  } else if (which == MPDPFT_FIELD_GRAD2 && c.d_g2) {
-    src = (char*)c.d_g2 + off;
-  } else if (which == MPDPFT_FIELD_LAPLACIAN && c.d_lap) {
-    src = (char*)c.d_lap + off;
-  } else {
-    return set_error(MPDPFT_ERR_ARG, "field not available");
-  }
-  return c.export_field(src, out, layout, mem);
+  cudaSetDevice(ctx->impl.device);
+  return ctx->impl.get_field(which, s, out, layout, mem);
+}
+
+int mpdpft_write_field_files(mpdpft_ctx* ctx, const char* v_path, const char* den_path) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return mpdpft::write_field_files(ctx->impl, v_path, den_path);
+}
+
+int mpdpft_interpolate_v_file(mpdpft_ctx* ctx, const char* path, double* const* v_out, int layout, int mem,
+                              int* n_file) {
+  CHECK_CTX(ctx);
+  cudaSetDevice(ctx->impl.device);
+  return mpdpft::interpolate_v_file(ctx->impl, path, v_out, layout, mem, n_file);
 }
 
 int mpdpft_energy(mpdpft_ctx* ctx, mpdpft_result* result) {

@@ -436,6 +436,31 @@ int Ctx::import_staged(const double* src, void* dst, int layout, int slot, bool 
   return MPDPFT_OK;
 }
 
+// One field of the current state (mpdpft_get_field): the input density of
+// the current ring slot, V, V_ext, |grad V|^2 or the Laplacian of species s.
+int Ctx::get_field(int which, int s, double* out, int layout, int mem) {
+  if (s < 0 || s >= S) return set_error(MPDPFT_ERR_ARG, "species index out of range");
+  const size_t off = (size_t)s * geom.n * rsize;
+  const void* src = nullptr;
+  if (which == MPDPFT_FIELD_DENSITY) {
+    ScState h;
+    int st = read_state(&h);
+    if (st) return st;
+    src = (char*)d_nin + (size_t)h.slot * S * geom.n * rsize + off;
+  } else if (which == MPDPFT_FIELD_POTENTIAL) {
+    src = (char*)d_V + off;
+  } else if (which == MPDPFT_FIELD_EXTERNAL) {
+    src = (char*)d_vext + off;
+  } else if (which == MPDPFT_FIELD_GRAD2 && d_g2) {
+    src = (char*)d_g2 + off;
+  } else if (which == MPDPFT_FIELD_LAPLACIAN && d_lap) {
+    src = (char*)d_lap + off;
+  } else {
+    return set_error(MPDPFT_ERR_ARG, "field not available");
+  }
+  return export_field(src, out, layout, mem);
+}
+
 int Ctx::export_field(const void* src, double* dst, int layout, int mem) {
   if (!dst) return set_error(MPDPFT_ERR_ARG, "null output array");
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;

@@ -106,6 +106,7 @@ struct Ctx {
   int import_staged(const double* src, void* dst, int layout, int slot, bool sync);
   double* host_stage(int slot);  // half slot of the pinned staging buffer
   int export_field(const void* src, double* dst, int layout, int mem);
+  int get_field(int which, int s, double* out, int layout, int mem);
   template <typename R>
   StepArgs<R> step_args(int mode);
   int launch_step(int mode, int parts = 7);  // parts: 1 mu, 2 density, 4 mixing kernel
@@ -154,5 +155,9 @@ struct Ctx {
                      double* dl_dpos);
   void adjoint_release();
 };
+
+// the reference's files (refio.cu)
+int write_field_files(Ctx& c, const char* v_path, const char* den_path);
+int interpolate_v_file(Ctx& c, const char* path, double* const* v_out, int layout, int mem, int* n_file);
 
 }  // namespace mpdpft

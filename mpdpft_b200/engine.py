@@ -33,6 +33,7 @@ EXPORTS = [
     "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
     "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei", "mpdpft_fft_config",
     "mpdpft_set_limits", "mpdpft_integrate_noalloc", "mpdpft_iteration_profile",
+    "mpdpft_read_input", "mpdpft_params_from_input", "mpdpft_write_field_files", "mpdpft_interpolate_v_file",
 ]
 
 
@@ -70,6 +71,10 @@ def load(path=LIB_PATH):
     L.mpdpft_ctx_stream.restype = vp
     L.mpdpft_set_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.mpdpft_iteration_profile.argtypes = [vp, C.c_int, C.POINTER(abi.LaunchRecord), C.POINTER(C.c_int)]
+    L.mpdpft_read_input.argtypes = [C.c_char_p, C.POINTER(abi.Input)]
+    L.mpdpft_params_from_input.argtypes = [C.POINTER(abi.Input), P]
+    L.mpdpft_write_field_files.argtypes = [vp, C.c_char_p, C.c_char_p]
+    L.mpdpft_interpolate_v_file.argtypes = [vp, C.c_char_p, _dpp, C.c_int, C.c_int, C.POINTER(C.c_int)]
     L.mpdpft_set_external_potential.argtypes = [vp, C.c_int, _dp, C.c_int, C.c_int]
     L.mpdpft_density.argtypes = [vp, C.c_int, _dp, C.c_double, _dp, _dp, C.c_int, C.c_int]
     L.mpdpft_vint.argtypes = [vp, C.c_int, C.c_int, _dpp, _dp, C.c_int, C.c_int]
@@ -120,6 +125,29 @@ def _ptr(a):
 
 def _ptrs(arrays):
     return (_dp * len(arrays))(*[_ptr(a) for a in arrays])
+
+
+def _check_lib(L, st):
+    if st != abi.OK:
+        raise MpdpftError(st, L.mpdpft_last_error().decode())
+
+
+def read_input(path):
+    """Parse an mpDPFT.input file (GetInputParameters): abi.Input.  Host
+    code only; needs no GPU."""
+    L = load()
+    inp = abi.Input()
+    _check_lib(L, L.mpdpft_read_input(os.fsencode(path), C.byref(inp)))
+    return inp
+
+
+def params_from_input(inp):
+    """Engine parameters of a parsed mpDPFT.input (abi.Params); raises on
+    options the engine does not implement."""
+    L = load()
+    p = abi.Params()
+    _check_lib(L, L.mpdpft_params_from_input(C.byref(inp), C.byref(p)))
+    return p
 
 
 class Engine:
@@ -307,6 +335,20 @@ class Engine:
     def stage_launch_counts(self):
         c, _ = self._launches()
         return {"sc_step": c[0], "z_r2c": c[1], "y": c[2], "x": c[3], "z_c2r": c[4], "other": c[5]}
+
+    def write_field_files(self, v_path=None, den_path=None):
+        """mpDPFT_V.dat / mpDPFT_Den.dat of the current state (ExportData)."""
+        self._check(self.lib.mpdpft_write_field_files(self.h, None if v_path is None else os.fsencode(v_path),
+                                                      None if den_path is None else os.fsencode(den_path)))
+
+    def interpolate_v_file(self, path, layout=abi.LAYOUT_PERIODIC):
+        """Start potentials interpolated from an mpDPFT_V.dat of any grid
+        (InterpolVQ = 1): ([V_s], n of the file)."""
+        outs = [np.empty(self._count(layout)) for _ in range(self.S)]
+        n = C.c_int()
+        self._check(self.lib.mpdpft_interpolate_v_file(self.h, os.fsencode(path), _ptrs(outs), layout, abi.MEM_HOST,
+                                                       C.byref(n)))
+        return outs, n.value
 
     def iteration_profile(self, cap=256):
         """One SC iteration replayed launch by launch from its CUDA graph:

@@ -42,6 +42,8 @@ def test_abi_version_and_struct_sizes(lib):
     assert lib.mpdpft_struct_size(0) == C.sizeof(abi.Params)
     assert lib.mpdpft_struct_size(1) == C.sizeof(abi.Result)
     assert lib.mpdpft_struct_size(2) == C.sizeof(abi.IterLog)
+    assert lib.mpdpft_struct_size(3) == C.sizeof(abi.Input)
+    assert lib.mpdpft_struct_size(4) == C.sizeof(abi.LaunchRecord)
 
 
 def test_params_default_matches_python_defaults(lib):
