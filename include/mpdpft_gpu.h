@@ -129,8 +129,8 @@ typedef struct {
   /* MPDPFT_DENS_GRADIENT in 3D (ABI version 2) */
   int gradient_form;        /* MPDPFT_GRADIENT_T0 or MPDPFT_GRADIENT_FINITE_T       */
   double airy_threshold;    /* line 17 Mpp[2]: Airy-averaged branch where
-                               ar = |grad V|^{2/3}/2 >= threshold (finite-T form
-                               only; <= 0: never)                                    */
+                               ar = |grad V|^{2/3}/2 >= |threshold| (finite-T form
+                               only; 0: everywhere, 1e300: nowhere)                 */
   int boole_pairs;          /* line 17 Mpp[0]: Boole pairs per half interval       */
   int boole_max_iter;       /* line 17 Mpp[1]: bisection depth of the Airy integral */
   double internal_acc;      /* line 12 InternalAcc: relative accuracy of the Airy

@@ -543,6 +543,7 @@ int Ctx::adjoint(const double* dl_dn, double* dl_dvext, int layout, int mem, dou
                  double* resid) {
   if (!initialised) return set_error(MPDPFT_ERR_ARG, "adjoint: no converged state (call sc_run first)");
   if (S != 1) return set_error(MPDPFT_ERR_ARG, "adjoint: one species only");
+  if (finite_t) return set_error(MPDPFT_ERR_ARG, "adjoint: the finite-T gradient form is not differentiated");
   if (layout != MPDPFT_LAYOUT_PERIODIC) return set_error(MPDPFT_ERR_ARG, "adjoint: periodic layout only");
   if (!dl_dn || !dl_dvext) return set_error(MPDPFT_ERR_ARG, "adjoint: null array");
   if (max_iter < 1) return set_error(MPDPFT_ERR_ARG, "adjoint: max_iter < 1");

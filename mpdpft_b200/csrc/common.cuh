@@ -186,13 +186,166 @@ struct DensParams {
   double floor_u;  // floor of mu - V in the 3D gradient terms
   double c2;       // |grad V|^2 coefficient (3D gradient form)
   int cut;         // 1: n and dn/dmu vanish wherever mu - V <= 0
+  // 3D gradient form at finite T (the reference's getDenEnAt)
+  int finite_t;        // 1: Fermi-Dirac form with the Airy-averaged branch
+  double airy_thr;     // Airy branch where |grad V|^{2/3}/2 >= airy_thr
+  int boole_pairs;     // Boole pairs per half interval
+  int boole_max_iter;  // bisection depth
+  double rtpna;        // relative accuracy of the Airy integral
+  double avg_density;  // AverageDensity = N* / L^D (NegligibleMagnitudeQ scale)
 };
 
 // Functionals with a classically forbidden region where n = 0 exactly (TF,
-// TF-inspired, 3D gradient-corrected); the finite-temperature forms are
-// positive everywhere.
-inline int density_has_cut(int expr, int dim) {
-  return expr == MPDPFT_DENS_TF || expr == MPDPFT_DENS_TF_INSPIRED || (expr == MPDPFT_DENS_GRADIENT && dim == 3);
+// TF-inspired, 3D gradient-corrected T -> 0 form); the finite-temperature
+// forms are positive everywhere.
+inline int density_has_cut(int expr, int dim, int finite_t = 0) {
+  return expr == MPDPFT_DENS_TF || expr == MPDPFT_DENS_TF_INSPIRED ||
+         (expr == MPDPFT_DENS_GRADIENT && dim == 3 && !finite_t);
+}
+
+}  // namespace mpdpft
+
+#include "special.cuh"
+
+namespace mpdpft {
+
+// ------------------------------------ 3D gradient form at finite T --------
+// getDenEnAt (EnergyQ = 0, Units 1: alpha = 1, tweak = 1; mpDPFT.cpp:
+// 3363-3453) with U = V - mu, tau = 1/T, beta0 = -g/(2 pi)^{3/2},
+// beta1 = (alpha tau)^{-3/2}, beta2 = -lap/(12 sqrt(alpha tau)),
+// ar = |grad V|^{2/3}/2:
+//   ar <  threshold  n = beta0 (beta1 Li_{3/2}(-e^{-tau U}) + beta2 Li_{-1/2}(-e^{-tau U}))
+//   ar >= threshold  n = int CurlyA(x) prefactor (Li_{1/2} + prefactor2 Li_{-3/2})(-e^{-(U - x ar)/T}) dx
+//                    over [2 x0, x0] and [x0, 100] by the reference's adaptive
+//                    Boole rule, x0 the first of -2, -4, ... where the
+//                    integrand falls below MP = 1e-12 (or -2^27 at most).
+// beta2 is taken exactly as the reference writes it (sqrt(T) where the
+// Wigner-Kirkwood correction has 1/sqrt(T): the reference's gradient term
+// is T times the textbook one); a NaN result counts as 0.
+struct AiryArgs {
+  double pre, pre2, U, ar, T;
+};
+
+__device__ __forceinline__ double airy_integrand(const AiryArgs& A, double x) {
+  // nAiTintegrand, 3D, EnergyQ = 0 (mpDPFT.cpp:3614-3619)
+  const double arg = -(A.U - x * A.ar) / A.T;
+  return A.pre * curly_a(x) * (fd_li(FD_1HALF, arg) + A.pre2 * fd_li(FD_M3HALF, arg));
+}
+
+// BooleRule1D (mpDPFT.cpp:8050-8058) over the 4 bp + 1 nodes
+// (a + i delta) + off of AdaptiveBoole_nAiT.
+__device__ __forceinline__ double airy_boole(const AiryArgs& A, int bp, double a, double delta, double off) {
+  const int n = 4 * bp + 1;
+  double res = 7.0 * airy_integrand(A, a + 0.0 * delta + off);
+  double last = 0.0;
+  for (int i = 1; i <= n - 4; i += 4) {
+    const double f1 = airy_integrand(A, (a + (double)i * delta) + off);
+    const double f2 = airy_integrand(A, (a + (double)(i + 1) * delta) + off);
+    const double f3 = airy_integrand(A, (a + (double)(i + 2) * delta) + off);
+    const double f4 = airy_integrand(A, (a + (double)(i + 3) * delta) + off);
+    res += (32.0 * f1 + 12.0 * f2 + 32.0 * f3 + 14.0 * f4);
+    last = f4;
+  }
+  res -= 14.0 * last;
+  res += 7.0 * last;
+  return res * (2.0 * delta / 45.0);
+}
+
+// NegligibleMagnitudeQ (mpDPFT.cpp:7094-7101)
+__device__ __forceinline__ bool negligible_magnitude(double big, double small, double max_exp) {
+  if (small == 0.0) return true;
+  if (big == 0.0 || big < small) return false;
+  return log10(fabs(big)) - log10(fabs(small)) > max_exp;
+}
+
+constexpr int kAiryMaxDepth = 24;  // boole_max_iter <= kAiryMaxDepth - 3
+
+// AdaptiveBoole_nAiT (mpDPFT.cpp:3553-3578) without recursion: a stack of
+// frames (a, b, previous integral, depth); a frame that does not return
+// evaluates its left half, then its right half, and returns their sum, in
+// the reference's order.
+static __device__ __noinline__ double airy_adaptive(const AiryArgs& A, const DensParams& d, double a0, double b0) {
+  struct Frame {
+    double a, b, prev, ib, left;
+    int iter, stage;
+  };
+  Frame st[kAiryMaxDepth];
+  int sp = 0;
+  double ret = 0.0;
+  const double mexp = -log10(d.rtpna);
+  st[0] = Frame{a0, b0, 0.0, 0.0, 0.0, 0, 0};
+  while (sp >= 0) {
+    Frame& f = st[sp];
+    const double half = 0.5 * (f.b - f.a);
+    if (f.stage == 0) {
+      const double delta = 0.25 * half / (double)d.boole_pairs;
+      const double ia = airy_boole(A, d.boole_pairs, f.a, delta, 0.0);
+      const double ib = airy_boole(A, d.boole_pairs, f.a, delta, half);
+      const double in = ia + ib;
+      bool done;
+      if (f.iter > 1 && fabs(in) > 0.0 && fabs((in - f.prev) / in) < d.rtpna) done = true;
+      else if (f.iter > d.boole_max_iter) done = true;
+      else if (negligible_magnitude(d.avg_density, pow(2.0, (double)f.iter) * in, mexp)) done = true;
+      else if (delta < 1.0e-12) done = true;
+      else done = sp + 1 >= kAiryMaxDepth;
+      if (done) {
+        ret = in;
+        --sp;
+        continue;
+      }
+      f.ib = ib;
+      f.stage = 1;
+      st[sp + 1] = Frame{f.a, f.a + half, ia, 0.0, 0.0, f.iter + 1, 0};
+      ++sp;
+    } else if (f.stage == 1) {
+      f.left = ret;
+      f.stage = 2;
+      st[sp + 1] = Frame{f.a + half, f.b, f.ib, 0.0, 0.0, f.iter + 1, 0};
+      ++sp;
+    } else {
+      ret = f.left + ret;
+      --sp;
+    }
+  }
+  return ret;
+}
+
+static __device__ __noinline__ double finite_t_density(const DensParams& d, double u, double lap, double g2) {
+  const double T = d.T, tau = 1.0 / T, U = -u;
+  const double beta0 = -d.g / 15.749609945722419;  // (2 pi)^{3/2}
+  const double beta1 = T * sqrt(T);
+  const double beta2 = -lap / (12.0 * sqrt(tau));
+  const double ar = 0.5 * cbrt(g2 > 0.0 ? g2 : 0.0);
+  double res;
+  if (ar < d.airy_thr) {
+    const double arg = -tau * U;
+    res = beta0 * (beta1 * fd_li(FD_3HALF, arg) + beta2 * fd_li(FD_M1HALF, arg));
+  } else {
+    const AiryArgs A{beta0 * ar * tau * beta1, beta2 / beta1, U, ar, T};
+    double x = -1.0, test;
+    do {  // lower integration limit (mpDPFT.cpp:3424-3433)
+      x *= 2.0;
+      const double arg = -tau * (U - x * ar);
+      test = beta0 * curly_a(x) * ar * tau * (beta1 * fd_li(FD_1HALF, arg) + beta2 * fd_li(FD_M3HALF, arg));
+      if (x < -1.0e8) break;
+    } while (fabs(test) > 1.0e-12);
+    res = airy_adaptive(A, d, 2.0 * x, x);
+    res += airy_adaptive(A, d, x, 100.0);
+  }
+  return res != res ? 0.0 : res;
+}
+
+// dn/dmu of the small-gradient finite-T form, beta0 (beta1 Li_{1/2} +
+// beta2 Li_{-3/2}) / T (also used at Airy points: it only places mu
+// candidates).
+static __device__ __noinline__ double finite_t_slope(const DensParams& d, double u, double lap) {
+  const double T = d.T, tau = 1.0 / T;
+  const double beta0 = -d.g / 15.749609945722419;
+  const double beta1 = T * sqrt(T);
+  const double beta2 = -lap / (12.0 * sqrt(tau));
+  const double arg = tau * u;
+  const double r = beta0 * (beta1 * fd_li(FD_1HALF, arg) + beta2 * fd_li(FD_M3HALF, arg)) * tau;
+  return r == r ? r : 0.0;
 }
 
 // Pointwise density at u = mu - V (R = float or double arithmetic).
@@ -224,6 +377,7 @@ __device__ __forceinline__ R density_at(const DensParams& d, R u, R lap, R g2) {
     return pref * t;
   }
   // MPDPFT_DENS_GRADIENT
+  if (d.finite_t) return R(finite_t_density(d, (double)u, (double)lap, (double)g2));
   if (d.dim == 2) {
     const R tau = R(1.0 / d.T);
     const R arg = tau * u;  // -tau (V - mu)
@@ -270,6 +424,7 @@ __device__ __forceinline__ double density_at_d(const DensParams& d, double u, do
     return (d.g / (2.0 * kPi)) * u;
   }
   if (d.expr == MPDPFT_DENS_GRADIENT && d.dim == 3) {
+    if (d.finite_t) return finite_t_density(d, u, lap, g2);
     if (!(u > 0.0)) return 0.0;
     const double ctf = 2.0 * 1.4142135623730951 * d.g / (6.0 * kPi * kPi);
     const double cg = 1.4142135623730951 * d.g / (48.0 * kPi * kPi);
@@ -308,6 +463,7 @@ __device__ __forceinline__ double density_slope_d(const DensParams& d, double u,
     return 1.0 / (1.0 + exp(-t2)) / (d.tau * d.tau);
   }
   // gradient-corrected
+  if (d.finite_t) return finite_t_slope(d, u, lap);
   if (d.dim == 2) {
     const double tau = 1.0 / d.T;
     const double arg = tau * u;

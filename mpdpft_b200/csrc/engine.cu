@@ -208,6 +208,18 @@ static int check_params(const mpdpft_params& p) {
       return set_error(MPDPFT_ERR_ARG, "Coulomb interactions need dim 3");
   }
   if (p.precision != MPDPFT_FP64 && p.precision != MPDPFT_MIXED) return set_error(MPDPFT_ERR_ARG, "bad precision");
+  if (p.gradient_form != MPDPFT_GRADIENT_T0 && p.gradient_form != MPDPFT_GRADIENT_FINITE_T)
+    return set_error(MPDPFT_ERR_ARG, "bad gradient_form");
+  if (p.gradient_form == MPDPFT_GRADIENT_FINITE_T && de == MPDPFT_DENS_GRADIENT) {
+    if (p.dim != 3) return set_error(MPDPFT_ERR_ARG, "the finite-T gradient form is 3D (2D uses its own finite-T form)");
+    if (p.boole_pairs < 1 || p.boole_pairs > 50)
+      return set_error(MPDPFT_ERR_ARG, "boole_pairs must be 1 to 50 (the reference caps Mpp[0] at 50)");
+    if (p.boole_max_iter < 0 || p.boole_max_iter > 21) return set_error(MPDPFT_ERR_ARG, "boole_max_iter must be 0 to 21");
+    if (!(p.internal_acc > 0.0)) return set_error(MPDPFT_ERR_ARG, "internal_acc must be positive");
+    for (int s = 0; s < p.species; ++s)
+      if (p.temperature[s] == 0.0)
+        return set_error(MPDPFT_ERR_ARG, "the finite-T gradient form needs T > 0 (or T < 0: automatic)");
+  }
   if (p.max_sc_count < 0) return set_error(MPDPFT_ERR_ARG, "max_sc_count < 0");
   return MPDPFT_OK;
 }
@@ -232,7 +244,13 @@ KParams Ctx::kparams() const {
     d.T = temperature[s];
     d.floor_u = P.gradient_floor;
     d.c2 = P.gradient_grad2;
-    d.cut = density_has_cut(d.expr, d.dim) && (d.expr != MPDPFT_DENS_TF_INSPIRED || d.tau > 0.0);
+    d.finite_t = finite_t ? 1 : 0;
+    d.airy_thr = std::fabs(P.airy_threshold);
+    d.boole_pairs = P.boole_pairs;
+    d.boole_max_iter = P.boole_max_iter;
+    d.rtpna = P.internal_acc;
+    d.avg_density = P.abundances[s] / std::pow(P.edge, (double)P.dim);  // AverageDensity (mpDPFT.cpp:1003)
+    d.cut = density_has_cut(d.expr, d.dim, d.finite_t) && (d.expr != MPDPFT_DENS_TF_INSPIRED || d.tau > 0.0);
     k.abundance[s] = P.abundances[s];
     k.charges[s] = P.charges[s];
   }
@@ -304,7 +322,9 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   // |grad V|^2 enters only the 3D form with a |grad V|^2 coefficient; the
   // reference's small-gradient branch (and the 2D form) use the Laplacian
   // alone, so the SC loop's DelField then skips the gradients
-  need_g2 = gradient && P.dim == 3 && P.gradient_grad2 != 0.0;
+  finite_t = gradient && P.dim == 3 && P.gradient_form == MPDPFT_GRADIENT_FINITE_T;
+  // the finite-T form reads |grad V|^2 for its Airy-branch test
+  need_g2 = gradient && P.dim == 3 && (finite_t || P.gradient_grad2 != 0.0);
   has_coulomb = has_interaction(MPDPFT_INT_HARTREE) || has_interaction(MPDPFT_INT_HARTREE_INTER) ||
                 has_interaction(MPDPFT_INT_COULOMB_CHARGED);
   for (int s = 0; s < S; ++s) temperature[s] = P.temperature[s];
@@ -337,7 +357,7 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   };
   const bool f64 = P.precision == MPDPFT_FP64;
   int occ_mu = 0, occ_dens = 0, occ_mix = 0;
-  fk = functional_kind(P.density_expression, P.dim);
+  fk = functional_kind(P.density_expression, P.dim, finite_t);
   if ((st = occupancy(f64 ? sc_kernel_ptr<double>(0, fk) : sc_kernel_ptr<float>(0, fk), kStepThreads, &occ_mu)))
     return st;
   dens_which = density_variant(P.mixer ? P.pulay_scope : 1);

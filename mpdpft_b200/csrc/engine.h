@@ -35,6 +35,7 @@ struct Ctx {
   int ring = 2;
   bool gradient = false;
   bool need_g2 = false;  // the SC loop's functional reads |grad V|^2
+  bool finite_t = false; // 3D gradient form at finite T (MPDPFT_GRADIENT_FINITE_T)
   int has_coulomb = 0;
   double temperature[kMaxS];
   bool initialised = false;

@@ -313,7 +313,8 @@ __device__ __forceinline__ void g2d_n_slope(const EvalK& k, double u, double l, 
 // gradient-corrected, 2 = 3D TF, 3 = 2D gradient-corrected, 0 = any
 // (density_at_d).  The point values are FP64 in both precisions: the mu
 // search resolves N to RelAcc (1e-10), below the rounding of FP32 values.
-inline int functional_kind(int expr, int dim) {
+inline int functional_kind(int expr, int dim, int finite_t = 0) {
+  if (expr == MPDPFT_DENS_GRADIENT && dim == 3 && finite_t) return 0;
   if (expr == MPDPFT_DENS_GRADIENT && dim == 3) return 1;
   if (expr == MPDPFT_DENS_TF && dim == 3) return 2;
   if (expr == MPDPFT_DENS_GRADIENT && dim == 2) return 3;

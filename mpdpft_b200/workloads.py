@@ -106,19 +106,23 @@ def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **
     Dirac exchange, g = 2, atomic units (gammaH = 1).  The density is the
     reference's small-gradient branch (mpDPFT.cpp:3376-3388) in its T -> 0
     form, n = g (2u)^{3/2}/(6 pi^2) - g lap V (2u)^{-1/2}/(24 pi^2),
-    u = mu - V, clamped at 0, with no |grad V|^2 term; the factor u^{-1/2}
-    is continued linearly below u = 1e-3 hartree (a floor for the singular
-    point at the classical turning surface).  Converges from 40^3 up (24 SC
-    iterations at 128^3).  The start mu = -30 lies within the reference's 20
-    bracket steps of the bare-nucleus root (the first density is computed
-    in V_ext alone)."""
+    u = mu - V, clamped at 0, with no |grad V|^2 term; the singular factor
+    u^{-1/2} is continued linearly below u = 0.5 hartree, where the
+    small-gradient expansion fails (the reference switches to its Airy
+    branch there).  12 SC iterations at 128^3.  With the floor at 1e-3
+    hartree the loop also converges (24 iterations at 128^3) but contracts
+    so slowly near its fixed point that where two correct loops stop differs
+    by ~1e-4 in L1/N at CC < 1e-8, which is why the benchmark keeps the 0.5
+    floor.  The start mu = -30 lies within
+    the reference's 20 bracket steps of the bare-nucleus root (the first
+    density is computed in V_ext alone)."""
     z = 18.0
     kw = dict(dim=3, steps=steps, species=1, edge=edge, abundances=[z],
               rel_acc=1e-10, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
               interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0,
               mu=[-30.0], mixer=1, pulay_scope=5, theta=[0.5], sc_criterion=1e-8,
               max_sc_count=300, smearing_extent=0.2, regularization_threshold=0.45,
-              gradient_floor=1e-3, gradient_grad2=0.0, potential_tol=0.0,
+              gradient_floor=0.5, gradient_grad2=0.0, potential_tol=0.0,
               precision=precision)
     kw.update(over)
     p = abi.make_params(**kw)

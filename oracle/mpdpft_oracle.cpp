@@ -367,6 +367,152 @@ void delfield(State& st, const std::vector<double>& f, std::vector<double>& grad
 }
 
 // ---------------------------------------------- densities MD:2142-2238 --
+// ------------------------- finite-T gradient form, MD:3363-3453, 3553-3620 --
+// Special functions from the same Chebyshev tables as the product
+// (mpdpft_b200/csrc/special_tables.inc, generated from mpmath and pinned by
+// tests/test_special_functions.py against mpmath and the reference's own
+// TabFunc_CurlyA.dat); the density algorithm around them is restated here.
+#include "../mpdpft_b200/csrc/special_tables.inc"
+const double kFdTab[5 * (MPDPFT_FD_X1 - MPDPFT_FD_X0) * MPDPFT_FD_DEG] = MPDPFT_FD_TABLE;
+const double kFdAsym[5 * MPDPFT_FD_ASYM] = MPDPFT_FD_ASYM_TABLE;
+const double kFdRGamma[5] = MPDPFT_FD_RGAMMA;
+const double kCaTab[MPDPFT_CA_N * MPDPFT_CA_DEG] = MPDPFT_CA_TABLE;
+const double kFdOrder[5] = {2.5, 1.5, 0.5, -0.5, -1.5};
+
+double cheb(const double* c, int n, double t) {
+  double b1 = 0., b2 = 0.;
+  for (int j = n - 1; j >= 1; --j) {
+    double b0 = std::fma(2. * t, b1, c[j] - b2);
+    b2 = b1;
+    b1 = b0;
+  }
+  return std::fma(t, b1, c[0] - b2);
+}
+
+// polylog(order, x) of MD:7000-7027 = Li_s(-e^x): 0 below -699, the leading
+// term -x^s/Gamma(s+1) above 699, else the series / table / Sommerfeld forms.
+double polylog(int o, double x) {
+  const double s = kFdOrder[o];
+  if (!(x >= -699.)) return x != x ? x : 0.;
+  if (x > 699.) return -std::pow(x, s) * kFdRGamma[o];
+  if (x < MPDPFT_FD_X0) {
+    const double z = std::exp(x);
+    double zk = z, sum = 0.;
+    for (int k = 1; k <= 40; ++k) {
+      const double t = zk * std::pow((double)k, -s);
+      sum += (k & 1) ? -t : t;
+      zk *= z;
+      if (zk < 1e-18 * std::fabs(sum)) break;
+    }
+    return sum;
+  }
+  if (x < MPDPFT_FD_X1) {
+    const double m = std::floor(x);
+    const double* c = kFdTab + ((long)o * (MPDPFT_FD_X1 - MPDPFT_FD_X0) + ((int)m - MPDPFT_FD_X0)) * MPDPFT_FD_DEG;
+    return cheb(c, MPDPFT_FD_DEG, 2. * (x - m) - 1.);
+  }
+  const double y = 1. / (x * x);
+  double sum = 0.;
+  for (int k = MPDPFT_FD_ASYM - 1; k >= 0; --k) sum = std::fma(sum, y, kFdAsym[o * MPDPFT_FD_ASYM + k]);
+  return -std::pow(x, s) * kFdRGamma[o] * sum;
+}
+
+// CurlyA(y) = int_y^inf Ai (mpDPFT.h:231-237), the reference's own forms
+// outside the table's range
+double CurlyA(double y) {
+  if (y < -1.0e50) return 1.;
+  if (y < -149.99) return 1. - std::cos(0.25 * PI + 0.6666666666666666666 * (-y) * std::sqrt(-y)) /
+                                   std::sqrt(PI * (-y) * std::sqrt(-y));
+  if (y < MPDPFT_CA_X1) {
+    const double u = (y - MPDPFT_CA_X0) / MPDPFT_CA_W;
+    int i = (int)std::floor(u);
+    if (i < 0) i = 0;
+    return cheb(kCaTab + (long)i * MPDPFT_CA_DEG, MPDPFT_CA_DEG, 2. * (u - i) - 1.);
+  }
+  const double z = 2. / 3. * y * std::sqrt(y);
+  return std::exp(-z) / (2. * std::sqrt(PI) * std::pow(y, 0.75));
+}
+
+struct NAiT {  // the arguments nAiTintegrand takes beside x (MD:3580)
+  double prefactor, U, ar, prefactor2, T, compare, rtpna;
+  int bp, max_iter;
+};
+
+double nAiT_integrand(const NAiT& a, double x) {  // MD:3614-3619, EnergyQ = 0
+  const double arg = -(a.U - x * a.ar) / a.T;
+  return a.prefactor * CurlyA(x) * (polylog(2, arg) + a.prefactor2 * polylog(4, arg));
+}
+
+double boole_1d(const std::vector<double>& f, int Lf, double a1, double b1, int bp) {  // MD:8050-8058
+  const double h = (b1 - a1) / (bp * 4.);
+  double res = 7. * f[0];
+  for (int i = 1; i <= Lf - 4; i += 4) res += (32. * f[i] + 12. * f[i + 1] + 32. * f[i + 2] + 14. * f[i + 3]);
+  res -= 14. * f[Lf - 1];
+  res += 7. * f[Lf - 1];
+  return res * (2. * h / 45.);
+}
+
+bool negligible_magnitude_q(double big, double small, double max_exp) {  // MD:7094-7101
+  if (small == 0.) return true;
+  if (big == 0. || big < small) return false;
+  return std::log10(std::fabs(big)) - std::log10(std::fabs(small)) > max_exp;
+}
+
+// AdaptiveBoole_nAiT (MD:3553-3578), recursive as the reference
+double adaptive_boole(const NAiT& A, double a, double b, double prev, int iter) {
+  const int BP = A.bp, n = 4 * BP + 1;
+  const double half = 0.5 * (b - a), Delta = 0.25 * half / (double)BP;
+  std::vector<double> fa(n), fb(n);
+  for (int yi = 0; yi < n; ++yi) {
+    const double x = a + (double)yi * Delta;
+    fa[yi] = nAiT_integrand(A, x);
+    fb[yi] = nAiT_integrand(A, x + half);
+  }
+  const double Inta = boole_1d(fa, n, a, a + half, BP);
+  const double Intb = boole_1d(fb, n, a + half, b, BP);
+  const double Int = Inta + Intb;
+  if (iter > 1 && std::fabs(Int) > 0. && std::fabs((Int - prev) / Int) < A.rtpna) return Int;
+  if (iter > A.max_iter) return Int;
+  if (negligible_magnitude_q(A.compare, std::pow(2., (double)iter) * Int, -std::log10(A.rtpna))) return Int;
+  if (Delta < MP) return Int;
+  return adaptive_boole(A, a, a + half, Inta, iter + 1) + adaptive_boole(A, a + half, b, Intb, iter + 1);
+}
+
+// getDenEnAt, DIM 3, EnergyQ = 0, Units 1 (alpha = 1, tweak = 1), MD:3365-3441
+double den_nAiT(const State& st, int s, long i, double mu) {
+  const mpdpft_params& P = st.P;
+  const double T = st.T[s], tau = 1. / T;
+  const double beta0 = -P.degeneracy / std::pow(2. * PI, 1.5), beta1 = std::pow(tau, -1.5);
+  const double U = st.V[s][i] - mu, ar = 0.5 * std::cbrt(st.Grad2[s][i]);
+  const double beta2 = -st.Lap[s][i] / (12. * std::sqrt(tau));
+  double res;
+  if (ar < std::fabs(P.airy_threshold)) {
+    const double arg = -tau * U;
+    res = beta0 * (beta1 * polylog(1, arg) + beta2 * polylog(3, arg));
+  } else {
+    NAiT A;
+    A.prefactor = beta0 * ar * tau * beta1;
+    A.prefactor2 = beta2 / beta1;
+    A.U = U;
+    A.ar = ar;
+    A.T = T;
+    A.compare = P.abundances[s] / std::pow(P.edge, (double)P.dim);  // AverageDensity (MD:1003)
+    A.rtpna = P.internal_acc;
+    A.bp = P.boole_pairs;
+    A.max_iter = P.boole_max_iter;
+    double test = 1., x = -1.;
+    while (std::fabs(test) > MP) {  // lower integration limit (MD:3424-3433)
+      x *= 2.;
+      const double arg = -tau * (U - x * ar);
+      test = beta0 * CurlyA(x) * ar * tau * (beta1 * polylog(2, arg) + beta2 * polylog(4, arg));
+      if (x < -1.0e8) break;
+    }
+    res = adaptive_boole(A, 2. * x, x, 0., 0);
+    res += adaptive_boole(A, x, 100., 0., 0);
+  }
+  return res != res ? 0. : res;
+}
+
 void density(State& st, int s) {
   const mpdpft_params& P = st.P;
   const long G = st.G;
@@ -419,6 +565,9 @@ void density(State& st, int s) {
         double r = g / (2. * PI) * (LOG / tau - tau * lap[i] / 12. * zeta / ((1. + zeta) * (1. + zeta)));
         n[i] = (r != r) ? 0. : r;
       }
+    } else if (P.gradient_form == MPDPFT_GRADIENT_FINITE_T) {  // MD:3365-3441
+#pragma omp parallel for schedule(dynamic, 256)
+      for (long i = 0; i < G; ++i) n[i] = den_nAiT(st, s, i, mu);
     } else {  // T -> 0 limit of the small-gradient branch in 3D (MD:3385-3386)
       const double floor_u = P.gradient_floor;
       const double c2 = P.gradient_grad2;
@@ -1142,6 +1291,25 @@ int oracle_num_threads(void) {
 #else
   return 1;
 #endif
+}
+
+// The special functions and one point of the finite-T gradient density
+// (species 0 of p, temperature T, u = mu - V), for the known-answer tests.
+double oracle_polylog(int order, double x) { return polylog(order, x); }
+double oracle_curly_a(double x) { return CurlyA(x); }
+double oracle_finite_t_point(const mpdpft_params* p, double T, double u, double lap, double grad2) {
+  State st;
+  mpdpft_params q = *p;
+  q.steps = 2;
+  q.dim = 3;
+  init_state(st, q);
+  st.T[0] = T;
+  st.V[0].assign(st.G, 0.);
+  st.Lap[0].assign(st.G, lap);
+  st.Grad2[0].assign(st.G, grad2);
+  st.P.edge = p->edge;
+  st.P.dim = p->dim;
+  return den_nAiT(st, 0, 0, u);
 }
 
 // OpenMP threads of later oracle calls (<= 0: all host threads).

@@ -52,6 +52,12 @@ def lib():
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_set_threads.restype = None
+        L.oracle_polylog.argtypes = [C.c_int, C.c_double]
+        L.oracle_polylog.restype = C.c_double
+        L.oracle_curly_a.argtypes = [C.c_double]
+        L.oracle_curly_a.restype = C.c_double
+        L.oracle_finite_t_point.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.oracle_finite_t_point.restype = C.c_double
         _lib = L
     return _lib
 
@@ -75,6 +81,24 @@ def num_threads():
 def set_threads(n):
     """OpenMP threads of later oracle calls (0: all host threads)."""
     lib().oracle_set_threads(int(n))
+
+
+FD_ORDERS = (2.5, 1.5, 0.5, -0.5, -1.5)
+
+
+def polylog(s, x):
+    """Li_s(-e^x) for s in FD_ORDERS (the reference's polylog())."""
+    return lib().oracle_polylog(FD_ORDERS.index(s), float(x))
+
+
+def curly_a(x):
+    """int_x^inf Ai(t) dt (the reference's CurlyA)."""
+    return lib().oracle_curly_a(float(x))
+
+
+def finite_t_point(p, T, u, lap, grad2):
+    """The finite-T gradient density of species 0 at one point (u = mu - V)."""
+    return lib().oracle_finite_t_point(C.byref(p), T, u, lap, grad2)
 
 
 def fft(p, field, sign):

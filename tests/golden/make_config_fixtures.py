@@ -4,8 +4,8 @@ Runs the FP64 CPU oracle (oracle/, OpenMP) once to convergence on
   argon_atom at 128^3 (the headline atom)     -> config_argon_atom_128.npz
   cluster_adjoint at 192^3 (13 Z = 3 nuclei)  -> config_cluster_adjoint_192.npz
   electron_hole at 256^3 (two charged species) -> config_electron_hole_256.npz
-to the SC criterion of CRITERIA below, and stores what the GPU parity
-tests compare against (after solving to the same criterion): the total energy, mu
+to the workloads' SC criterion (CC < 1e-8 three times) and stores what the
+GPU parity tests compare against: the total energy, mu
 and N per species, the iteration count, the final CC and potential
 residual, and the density and potential summed over 16^3 coarse blocks
 (oracle.block_sums; density sums times dvol, potential block means).
@@ -57,22 +57,15 @@ def run(name, p, vext, v0):
     save(name, p, res, log, dens, pot, time.time() - t)
 
 
-# SC criteria of the fixtures: tight enough that the stopping point does not
-# dominate the comparison (CC ~ |dn|^2 / 2|n|^2, so CC < 1e-8 still allows
-# ~1e-4 relative changes per iteration); the cluster's loop stalls near
-# CC ~ 1e-9 (its TF-Dirac edge points flip branch), so it keeps 1e-8.
-CRITERIA = {"argon_atom_128": 1e-12, "electron_hole_256": 1e-11, "cluster_adjoint_192": 1e-8}
-
-
 def main(which):
     if which in ("argon", "all"):
-        p, vext, v0 = W.argon_atom(steps=128, precision=abi.FP64, sc_criterion=CRITERIA["argon_atom_128"])
+        p, vext, v0 = W.argon_atom(steps=128, precision=abi.FP64, sc_criterion=1e-8)
         run("argon_atom_128", p, vext, v0)
     if which in ("electron_hole", "all"):
-        p, vext, v0 = W.electron_hole(steps=256, precision=abi.FP64, sc_criterion=CRITERIA["electron_hole_256"])
+        p, vext, v0 = W.electron_hole(steps=256, precision=abi.FP64, sc_criterion=1e-8)
         run("electron_hole_256", p, vext, v0)
     if which in ("cluster", "all"):
-        p, vext, v0, _ = W.cluster_adjoint(steps=192, precision=abi.FP64, sc_criterion=CRITERIA["cluster_adjoint_192"])
+        p, vext, v0, _ = W.cluster_adjoint(steps=192, precision=abi.FP64, sc_criterion=1e-8)
         run("cluster_adjoint_192", p, vext, v0)
 
 
