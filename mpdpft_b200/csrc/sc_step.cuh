@@ -322,6 +322,25 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
         if (est + e < m.hi) m.cand[m.ncand++] = est + e;
       }
     }
+    // the quadratic through N at both bracket ends with the slope at
+    // candidate 0 (one of them): a third-order estimate that usually meets
+    // the tolerance here, so a steady-state search ends after two passes
+    if (slope > 0.0 && isfinite(slope) && isfinite(m.N_prev0) && m.ncand + 3 <= kMuCand - 2) {
+      const double c0 = m.cand_prev0, N0 = m.N_prev0;
+      const bool at_lo = c0 == m.lo;
+      const double h = (at_lo ? m.hi : m.lo) - c0, N1 = at_lo ? m.Nhi : m.Nlo;
+      const double qa = (N1 - N0 - slope * h) / (h * h), qc = N0 - target;
+      const double disc = slope * slope - 4.0 * qa * qc;
+      if (h != 0.0 && disc >= 0.0 && isfinite(qa)) {
+        const double est = c0 - 2.0 * qc / (slope + sqrt(disc));
+        if (est > m.lo && est < m.hi) {
+          const double e = fmax(1e-6 * fabs(est - c0), 1e-13 * fabs(est) + 1e-300);
+          m.cand[m.ncand++] = est;
+          if (est - e > m.lo) m.cand[m.ncand++] = est - e;
+          if (est + e < m.hi) m.cand[m.ncand++] = est + e;
+        }
+      }
+    }
     const double rf = m.lo + (target - m.Nlo) * (m.hi - m.lo) / (m.Nhi - m.Nlo);
     if (rf > m.lo && rf < m.hi) m.cand[m.ncand++] = rf;
     m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
