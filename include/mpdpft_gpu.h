@@ -48,7 +48,14 @@ typedef enum {
   MPDPFT_ERR_PULAY_SINGULAR = 5,/* Pulay Gram matrix rejected; linear mixing   */
   MPDPFT_ERR_TIMEOUT = 6,       /* a device loop reached its iteration cap     */
   MPDPFT_ERR_NOT_CONVERGED = 7, /* maxSCcount reached before convergence       */
-  MPDPFT_ERR_NO_DEVICE = 8      /* no usable sm_100 device                     */
+  MPDPFT_ERR_NO_DEVICE = 8,     /* no usable sm_100 device                     */
+  /* warning: the mu search ended inside its bracket without meeting
+   * rel_acc (a step of N(mu) at the target), the reference's TrappedQ
+   * (mpDPFT.cpp:4690-4703).  Returned by mpdpft_mu_search (mu and N are
+   * the search's end point); in an SC iteration a status bit only, and the
+   * iteration mixes with theta scaled by min(1, |1 - RelDiff|^30),
+   * RelDiff = |N* - N| / |N*| (AdmixDensities, mpDPFT.cpp:4929-4934)     */
+  MPDPFT_WARN_MU_TRAPPED = 9
 } mpdpft_status;
 
 enum { MPDPFT_FP64 = 0, MPDPFT_MIXED = 1 };
@@ -163,6 +170,9 @@ typedef struct {
   int iterations;           /* SC iterations run                                   */
   int converged;            /* 1 if the exit rule was met                          */
   int total_mu_trials;
+  int device_loop;          /* 1 if the SC loop ran as one device-side graph loop
+                               (no host round trip per iteration), 0 if the host
+                               replayed one iteration at a time                 */
   double cc;
   double v_residual;
   double mu[MPDPFT_MAX_SPECIES];
@@ -237,7 +247,9 @@ int mpdpft_update_v(mpdpft_ctx* ctx, const double* const* n, double incremental,
  * (mpDPFT.cpp:4569-4743) for one species.  *mu_io holds the starting mu on
  * entry and the result on exit; the final density is left in n_out when it
  * is not NULL.  Returns MPDPFT_ERR_MU_BRACKET (mu reset to the start value)
- * when no bracket is found, as the reference does. */
+ * when no bracket is found, as the reference does, and
+ * MPDPFT_WARN_MU_TRAPPED when the bracket closes on a step of N(mu) that
+ * the tolerance cannot resolve (the reference's trapped bisection). */
 int mpdpft_mu_search(mpdpft_ctx* ctx, int s, const double* v, double n_target,
                      double* mu_io, double* abundance_out, int* trials_out,
                      double* n_out, int layout, int mem);

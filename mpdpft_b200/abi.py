@@ -20,6 +20,7 @@ ERR_PULAY_SINGULAR = 5
 ERR_TIMEOUT = 6
 ERR_NOT_CONVERGED = 7
 ERR_NO_DEVICE = 8
+WARN_MU_TRAPPED = 9  # status_bits only
 
 FP64 = 0
 MIXED = 1
@@ -140,6 +141,7 @@ class Result(C.Structure):
         ("iterations", C.c_int),
         ("converged", C.c_int),
         ("total_mu_trials", C.c_int),
+        ("device_loop", C.c_int),
         ("cc", C.c_double),
         ("v_residual", C.c_double),
         ("mu", _D4),

@@ -81,6 +81,7 @@ const char* mpdpft_status_string(int status) {
     case MPDPFT_ERR_TIMEOUT: return "device loop cap reached";
     case MPDPFT_ERR_NOT_CONVERGED: return "not converged";
     case MPDPFT_ERR_NO_DEVICE: return "no usable device";
+    case MPDPFT_WARN_MU_TRAPPED: return "mu search trapped (warning)";
     default: return "unknown status";
   }
 }

@@ -22,6 +22,7 @@ constexpr int kBitNonfinite = 1 << MPDPFT_ERR_NONFINITE;
 constexpr int kBitBracket = 1 << MPDPFT_ERR_MU_BRACKET;
 constexpr int kBitPulay = 1 << MPDPFT_ERR_PULAY_SINGULAR;
 constexpr int kBitTimeout = 1 << MPDPFT_ERR_TIMEOUT;
+constexpr int kBitTrapped = 1 << MPDPFT_WARN_MU_TRAPPED;
 
 inline int grid_blocks(long n) {
   long b = (n + kThreads - 1) / kThreads;
@@ -521,6 +522,33 @@ __device__ __forceinline__ R density_slope(const DensParams& d, R u) {
   if (!(u > R(0))) return R(0);
   if (d.dim == 3) return R(1.5 * 1.4142135623730951 * d.g / (3.0 * kPi * kPi)) * sqrt(u);
   return R(d.g / (2.0 * kPi));
+}
+
+// e^{-x} I0(x) for x >= 0 (the exponentially scaled modified Bessel function
+// of the 2D Coulomb compensation term, mpDPFT.cpp:2659).  Below x = 30 the
+// power series I0(x) = sum_k (x^2/4)^k / (k!)^2 (positive terms, no
+// cancellation) times e^{-x}; above, the asymptotic expansion
+// e^{-x} I0(x) ~ (2 pi x)^{-1/2} sum_k [(2k-1)!!]^2 / (k! (8x)^k), whose
+// terms fall below 1e-17 of the sum long before they start to grow.
+__host__ __device__ inline double bessel_i0e(double x) {
+  if (x < 30.0) {
+    const double q = 0.25 * x * x;
+    double t = 1.0, sum = 1.0;
+    for (int k = 1; k < 200; ++k) {
+      t *= q / ((double)k * (double)k);
+      sum += t;
+      if (t < 1.0e-17 * sum) break;
+    }
+    return sum * exp(-x);
+  }
+  double t = 1.0, sum = 1.0;
+  for (int k = 1; k < 40; ++k) {
+    const double a = 2.0 * k - 1.0;
+    t *= a * a / (8.0 * k * x);
+    sum += t;
+    if (t < 1.0e-17 * sum) break;
+  }
+  return sum / sqrt(2.0 * kPi * x);
 }
 
 }  // namespace mpdpft

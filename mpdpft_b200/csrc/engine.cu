@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mpdpft_gpu.h"
@@ -168,8 +169,7 @@ Ctx::~Ctx() { release(); }
 
 void Ctx::release() {
   adjoint_release();
-  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  drop_graphs();
   for (void* p : allocations) cudaFree(p);
   allocations.clear();
   if (pinned) { cudaFreeHost(pinned); pinned = nullptr; }
@@ -204,8 +204,8 @@ static int check_params(const mpdpft_params& p) {
     int t = p.interactions[a];
     if (t != 0 && t != 1 && t != 8 && t != 10 && t != 11 && t != 21 && t != 100)
       return set_error(MPDPFT_ERR_ARG, "unsupported interaction type " + std::to_string(t));
-    if ((t == 8 || t == 21 || t == 100) && p.dim != 3)
-      return set_error(MPDPFT_ERR_ARG, "Coulomb interactions need dim 3");
+    if ((t == 8 || t == 21 || t == 100) && p.dim == 2 && p.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED)
+      return set_error(MPDPFT_ERR_ARG, "2D Coulomb interactions use the reference's regularised 2D kernel only");
   }
   if (p.precision != MPDPFT_FP64 && p.precision != MPDPFT_MIXED) return set_error(MPDPFT_ERR_ARG, "bad precision");
   if (p.gradient_form != MPDPFT_GRADIENT_T0 && p.gradient_form != MPDPFT_GRADIENT_FINITE_T)
@@ -285,8 +285,7 @@ int Ctx::set_limits(int mu_passes, long long spins) {
   if (mu_passes == 0) return set_error(MPDPFT_ERR_ARG, "mu pass cap must be at least 1");
   mu_max_passes = mu_passes < 0 ? kMuMaxPasses : mu_passes;
   spin_limit = spins < 0 ? kBarrierSpinLimit : (long)spins;
-  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  drop_graphs();
   return MPDPFT_OK;
 }
 
@@ -413,8 +412,6 @@ int Ctx::reset_state(bool sync) {
   // a pageable source: the copy has read h when the call returns
   CU(cudaMemcpyAsync(d_state, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
   if (sync) CU(cudaStreamSynchronize(stream));
-  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
   return MPDPFT_OK;
 }
 
@@ -430,11 +427,42 @@ int Ctx::read_state(ScState* h) {
 // caller synchronises the stream before that half is used again.
 double* Ctx::host_stage(int slot) { return (double*)pinned + (slot ? std::max(n_ref, geom.n) : 0); }
 
+// Host copy of a large grid by several threads (one thread copies well
+// under the bandwidth of the host's memory).
+static void par_memcpy(void* dst, const void* src, size_t bytes) {
+  const size_t min_part = (size_t)1 << 20;
+  size_t nt = std::min<size_t>(8, std::max<size_t>(1, std::thread::hardware_concurrency()));
+  nt = std::min(nt, bytes / min_part);
+  if (nt <= 1) { std::memcpy(dst, src, bytes); return; }
+  const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nt; ++t) {
+    const size_t b = t * part;
+    if (b >= bytes) break;
+    pool.emplace_back([=] { std::memcpy((char*)dst + b, (const char*)src + b, std::min(part, bytes - b)); });
+  }
+  std::memcpy(dst, src, std::min(part, bytes));
+  for (std::thread& th : pool) th.join();
+}
+
 int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slot, bool sync) {
   if (!src) return set_error(MPDPFT_ERR_ARG, "null input array");
+  if (mem != MPDPFT_MEM_HOST) return import_staged(src, dst, layout, slot, sync);
+  // host grids cross in 4 MB chunks: the host copies chunk k into the pinned
+  // buffer while the DMA of chunk k - 1 runs
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
-  if (mem == MPDPFT_MEM_HOST) std::memcpy(host_stage(slot), src, sizeof(double) * cnt);
-  return import_staged(mem == MPDPFT_MEM_HOST ? nullptr : src, dst, layout, slot, sync);
+  double* hs = host_stage(slot);
+  double* dstage = d_io + (slot ? std::max(n_ref, geom.n) : 0);  // d_io holds two grids
+  const long chunk = 1L << 19;
+  for (long off = 0; off < cnt; off += chunk) {
+    const long len = std::min(chunk, cnt - off);
+    par_memcpy(hs + off, src + off, sizeof(double) * len);
+    CU(cudaMemcpyAsync(dstage + off, hs + off, sizeof(double) * len, cudaMemcpyHostToDevice, stream));
+  }
+  int st = import_staged(dstage, dst, layout, slot, false);
+  if (st) return st;
+  if (sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
+  return MPDPFT_OK;
 }
 
 // The device half of import_field: src (device) or, when src is null, the
@@ -492,7 +520,7 @@ int Ctx::export_field(const void* src, double* dst, int layout, int mem) {
   if (mem == MPDPFT_MEM_HOST) {
     CU(cudaMemcpyAsync(pinned, d_io, sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
-    std::memcpy(dst, pinned, sizeof(double) * cnt);
+    par_memcpy(dst, pinned, sizeof(double) * cnt);
   }
   return MPDPFT_OK;
 }
@@ -624,12 +652,13 @@ int Ctx::sc_init(const double* const* v0, int layout, int mem) {
     }
   }
   // automatic temperature (PreparationsForSCdensity, mpDPFT.cpp:4523-4528)
+  // (every solve takes its own from its V_0)
   bool need_t = false;
-  for (int s = 0; s < S; ++s) need_t |= temperature[s] < 0.0;
+  for (int s = 0; s < S; ++s) need_t |= P.temperature[s] < 0.0;
   if (need_t) {
     std::vector<double> h(geom.n);
     for (int s = 0; s < S; ++s) {
-      if (temperature[s] >= 0.0) continue;
+      if (P.temperature[s] >= 0.0) continue;
       if ((st = export_field((char*)d_V + (size_t)s * geom.n * rsize, h.data(), MPDPFT_LAYOUT_PERIODIC, MPDPFT_MEM_HOST))) return st;
       double vmin = h[0], vmax = h[0];
       for (double x : h) { vmin = std::min(vmin, x); vmax = std::max(vmax, x); }
@@ -648,11 +677,90 @@ int Ctx::sc_init(const double* const* v0, int layout, int mem) {
   return MPDPFT_OK;
 }
 
+void Ctx::drop_graphs() {
+  if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+  if (loop_exec) { cudaGraphExecDestroy(loop_exec); loop_exec = nullptr; }
+  if (loop_graph) { cudaGraphDestroy(loop_graph); loop_graph = nullptr; }
+  if (loop_state > 0) loop_state = 0;
+}
+
+// The captured graphs hold the kernel parameters by value; the only ones
+// that change after context creation are the automatic temperatures (set
+// per solve from V_0) and the device loop limits, so a graph is kept while
+// kparams() is what it was captured with.
+void Ctx::check_graphs() {
+  if (!graph_exec && !loop_exec) return;
+  const KParams k = kparams();
+  if (std::memcmp(&k, &graph_kp, sizeof(k)) != 0) drop_graphs();
+}
+
+// Last node of the device-side loop's body: loop again unless the exit test
+// has been met, a kernel aborted, or `cap` iterations have run.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const ScState* st, int cap) {
+  const bool stop = __ldcg(&st->exit_loop) != 0 || __ldcg(&st->abort) != 0 || __ldcg(&st->sc_count) >= cap;
+  cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+// The SC loop as one graph: a WHILE node whose body is one captured
+// iteration followed by k_loop_cond, so a solve runs without host round
+// trips between iterations.  Where the driver cannot build or instantiate
+// it (loop_state -1), sc_run replays the one-iteration graph from the host.
+int Ctx::build_loop() {
+  check_graphs();
+  if (loop_exec || loop_state < 0) return MPDPFT_OK;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle h = 0;
+  cudaGraphNode_t node = nullptr;
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  }
+  cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    loop_state = -1;
+    return MPDPFT_OK;
+  }
+  const KParams k = kparams();
+  int st = issue_iteration();
+  if (st == MPDPFT_OK) {
+    k_loop_cond<<<1, 1, 0, stream>>>(h, d_state, P.max_sc_count + 3);
+    if (cudaGetLastError() != cudaSuccess) st = -1;
+  }
+  cudaGraph_t out = nullptr;
+  e = cudaStreamEndCapture(stream, &out);
+  if (st == MPDPFT_OK && e == cudaSuccess) e = cudaGraphInstantiate(&loop_exec, g, 0);
+  // any failure here (a launch the driver does not take inside a loop body,
+  // say) leaves the host-driven loop, which reports real errors itself
+  if (st != MPDPFT_OK || e != cudaSuccess || !loop_exec) {
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    loop_exec = nullptr;
+    loop_state = -1;
+    g_last_error.clear();
+    return MPDPFT_OK;
+  }
+  loop_graph = g;
+  loop_state = 1;
+  graph_kp = k;
+  return MPDPFT_OK;
+}
+
 int Ctx::sc_step(int use_graph) {
   if (!initialised) return set_error(MPDPFT_ERR_ARG, "sc_init has not been called");
   int st;
   if (!use_graph) return issue_iteration();
+  check_graphs();
   if (!graph_exec) {
+    graph_kp = kparams();
     CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < 6; ++i) cnt[i] = 0;
     notes.clear();
@@ -772,9 +880,20 @@ int Ctx::sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_gr
   auto t0 = std::chrono::steady_clock::now();
   int st;
   ScState h;
+  bool looped = false;
+  if (use_graph) {
+    if (!initialised) return set_error(MPDPFT_ERR_ARG, "sc_init has not been called");
+    if ((st = build_loop())) return st;
+    if (loop_exec) {
+      CU(cudaGraphLaunch(loop_exec, stream));
+      if ((st = read_state(&h))) return st;
+      if ((st = status_from_state(h))) return st;
+      looped = true;
+    }
+  }
   const int chunk = 4;
   int issued = 0;
-  for (;;) {
+  while (!looped) {
     for (int c = 0; c < chunk; ++c, ++issued)
       if ((st = sc_step(use_graph))) return st;
     CU(cudaStreamSynchronize(stream));
@@ -787,6 +906,7 @@ int Ctx::sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_gr
     std::memset(result, 0, sizeof(*result));
     if ((st = fill_result(result, h))) return st;
     result->seconds = std::chrono::duration<double>(t1 - t0).count();
+    result->device_loop = looped ? 1 : 0;
   }
   if (log && cap > 0) {
     int nlog = std::min(cap, std::min(h.sc_count, log_cap));
@@ -912,6 +1032,8 @@ int Ctx::op_mu_search(int s, const double* v, double target, double* mu_io, doub
   }
   if (h.status_bits & kBitBracket) return set_error(MPDPFT_ERR_MU_BRACKET, "mu bracket not found; mu reset");
   if (h.status_bits & kBitTimeout) return set_error(MPDPFT_ERR_TIMEOUT, "mu search reached its pass cap");
+  if (h.status_bits & kBitTrapped)
+    return set_error(MPDPFT_WARN_MU_TRAPPED, "mu search trapped at a step of N(mu) (TrappedQ); mu and N are its end point");
   return MPDPFT_OK;
 }
 

@@ -72,8 +72,14 @@ struct Ctx {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
   std::vector<void*> allocations;
-  cudaGraph_t graph = nullptr;
+  cudaGraph_t graph = nullptr;          // one SC iteration (mpdpft_sc_step)
   cudaGraphExec_t graph_exec = nullptr;
+  // the whole SC loop on the device: a WHILE conditional node around one
+  // iteration whose last kernel clears the condition at the exit test
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_state = 0;  // 0: not built yet, 1: built, -1: not available (host loop)
+  KParams graph_kp;    // kernel parameters the captured graphs were built with
   FftPlan* fft = nullptr;
   Adjoint* adj = nullptr;  // adjoint work fields (allocated on first use)
   // launches of the iteration being captured, in issue order: kernel name
@@ -114,6 +120,9 @@ struct Ctx {
   int issue_iteration();
   int sc_init(const double* const* v0, int layout, int mem);
   int sc_step(int use_graph);
+  void drop_graphs();
+  void check_graphs();  // drop captured graphs whose kernel parameters changed
+  int build_loop();
   int sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph);
   int fill_result(mpdpft_result* r, const ScState& h);
   int energy(mpdpft_result* r, const ScState& h);

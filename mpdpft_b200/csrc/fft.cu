@@ -103,7 +103,8 @@ enum { PRO_NONE = 0, PRO_TAPER = 1, PRO_CHARGE = 2 };
 // species (k_assemble_v fused into the transform; plane kernels only)
 enum { EPI_STORE = 0, EPI_POS = 1, EPI_GRAD = 2, EPI_COULOMB = 3, EPI_SCALE = 4, EPI_COULOMB_V = 5 };
 // MUL_LAP: the Laplacian output of MUL_DERIV alone (one output)
-enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3, MUL_LAP = 4 };
+// MUL_COULOMB_2D: the reference's 2D kernel (n~ - n~0 e^{-k^2})/k, k = 0 -> 0
+enum { MUL_COULOMB_REG = 0, MUL_COULOMB_TRUNC = 1, MUL_DERIV = 2, MUL_SMOOTH = 3, MUL_LAP = 4, MUL_COULOMB_2D = 5 };
 
 template <typename R>
 struct ZArgs {
@@ -179,8 +180,13 @@ __device__ __forceinline__ R taper_value(const ZArgs<R>& a, long p, R x, double 
 
 // Coulomb epilogue value at (x, y, z): coef (v + f0 pi erf(r/2)/r / (4 pi^2))
 // (mpDPFT.cpp:2704-2711).
+// 2D (mpDPFT.cpp:2657-2662): coef (v + f0 e^{-r^2/8} I0(r^2/8) / (4 sqrt pi)).
 template <typename R>
 __device__ __forceinline__ R coulomb_xyz(const ZArgs<R>& a, double x, double y, double z, R v, double f0) {
+  if (a.g.dim == 2) {
+    const double q = 0.125 * (x * x + y * y);
+    return R(a.coul_coef * ((double)v + f0 * bessel_i0e(q) / (4.0 * 1.7724538509055159)));
+  }
   if constexpr (sizeof(R) == sizeof(float)) {  // FP32 fields: the term in FP32
     const float r = sqrtf(float(x) * float(x) + float(y) * float(y) + float(z) * float(z));
     const float zf = r > 1.0e-10f ? float(kPi) * erff(0.5f * r) / r : float(1.7724538509055159);
@@ -562,6 +568,17 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier(const AxisArgs<R>&
   const double ky = a.dk * (double)qy;
   const double kz = a.dk * (col == a.M ? -(double)a.M : (double)col);  // col M: Nyquist
   const double k2 = kx * kx + ky * ky + kz * kz;  // 2D: ky = 0, kz is the contiguous axis
+  if (a.mul == MUL_COULOMB_2D) {
+    // (n~ - n~0 e^{-k^2})/k on the real part, n~/k on the imaginary part,
+    // k <= 1e-5 dk -> 0 (mpDPFT.cpp:2647-2657); phase as below
+    const double k = sqrt(k2);
+    if (k > 0.00001 * a.dk) {
+      const int par = (t + col) & 1;
+      const double g = exp(-k2) * f0 * (par ? -1.0 : 1.0);
+      return C{R(((double)v.x - g) / k * a.scale), R((double)v.y / k * a.scale)};
+    }
+    return C{R(0), R(0)};
+  }
   if (a.mul == MUL_COULOMB_REG) {
     // (n~ - n~0 e^{-k^2})/k^2, k = 0 -> n~0 (mpDPFT.cpp:2686-2701); the
     // centred transform's phase (-1)^{qx+qy+qz} carries over to the
@@ -617,6 +634,16 @@ __device__ __forceinline__ typename Cx<R>::T apply_multiplier_tab(const AxisArgs
   if (a.mul == MUL_COULOMB_TRUNC) return apply_multiplier<R>(a, v, t, outer, col, o, f0);
   const R kx = T.kx[t];
   const R k2 = kx * kx + T.k2yz[l];
+  if (a.mul == MUL_COULOMB_2D) {
+    const R k = sqrt(k2);
+    if ((double)k > 0.00001 * a.dk) {
+      const int par = (t + T.par[l]) & 1;
+      const R g = T.gx[t] * T.gyz[l] * R(f0) * (par ? R(-1) : R(1));
+      const R ik = sc / k;
+      return C{(v.x - g) * ik, v.y * ik};
+    }
+    return C{R(0), R(0)};
+  }
   if (a.mul == MUL_COULOMB_REG) {
     if ((double)k2 > 1.0e-6 * a.dk * a.dk) {
       const int par = (t + T.par[l]) & 1;
@@ -647,7 +674,7 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double s_f0;
-  if (a.mul == MUL_COULOMB_REG) {
+  if (a.mul == MUL_COULOMB_REG || a.mul == MUL_COULOMB_2D) {
     if (threadIdx.x < 32) {
       double t = 0.0;
       for (int b = threadIdx.x; b < a.f0_blocks; b += 32) t += a.f0_part[b];
@@ -701,7 +728,7 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
     auto gload = [&](int t, int l) -> C { return s_ok[l] ? data[s_base[l] + t * as] : C{R(0), R(0)}; };
     auto fstore = [&](int t, int l, C v) { F[t * (NL + 1) + l] = v; };
     fft_lines<C, NC, NL, false>(A, B, twf, -1, gload, fstore);
-    const double f0 = a.mul == MUL_COULOMB_REG ? s_f0 : 0.0;
+    const double f0 = (a.mul == MUL_COULOMB_REG || a.mul == MUL_COULOMB_2D) ? s_f0 : 0.0;
     for (int o = 0; o < a.nout; ++o) {
       C* dst = a.out[o];
       auto mload = [&](int t, int l) -> C {
@@ -728,7 +755,7 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
     __syncthreads();
     C* F = tile_fft<C>(A, B, a.plan, tk, a.twf, -1);
     C* spare = (F == A) ? B : A;  // two free buffers: spare and W
-    const double f0 = a.mul == MUL_COULOMB_REG ? s_f0 : 0.0;
+    const double f0 = (a.mul == MUL_COULOMB_REG || a.mul == MUL_COULOMB_2D) ? s_f0 : 0.0;
     for (int o = 0; o < a.nout; ++o) {
       for (int w = threadIdx.x; w < n * tk; w += blockDim.x) {
         const int t = w / tk, l = w % tk;
@@ -1443,6 +1470,11 @@ static int coulomb_into(Ctx& c, const R* src, int nsrc, const double* qcoef, R* 
   FftPlan& f = *c.fft;
   int st;
   const int pro = nsrc > 1 || (qcoef && qcoef[0] != 1.0) ? PRO_CHARGE : PRO_NONE;
+  if (f.dim == 2) {  // HartreeRepulsion 2D (mpDPFT.cpp:2636-2665): V = 2 pi gammaH (...)
+    if ((st = launch_z_r2c<R>(c, src, pro, nsrc, qcoef, f.spec[0], true))) return st;
+    if ((st = launch_x<R>(c, f.spec[0], &f.spec[0], 1, MUL_COULOMB_2D, 0.0))) return st;
+    return launch_z_c2r<R>(c, &f.spec[0], 1, EPI_COULOMB, out, nullptr, 2.0 * kPi * coef);
+  }
   const int mul = c.P.coulomb_kernel == MPDPFT_COULOMB_TRUNCATED ? MUL_COULOMB_TRUNC : MUL_COULOMB_REG;
   if (f.plane && pro == PRO_NONE) {
     if ((st = launch_plane_fwd<R>(c, src, pro, f.spec[0], true))) return st;
@@ -1727,9 +1759,9 @@ int Ctx::op_vint(int type, int s, const double* const* nn, double* v_out, int la
   P.interactions[0] = type;
   P.incremental_v = 1.0;
   const bool coul = type == MPDPFT_INT_HARTREE || type == MPDPFT_INT_HARTREE_INTER || type == MPDPFT_INT_COULOMB_CHARGED;
-  if (coul && (!fft || !fft->spec[0] || geom.dim != 3)) {
+  if (coul && (!fft || !fft->spec[0])) {
     P = saved;
-    return set_error(MPDPFT_ERR_ARG, "Coulomb terms need a 3D context created with a Coulomb interaction");
+    return set_error(MPDPFT_ERR_ARG, "Coulomb terms need a context created with a Coulomb interaction");
   }
   void* out = (char*)d_V + (size_t)s * geom.n * rsize;  // staging
   if (coul) {

@@ -1013,6 +1013,22 @@ __device__ __forceinline__ void sc_phase_d(const StepArgs<R>& a, const int nblk,
   __syncthreads();
   if (threadIdx.x == 0) {
     const int sc = ls->sc_count;
+    // TrappedQ (mpDPFT.cpp:4926-4934): a mu search that ended without
+    // meeting the tolerance lowers this iteration's mixing weight theta by
+    // min(1, |1 - RelDiff|^30), RelDiff = |N* - N| / |N*| over the species
+    int trapped = 0;
+    for (int s = 0; s < S; ++s) trapped |= ls->ms[s].trapped;
+    double tmod = 1.0;
+    if (trapped) {
+      double na = 0.0, nd = 0.0;
+      for (int s = 0; s < S; ++s) {
+        na += kp.abundance[s] * kp.abundance[s];
+        nd += (kp.abundance[s] - ls->ab[s]) * (kp.abundance[s] - ls->ab[s]);
+      }
+      const double rd = sqrt(nd) / sqrt(na);
+      if (rd > 1.0e-12) tmod = fmin(1.0, pow(fabs(1.0 - rd), 30.0));
+      ls->iter_bits |= kBitTrapped;
+    }
     if (a.mode == 1) {
       ls->status_bits |= ls->iter_bits;
       ls->mu_passes_total += ls->mu_passes;
@@ -1020,7 +1036,7 @@ __device__ __forceinline__ void sc_phase_d(const StepArgs<R>& a, const int nblk,
       const int used = pulay_now ? ls->pulay_used : 0;
       if (!pulay_now) { ls->pulay_used = 0; ls->ncoeff = 0; }
       ls->iter_bits |= s_pbits;
-      for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s];
+      for (int s = 0; s < S; ++s) ls->theta_mix[s] = ls->theta[s] * tmod;
       // InjectSchedule (mpDPFT.cpp:5229-5315)
       if (kp.schedule == 5) {
         for (int s = 0; s < S; ++s) {

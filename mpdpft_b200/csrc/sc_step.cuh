@@ -66,6 +66,7 @@ struct MuState {
   double step;     // size of the last Newton step
   double last_mu, last_N;     // last bracket-step position and its N
   double cand_prev0, N_prev0; // candidate 0 of the evaluated pass and its N
+  int trapped;  // ended inside a bracket without meeting the tolerance
 };
 
 // SC loop state, resident in device memory.
@@ -222,6 +223,7 @@ __device__ inline void mu_begin(MuState& m, double mu, double prev_abs, double d
   m.best_N = 0.0;
   m.best_err = 1e300;
   m.step = 0.0;
+  m.trapped = 0;
   m.ncand = 0;
   m.cand[m.ncand++] = mu;
   m.cand[m.ncand++] = mu - m.delta0;  // first reference step, both directions
@@ -248,6 +250,7 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
   for (int c = 0; c < m.ncand; ++c)
     if (!isfinite(N[c])) bits |= kBitNonfinite;
   const bool bracket_before = m.have_lo && m.have_hi;
+  bool poor = false;  // an in-bracket pass that left more than a quarter of the bracket
   m.cand_prev0 = m.cand[0];
   m.N_prev0 = N[0];
   if (m.pass == 0) {
@@ -275,6 +278,7 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
     m.last_mu = pm; m.last_N = pN;
   } else {
     // inside the bracket: tighten it and track the best point
+    const double w0 = m.hi - m.lo;
     for (int c = 0; c < m.ncand; ++c) {
       const double mu = m.cand[c], n = N[c];
       if (!(mu > m.lo && mu < m.hi) || !isfinite(n)) continue;
@@ -283,11 +287,17 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
       if (n < target) { m.lo = mu; m.Nlo = n; }
       else if (n > target) { m.hi = mu; m.Nhi = n; }
     }
+    poor = !(m.hi - m.lo <= 0.25 * w0);
   }
   m.pass++;
   m.dens_mu = m.best_mu;
   if (m.best_err <= rel_acc) { m.done = 1; return; }
-  if (m.pass >= max_passes) { m.done = 1; bits |= kBitTimeout; return; }
+  if (m.pass >= max_passes) {
+    m.done = 1;
+    m.trapped = m.have_lo && m.have_hi;
+    bits |= kBitTimeout;
+    return;
+  }
   m.ncand = 0;
   if (!(m.have_lo && m.have_hi)) {
     if (m.next_c > 20) {
@@ -303,7 +313,18 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
     while (m.next_c <= 20 && m.ncand < kMuCand) m.cand[m.ncand++] = m.start + m.dir * step_offset(m, m.next_c++);
     return;
   }
-  if (!(m.hi - m.lo > 1.0e-12)) { m.done = 1; return; }  // Deltamu below MP (:4711)
+  // the bracket has closed to MP (1e-12) without meeting the tolerance.  The
+  // reference's bisection stops either on Deltamu < MP (:4711, a warning:
+  // N(mu) too steep for the tolerance) or, earlier, on its trap test
+  // (:4690-4703: abundances repeating within RelAcc N*, i.e. N(mu) changes
+  // by less than that over the remaining steps while a step of N straddles
+  // the target), which sets TrappedQ: the latter where the local slope
+  // moves N by less than RelAcc N* over MP
+  if (!(m.hi - m.lo > 1.0e-12)) {
+    m.done = 1;
+    m.trapped = !(slope * 1.0e-12 >= rel_acc * fabs(target));
+    return;
+  }
   if (!bracket_before) {
     // the reference starts bisecting at the bracket midpoint (:4667-4672);
     // its first evaluation also provides the slope for Newton steps
@@ -320,25 +341,6 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
         m.cand[m.ncand++] = est;  // candidate 0 carries the slope
         if (est - e > m.lo) m.cand[m.ncand++] = est - e;
         if (est + e < m.hi) m.cand[m.ncand++] = est + e;
-      }
-    }
-    // the quadratic through N at both bracket ends with the slope at
-    // candidate 0 (one of them): a third-order estimate that usually meets
-    // the tolerance here, so a steady-state search ends after two passes
-    if (slope > 0.0 && isfinite(slope) && isfinite(m.N_prev0) && m.ncand + 3 <= kMuCand - 2) {
-      const double c0 = m.cand_prev0, N0 = m.N_prev0;
-      const bool at_lo = c0 == m.lo;
-      const double h = (at_lo ? m.hi : m.lo) - c0, N1 = at_lo ? m.Nhi : m.Nlo;
-      const double qa = (N1 - N0 - slope * h) / (h * h), qc = N0 - target;
-      const double disc = slope * slope - 4.0 * qa * qc;
-      if (h != 0.0 && disc >= 0.0 && isfinite(qa)) {
-        const double est = c0 - 2.0 * qc / (slope + sqrt(disc));
-        if (est > m.lo && est < m.hi) {
-          const double e = fmax(1e-6 * fabs(est - c0), 1e-13 * fabs(est) + 1e-300);
-          m.cand[m.ncand++] = est;
-          if (est - e > m.lo) m.cand[m.ncand++] = est - e;
-          if (est + e < m.hi) m.cand[m.ncand++] = est + e;
-        }
       }
     }
     const double rf = m.lo + (target - m.Nlo) * (m.hi - m.lo) / (m.Nhi - m.Nlo);
@@ -365,7 +367,15 @@ __device__ inline void mu_decide(MuState& m, const double* N, double slope, doub
   m.cand[m.ncand++] = est;
   if (est - e > m.lo) m.cand[m.ncand++] = est - e;
   if (est + e < m.hi) m.cand[m.ncand++] = est + e;
-  if (m.pass > 3) m.cand[m.ncand++] = 0.5 * (m.lo + m.hi);
+  // a pass that left more than a quarter of the bracket (N(mu) too rough
+  // for the Newton placement, e.g. where the adaptive Airy quadrature
+  // changes its subdivision with mu), and every pass after the third, puts
+  // the free candidates on an even subdivision of the bracket, so such a
+  // pass shrinks it at least (free + 1)-fold
+  if (poor || m.pass > 3) {
+    const int nfree = kMuCand - m.ncand;
+    for (int k = 1; k <= nfree; ++k) m.cand[m.ncand++] = m.lo + (m.hi - m.lo) * ((double)k / (double)(nfree + 1));
+  }
 }
 
 }  // namespace mpdpft

@@ -99,6 +99,25 @@ def harmonic_tf(steps=64, edge=24.0, precision=abi.FP64, seed=SEED_BASE + 1, **o
     return p, [vext], [v0]
 
 
+def quantum_dot_2d(steps=64, edge=24.0, precision=abi.FP64, n_target=20.0, seed=SEED_BASE + 6, **over):
+    """A 2D electron droplet: N = 20 electrons (g = 2) in the harmonic trap
+    V_ext = r^2/2, TF density n = g (mu - V)_+ / (2 pi) (DenExpr 7), Hartree
+    repulsion by the reference's 2D kernel (HartreeRepulsion,
+    mpDPFT.cpp:2636-2665) and 2D Dirac exchange, Pulay history 5, theta 0.3;
+    V_0 = V_ext + U(-1e-3, 1e-3)."""
+    mu0 = np.sqrt(2.0 * n_target / 2.0)  # noninteracting 2D TF estimate
+    kw = dict(dim=2, steps=steps, species=1, edge=edge, abundances=[n_target],
+              rel_acc=1e-10, density_expression=abi.DENS_TF, degeneracy=2.0,
+              interactions=[abi.INT_HARTREE, abi.INT_DIRAC], gamma_h=1.0, mu=[mu0],
+              mixer=1, pulay_scope=5, theta=[0.3], sc_criterion=1e-12,
+              max_sc_count=400, potential_tol=1e-8, precision=precision)
+    kw.update(over)
+    p = abi.make_params(**kw)
+    vext = 0.5 * radius2(2, steps, edge).reshape(-1)
+    v0 = vext + noise(vext.shape, 1e-3, seed)
+    return p, [vext], [v0]
+
+
 def argon_atom(steps=128, edge=20.0, precision=abi.MIXED, seed=SEED_BASE + 2, **over):
     """Neutral atom Z = 18: Gaussian nucleus (sigma 0.1 bohr) at the centre of
     [-10, 10]^3, TF + gradient correction (spectral grad V and Laplacian,

@@ -595,13 +595,57 @@ void get_density_and_abundance(State& st, int s) {
   st.mu_trials++;
 }
 
-// ------------------------------------------ Hartree MD:2583-2717 (3D) --
+// e^{-x} I0(x), x >= 0, for the 2D compensation term (gsl_sf_bessel_I0 times
+// EXP(-x) at MD:2659): the power series of I0 below x = 30 (positive terms),
+// the asymptotic series (2 pi x)^{-1/2} sum [(2k-1)!!]^2 / (k! (8x)^k) above.
+double i0e(double x) {
+  if (x < 30.) {
+    const double q = 0.25 * x * x;
+    double t = 1., sum = 1.;
+    for (int k = 1; k < 200 && t >= 1e-17 * sum; ++k) {
+      t *= q / ((double)k * k);
+      sum += t;
+    }
+    return sum * std::exp(-x);
+  }
+  double t = 1., sum = 1.;
+  for (int k = 1; k < 40 && t >= 1e-17 * sum; ++k) {
+    t *= (2. * k - 1.) * (2. * k - 1.) / (8. * k * x);
+    sum += t;
+  }
+  return sum / std::sqrt(2. * PI * x);
+}
+
+// ------------------------------------------ Hartree MD:2583-2717 --------
 // Coulomb potential of rho, gammaH * int rho(r')/|r-r'| (no prefactor here).
+// 2D (HartreeType 0, MD:2636-2665): n~ -> (n~ - n~0 e^{-k^2})/k (imaginary
+// part / k), k = 0 -> 0, then 2 pi (IFT + n~0 e^{-z^2/8} I0(z^2/8)/(4 sqrt pi)).
 void coulomb(State& st, const std::vector<double>& rho, std::vector<double>& out) {
   const long G = st.G;
   for (long i = 0; i < G; ++i) st.CF[i] = cplx(rho[i], 0.);
   fft_parallel(st, -1, st.CF);
   const double f0 = st.CF[st.centre].real();
+  if (st.D == 2) {
+    const double kmin = 0.00001 * st.dk;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < G; ++i) {
+      double k = std::sqrt(knorm2(st, i));
+      if (k > kmin) st.CF[i] = cplx((st.CF[i].real() - f0 * EXPc(-k * k)) / k, st.CF[i].imag() / k);
+      else st.CF[i] = cplx(0., 0.);
+    }
+    fft_parallel(st, +1, st.CF);
+    out.resize(G);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < G; ++i) {
+      double r3[3];
+      coords(st, i, r3);
+      const double z2 = r3[0] * r3[0] + r3[1] * r3[1];
+      const double x = z2 / 8.;
+      const double ebi = x < 1.0e+300 ? i0e(x) : 1. / std::sqrt(2. * PI * x);
+      out[i] = 2. * PI * (st.CF[i].real() + f0 * ebi / (4. * std::sqrt(PI)));
+    }
+    return;
+  }
   if (st.P.coulomb_kernel == MPDPFT_COULOMB_REGULARISED) {
     const double kzero = 0.000001 * st.dk * st.dk;
 #pragma omp parallel for schedule(static)
@@ -775,6 +819,7 @@ void enforce_constraints(State& st) {
                 if (h >= 0 && hp > h && std::fabs(hist[h] - hist[hp]) < st.relacc_orig * Ab[s]) {
                   trap++;
                   st.trapped = true;
+                  st.status_bits |= 1 << MPDPFT_WARN_MU_TRAPPED;
                   break;
                 }
           }
@@ -1167,10 +1212,17 @@ void oracle_vint(const mpdpft_params* p, int type, int s, const double* dens, do
 
 // EnforceConstraints for all species from potentials v (S grids) and the
 // starting mu in p->mu.  Writes mu, N, trials and densities.
+static int g_last_status_bits = 0;
+
+// status bits of the last oracle_mu_search (MPDPFT_WARN_MU_TRAPPED: the
+// bisection ended on the reference's trap test)
+int oracle_last_status_bits() { return g_last_status_bits; }
+
 int oracle_mu_search(const mpdpft_params* p, const double* v, double* mu_out, double* ab_out,
                      double* dens_out, double* deltamu_modifier_io) {
   State st;
   init_state(st, *p);
+  st.status_bits = 0;
   if (deltamu_modifier_io) st.dmm = *deltamu_modifier_io;
   for (int q = 0; q < st.S; ++q) st.V[q].assign(v + q * st.G, v + (q + 1) * st.G);
   get_densities(st);
@@ -1180,6 +1232,7 @@ int oracle_mu_search(const mpdpft_params* p, const double* v, double* mu_out, do
     if (dens_out) std::memcpy(dens_out + q * st.G, st.Den[q].data(), sizeof(double) * st.G);
   }
   if (deltamu_modifier_io) *deltamu_modifier_io = st.dmm;
+  g_last_status_bits = st.status_bits;
   return (int)st.mu_trials;
 }
 
@@ -1297,6 +1350,7 @@ int oracle_num_threads(void) {
 // (species 0 of p, temperature T, u = mu - V), for the known-answer tests.
 double oracle_polylog(int order, double x) { return polylog(order, x); }
 double oracle_curly_a(double x) { return CurlyA(x); }
+double oracle_i0e(double x) { return i0e(x); }
 double oracle_finite_t_point(const mpdpft_params* p, double T, double u, double lap, double grad2) {
   State st;
   mpdpft_params q = *p;

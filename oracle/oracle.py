@@ -43,6 +43,7 @@ def lib():
         L.oracle_vint.argtypes = [P, C.c_int, C.c_int, _dp, _dp]
         L.oracle_mu_search.argtypes = [P, _dp, _dp, _dp, _dp, _dp]
         L.oracle_mu_search.restype = C.c_int
+        L.oracle_last_status_bits.restype = C.c_int
         L.oracle_sc_run.argtypes = [P, _dp, _dp, C.POINTER(abi.Result), C.POINTER(abi.IterLog),
                                     C.c_int, _dp, _dp]
         L.oracle_sc_run.restype = C.c_int
@@ -56,6 +57,8 @@ def lib():
         L.oracle_polylog.restype = C.c_double
         L.oracle_curly_a.argtypes = [C.c_double]
         L.oracle_curly_a.restype = C.c_double
+        L.oracle_i0e.argtypes = [C.c_double]
+        L.oracle_i0e.restype = C.c_double
         L.oracle_finite_t_point.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_double]
         L.oracle_finite_t_point.restype = C.c_double
         _lib = L
@@ -94,6 +97,11 @@ def polylog(s, x):
 def curly_a(x):
     """int_x^inf Ai(t) dt (the reference's CurlyA)."""
     return lib().oracle_curly_a(float(x))
+
+
+def i0e(x):
+    """e^{-x} I0(x) of the 2D Hartree compensation term."""
+    return lib().oracle_i0e(float(x))
 
 
 def finite_t_point(p, T, u, lap, grad2):
@@ -141,6 +149,12 @@ def density(p, s, v, mu):
     n = np.empty_like(r)
     N = lib().oracle_density(C.byref(p), s, _ptr(r), mu, _ptr(n))
     return _per(p, n), N
+
+
+def last_status_bits():
+    """Status bits of the last mu_search (1 << abi.WARN_MU_TRAPPED: the
+    bisection ended on the reference's trap test)."""
+    return lib().oracle_last_status_bits()
 
 
 def vint(p, type_, s, dens):

@@ -61,6 +61,31 @@ def test_barrier_spin_limit_times_out_and_context_recovers(eng):
         assert abs(res.abundance[0] - 1000.0) <= 2e-7
 
 
+def test_trapped_search_damps_the_mixing_weight(eng):
+    """A mu search that ends inside its bracket without meeting rel_acc (here
+    stopped by a pass cap of 2) is the reference's TrappedQ case
+    (EnforceConstraints, mpDPFT.cpp:4690-4703): the iteration's status bits
+    carry MPDPFT_WARN_MU_TRAPPED and it mixes with theta * min(1,
+    |1 - RelDiff|^30), RelDiff = |N* - N| / |N*| (AdmixDensities,
+    mpDPFT.cpp:4926-4934); iterations whose search met the tolerance, or
+    found no bracket, mix with theta itself."""
+    p, vext, v0 = W.harmonic_tf(steps=32, precision=abi.FP64)
+    bit = 1 << abi.WARN_MU_TRAPPED
+    with eng.Engine(p) as e:
+        e.sc_init(vext, v0)
+        e.set_limits(mu_max_passes=2)
+        logs = [e.sc_step(graph=True, want_log=True) for _ in range(8)]
+    trapped = [L for L in logs if L.status_bits & bit]
+    print("trapped iterations %d of %d; RelDiff %s" %
+          (len(trapped), len(logs), [abs(1000.0 - L.abundance[0]) / 1000.0 for L in trapped]))
+    assert trapped
+    for L in logs:
+        rd = abs(1000.0 - L.abundance[0]) / 1000.0
+        mod = min(1.0, abs(1.0 - rd) ** 30) if (L.status_bits & bit) and rd > 1e-12 else 1.0
+        assert abs(L.theta[0] - p.theta[0] * mod) <= 1e-15 * p.theta[0]
+    assert any(L.theta[0] < p.theta[0] for L in trapped)
+
+
 def test_set_limits_rejects_bad_values(eng):
     p, _, _ = W.harmonic_tf(steps=16)
     with eng.Engine(p) as e:

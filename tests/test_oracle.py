@@ -190,3 +190,22 @@ def test_mu_search_two_species_gradient(oracle_lib):
         n, N = oracle_lib.density(p, s, v[s], mu[s])
         assert np.abs(dens[s] - n).max() <= 1e-12 * np.abs(n).max()
         assert abs(N - ab[s]) <= 1e-9 * ab[s]
+
+
+def test_hartree_2d_gaussian_known_answer(oracle_lib):
+    """2D Hartree (HartreeRepulsion, mpDPFT.cpp:2636-2665): the potential of
+    a Gaussian sheet of charge N, variance 1 per axis, is
+    N sqrt(pi/2) e^{-r^2/4} I0(r^2/4).  The regularised kernel removes the
+    Gaussian part analytically, so what remains is the periodic images of a
+    neutral residual: 6e-5 of the peak on [-20, 20]^2, independent of the
+    grid."""
+    import scipy.special as sp
+    s, L, N = 128, 40.0, 5.0
+    p = abi.make_params(dim=2, steps=s, edge=L, gamma_h=1.0, interactions=[abi.INT_HARTREE], precision=abi.FP64)
+    x = W.axis(s, L)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    r2 = (X * X + Y * Y).reshape(-1)
+    n = N / (2.0 * np.pi) * np.exp(-r2 / 2.0)
+    v = oracle_lib.vint(p, abi.INT_HARTREE, 0, [n])
+    exact = N * np.sqrt(np.pi / 2.0) * sp.i0e(r2 / 4.0)
+    assert np.abs(v - exact).max() < 1e-4 * exact.max()

@@ -123,3 +123,13 @@ def test_finite_t_airy_branch_point(oracle_lib, T, u, lap, g2):
                              gradient_form=abi.GRADIENT_FINITE_T, airy_threshold=0.0, boole_pairs=1,
                              boole_max_iter=1, internal_acc=0.01, abundances=[1e3])
     assert abs(oracle_lib.finite_t_point(coarse, T, u, lap, g2) - ref) <= 0.5 * abs(ref)
+
+
+def test_bessel_i0e_against_scipy(oracle_lib):
+    """e^{-x} I0(x) of the 2D Hartree compensation term (gsl_sf_bessel_I0
+    times EXP(-x), mpDPFT.cpp:2659) against scipy's Cephes implementation,
+    over the series range, the switch at x = 30 and the asymptotic range."""
+    import scipy.special as sp
+    xs = np.concatenate([np.linspace(0.0, 40.0, 801), np.geomspace(1e-8, 1e4, 200)])
+    err = max(abs(oracle_lib.i0e(x) - sp.i0e(x)) / sp.i0e(x) for x in xs)
+    assert err < 1e-14, err
