@@ -195,8 +195,9 @@ int Batch::init(const mpdpft_params* params, int n, int dev) {
     for (int a = 0; a < p.n_interactions; ++a) {
       const int t = p.interactions[a];
       if (t != p0.interactions[a] || (t != MPDPFT_INT_CONTACT_MUTUAL && t != MPDPFT_INT_CONTACT_SELF &&
-                                      t != MPDPFT_INT_DIRAC))
-        return set_error(MPDPFT_ERR_ARG, "batch: pointwise interactions (types 1, 10, 11) only");
+                                      t != MPDPFT_INT_DIRAC && t != MPDPFT_INT_HARTREE &&
+                                      t != MPDPFT_INT_HARTREE_INTER && t != MPDPFT_INT_COULOMB_CHARGED))
+        return set_error(MPDPFT_ERR_ARG, "batch: interaction types 1, 8, 10, 11, 21 and 100 only");
     }
   }
   int ndev = 0;
@@ -381,6 +382,16 @@ int Batch::issue_sc(int mode) {
 int Batch::issue_iteration() {
   int st;
   CU(cudaMemsetAsync(d_vmax, 0, sizeof(unsigned long long) * kMaxS * count, stream));
+  // Coulomb terms of the current densities, every grid size on its own stream
+  if (!classes.empty() && batch_fft_has_coulomb(classes[0])) {
+    CU(cudaEventRecord(events[0], stream));
+    for (size_t k = 0; k < classes.size(); ++k) {
+      CU(cudaStreamWaitEvent(side[k], events[0], 0));
+      if ((st = batch_fft_issue_coulomb(classes[k], side[k]))) return st;
+      CU(cudaEventRecord(events[1 + k], side[k]));
+      CU(cudaStreamWaitEvent(stream, events[1 + k], 0));
+    }
+  }
   if ((st = batch_assemble_issue(assemble, 1, stream))) return st;
   // DelField of every grid size on its own stream
   CU(cudaEventRecord(events[0], stream));

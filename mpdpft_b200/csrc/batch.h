@@ -23,6 +23,10 @@ struct BatchMember {
 struct BatchFftClass;
 int batch_fft_create(const std::vector<BatchMember>& members, unsigned long long* vmax_all, BatchFftClass** out);
 int batch_fft_issue(BatchFftClass* b, cudaStream_t st);
+// the Coulomb terms of every argument set of the class (2D kernel, into each
+// member's vh), when its solves have Coulomb interactions
+bool batch_fft_has_coulomb(const BatchFftClass* b);
+int batch_fft_issue_coulomb(BatchFftClass* b, cudaStream_t st);
 void batch_fft_destroy(BatchFftClass* b);
 
 // Rows of V-residual partial sums the V assembly of c writes.

@@ -524,6 +524,36 @@ __device__ __forceinline__ R density_slope(const DensParams& d, R u) {
   return R(d.g / (2.0 * kPi));
 }
 
+// Programmatic dependent launch.  A kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may begin while the
+// kernel before it on the stream is still running: pdl_wait() returns once
+// that kernel has completed and its memory is visible (a no-op for a kernel
+// launched without the attribute), pdl_trigger() lets the next kernel begin
+// once every block of this one has called it or exited.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Kernel launch with programmatic stream serialization (the kernels of the
+// SC iteration call pdl_wait before touching memory and pdl_trigger when
+// their block is done), process-wide unless a captured graph with
+// programmatic edges could not be built (pdl_disable).
+bool pdl_enabled();
+void pdl_disable();
+template <typename... P, typename... A>
+inline cudaError_t launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+}
+
 // e^{-x} I0(x) for x >= 0 (the exponentially scaled modified Bessel function
 // of the 2D Coulomb compensation term, mpDPFT.cpp:2659).  Below x = 30 the
 // power series I0(x) = sum_k (x^2/4)^k / (k!)^2 (positive terms, no

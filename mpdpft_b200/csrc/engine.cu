@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,11 @@
 namespace mpdpft {
 
 thread_local std::string g_last_error;
+
+// programmatic dependent launch of the SC iteration's kernels (launch_k)
+static std::atomic<bool> g_pdl{true};
+bool pdl_enabled() { return g_pdl.load(std::memory_order_relaxed); }
+void pdl_disable() { g_pdl.store(false, std::memory_order_relaxed); }
 
 int set_error(int status, const std::string& msg) {
   g_last_error = msg;
@@ -378,7 +384,9 @@ int Ctx::init(const mpdpft_params& params, int dev) {
     chunk = (geom.n + warps - 1) / warps;
     chunk = (chunk + kSegPts - 1) / kSegPts * kSegPts;
     if ((st = alloc((void**)&d_bcount, sizeof(int) * (size_t)kMaxS * step_blocks))) return st;
-    if ((st = alloc((void**)&d_plist, sizeof(int) * (size_t)S * geom.n))) return st;
+    // a warp's region holds its owned points, whole 32-point segments
+    plist_stride = geom.n + 32L * (warps + 1);
+    if ((st = alloc((void**)&d_plist, sizeof(int) * (size_t)S * plist_stride))) return st;
     if ((st = alloc((void**)&d_part2, sizeof(double) * (size_t)dens_blocks * kNPart))) return st;
   }
   part_vals = std::max(kNPart, kNEnergy);
@@ -543,6 +551,7 @@ StepArgs<R> Ctx::step_args(int mode) {
   a.part2 = d_part2;
   a.bcount = d_bcount;
   a.plist = d_plist;
+  a.plist_stride = plist_stride;
   a.vres_part = vres_part_ext;
   a.vres_blocks = vres_blocks_ext;
   a.log = d_log;
@@ -597,20 +606,30 @@ static cudaError_t launch_sc_kernels(Ctx& c, int mode, int fk, int parts = 7) {
   cudaError_t e = cudaSuccess;
   if (parts & 2) {
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
-    e = cudaLaunchKernel(sc_kernel_ptr<R>(c.dens_which, fk), dim3(c.dens_blocks), dim3(kDensityThreads), params, 0,
-                         c.stream);
+    {
+      cudaLaunchConfig_t dc;
+      std::memset(&dc, 0, sizeof(dc));
+      dc.gridDim = dim3(c.dens_blocks);
+      dc.blockDim = dim3(kDensityThreads);
+      dc.stream = c.stream;
+      cudaLaunchAttribute pa[1];
+      pa[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      pa[0].val.programmaticStreamSerializationAllowed = 1;
+      dc.attrs = pa;
+      dc.numAttrs = pdl_enabled() ? 1 : 0;
+      e = cudaLaunchKernelExC(&dc, sc_kernel_ptr<R>(c.dens_which, fk), params);
+    }
     if (e != cudaSuccess) return e;
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
-    if (c.dens_which == 1) sc_phase_d_kernel<R, 5><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
-    else if (c.dens_which == 3) sc_phase_d_kernel<R, 8><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
-    else sc_phase_d_kernel<R, kMaxP><<<1, kDensityThreads, 0, c.stream>>>(args, c.dens_blocks);
-    e = cudaGetLastError();
+    const int nb = c.dens_blocks;
+    if (c.dens_which == 1) e = launch_k(sc_phase_d_kernel<R, 5>, dim3(1), dim3(kDensityThreads), 0, c.stream, args, nb);
+    else if (c.dens_which == 3) e = launch_k(sc_phase_d_kernel<R, 8>, dim3(1), dim3(kDensityThreads), 0, c.stream, args, nb);
+    else e = launch_k(sc_phase_d_kernel<R, kMaxP>, dim3(1), dim3(kDensityThreads), 0, c.stream, args, nb);
     if (e != cudaSuccess) return e;
   }
   if (mode != 1 && (parts & 4)) {
     c.cnt[MPDPFT_STAGE_SC_STEP]++;
-    sc_mix_kernel<R><<<c.mix_blocks, kDensThreads, 0, c.stream>>>(args);
-    e = cudaGetLastError();
+    e = launch_k(sc_mix_kernel<R>, dim3(c.mix_blocks), dim3(kDensThreads), 0, c.stream, args);
   }
   return e;
 }
@@ -761,19 +780,31 @@ int Ctx::sc_step(int use_graph) {
   check_graphs();
   if (!graph_exec) {
     graph_kp = kparams();
-    CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < 6; ++i) cnt[i] = 0;
-    notes.clear();
-    noting = true;
-    st = issue_iteration();
-    noting = false;
-    for (int i = 0; i < 6; ++i) iter_cnt[i] = cnt[i];
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(stream, &g);
-    if (st) { if (g) cudaGraphDestroy(g); return st; }
-    if (e != cudaSuccess) return set_error(MPDPFT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    graph = g;
-    CU(cudaGraphInstantiate(&graph_exec, graph, 0));
+    // a driver that does not take the programmatic launches inside a
+    // captured graph gets the iteration captured again without them
+    for (int attempt = 0;; ++attempt) {
+      CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      for (int i = 0; i < 6; ++i) cnt[i] = 0;
+      notes.clear();
+      noting = true;
+      st = issue_iteration();
+      noting = false;
+      for (int i = 0; i < 6; ++i) iter_cnt[i] = cnt[i];
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(stream, &g);
+      if (st == MPDPFT_OK && e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec, g, 0);
+      if (st == MPDPFT_OK && e == cudaSuccess) { graph = g; break; }
+      if (g) cudaGraphDestroy(g);
+      graph_exec = nullptr;
+      if (attempt == 0 && pdl_enabled()) {
+        cudaGetLastError();
+        g_last_error.clear();
+        pdl_disable();
+        continue;
+      }
+      if (st) return st;
+      return set_error(MPDPFT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
   }
   CU(cudaGraphLaunch(graph_exec, stream));
   return MPDPFT_OK;

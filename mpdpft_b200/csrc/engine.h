@@ -64,7 +64,8 @@ struct Ctx {
   int mix_blocks = 0;    // grid of the mixing kernel
   long chunk = kSegPts;  // points per warp in the mu kernel's list sweeps
   int* d_bcount = nullptr;    // [kMaxS][step_blocks] active points per block
-  int* d_plist = nullptr;     // [S][n] active-point lists
+  int* d_plist = nullptr;     // [S][plist_stride] active-point lists (a region per warp)
+  long plist_stride = 0;      // >= n + 32 (warps of the largest mu grid + 1)
   double* d_part2 = nullptr;  // [dens_blocks][kNPart] density-kernel partial sums
   int assemble_in_step = 1;
   const double* vres_part_ext = nullptr;

@@ -296,7 +296,9 @@ __device__ __forceinline__ void z_r2c_body(const ZArgs<R>& a, const long blk) {
 
 template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_z_r2c(ZArgs<R> a) {
+  pdl_wait();
   z_r2c_body<R, NC, NL>(a, blockIdx.x);
+  pdl_trigger();
 }
 
 // Batched launch: blockIdx.y selects the transform's arguments (one solve
@@ -442,7 +444,9 @@ __device__ __forceinline__ void z_c2r_body(const ZArgs<R>& a, const long blk) {
 
 template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_z_c2r(ZArgs<R> a) {
+  pdl_wait();
   z_c2r_body<R, NC, NL>(a, blockIdx.x);
+  pdl_trigger();
 }
 
 template <typename R, int NC, int NL>
@@ -499,6 +503,7 @@ __device__ __forceinline__ bool axis_line(const AxisArgs<R>& a, long b, int l, l
 
 template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_axis_c2c(AxisArgs<R> a) {
+  pdl_wait();
   using C = typename Cx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   const long blk = blockIdx.x;
@@ -781,7 +786,9 @@ __device__ __forceinline__ void x_roundtrip_body(const AxisArgs<R>& a, const lon
 
 template <typename R, int NC, int NL>
 __global__ void __launch_bounds__(kFftThreads) k_x_roundtrip(AxisArgs<R> a) {
+  pdl_wait();
   x_roundtrip_body<R, NC, NL>(a, blockIdx.x);
+  pdl_trigger();
 }
 
 template <typename R, int NC, int NL>
@@ -987,7 +994,7 @@ static bool launch_z_r2c_ct(int M, unsigned grid, size_t smem, cudaStream_t st, 
 #define CASE(N)                                                                                   \
   case N:                                                                                         \
     smem_optin(k_z_r2c<R, N, NL>); \
-    k_z_r2c<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    launch_k(k_z_r2c<R, N, NL>, dim3(grid), dim3(kFftThreads), smem, st, a);                                        \
     return true;
     MPDPFT_CT_LENGTHS(CASE)
 #undef CASE
@@ -1001,7 +1008,7 @@ static bool launch_z_c2r_ct(int M, unsigned grid, size_t smem, cudaStream_t st, 
 #define CASE(N)                                                                                   \
   case N:                                                                                         \
     smem_optin(k_z_c2r<R, N, NL>); \
-    k_z_c2r<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    launch_k(k_z_c2r<R, N, NL>, dim3(grid), dim3(kFftThreads), smem, st, a);                                        \
     return true;
     MPDPFT_CT_LENGTHS(CASE)
 #undef CASE
@@ -1015,7 +1022,7 @@ static bool launch_axis_ct(int n, dim3 grid, size_t smem, cudaStream_t st, const
 #define CASE(N)                                                                                      \
   case N:                                                                                            \
     smem_optin(k_axis_c2c<R, N, NL>); \
-    k_axis_c2c<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    launch_k(k_axis_c2c<R, N, NL>, dim3(grid), dim3(kFftThreads), smem, st, a);                                        \
     return true;
     MPDPFT_CT_LENGTHS(CASE)
 #undef CASE
@@ -1029,7 +1036,7 @@ static bool launch_x_ct(int n, unsigned grid, size_t smem, cudaStream_t st, cons
 #define CASE(N)                                                                                         \
   case N:                                                                                               \
     smem_optin(k_x_roundtrip<R, N, NL>); \
-    k_x_roundtrip<R, N, NL><<<grid, kFftThreads, smem, st>>>(a);                                        \
+    launch_k(k_x_roundtrip<R, N, NL>, dim3(grid), dim3(kFftThreads), smem, st, a);                                        \
     return true;
     MPDPFT_CT_LENGTHS(CASE)
 #undef CASE
@@ -1215,7 +1222,7 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
   c.note("k_z_r2c", nsrc * c.field_bytes() + c.spec_bytes());
   if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
-    k_z_r2c<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+    launch_k(k_z_r2c<R, 0, 0>, dim3(f.zblocks), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1251,7 +1258,7 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   c.note("k_z_c2r", nin * c.spec_bytes() + ((out0 ? 1 : 0) + (out1 ? 1 : 0)) * c.field_bytes());
   if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
-    k_z_c2r<R, 0, 0><<<f.zblocks, kFftThreads, smem, c.stream>>>(a);
+    launch_k(k_z_c2r<R, 0, 0>, dim3(f.zblocks), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1301,7 +1308,7 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   c.cnt[MPDPFT_STAGE_FFT_Y]++;
   c.note("k_axis_c2c", 2.0 * nfield * c.spec_bytes());
   if (f.tk != ct_width<R>() || !launch_axis_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
-    k_axis_c2c<R, 0, 0><<<grid, kFftThreads, smem, c.stream>>>(a);
+    launch_k(k_axis_c2c<R, 0, 0>, dim3(grid), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1349,7 +1356,7 @@ static int launch_x_args(Ctx& c, const AxisArgs<R>& a) {
   c.cnt[MPDPFT_STAGE_FFT_X]++;
   c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
   if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
-    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
+    launch_k(k_x_roundtrip<R, 0, 0>, dim3(grid), dim3(kFftThreads), x_smem_rt<R>(f), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1362,7 +1369,7 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   c.cnt[MPDPFT_STAGE_FFT_X]++;
   c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
   if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
-    k_x_roundtrip<R, 0, 0><<<grid, kFftThreads, x_smem_rt<R>(f), c.stream>>>(a);
+    launch_k(k_x_roundtrip<R, 0, 0>, dim3(grid), dim3(kFftThreads), x_smem_rt<R>(f), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
@@ -1372,13 +1379,13 @@ template <typename R, int S>
 static void plane_fwd_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
   constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
   smem_optin(k_plane_fwd<R, S, NLY, NLZ>);
-  k_plane_fwd<R, S, NLY, NLZ><<<grid, kPlaneThreads, smem, st>>>(a);
+  launch_k(k_plane_fwd<R, S, NLY, NLZ>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
 }
 template <typename R, int S>
 static void plane_inv_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
   constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
   smem_optin(k_plane_inv<R, S, NLY, NLZ>);
-  k_plane_inv<R, S, NLY, NLZ><<<grid, kPlaneThreads, smem, st>>>(a);
+  launch_k(k_plane_inv<R, S, NLY, NLZ>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
 }
 
 template <typename R>
@@ -2073,12 +2080,34 @@ struct BatchFftClass {
   bool xct = false;
   void* d_z[4] = {nullptr, nullptr, nullptr, nullptr};  // ZArgs<R>[count]
   void* d_x[2] = {nullptr, nullptr};                    // AxisArgs<R>[count]
+  // Coulomb terms (2D kernel): per argument set one transform of the
+  // weighted densities sum_q w_q n_q into that species' vh
+  bool coulomb = false;
+  void* d_cz[2] = {nullptr, nullptr};  // ZArgs<R>[count]: R2C, C2R
+  void* d_cx = nullptr;                // AxisArgs<R>[count]
 };
+
+// Weights w_q of the densities whose Coulomb potential is species s's
+// Coulomb term, V_s = gammaH V_H[sum_q w_q n_q] (V_H linear): type 8 its
+// own density, 21 the other species' (mpDPFT.cpp:2266-2285), 100 the
+// charge density times q_s.
+static void coulomb_weights(const Ctx& c, int s, double* w) {
+  for (int q = 0; q < kMaxS; ++q) w[q] = 0.0;
+  for (int a = 0; a < c.P.n_interactions; ++a) {
+    const int t = c.P.interactions[a];
+    if (t == MPDPFT_INT_HARTREE) w[s] += 1.0;
+    else if (t == MPDPFT_INT_HARTREE_INTER)
+      for (int q = 0; q < c.S; ++q) w[q] += q == s ? 0.0 : 1.0;
+    else if (t == MPDPFT_INT_COULOMB_CHARGED)
+      for (int q = 0; q < c.S; ++q) w[q] += c.P.charges[s] * c.P.charges[q];
+  }
+}
 
 template <typename R>
 static int batch_fft_build(const std::vector<BatchMember>& members, unsigned long long* vmax_all, BatchFftClass* b) {
-  std::vector<ZArgs<R>> z[4];
-  std::vector<AxisArgs<R>> x[2];
+  std::vector<ZArgs<R>> z[4], cz[2];
+  std::vector<AxisArgs<R>> x[2], cx;
+  const bool coul = members[0].c->has_coulomb;
   for (const BatchMember& m : members) {
     Ctx& c = *m.c;
     FftPlan& f = *c.fft;
@@ -2086,6 +2115,7 @@ static int batch_fft_build(const std::vector<BatchMember>& members, unsigned lon
     for (int s = 0; s < c.S; ++s) {
       void* spec[4];
       void* rtmp;
+      double* zpart = f.zpart;
       if (s == 0) {
         for (int i = 0; i < 4; ++i) spec[i] = f.spec[i];
         rtmp = f.rtmp;
@@ -2094,6 +2124,7 @@ static int batch_fft_build(const std::vector<BatchMember>& members, unsigned lon
         for (int i = 0; i < 4; ++i)
           if ((st = c.alloc(&spec[i], 2 * c.rsize * f.nspec))) return st;
         if ((st = c.alloc(&rtmp, c.rsize * n))) return st;
+        if (coul && (st = c.alloc((void**)&zpart, sizeof(double) * (f.zblocks + 1)))) return st;
       }
       Delfield2D<R> d = delfield2d_args<R>(c, (const R*)c.d_V + (long)s * n, (R*)c.d_g2 + (long)s * n,
                                            (R*)c.d_lap + (long)s * n, spec, rtmp,
@@ -2101,6 +2132,27 @@ static int batch_fft_build(const std::vector<BatchMember>& members, unsigned lon
       const int* skip = &c.d_state->exit_loop;
       for (int i = 0; i < 4; ++i) { d.z[i].skip = skip; z[i].push_back(d.z[i]); }
       for (int i = 0; i < 2; ++i) { d.x[i].skip = skip; x[i].push_back(d.x[i]); }
+      if (coul) {  // HartreeRepulsion 2D of the weighted current densities into vh of species s
+        double w[kMaxS];
+        coulomb_weights(c, s, w);
+        const bool plain = c.S == 1 && w[0] == 1.0;
+        ZArgs<R> a0 = r2c_args<R>(c, (const R*)c.d_cur, plain ? PRO_NONE : PRO_CHARGE, c.S, w, spec[0], true,
+                                  vmax_all + (long)m.index * kMaxS + s);
+        a0.part = zpart;
+        AxisArgs<R> ax = x_args<R>(c, spec[0], &spec[0], 1, MUL_COULOMB_2D, 0.0);
+        ax.f0_part = zpart;
+        ax.f0_blocks = f.zblocks;
+        ZArgs<R> a1 = c2r_args<R>(c, &spec[0], 1, EPI_COULOMB, (R*)c.d_vh + (long)s * n, nullptr,
+                                  2.0 * kPi * c.P.gamma_h);
+        a1.f0_part = zpart;
+        a1.f0_blocks = f.zblocks;
+        a0.skip = skip;
+        ax.skip = skip;
+        a1.skip = skip;
+        cz[0].push_back(a0);
+        cz[1].push_back(a1);
+        cx.push_back(ax);
+      }
     }
   }
   Ctx& c0 = *members[0].c;
@@ -2125,6 +2177,15 @@ static int batch_fft_build(const std::vector<BatchMember>& members, unsigned lon
   for (int i = 0; i < 2; ++i) {
     CU(cudaMalloc(&b->d_x[i], sizeof(AxisArgs<R>) * b->count));
     CU(cudaMemcpy(b->d_x[i], x[i].data(), sizeof(AxisArgs<R>) * b->count, cudaMemcpyHostToDevice));
+  }
+  b->coulomb = coul;
+  if (coul) {
+    for (int i = 0; i < 2; ++i) {
+      CU(cudaMalloc(&b->d_cz[i], sizeof(ZArgs<R>) * b->count));
+      CU(cudaMemcpy(b->d_cz[i], cz[i].data(), sizeof(ZArgs<R>) * b->count, cudaMemcpyHostToDevice));
+    }
+    CU(cudaMalloc(&b->d_cx, sizeof(AxisArgs<R>) * b->count));
+    CU(cudaMemcpy(b->d_cx, cx.data(), sizeof(AxisArgs<R>) * b->count, cudaMemcpyHostToDevice));
   }
   return MPDPFT_OK;
 }
@@ -2151,7 +2212,7 @@ int batch_fft_create(const std::vector<BatchMember>& members, unsigned long long
 }
 
 template <typename R>
-static int batch_fft_issue_t(BatchFftClass* b, cudaStream_t st) {
+static int batch_fft_issue_t(BatchFftClass* b, cudaStream_t st, bool coulomb_only) {
   const ZArgs<R>* z[4];
   const AxisArgs<R>* x[2];
   for (int i = 0; i < 4; ++i) z[i] = (const ZArgs<R>*)b->d_z[i];
@@ -2169,6 +2230,13 @@ static int batch_fft_issue_t(BatchFftClass* b, cudaStream_t st) {
     if (!b->xct || !launch_x_b_ct<R, ct_width<R>()>(b->s, xg, b->smem_xct, st, a))
       k_x_roundtrip_b<R, 0, 0><<<xg, kFftThreads, b->smem_xrt, st>>>(a);
   };
+  if (coulomb_only) {
+    r2c((const ZArgs<R>*)b->d_cz[0]);
+    xrt((const AxisArgs<R>*)b->d_cx);
+    c2r((const ZArgs<R>*)b->d_cz[1]);
+    CU(cudaGetLastError());
+    return MPDPFT_OK;
+  }
   r2c(z[0]);
   xrt(x[0]);
   c2r(z[1]);
@@ -2180,13 +2248,22 @@ static int batch_fft_issue_t(BatchFftClass* b, cudaStream_t st) {
 }
 
 int batch_fft_issue(BatchFftClass* b, cudaStream_t st) {
-  return b->rsize == sizeof(double) ? batch_fft_issue_t<double>(b, st) : batch_fft_issue_t<float>(b, st);
+  return b->rsize == sizeof(double) ? batch_fft_issue_t<double>(b, st, false) : batch_fft_issue_t<float>(b, st, false);
+}
+
+bool batch_fft_has_coulomb(const BatchFftClass* b) { return b && b->coulomb; }
+
+int batch_fft_issue_coulomb(BatchFftClass* b, cudaStream_t st) {
+  if (!b->coulomb) return MPDPFT_OK;
+  return b->rsize == sizeof(double) ? batch_fft_issue_t<double>(b, st, true) : batch_fft_issue_t<float>(b, st, true);
 }
 
 void batch_fft_destroy(BatchFftClass* b) {
   if (!b) return;
   for (int i = 0; i < 4; ++i) cudaFree(b->d_z[i]);
   for (int i = 0; i < 2; ++i) cudaFree(b->d_x[i]);
+  for (int i = 0; i < 2; ++i) cudaFree(b->d_cz[i]);
+  cudaFree(b->d_cx);
   delete b;
 }
 
@@ -2335,6 +2412,7 @@ struct AssembleArgs {
   KParams kp;
   const ScState* st;
   const R* vext;
+  const R* vh;  // Coulomb terms [S][n] or null
   const R* nin;
   R* V;
   double* vres_part;
@@ -2346,7 +2424,7 @@ template <typename R>
 __global__ void k_assemble_v_b(const AssembleArgs<R>* __restrict__ args, const int4* __restrict__ tab, int update) {
   const int4 t = tab[blockIdx.x];  // (member, block, blocks)
   const AssembleArgs<R>& a = args[t.x];
-  assemble_v_body<R>(a.kp, a.st, a.vext, nullptr, a.nin, a.V, a.vres_part, a.vmax, a.shell_r, a.shell_w, a.kp.S,
+  assemble_v_body<R>(a.kp, a.st, a.vext, a.vh, a.nin, a.V, a.vres_part, a.vmax, a.shell_r, a.shell_w, a.kp.S,
                      update, t.y, t.z);
 }
 
@@ -2370,6 +2448,7 @@ static int batch_assemble_build(const std::vector<BatchMember>& members, unsigne
     a.kp = c.kparams();
     a.st = c.d_state;
     a.vext = (const R*)c.d_vext;
+    a.vh = c.has_coulomb ? (const R*)c.d_vh : nullptr;
     a.nin = (const R*)c.d_nin;
     a.V = (R*)c.d_V;
     a.vres_part = c.fft->vres_part;
@@ -2397,7 +2476,8 @@ int batch_assemble_create(const std::vector<BatchMember>& members, unsigned long
   *out = nullptr;
   if (members.empty()) return set_error(MPDPFT_ERR_ARG, "empty batch");
   for (const BatchMember& m : members)
-    if (m.c->has_coulomb || !m.c->fft) return set_error(MPDPFT_ERR_ARG, "batched V assembly: no Coulomb terms");
+    if (!m.c->fft || m.c->has_coulomb != members[0].c->has_coulomb)
+      return set_error(MPDPFT_ERR_ARG, "batched V assembly: the solves share their interactions");
   BatchAssemble* b = new BatchAssemble;
   const int st = members[0].c->rsize == sizeof(double) ? batch_assemble_build<double>(members, vmax_all, b, blocks_out)
                                                        : batch_assemble_build<float>(members, vmax_all, b, blocks_out);

@@ -124,6 +124,7 @@ __device__ __forceinline__ void plane_y_pass(C* plane, C* A, C* B, const C* tw, 
 // plane index is blockIdx.x.
 template <typename R, int S, int NLY, int NLZ>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
+  pdl_wait();
   using C = typename Cx<R>::T;
   constexpr int M = S / 2, H = M + 1;
   constexpr int TILE = (int)plane_tile<R>(S, NLY, NLZ);
@@ -217,6 +218,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
 // writes field nin-1 to rout[1]; the others write rout[0]).
 template <typename R, int S, int NLY, int NLZ>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
+  pdl_wait();
   using C = typename Cx<R>::T;
   constexpr int M = S / 2, H = M + 1;
   constexpr int TILE = (int)plane_tile<R>(S, NLY, NLZ);

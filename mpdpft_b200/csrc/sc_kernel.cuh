@@ -566,8 +566,10 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   __shared__ double s_dmm;
   __shared__ double s_kx[kMaxS][2 * kMuCand];  // 2D form: shared exponentials of the candidates
   // active-point lists as this block sees them (identical in every block)
-  __shared__ int s_wcnt[kMaxS][kStepWarps];
-  __shared__ int s_need[kMaxS], s_lok[kMaxS], s_llen[kMaxS];
+  // list length of each warp of this block (-1: the warp evaluates all the
+  // points it owns)
+  __shared__ int s_wlen[kMaxS][kStepWarps];
+  __shared__ int s_need[kMaxS], s_lok[kMaxS];
   __shared__ double s_cap[kMaxS], s_lcap[kMaxS];
 
   if (a.mode == 0) {
@@ -638,8 +640,15 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
   if (threadIdx.x < kMaxS) {
     s_need[threadIdx.x] = 0;
     s_lok[threadIdx.x] = 0;
-    s_llen[threadIdx.x] = 0;
   }
+  if (lane == 0)
+    for (int s = 0; s < kMaxS; ++s) s_wlen[s][wib] = -1;
+  // the points a warp owns: the 32-point segments gw, gw + nwarps, ... of
+  // the grid (spread over the whole grid, so that the warps' shares of the
+  // active points are alike)
+  const long nseg = (n + 31) / 32;
+  const long own = gw < nseg ? 32 * ((nseg - gw + nwarps - 1) / nwarps) : 0;
+  const long wcap = 32 * ((nseg + nwarps - 1) / nwarps);  // list capacity of a warp
   __syncthreads();
   if (bid == 0 && threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) { ls->ms[s] = s_ms[s]; ls->prev_mu[s] = s_ms[s].start; }
@@ -681,84 +690,44 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
     for (int s = 0; s < S; ++s) { any |= !s_ms[s].done; need |= s_need[s]; }
     if (!any) break;
     if (need) {
-      // (re)build the active-point lists: count, offsets, write (grid order)
-      const long beg = gw * kp.chunk;
-      const long end = beg + kp.chunk < n ? beg + kp.chunk : n;
+      // (re)build the active-point lists: every warp lists the points it owns
+      // below the largest candidate, in its own region of plist (no count
+      // pass, no offsets, no grid barrier); a warp that finds most of its
+      // points active keeps no list and evaluates all of them
+      const unsigned lt = (1u << lane) - 1u;
       for (int s = 0; s < S; ++s) {
         if (!s_need[s]) continue;
         const R* Vs = V + (long)s * n;
+        int* pl = a.plist + (long)s * a.plist_stride + gw * wcap;
         const double cap = s_cap[s];
         int cnt = 0;
-        for (long b = beg; b < end; b += kSegPts) {
-          const long p0 = b + 4 * lane;
-          R v4[4];
-          load4(Vs, p0, n, kp.vec4, v4);
-          int c = 0;
+        for (long seg = gw; seg < nseg; seg += 4 * nwarps) {
+          R vv[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) c += (p0 + i < n && cap - (double)v4[i] > 0.0) ? 1 : 0;
-          cnt += __reduce_add_sync(0xffffffffu, c);
-        }
-        if (lane == 0) s_wcnt[s][wib] = cnt;
-      }
-      __syncthreads();
-      if (threadIdx.x < S && s_need[threadIdx.x]) {
-        int c = 0;
-        for (int w = 0; w < kStepWarps; ++w) c += s_wcnt[threadIdx.x][w];
-        a.bcount[(long)threadIdx.x * nblk + bid] = c;
-      }
-      if (!grid_barrier(st, nblk, kp.spin_limit)) return;
-      for (int s = 0; s < S; ++s) {
-        if (!s_need[s]) continue;
-        int before = 0, total = 0;
-        for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-          const int c = __ldcg(a.bcount + (long)s * nblk + b);
-          total += c;
-          if (b < (int)bid) before += c;
-        }
-        block_sum2(before, total);
-        if (2L * total > n) {  // most points active: the pass sweeps the whole grid
-          if (threadIdx.x == 0) s_llen[s] = -1;
-          continue;
-        }
-        int off = before;
-        for (int w = 0; w < wib; ++w) off += s_wcnt[s][w];
-        const R* Vs = V + (long)s * n;
-        int* pl = a.plist + (long)s * n;
-        const double cap = s_cap[s];
-        const unsigned lt = (1u << lane) - 1u;
-        for (long b = beg; b < end; b += kSegPts) {
-          const long p0 = b + 4 * lane;
-          R v4[4];
-          load4(Vs, p0, n, kp.vec4, v4);
-          bool f[4];
-          unsigned m[4];
-          int pos = off, tot = 0;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            f[i] = p0 + i < n && cap - (double)v4[i] > 0.0;
-            m[i] = __ballot_sync(0xffffffffu, f[i]);
-            pos += __popc(m[i] & lt);
-            tot += __popc(m[i]);
+          for (int u = 0; u < 4; ++u) {
+            const long p = (seg + u * nwarps) * 32 + lane;
+            vv[u] = p < n ? __ldcg(Vs + p) : R(0);
           }
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (f[i]) pl[pos++] = (int)(p0 + i);
-          off += tot;
+          for (int u = 0; u < 4; ++u) {
+            const long p = (seg + u * nwarps) * 32 + lane;
+            const bool f = p < n && cap - (double)vv[u] > 0.0;
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (f) pl[cnt + __popc(m & lt)] = (int)p;
+            cnt += __popc(m);
+          }
         }
-        if (threadIdx.x == 0) s_llen[s] = total;
+        __syncwarp();  // the warp's list entries are visible to all its lanes
+        if (lane == 0) s_wlen[s][wib] = 2L * cnt > own ? -1 : cnt;
       }
-      __syncthreads();
-      // (the same decisions in every block: `total` sums the same counts)
-      int written = 0;
-      for (int s = 0; s < S; ++s) written |= s_need[s] && s_llen[s] >= 0;
       __syncthreads();
       if (threadIdx.x < S && s_need[threadIdx.x]) {
         const int s = threadIdx.x;
         s_lok[s] = 1;
-        s_lcap[s] = s_llen[s] >= 0 ? s_cap[s] : 1e300;  // no rebuild after a whole-grid decision
+        s_lcap[s] = s_cap[s];
         s_need[s] = 0;
       }
-      if (written && !grid_barrier(st, nblk, kp.spin_limit)) return;  // the lists are complete
+      __syncthreads();
     }
     for (int s = 0; s < S; ++s) {
       if (s_ms[s].done) continue;
@@ -775,22 +744,26 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
       const R* Vs = V + (long)s * n;
       const R* Ls = a.lap ? a.lap + (long)s * n : nullptr;
       const R* Gs = a.g2 ? a.g2 + (long)s * n : nullptr;
-      const int* pl = a.plist + (long)s * n;
-      const bool listed = d.cut && s_llen[s] >= 0;  // s_llen < 0: the whole grid
-      const long len = listed ? (long)s_llen[s] : n;
-      // a warp takes 32 NPT consecutive list entries per trip, entry
-      // lane + 32 i on lane `lane` (coalesced loads), in a three-stage
-      // pipeline: the list indices of trip t + 2 and the field values of
-      // trip t + 1 are loaded while trip t is evaluated (index -1: past the
-      // end).  NPT = 4 points per lane for FP32 fields, 2 for FP64 (the
-      // registers of two stages of values).
+      const int* pl = a.plist + (long)s * a.plist_stride + gw * wcap;
+      const int wl = s_wlen[s][wib];
+      const bool listed = d.cut && wl >= 0;  // else every owned point
+      const long len = listed ? (long)wl : own;
+      // a warp takes 32 NPT consecutive entries of its own list (or of its
+      // owned points) per trip, entry lane + 32 i on lane `lane` (coalesced
+      // loads), in a three-stage pipeline: the indices of trip t + 2 and the
+      // field values of trip t + 1 are loaded while trip t is evaluated
+      // (index -1: past the end).  NPT = 4 points per lane for FP32 fields,
+      // 2 for FP64 (the registers of two stages of values).
       constexpr int NPT = sizeof(R) == sizeof(float) ? 4 : 2;
-      const long step = nwarps * 32 * NPT;
+      const long step = 32 * NPT;
       auto indices = [&](long jb, int (&q)[NPT]) {
 #pragma unroll
         for (int i = 0; i < NPT; ++i) {
           const long j = jb + 32 * i + lane;
-          q[i] = j < len ? (listed ? __ldcg(pl + j) : (int)j) : -1;
+          if (j >= len) { q[i] = -1; continue; }
+          if (listed) { q[i] = __ldcg(pl + j); continue; }
+          const long p = (gw + (j >> 5) * nwarps) * 32 + (j & 31);
+          q[i] = p < n ? (int)p : -1;
         }
       };
       auto values = [&](const int (&q)[NPT], R (&v)[NPT], R (&l)[NPT], R (&g)[NPT]) {
@@ -802,7 +775,7 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
           g[i] = (ok && Gs) ? __ldcg(Gs + q[i]) : R(0);
         }
       };
-      long jb = gw * 32 * NPT;
+      long jb = 0;
       int qa[NPT], qb[NPT];
       R v[NPT], l[NPT], g[NPT];
       indices(jb, qa);
@@ -871,7 +844,9 @@ __device__ __forceinline__ void sc_mu_body(const StepArgs<R>& a, const int bid, 
 
 template <typename R, int FK>
 __global__ void __launch_bounds__(kStepThreads, 1) sc_mu_kernel(StepArgs<R> a) {
+  pdl_wait();
   sc_mu_body<R, FK>(a, blockIdx.x, gridDim.x);
+  pdl_trigger();
 }
 
 // Batched launches: entry b of the block table names the solve (x), the
@@ -1243,7 +1218,9 @@ __device__ __forceinline__ void sc_density_body(const StepArgs<R>& a, const int 
 
 template <typename R, int FK, int PW>
 __global__ void __launch_bounds__(kDensityThreads, 2) sc_density_kernel(StepArgs<R> a) {
+  pdl_wait();
   sc_density_body<R, FK, PW>(a, blockIdx.x, gridDim.x);
+  pdl_trigger();
 }
 
 template <typename R, int FK, int PW>
@@ -1257,6 +1234,7 @@ __global__ void __launch_bounds__(kDensityThreads, 2) sc_density_kernel_b(const 
 // kernel's occupancy.
 template <typename R, int PW>
 __global__ void __launch_bounds__(kDensityThreads, 1) sc_phase_d_kernel(StepArgs<R> a, int nblk) {
+  pdl_wait();
   const KParams& kp = a.kp;
   ScState* st = a.st;
   const int S = kp.S;
@@ -1336,7 +1314,9 @@ __device__ __forceinline__ void sc_mix_body(const StepArgs<R>& a, const int bid,
 
 template <typename R>
 __global__ void __launch_bounds__(kDensThreads, 4) sc_mix_kernel(StepArgs<R> a) {
+  pdl_wait();
   sc_mix_body<R>(a, blockIdx.x, gridDim.x);
+  pdl_trigger();
 }
 
 template <typename R>

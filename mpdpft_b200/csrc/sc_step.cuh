@@ -110,11 +110,12 @@ struct StepArgs {
   double* part;   // [mu_blocks][kNPart]: mu-pass sums, V-update residual
   double* part2;  // [density blocks][kNPart]: density-pass sums
   // active-point lists of the mu search (functionals that vanish for
-  // mu <= V): the points below the largest candidate of the pass that built
-  // the list, in grid order; later passes whose candidates stay below that
-  // bound visit only those
-  int* bcount;  // [kMaxS][mu_blocks] active points found by each block
-  int* plist;   // [kMaxS][n]
+  // mu <= V): every warp's list of the points it owns below the largest
+  // candidate of the pass that built the lists; later passes whose
+  // candidates stay below that bound visit only those
+  int* bcount;  // [kMaxS][mu_blocks] (unused by the mu search)
+  int* plist;   // [S][plist_stride]: per species, one region per warp
+  long plist_stride;
   const double* vres_part;  // partials of |V_new - V_old|^2 from an external
   int vres_blocks;          //   V assembly (when assemble_v == 0), or null
   mpdpft_iter_log* log;
