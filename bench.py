@@ -598,6 +598,53 @@ def adjoint_cluster(device, max_iter=60):
     out["max_abs_dL_dR_fp64"] = float(np.abs(dR["fp64"]).max())
     out["dL_dR_rel_diff_mixed_vs_fp64"] = float(np.abs(dR["mixed"] - dR["fp64"]).max() / np.abs(dR["fp64"]).max())
     out["accuracy_vs_fp64_oracle"] = acc
+    out["hartree_only"] = adjoint_cluster_hartree(device, max_iter=300)
+    return out
+
+
+def adjoint_cluster_hartree(device, max_iter=300, h=1e-4, coords=((0, 0), (3, 1), (7, 2), (12, 0))):
+    """The same cluster with the Hartree functional (Dirac off: with it the
+    fixed point is not unique at the TF-Dirac edge and the adjoint system
+    does not converge): adjoint residuals in FP64 and mixed precision,
+    dL/dR against central differences of whole FP64 solves (step h) for a
+    few coordinates, mixed vs FP64 gradient."""
+    from mpdpft_b200 import abi, engine, workloads as W
+    out = {"interactions": "Hartree", "fd_step": h}
+    dR = {}
+    for name, prec in (("fp64", abi.FP64), ("mixed", abi.MIXED)):
+        pt, vt, v0t, _ = W.cluster_adjoint(precision=prec, jitter=0.0, interactions=[abi.INT_HARTREE])
+        with engine.Engine(pt, device=device) as et:
+            et.sc_run(vt, v0t, check=False)
+            nt = et.field(abi.FIELD_DENSITY, 0)
+        p, vext, v0, nuc = W.cluster_adjoint(precision=prec, interactions=[abi.INT_HARTREE])
+        dvol = (p.edge / p.steps) ** 3
+        with engine.Engine(p, device=device) as e:
+            e.sc_run(vext, v0, check=False)
+            n = e.field(abi.FIELD_DENSITY, 0)
+            t0 = time.perf_counter()
+            grad, it, resid, ast = e.adjoint(2.0 * dvol * (n - nt), max_iter=max_iter,
+                                             tol=1e-10 if prec == abi.FP64 else 1e-7, check=False)
+            out["adjoint_s_%s" % name] = time.perf_counter() - t0
+            dR[name] = e.adjoint_nuclei(grad, nuc["z"], nuc["pos"], nuc["sigma"])
+        out["adjoint_iters_%s" % name] = it
+        out["adjoint_residual_%s" % name] = resid
+        if prec == abi.FP64:
+            fd_rows = []
+            for a, k in coords:
+                lp = []
+                for sgn in (1, -1):
+                    pos = nuc["pos"].copy()
+                    pos[a, k] += sgn * h
+                    v2 = W.nuclei_potential(p.steps, p.edge, pos, 3.0, nuc["sigma"])
+                    with engine.Engine(p, device=device) as e2:
+                        e2.sc_run([v2], v0, check=False)
+                        n2 = e2.field(abi.FIELD_DENSITY, 0)
+                    lp.append(dvol * float(((n2 - nt) ** 2).sum()))
+                fd = (lp[0] - lp[1]) / (2 * h)
+                fd_rows.append({"nucleus": a, "coord": k, "adjoint": float(dR[name][a, k]), "fd": fd,
+                                "rel": abs(float(dR[name][a, k]) - fd) / abs(fd)})
+            out["fd_check_fp64"] = fd_rows
+    out["dL_dR_rel_diff_mixed_vs_fp64"] = float(np.abs(dR["mixed"] - dR["fp64"]).max() / np.abs(dR["fp64"]).max())
     return out
 
 

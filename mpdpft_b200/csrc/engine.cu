@@ -836,10 +836,12 @@ int Ctx::iteration_profile(int cap, mpdpft_launch_record* out, int* n_out) {
     bool progress = false;
     for (size_t i = 0; i < nn; ++i) {
       if (done[i]) continue;
+      // (the edge-data form: programmatic edges refuse the plain query)
       size_t nd = 0;
-      CU(cudaGraphNodeGetDependencies(nodes[i], nullptr, &nd));
+      CU(cudaGraphNodeGetDependencies_v2(nodes[i], nullptr, nullptr, &nd));
       std::vector<cudaGraphNode_t> deps(nd);
-      if (nd) CU(cudaGraphNodeGetDependencies(nodes[i], deps.data(), &nd));
+      std::vector<cudaGraphEdgeData> edata(nd);
+      if (nd) CU(cudaGraphNodeGetDependencies_v2(nodes[i], deps.data(), edata.data(), &nd));
       bool ready = true;
       for (cudaGraphNode_t d : deps) {
         size_t j = 0;
