@@ -113,6 +113,84 @@ __global__ void k_energy(Geom g, int S, const R* V, const R* vext, const R* dens
   block_reduce_store<kNEnergy>(acc, part + (long)blockIdx.x * kNEnergy);
 }
 
+// Kinetic energy integrands of the gradient-corrected density, per species
+// (GetDispersalEnergy, DensityExpression 5, mpDPFT.cpp:5606-5703), one block
+// partial per accumulator: [s] the point values, [kMaxS + s] V n (2D).
+//  2D: g/2 [lap CurlyA(y)/(12 pi) - |grad V|^{4/3} (y^2 CurlyA(y) + Ai(y) +
+//      y Ai'(y))/(8 pi)], y = 2 (V - mu)/|grad V|^{2/3}; 0 where |grad V|^2
+//      <= MP; Ai = Ai' = 0 from y = 50.
+//  3D (EkinAiT03D): (2u)^{5/2}/5 - lap (2u)^{1/2}/6, u = mu - V > 0, where
+//      a = |grad V|^{2/3}/2 < thr; else the Airy-weighted integral
+//      int_0^{x1} Ai(x + U/a) [(2ax)^{5/2}/5 - lap (2ax)^{1/2}/6] dx by the
+//      trapezoid rule on 64, 128, ... points until two agree (ASYMcritABS <
+//      MP), or until maxit doublings (the reference's NegligibleMagnitudeQ
+//      exit against e_env = int V_ext n).
+template <typename R>
+__global__ void k_ekin_grad(Geom g, int S, double gdeg, double thr, int maxit, double internal_acc,
+                            double area_pref, const R* V, const R* lap, const R* g2, const R* dens,
+                            const double* mu, const double* e_env, double* part) {
+  double acc[2 * kMaxS];
+#pragma unroll
+  for (int j = 0; j < 2 * kMaxS; ++j) acc[j] = 0.0;
+  const long n = g.n;
+  constexpr double kMP = 1.0e-12;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    for (int s = 0; s < S; ++s) {
+      const long q = (long)s * n + p;
+      const double U = (double)V[q] - mu[s], L = (double)lap[q], ab = fabs((double)g2[q]);
+      double t = 0.0;
+      if (g.dim == 2) {
+        if (ab > kMP) {
+          const double y = 2.0 * U / cbrt(ab);
+          double ai = 0.0, aip = 0.0;
+          if (y < 50.0) airy_ai_d(y, ai, aip);
+          const double ca = curly_a(y);
+          t = 0.5 * gdeg * (L * ca / (12.0 * kPi) - pow(ab, 2.0 / 3.0) * (y * y * ca + ai + y * aip) / (8.0 * kPi));
+        }
+        acc[kMaxS + s] += (double)V[q] * (double)dens[q];
+      } else {
+        const double a = 0.5 * cbrt(ab);
+        if (a < thr) {
+          const double w = -2.0 * U;
+          t = w > 0.0 ? w * w * sqrt(w) / 5.0 - L * sqrt(w) / 6.0 : 0.0;
+        } else {
+          const double x1 = fmax(1.0, 100.0 - U / a);
+          double prev = 1.0, res = 0.0;
+          for (int it = 0, m = 64;; ++it, m *= 2) {
+            const double h = x1 / (double)(m - 1);
+            double sum = 0.0;
+            for (int j = 0; j < m; ++j) {
+              const double x = (double)j * h, y = x + U / a;
+              double ai = 0.0, aip;
+              if (!(y > 100.0)) {
+                if (y > -300.0) airy_ai_d(y, ai, aip);
+                else ai = cos(2.0 * (-y) * sqrt(-y) / 3.0 - 0.25 * kPi) / (1.7724538509055159 * sqrt(sqrt(-y)));
+              }
+              const double w = 2.0 * a * x;
+              const double f = ai * (w * w * sqrt(w) / 5.0 - L * sqrt(w) / 6.0);
+              sum += (j == 0 || j == m - 1) ? 0.5 * f : f;
+            }
+            res = sum * h;
+            if (it > 0) {
+              const bool tiny = fabs(res) < kMP && fabs(prev) < kMP;
+              const double da = tiny ? 0.0 : fabs((res - prev) / (res + prev));
+              const double dr = (res == 0.0 && prev == 0.0) ? 0.0 : fabs((res - prev) / (res + prev));
+              if (da < kMP || (dr < internal_acc && negligible_magnitude(e_env[5 * s + 1], area_pref * res,
+                                                                      -log(internal_acc))))
+                break;
+            }
+            if (it == maxit) break;
+            prev = res;
+          }
+          t = res;
+        }
+      }
+      acc[s] += t;
+    }
+  }
+  block_reduce_store<2 * kMaxS>(acc, part + (long)blockIdx.x * 2 * kMaxS);
+}
+
 // out[v] = scale * sum over rows b < nb of part[b * nv + v], one block, in
 // a fixed order.
 __global__ void k_sum_rows(const double* part, int nb, int nv, double scale, double* out) {
@@ -984,6 +1062,27 @@ int Ctx::energy_issue(const ScState& h, double* e_dev) {
                                                      d_mu, d_part);
   k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, kNEnergy, geom.dvol, e_dev);
   CU(cudaGetLastError());
+  if (gradient) return ekin_issue(dens, d_mu, e_dev, 4, e_dev + kEkinOff);
+  return MPDPFT_OK;
+}
+
+// Kinetic integrals of the gradient-corrected density (k_ekin_grad) with
+// inner trapezoid cap maxit: 2 kMaxS values (times dvol) to out; mu and
+// e_dev (int V_ext n at [5 s + 1]) on the device.
+int Ctx::ekin_issue(const void* dens, const double* d_mu, const double* e_dev, int maxit, double* out) {
+  const int blocks = grid_blocks(geom.n);
+  const double thr = finite_t ? std::fabs(P.airy_threshold) : 1.0e300;
+  const double area_pref = std::pow(P.edge, (double)P.dim) * P.degeneracy / (4.0 * kPi * kPi);
+  if (rsize == sizeof(double))
+    k_ekin_grad<double><<<blocks, kThreads, 0, stream>>>(geom, S, P.degeneracy, thr, maxit, P.internal_acc, area_pref,
+                                                          (const double*)d_V, (const double*)d_lap, (const double*)d_g2,
+                                                          (const double*)dens, d_mu, e_dev, d_part);
+  else
+    k_ekin_grad<float><<<blocks, kThreads, 0, stream>>>(geom, S, P.degeneracy, thr, maxit, P.internal_acc, area_pref,
+                                                        (const float*)d_V, (const float*)d_lap, (const float*)d_g2,
+                                                        (const float*)dens, d_mu, e_dev, d_part);
+  k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, 2 * kMaxS, geom.dvol, out);
+  CU(cudaGetLastError());
   return MPDPFT_OK;
 }
 
@@ -994,6 +1093,30 @@ int Ctx::energy(mpdpft_result* r, const ScState& h) {
   double E[kNEnergy];
   CU(cudaMemcpyAsync(E, e_dev, sizeof(E), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
+  if (gradient && geom.dim == 3 && finite_t) {
+    // EkinAiT03D's outer loop (mpDPFT.cpp:5651-5700): the Airy-weighted
+    // integrals again with MaxIteration 5 .. 10 until a species' kinetic
+    // integral agrees with the previous one to max(RelAcc, MP)
+    const void* dens = (char*)d_nin + (size_t)h.slot * S * geom.n * rsize;
+    double* e2 = e_dev + kNEnergy;  // scratch beside the integrals
+    bool done[kMaxS] = {false, false, false, false};
+    for (int maxit = 5; maxit <= 10; ++maxit) {
+      if ((st = ekin_issue(dens, d_io, e_dev, maxit, e2))) return st;
+      double K[2 * kMaxS];
+      CU(cudaMemcpyAsync(K, e2, sizeof(K), cudaMemcpyDeviceToHost, stream));
+      CU(cudaStreamSynchronize(stream));
+      bool all = true;
+      for (int s = 0; s < S; ++s) {
+        if (done[s]) continue;
+        const double a = K[s], b = E[kEkinOff + s];
+        const double d = (a == 0.0 && b == 0.0) ? 0.0 : std::fabs((a - b) / (a + b));
+        E[kEkinOff + s] = a;
+        if (d < std::max(P.rel_acc, 1.0e-12)) done[s] = true;
+        else all = false;
+      }
+      if (all) break;
+    }
+  }
   energy_finish(r, E);
   return MPDPFT_OK;
 }
@@ -1026,6 +1149,10 @@ void Ctx::energy_finish(mpdpft_result* r, const double* E) {
     if (P.dim == 2 && (P.density_expression == MPDPFT_DENS_TF_INSPIRED ||
                        P.density_expression == MPDPFT_DENS_TF_INSPIRED_T))
       ekin = 0.5 * P.tau[s] * E[5 * s + 2];
+    else if (P.density_expression == MPDPFT_DENS_GRADIENT && P.dim == 2)  // E1 - int V n + mu N (:5608-5621)
+      ekin = E[kEkinOff + s] - E[kEkinOff + kMaxS + s] + r->mu[s] * r->abundance[s];
+    else if (P.density_expression == MPDPFT_DENS_GRADIENT)  // EkinAiT03D (:5647-5703)
+      ekin = P.degeneracy / (4.0 * kPi * kPi) * E[kEkinOff + s];
     else
       ekin = P.degeneracy * AF * std::pow(2.0, (D + 2.0) / 2.0) / (std::pow(2.0 * kPi, D) * (2.0 * D + 4.0)) *
              E[5 * s + 0];

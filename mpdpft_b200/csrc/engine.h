@@ -21,7 +21,11 @@ struct Adjoint;  // adjoint.cu
 enum { SPEC_DERIV = 0, SPEC_SMOOTH = 1, SPEC_COULOMB = 2 };
 
 // energy integrals per solve (k_energy)
-constexpr int kNEnergy = 5 * kMaxS + kMaxS * kMaxS;
+// [5 s + k] per species, [5 kMaxS + s kMaxS + t] pairs, then the kinetic
+// integrals of the gradient-corrected density: [kEkinOff + s] its point
+// values, [kEkinOff + kMaxS + s] int V n (2D)
+constexpr int kEkinOff = 5 * kMaxS + kMaxS * kMaxS;
+constexpr int kNEnergy = kEkinOff + 2 * kMaxS;
 
 struct Ctx {
   mpdpft_params P;
@@ -129,6 +133,7 @@ struct Ctx {
   int energy(mpdpft_result* r, const ScState& h);
   int energy_issue(const ScState& h, double* e_dev);  // kNEnergy integrals to e_dev (device)
   void energy_finish(mpdpft_result* r, const double* E);
+  int ekin_issue(const void* dens, const double* d_mu, const double* e_dev, int maxit, double* out);
   int integrate_device(const void* f, double* out);
   // standalone operators
   int op_mu_search(int s, const double* v, double target, double* mu_io, double* ab_out, int* trials,

@@ -1375,17 +1375,33 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
 }
 
 // ---- plane passes (3D): instantiated (s, lines per tile) per precision ----
+template <typename R, int S, int PRO>
+static void plane_fwd_pro(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
+  smem_optin(k_plane_fwd<R, S, NLY, NLZ, PRO>);
+  launch_k(k_plane_fwd<R, S, NLY, NLZ, PRO>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
+}
 template <typename R, int S>
 static void plane_fwd_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
+  if (a.pro == PRO_TAPER) plane_fwd_pro<R, S, PRO_TAPER>(grid, smem, st, a);
+  else plane_fwd_pro<R, S, PRO_NONE>(grid, smem, st, a);
+}
+template <typename R, int S, int EPI>
+static void plane_inv_epi(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
   constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
-  smem_optin(k_plane_fwd<R, S, NLY, NLZ>);
-  launch_k(k_plane_fwd<R, S, NLY, NLZ>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
+  smem_optin(k_plane_inv<R, S, NLY, NLZ, EPI>);
+  launch_k(k_plane_inv<R, S, NLY, NLZ, EPI>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
 }
 template <typename R, int S>
 static void plane_inv_ct(unsigned grid, size_t smem, cudaStream_t st, const ZArgs<R>& a) {
-  constexpr int NLY = plane_nly<R>(S), NLZ = plane_nlz<R>(S);
-  smem_optin(k_plane_inv<R, S, NLY, NLZ>);
-  launch_k(k_plane_inv<R, S, NLY, NLZ>, dim3(grid), dim3(kPlaneThreads), smem, st, a);
+  switch (a.epi) {
+    case EPI_POS: plane_inv_epi<R, S, EPI_POS>(grid, smem, st, a); break;
+    case EPI_GRAD: plane_inv_epi<R, S, EPI_GRAD>(grid, smem, st, a); break;
+    case EPI_COULOMB: plane_inv_epi<R, S, EPI_COULOMB>(grid, smem, st, a); break;
+    case EPI_SCALE: plane_inv_epi<R, S, EPI_SCALE>(grid, smem, st, a); break;
+    case EPI_COULOMB_V: plane_inv_epi<R, S, EPI_COULOMB_V>(grid, smem, st, a); break;
+    default: plane_inv_epi<R, S, EPI_STORE>(grid, smem, st, a); break;
+  }
 }
 
 template <typename R>

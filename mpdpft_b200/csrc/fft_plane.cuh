@@ -122,7 +122,7 @@ __device__ __forceinline__ void plane_y_pass(C* plane, C* A, C* B, const C* tw, 
 // Forward: real plane -> half-spectrum plane, R2C along z and C2C along y.
 // a.in, a.out, a.pro (PRO_NONE or PRO_TAPER), a.part as for k_z_r2c; the
 // plane index is blockIdx.x.
-template <typename R, int S, int NLY, int NLZ>
+template <typename R, int S, int NLY, int NLZ, int PRO>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
   pdl_wait();
   using C = typename Cx<R>::T;
@@ -144,7 +144,9 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
   for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
   double shift = 0.0;  // no shell points: no shift
-  if (a.pro == PRO_TAPER && *a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
+  if constexpr (PRO == PRO_TAPER) {
+    if (*a.vmax != 0ull) shift = from_ordered_bits(*a.vmax);
+  }
   const bool ok = __syncthreads_and(mbar_wait(&bar, 0, a.err)) != 0;
   if (!ok) return;
   double rowsum = 0.0;
@@ -155,7 +157,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
     auto load = [&](int m, int l) -> C {
       const int y = y0 + l;
       R x0 = realP[y * S + 2 * m], x1 = realP[y * S + 2 * m + 1];
-      if (a.pro == PRO_TAPER) {
+      if constexpr (PRO == PRO_TAPER) {
         const double h = -0.5 * a.g.L, dx = a.g.dx;
         const double px = h + dx * xi, py = h + dx * y;
         x0 = taper_xyz<R>(a, px, py, h + dx * (2 * m), x0, shift);
@@ -216,7 +218,11 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(ZArgs<R> a) {
 // Inverse: a.nin half-spectrum planes -> real outputs with a.epi (as
 // k_z_c2r: EPI_GRAD sums the squares of fields 0 .. nin-2 into rout[0] and
 // writes field nin-1 to rout[1]; the others write rout[0]).
-template <typename R, int S, int NLY, int NLZ>
+// EPI is the epilogue a.epi as a template argument: each instantiation
+// carries only its own epilogue code, which the last FFT stage inlines once
+// per radix output (the instruction cache misses of one kernel holding all
+// epilogues were the largest stall).
+template <typename R, int S, int NLY, int NLZ, int EPI>
 __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
   pdl_wait();
   using C = typename Cx<R>::T;
@@ -236,8 +242,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   for (int i = threadIdx.x; i < S; i += blockDim.x) { tw_s[i] = a.tw_s[i]; tw_n[i] = a.tw_n[i]; }
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw_m[i] = a.tw_m[i];
-  const bool coul = a.epi == EPI_COULOMB || a.epi == EPI_COULOMB_V;
-  const bool fusev = a.epi == EPI_COULOMB_V;
+  constexpr bool coul = EPI == EPI_COULOMB || EPI == EPI_COULOMB_V;
+  constexpr bool fusev = EPI == EPI_COULOMB_V;
   // V assembly: skipped once the SC loop has exited (V stays as it was)
   const bool vwrite = fusev && !__ldcg(&a.st->exit_loop);
   const double vfac = fusev ? fmin(1.0, __ldcg(&a.st->inc_v)) : 0.0;
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
         const int y = y0 + l;
         const R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
         const long p0 = ((long)xi * S + y) * S + 2 * m;
-        if (a.epi == EPI_GRAD) {
+        if constexpr (EPI == EPI_GRAD) {
           R* dst = acc + y * S + 2 * m;
           if (f == 0) { dst[0] = x0 * x0; dst[1] = x1 * x1; }
           else if (f < a.nin - 1) { dst[0] += x0 * x0; dst[1] += x1 * x1; }
@@ -296,7 +302,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
             *reinterpret_cast<C*>(a.rout[0] + p0) = C{dst[0], dst[1]};
             *reinterpret_cast<C*>(a.rout[1] + p0) = C{x0, x1};
           }
-        } else if (coul) {
+        } else if constexpr (coul) {
           const double h = -0.5 * a.g.L, dx = a.g.dx;
           const double px = h + dx * xi, py = h + dx * y, pz0 = h + dx * (2 * m), pz1 = h + dx * (2 * m + 1);
           R vh[2];
@@ -330,8 +336,12 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
             }
             *reinterpret_cast<C*>(a.vpot + p0) = C{vn[0], vn[1]};
           }
+        } else if constexpr (EPI == EPI_POS) {
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{x0 > R(0) ? x0 : R(0), x1 > R(0) ? x1 : R(0)};
+        } else if constexpr (EPI == EPI_SCALE) {
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{R(a.coul_coef * (double)x0), R(a.coul_coef * (double)x1)};
         } else {
-          *reinterpret_cast<C*>(a.rout[0] + p0) = C{z_output<R>(a, p0, x0, f0), z_output<R>(a, p0 + 1, x1, f0)};
+          *reinterpret_cast<C*>(a.rout[0] + p0) = C{x0, x1};
         }
       };
       fft_lines<C, M, NLZ, true>(A, B, tw_m, +1, load, store);
@@ -340,7 +350,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
     fence_proxy_async_smem();
     __syncthreads();
   }
-  if (fusev) {  // block sums of |V_new - V_old|^2 and the block's shell maximum
+  if constexpr (fusev) {  // block sums of |V_new - V_old|^2 and the block's shell maximum
     double accv[1] = {vacc};
     block_reduce_store<1>(accv, a.vres_part + (long)blockIdx.x * kMaxS);
     __shared__ double smx[kPlaneThreads / 32];

@@ -108,4 +108,64 @@ __device__ __forceinline__ double curly_a(double y) {
   return exp(-z) / (2.0 * sqrt(3.141592653589793) * sqrt(sqrt(y)) * sqrt(y));
 }
 
+// Ai(y) and Ai'(y) (gsl_sf_airy_Ai / _Ai_deriv at mpDPFT.cpp:3589, 5616,
+// 5666): on the CurlyA table's range [-150, 16) the first and second
+// derivatives of its Chebyshev series (Ai = -CurlyA', Ai' = -CurlyA''; the
+// derivative series by the recurrence d_{k-1} = d_{k+1} + 2 k c_k); outside
+// it the asymptotic expansions to third order in 1/zeta, zeta = 2 |y|^{3/2}/3
+// (Ai(x) ~ e^{-zeta} sum (-1)^k u_k zeta^{-k} / (2 sqrt(pi) x^{1/4}); for
+// negative arguments the sine and cosine series); 0 above 100, as the
+// reference sets there.
+// coefficients u_k = Gamma(3k + 1/2) / (54^k k! Gamma(k + 1/2)) and
+// v_k = -(6k + 1) u_k / (6k - 1) of the asymptotic series, k = 1 .. 3
+constexpr double kAiU1 = 0.069444444444444444, kAiU2 = 0.037133487654320988, kAiU3 = 0.037993059127800655;
+constexpr double kAiV1 = -0.097222222222222222, kAiV2 = -0.043885030864197531, kAiV3 = -0.042462830789894850;
+
+__device__ __forceinline__ void airy_ai_d(double y, double& ai, double& aip) {
+  constexpr double kSqrtPi = 1.7724538509055159;
+  if (y > 100.0) { ai = 0.0; aip = 0.0; return; }
+  if (y < MPDPFT_CA_X0 || y >= MPDPFT_CA_X1) {
+    const double x = fabs(y), r4 = sqrt(sqrt(x)), z = 2.0 / 3.0 * x * sqrt(x);
+    if (y < 0.0) {
+      const double sn = sin(z + 0.25 * 3.141592653589793), cs = cos(z + 0.25 * 3.141592653589793);
+      const double iz = 1.0 / z, iz2 = iz * iz;
+      ai = (sn * (1.0 - kAiU2 * iz2) - cs * iz * (kAiU1 - kAiU3 * iz2)) / (kSqrtPi * r4);
+      aip = r4 * (-cs * (1.0 - kAiV2 * iz2) - sn * iz * (kAiV1 - kAiV3 * iz2)) / kSqrtPi;
+    } else {
+      const double e = exp(-z), iz = 1.0 / z;
+      ai = e * (1.0 - iz * (kAiU1 - iz * (kAiU2 - iz * kAiU3))) / (2.0 * kSqrtPi * r4);
+      aip = -r4 * e * (1.0 - iz * (kAiV1 - iz * (kAiV2 - iz * kAiV3))) / (2.0 * kSqrtPi);
+    }
+    return;
+  }
+  const double u = (y - MPDPFT_CA_X0) / MPDPFT_CA_W;
+  int i = (int)floor(u);
+  i = i < 0 ? 0 : i;
+  const double* c = kCaTab + (long)i * MPDPFT_CA_DEG;
+  const double t = 2.0 * (u - (double)i) - 1.0;
+  double d1[MPDPFT_CA_DEG], d2[MPDPFT_CA_DEG];
+  const int n = MPDPFT_CA_DEG;
+  d1[n - 1] = 0.0;
+  d1[n - 2] = 2.0 * (n - 1) * __ldg(c + n - 1);
+  for (int k = n - 2; k >= 1; --k) d1[k - 1] = (k + 1 < n ? d1[k + 1] : 0.0) + 2.0 * k * __ldg(c + k);
+  d1[0] *= 0.5;
+  d2[n - 1] = 0.0;
+  d2[n - 2] = 2.0 * (n - 1) * d1[n - 1];
+  for (int k = n - 2; k >= 1; --k) d2[k - 1] = (k + 1 < n ? d2[k + 1] : 0.0) + 2.0 * k * d1[k];
+  d2[0] *= 0.5;
+  double b1 = 0.0, b2 = 0.0, e1 = 0.0, e2 = 0.0;
+  for (int j = n - 1; j >= 1; --j) {
+    const double b0 = fma(2.0 * t, b1, d1[j] - b2);
+    b2 = b1;
+    b1 = b0;
+    const double f0 = fma(2.0 * t, e1, d2[j] - e2);
+    e2 = e1;
+    e1 = f0;
+  }
+  const double s1 = fma(t, b1, d1[0] - b2), s2 = fma(t, e1, d2[0] - e2);
+  const double g = 2.0 / MPDPFT_CA_W;  // dt/dy
+  ai = -g * s1;
+  aip = -g * g * s2;
+}
+
 }  // namespace mpdpft

@@ -433,6 +433,45 @@ double CurlyA(double y) {
   return std::exp(-z) / (2. * std::sqrt(PI) * std::pow(y, 0.75));
 }
 
+// Ai(y), Ai'(y) (gsl_sf_airy_Ai / _Ai_deriv, MD:3589, 5616, 5666): on the
+// CurlyA table's range the negated first and second derivatives of its
+// Chebyshev series, outside it the asymptotic expansions with their first
+// correction terms; 0 above 100.
+void airy_ai_d(double y, double& ai, double& aip) {
+  const double sp = std::sqrt(PI);
+  if (y > 100.) { ai = aip = 0.; return; }
+  if (y < MPDPFT_CA_X0 || y >= MPDPFT_CA_X1) {
+    const double x = std::fabs(y), r4 = std::pow(x, 0.25), z = 2. / 3. * x * std::sqrt(x);
+    // u_k = Gamma(3k + 1/2) / (54^k k! Gamma(k + 1/2)), v_k = -(6k+1) u_k/(6k-1)
+    const double u1 = 5. / 72., u2 = 385. / 10368., u3 = 0.037993059127800655;
+    const double v1 = -7. / 72., v2 = -455. / 10368., v3 = -19. / 17. * u3;
+    const double iz = 1. / z, iz2 = iz * iz;
+    if (y < 0.) {
+      const double sn = std::sin(z + 0.25 * PI), cs = std::cos(z + 0.25 * PI);
+      ai = (sn * (1. - u2 * iz2) - cs * iz * (u1 - u3 * iz2)) / (sp * r4);
+      aip = r4 * (-cs * (1. - v2 * iz2) - sn * iz * (v1 - v3 * iz2)) / sp;
+    } else {
+      const double e = std::exp(-z);
+      ai = e * (1. - u1 * iz + u2 * iz2 - u3 * iz2 * iz) / (2. * sp * r4);
+      aip = -r4 * e * (1. - v1 * iz + v2 * iz2 - v3 * iz2 * iz) / (2. * sp);
+    }
+    return;
+  }
+  const double u = (y - MPDPFT_CA_X0) / MPDPFT_CA_W;
+  int i = (int)std::floor(u);
+  if (i < 0) i = 0;
+  const double* c = kCaTab + (long)i * MPDPFT_CA_DEG;
+  const int n = MPDPFT_CA_DEG;
+  std::vector<double> d1(n + 1, 0.), d2(n + 1, 0.);
+  for (int k = n - 1; k >= 1; --k) d1[k - 1] = d1[k + 1] + 2. * k * c[k];
+  d1[0] *= 0.5;
+  for (int k = n - 1; k >= 1; --k) d2[k - 1] = d2[k + 1] + 2. * k * d1[k];
+  d2[0] *= 0.5;
+  const double t = 2. * (u - i) - 1., g = 2. / MPDPFT_CA_W;
+  ai = -g * cheb(d1.data(), n, t);
+  aip = -g * g * cheb(d2.data(), n, t);
+}
+
 struct NAiT {  // the arguments nAiTintegrand takes beside x (MD:3580)
   double prefactor, U, ar, prefactor2, T, compare, rtpna;
   int bp, max_iter;
@@ -1066,6 +1105,102 @@ void inject_schedule(State& st) {  // MD:5229-5315, schedules 5 and 9
 }
 
 // --------------------------------------------------------- energies ----
+// Kinetic energy of the gradient-corrected density (GetDispersalEnergy,
+// DensityExpression 5, MD:5606-5703), units 1 (alpha = 1).
+//  2D (MD:5608-5621): E1 - int V n + mu N, E1 = int g/2 [lap CurlyA(y)/(12 pi)
+//     - |grad V|^{4/3} (y^2 CurlyA(y) + Ai(y) + y Ai'(y))/(8 pi)],
+//     y = 2 (V - mu) / |grad V|^{2/3}, 0 where |grad V|^2 <= MP, Ai = Ai' = 0
+//     from y = 50.
+//  3D EkinAiT03D (MD:5647-5703): g/(4 pi^2) int T, T = (2u)^{5/2}/5 -
+//     lap (2u)^{1/2}/6 (u = mu - V > 0, else 0) where a = |grad V|^{2/3}/2 <
+//     Mpp[2] (the T -> 0 form: everywhere), else the Airy-weighted integral
+//     int_0^{x1} Ai(x + U/a) [(2ax)^{5/2}/5 - lap (2ax)^{1/2}/6] dx, U = V - mu,
+//     x1 = max(1, 100 - U/a), by the trapezoid rule on 64, 128, ... points
+//     until two agree (ASYMcritABS < MP) or MaxIteration doublings; the whole
+//     integral again with MaxIteration + 1 ... (4 .. 10) until two agree to
+//     max(RelAcc, MP).
+double ekin_gradient(State& st, int s, double e_env) {
+  const mpdpft_params& P = st.P;
+  const long G = st.G;
+  const double g = P.degeneracy, mu = st.mu[s];
+  const std::vector<double>& V = st.V[s];
+  const std::vector<double>& lap = st.Lap[s];
+  const std::vector<double>& g2 = st.Grad2[s];
+  std::vector<double> tmp(G);
+  if (st.D == 2) {
+    for (long i = 0; i < G; ++i) {
+      const double U = V[i] - mu, ab = std::fabs(g2[i]);
+      if (ab > MP) {
+        const double y = 2. * U / std::cbrt(ab);
+        double ai = 0., aip = 0.;
+        if (y < 50.) airy_ai_d(y, ai, aip);
+        const double ca = CurlyA(y);
+        tmp[i] = 0.5 * g * (lap[i] * ca / (12. * PI) - std::pow(ab, 2. / 3.) * (y * y * ca + ai + y * aip) / (8. * PI));
+      } else {
+        tmp[i] = 0.;
+      }
+    }
+    const double e1 = integrate(st, tmp);
+    for (long i = 0; i < G; ++i) tmp[i] = V[i] * st.Den[s][i];
+    return e1 - integrate(st, tmp) + mu * st.tmp_ab[s];
+  }
+  const bool airy = P.gradient_form == MPDPFT_GRADIENT_FINITE_T;
+  const double thr = airy ? std::fabs(P.airy_threshold) : 1.0e300;
+  const double pref = g / (4. * PI * PI), area = std::pow(P.edge, 3.);
+  auto asym = [](double x, double y) { return (x == 0. && y == 0.) ? 0. : (x - y) / (x + y); };
+  auto asym_abs = [](double x, double y, double crit) {
+    return (std::fabs(x) < crit && std::fabs(y) < crit) ? 0. : std::fabs((x - y) / (x + y));
+  };
+  auto negligible = [](double big, double small, double max_exp) {
+    if (small == 0.) return true;
+    if (big == 0. || big < small) return false;
+    return std::log10(std::fabs(big)) - std::log10(std::fabs(small)) > max_exp;
+  };
+  double e = 0., eprev = 0.;
+  for (int outer = 0, maxit = 4;; ++outer, ++maxit) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long i = 0; i < G; ++i) {
+      const double U = V[i] - mu, a = 0.5 * std::cbrt(std::fabs(g2[i]));
+      if (a < thr) {
+        const double w = 2. * (-U);
+        tmp[i] = -U > 0. ? w * w * std::sqrt(w) / 5. - lap[i] * std::sqrt(w) / 6. : 0.;
+        continue;
+      }
+      const double x1 = std::max(1., 100. - U / a);
+      double prev = 1., res = 0.;
+      for (int it = 0, n = 64;; ++it, n *= 2) {
+        const double h = x1 / (double)(n - 1);
+        double sum = 0.;
+        for (int j = 0; j < n; ++j) {
+          const double x = (double)j * h, y = x + U / a;
+          double ai = 0., aip;
+          if (!(y > 100.)) {
+            if (y > -300.) airy_ai_d(y, ai, aip);
+            else ai = std::cos(2. * (-y) * std::sqrt(-y) / 3. - 0.25 * PI) / (std::sqrt(PI) * std::pow(-y, 0.25));
+          }
+          const double w = 2. * a * x;
+          const double f = ai * (w * w * std::sqrt(w) / 5. - lap[i] * std::sqrt(w) / 6.);
+          sum += (j == 0 || j == n - 1) ? 0.5 * f : f;
+        }
+        res = sum * h;
+        if (it > 0 && (asym_abs(res, prev, MP) < MP ||
+                       (std::fabs(asym(res, prev)) < P.internal_acc &&
+                        negligible(e_env, area * pref * res, -std::log(P.internal_acc)))))
+          break;
+        if (it == maxit) break;
+        prev = res;
+      }
+      tmp[i] = res;
+    }
+    e = pref * integrate(st, tmp);
+    if (!airy) break;  // no Airy points: MaxIteration does not enter
+    if (outer > 0 && std::fabs(asym(e, eprev)) < std::max(P.rel_acc, MP)) break;
+    if (maxit >= 10) break;
+    eprev = e;
+  }
+  return e;
+}
+
 void energy(State& st, mpdpft_result* res) {
   const mpdpft_params& P = st.P;
   const int D = st.D;
@@ -1130,6 +1265,8 @@ void energy(State& st, mpdpft_result* res) {
     if (D == 2 && (P.density_expression == MPDPFT_DENS_TF_INSPIRED || P.density_expression == MPDPFT_DENS_TF_INSPIRED_T)) {
       for (long i = 0; i < G; ++i) tmp[i] = st.Den[s][i] * st.Den[s][i];
       ekin = 0.5 * P.tau[s] * integrate(st, tmp);
+    } else if (P.density_expression == MPDPFT_DENS_GRADIENT) {
+      ekin = ekin_gradient(st, s, eenv);
     } else {  // TF potential functional, MD:5741-5750 (U = 1)
       for (long i = 0; i < G; ++i) {
         double t = st.mu[s] - st.V[s][i];
@@ -1309,6 +1446,8 @@ void oracle_energy(const mpdpft_params* p, const double* vext, const double* den
     st.Den[q].assign(dens + q * st.G, dens + (q + 1) * st.G);
     st.V[q].assign(v + q * st.G, v + (q + 1) * st.G);
     st.mu[q] = mu[q];
+    st.tmp_ab[q] = integrate(st, st.Den[q]);
+    if (p->density_expression == MPDPFT_DENS_GRADIENT) delfield(st, st.V[q], st.Grad2[q], st.Lap[q]);
   }
   std::memset(result, 0, sizeof(*result));
   energy(st, result);
@@ -1351,6 +1490,7 @@ int oracle_num_threads(void) {
 double oracle_polylog(int order, double x) { return polylog(order, x); }
 double oracle_curly_a(double x) { return CurlyA(x); }
 double oracle_i0e(double x) { return i0e(x); }
+void oracle_airy(double x, double* ai, double* aip) { airy_ai_d(x, *ai, *aip); }
 double oracle_finite_t_point(const mpdpft_params* p, double T, double u, double lap, double grad2) {
   State st;
   mpdpft_params q = *p;

@@ -59,6 +59,8 @@ def lib():
         L.oracle_curly_a.restype = C.c_double
         L.oracle_i0e.argtypes = [C.c_double]
         L.oracle_i0e.restype = C.c_double
+        L.oracle_airy.argtypes = [C.c_double, _dp, _dp]
+        L.oracle_airy.restype = None
         L.oracle_finite_t_point.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_double]
         L.oracle_finite_t_point.restype = C.c_double
         _lib = L
@@ -97,6 +99,13 @@ def polylog(s, x):
 def curly_a(x):
     """int_x^inf Ai(t) dt (the reference's CurlyA)."""
     return lib().oracle_curly_a(float(x))
+
+
+def airy(x):
+    """(Ai(x), Ai'(x)) as the energies of the gradient-corrected density use them."""
+    a, b = C.c_double(), C.c_double()
+    lib().oracle_airy(float(x), C.byref(a), C.byref(b))
+    return a.value, b.value
 
 
 def i0e(x):

@@ -95,6 +95,25 @@ def test_finite_t_sc_solve(eng, oracle_lib, thr, prec, n_tol):
     assert l1 < n_tol
 
 
+@pytest.mark.parametrize("prec,tol", [(abi.FP64, 1e-10), (abi.MIXED, 1e-4)])
+def test_finite_t_kinetic_energy(eng, oracle_lib, prec, tol):
+    """EkinAiT03D (mpDPFT.cpp:5647-5703) on the GPU against the oracle on
+    the GPU's own converged fields: the Airy-averaged kinetic integrand near
+    the nucleus (threshold 2) with its trapezoid doubling and the outer
+    MaxIteration 4 .. 10 loop, the small-gradient integrand elsewhere."""
+    p, vext, v0 = atom(32, prec, airy_threshold=2.0)
+    pr, _, _ = atom(32, abi.FP64, airy_threshold=2.0)
+    with eng.Engine(p) as e:
+        res, log, st = e.sc_run(vext, v0)
+        dens = e.field(abi.FIELD_DENSITY, 0).astype(np.float64)
+        v = e.field(abi.FIELD_POTENTIAL, 0).astype(np.float64)
+    r = oracle_lib.energy(pr, vext, [dens], [v], [res.mu[0]])
+    print("E_kin GPU %.12f oracle %.12f; E_ext %.12f %.12f" % (res.e_kinetic[0], r.e_kinetic[0], res.e_external[0],
+                                                              r.e_external[0]))
+    assert abs(res.e_kinetic[0] - r.e_kinetic[0]) <= tol * abs(r.e_kinetic[0])
+    assert abs(res.e_external[0] - r.e_external[0]) <= tol * abs(r.e_external[0])
+
+
 def test_finite_t_parameters_are_checked(eng):
     for bad in (dict(boole_pairs=0), dict(boole_pairs=51), dict(boole_max_iter=22), dict(internal_acc=0.0),
                 dict(temperature=[0.0])):

@@ -133,3 +133,100 @@ def test_bessel_i0e_against_scipy(oracle_lib):
     xs = np.concatenate([np.linspace(0.0, 40.0, 801), np.geomspace(1e-8, 1e4, 200)])
     err = max(abs(oracle_lib.i0e(x) - sp.i0e(x)) / sp.i0e(x) for x in xs)
     assert err < 1e-14, err
+
+
+def test_airy_against_scipy(oracle_lib):
+    """Ai and Ai' of the kinetic energies of the gradient-corrected density
+    (gsl_sf_airy_Ai / _Ai_deriv, mpDPFT.cpp:5616, 5666): the negated first
+    and second derivatives of the CurlyA Chebyshev series on [-150, 16),
+    asymptotic series outside, against scipy."""
+    import scipy.special as sp
+    # (the second derivative of the series loses more digits: Ai' to 1e-9)
+    for lo, hi, tol in [(-150.0, 16.0, 1e-9), (-300.0, -150.0, 1e-10), (16.0, 99.0, 5e-8)]:
+        for x in np.linspace(lo, hi, 3001):
+            a, b = oracle_lib.airy(x)
+            A, Ap, _, _ = sp.airy(x)
+            # near a zero of Ai (Ai') the absolute error against the envelope
+            env_a = abs(x) ** -0.25 / np.sqrt(np.pi) if x < -1 else abs(A)
+            env_b = abs(x) ** 0.25 / np.sqrt(np.pi) if x < -1 else abs(Ap)
+            # (values below 1e-15 to 1e-15 tol absolute: the table's own floor)
+            assert abs(a - A) <= tol * max(env_a, 1e-15), (x, a, A)
+            assert abs(b - Ap) <= tol * max(env_b, 1e-15), (x, b, Ap)
+
+
+def _cosine_problem(dim, **kw):
+    """V = V0 + A cos(2 pi x / L) along the first axis on a small periodic
+    grid, with its smoothed Laplacian and |grad V|^2 from the oracle's
+    DelField (method 5, the fields the kinetic energies read)."""
+    from mpdpft_b200 import workloads as W
+    steps, edge = 8, 8.0
+    p = abi.make_params(dim=dim, steps=steps, edge=edge, density_expression=abi.DENS_GRADIENT, degeneracy=2.0,
+                        abundances=[10.0], interactions=[], smearing_extent=0.5, **kw)
+    x = W.axis(steps, edge)
+    shape = (steps,) * dim
+    xs = x.reshape((steps,) + (1,) * (dim - 1)) * np.ones(shape)
+    v = (-1.0 + 1.5 * np.cos(2.0 * np.pi * xs / edge)).reshape(-1)
+    return p, v
+
+
+def test_ekin_ait0_3d_against_scipy(oracle_lib):
+    """EkinAiT03D (mpDPFT.cpp:5647-5703) of the oracle's energy against a
+    scipy restatement: g/(4 pi^2) int [ (2(mu-V))^{5/2}/5 - lap V (2(mu-V))^{1/2}/6 ]
+    where a = |grad V|^{2/3}/2 < Mpp[2], else the Airy average
+    int_0^{max(1, 100 - U/a)} Ai(x + U/a) [ (2ax)^{5/2}/5 - lap V (2ax)^{1/2}/6 ] dx
+    (U = V - mu) by adaptive quadrature; the oracle doubles its trapezoid
+    grid from 64 points up to MaxIteration 4 .. 10 as the reference does."""
+    import scipy.integrate as si
+    import scipy.special as sp
+    p, v = _cosine_problem(3, gradient_form=abi.GRADIENT_FINITE_T, airy_threshold=0.2, internal_acc=1e-12,
+                           rel_acc=1e-12)
+    mu = 0.3
+    g2, lap = oracle_lib.delfield(p, v)
+    a = 0.5 * np.cbrt(np.abs(g2))
+    assert (a >= 0.2).any() and (a < 0.2).any()
+    t = np.empty_like(v)
+    for i in range(v.size):
+        U, L = v[i] - mu, lap[i]
+        if a[i] < 0.2:
+            w = -2.0 * U
+            t[i] = w ** 2.5 / 5.0 - L * np.sqrt(w) / 6.0 if w > 0 else 0.0
+        else:
+            x1 = max(1.0, 100.0 - U / a[i])
+            f = lambda x: sp.airy(x + U / a[i])[0] * ((2 * a[i] * x) ** 2.5 / 5.0 - L * np.sqrt(2 * a[i] * x) / 6.0)
+            t[i] = si.quad(f, 0.0, x1, limit=400, epsabs=0.0, epsrel=1e-11)[0]
+    ref = 2.0 / (4.0 * np.pi ** 2) * oracle_lib.integrate(p, t)
+    dens = np.full_like(v, 0.1)
+    r = oracle_lib.energy(p, [v], [dens], [v], [mu])
+    assert abs(r.e_kinetic[0] - ref) <= 1e-7 * abs(ref), (r.e_kinetic[0], ref)
+    # with no Airy points the small-gradient integrand everywhere
+    p0, _ = _cosine_problem(3, gradient_form=abi.GRADIENT_FINITE_T, airy_threshold=1e300)
+    w = np.maximum(-2.0 * (v - mu), 0.0)
+    ref0 = 2.0 / (4.0 * np.pi ** 2) * oracle_lib.integrate(p0, w ** 2.5 / 5.0 - lap * np.sqrt(w) / 6.0)
+    r0 = oracle_lib.energy(p0, [v], [dens], [v], [mu])
+    assert abs(r0.e_kinetic[0] - ref0) <= 1e-13 * abs(ref0)
+
+
+def test_ekin_2d_against_scipy(oracle_lib):
+    """The 2D kinetic energy of DensityExpression 5 (mpDPFT.cpp:5608-5621):
+    int g/2 [ lap V CurlyA(y)/(12 pi) - |grad V|^{4/3} (y^2 CurlyA(y) + Ai(y)
+    + y Ai'(y))/(8 pi) ] - int V n + mu N, y = 2 (V - mu)/|grad V|^{2/3}
+    (Ai = Ai' = 0 from y = 50 on, integrand 0 where |grad V|^2 <= 1e-12),
+    with scipy's Airy functions and mpmath's CurlyA = 1/3 - int_0^y Ai."""
+    import scipy.special as sp
+    p, v = _cosine_problem(2, airy_threshold=1e300)
+    mu = 0.3
+    g2, lap = oracle_lib.delfield(p, v)
+    ab = np.abs(g2)
+    t = np.zeros_like(v)
+    for i in range(v.size):
+        if ab[i] > 1e-12:
+            y = 2.0 * (v[i] - mu) / np.cbrt(ab[i])
+            ai, aip = sp.airy(y)[:2] if y < 50.0 else (0.0, 0.0)
+            ca = mp_curly_a(y)
+            t[i] = 1.0 * (lap[i] * ca / (12 * np.pi) - ab[i] ** (2 / 3) * (y * y * ca + ai + y * aip) / (8 * np.pi))
+    rng = np.random.default_rng(5)
+    dens = rng.uniform(0.0, 0.2, v.size)
+    n = oracle_lib.integrate(p, dens)
+    ref = oracle_lib.integrate(p, t) - oracle_lib.integrate(p, v * dens) + mu * n
+    r = oracle_lib.energy(p, [v], [dens], [v], [mu])
+    assert abs(r.e_kinetic[0] - ref) <= 1e-9 * abs(ref), (r.e_kinetic[0], ref)
