@@ -516,7 +516,7 @@ int Batch::run(mpdpft_result* results, int* status) {
     CU(cudaMemcpyAsync(&h[i], members[i]->d_state, sizeof(ScState), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
   for (int i = 0; i < count; ++i)
-    if ((st = members[i]->energy_issue(h[i], d_energy + (size_t)i * kNEnergy))) return st;
+    if ((st = members[i]->energy_issue(h[i], d_energy + (size_t)i * kNEnergy, /*g2_current=*/true))) return st;
   std::vector<double> E((size_t)count * kNEnergy);
   CU(cudaMemcpyAsync(E.data(), d_energy, sizeof(double) * E.size(), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));

@@ -1043,11 +1043,19 @@ int Ctx::fill_result(mpdpft_result* r, const ScState& h) {
 // of the last density evaluation, as in the reference's ExportData.
 // energy_issue leaves the kNEnergy integrals (times dvol) at e_dev on the
 // stream; energy_finish forms the energies from them on the host.
-int Ctx::energy_issue(const ScState& h, double* e_dev) {
+int Ctx::energy_issue(const ScState& h, double* e_dev, bool g2_current) {
   int st;
   double* d_mu = d_io;  // scratch
   CU(cudaMemcpyAsync(d_mu, h.mu, sizeof(double) * kMaxS, cudaMemcpyHostToDevice, stream));
   const void* dens = (char*)d_nin + (size_t)h.slot * S * geom.n * rsize;
+  if (gradient && geom.dim == 2 && !need_g2 && !g2_current) {
+    // the 2D kinetic energy reads |grad V|^2, which the iterations' DelField
+    // leaves out (the 2D density does not use it)
+    need_g2 = true;
+    st = issue_delfield_of_V();
+    need_g2 = false;
+    if (st) return st;
+  }
   if (has_coulomb) {
     if ((st = issue_coulomb(dens, d_vh, /*for_energy=*/1))) return st;
   }

@@ -131,7 +131,9 @@ struct Ctx {
   int sc_run(mpdpft_result* result, mpdpft_iter_log* log, int cap, int use_graph);
   int fill_result(mpdpft_result* r, const ScState& h);
   int energy(mpdpft_result* r, const ScState& h);
-  int energy_issue(const ScState& h, double* e_dev);  // kNEnergy integrals to e_dev (device)
+  // kNEnergy integrals to e_dev (device); g2_current: d_g2 already holds
+  // |grad V|^2 of the current V (the batch's 2D transforms always write it)
+  int energy_issue(const ScState& h, double* e_dev, bool g2_current = false);
   void energy_finish(mpdpft_result* r, const double* E);
   int ekin_issue(const void* dens, const double* d_mu, const double* e_dev, int maxit, double* out);
   int integrate_device(const void* f, double* out);
