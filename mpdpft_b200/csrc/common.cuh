@@ -403,13 +403,24 @@ __device__ __forceinline__ R density_at(const DensParams& d, R u, R lap, R g2) {
   return r > R(0) ? r : R(0);
 }
 
-// 1/sqrt(u) for u > 0 to double precision: FP32 hardware estimate refined by
-// two Newton steps r <- r (3 - u r^2)/2 in double (the error squares each
-// step: ~2^-23 -> ~2^-46 -> below double rounding).  Inputs below the FP32
-// normal range fall back to the library division.
+// Start value of a double-precision 1/sqrt(u), u > 0 normal: the PTX
+// approximation rsqrt.approx.ftz.f64, which reads the double itself (an
+// FP32 estimate would need two conversions to and from 64-bit types, which
+// issue at a quarter of the FP64 FMA rate).  Its error is squared by each
+// Newton step of the callers.
+__device__ __forceinline__ double rsqrt_seed(double u) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(u));
+  return r;
+}
+
+// 1/sqrt(u) for u > 0 to double precision: the estimate refined by two
+// Newton steps r <- r (3 - u r^2)/2 in double (the error squares each step
+// and ends below double rounding).  Inputs outside [1e-30, 1e30] fall back
+// to the library division.
 __device__ __forceinline__ double rsqrt_d(double u) {
   if (u < 1.0e-30 || u > 1.0e30) return 1.0 / sqrt(u);
-  double r = (double)rsqrtf((float)u);
+  double r = rsqrt_seed(u);
   double h = 0.5 * u;
   r = r * fma(-h * r, r, 1.5);
   r = r * fma(-h * r, r, 1.5);

@@ -211,9 +211,9 @@ __device__ __forceinline__ EvalK eval_constants(const DensParams& d) {
   return k;
 }
 
-// rsqrt_d without its range branch (callers clamp u to [1e-30, 1e30]).
+// rsqrt_d without its range branch (callers keep u normal and positive).
 __device__ __forceinline__ double rsqrt_nr(double u) {
-  double r = (double)rsqrtf((float)u);
+  double r = rsqrt_seed(u);
   const double h = 0.5 * u;
   r = r * fma(-h * r, r, 1.5);
   r = r * fma(-h * r, r, 1.5);
@@ -223,27 +223,38 @@ __device__ __forceinline__ double rsqrt_nr(double u) {
 // n(u) of the 3D gradient-corrected form for A = cg lap, B = cg c2/4 |grad V|^2
 // (density_at_d without branches: u^{-1/2}, u^{-3/2} continued linearly below
 // the floor, n = 0 for u <= 0 or a negative value).
+// HB: the |grad V|^2 term is present (B != 0); without it the u^{-3/2}
+// factor is not formed.  u is replaced by 1 where it is not in
+// [1e-30, 1e30] before the square root (the result is 0 for u <= 0, and u
+// stays far inside the range elsewhere), with selects rather than FP64
+// min/max instructions.
+template <bool HB = true>
 __device__ __forceinline__ double grad3_n(const EvalK& k, double u, double A, double B) {
-  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const bool pos = u > 0.0;
+  const double r = rsqrt_nr(u > 1.0e-30 && u < 1.0e30 ? u : 1.0);
   const bool hi = u >= k.floor_u;
   const double m1 = hi ? r : u * k.c1;
-  const double m3 = hi ? r * r * r : u * k.c3;
-  const double v = k.ctf * u * u * r - (A * m1 + B * m3);
-  return (u > 0.0 && v > 0.0) ? v : 0.0;
+  double v = k.ctf * u * u * r - A * m1;
+  if constexpr (HB) v -= B * (hi ? r * r * r : u * k.c3);
+  return (pos && v > 0.0) ? v : 0.0;
 }
 
 // n(u) and dn/du of the same form with one reciprocal square root.
+template <bool HB = true>
 __device__ __forceinline__ double grad3_n_slope(const EvalK& k, double u, double A, double B, double& sl) {
-  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const double r = rsqrt_nr(u > 1.0e-30 && u < 1.0e30 ? u : 1.0);
   const bool hi = u >= k.floor_u;
   const double r3 = r * r * r;
   const double m1 = hi ? r : u * k.c1;
-  const double m3 = hi ? r3 : u * k.c3;
   const double dm1 = hi ? -0.5 * r3 : k.c1;
-  const double dm3 = hi ? -1.5 * r3 * r * r : k.c3;
-  const double v = k.ctf * u * u * r - (A * m1 + B * m3);
+  double v = k.ctf * u * u * r - A * m1;
+  double dv = 1.5 * k.ctf * u * r - A * dm1;
+  if constexpr (HB) {
+    v -= B * (hi ? r3 : u * k.c3);
+    dv -= B * (hi ? -1.5 * r3 * r * r : k.c3);
+  }
   const bool pos = u > 0.0 && v > 0.0;
-  sl = pos ? 1.5 * k.ctf * u * r - (A * dm1 + B * dm3) : 0.0;
+  sl = pos ? dv : 0.0;
   return pos ? v : 0.0;
 }
 
@@ -262,12 +273,12 @@ __device__ __forceinline__ double grad3_slope(const EvalK& k, double u, double A
 }
 
 __device__ __forceinline__ double tf3_n(const EvalK& k, double u) {
-  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const double r = rsqrt_nr(u > 1.0e-30 && u < 1.0e30 ? u : 1.0);
   return u > 0.0 ? k.ctf * u * u * r : 0.0;
 }
 
 __device__ __forceinline__ double tf3_slope(const EvalK& k, double u) {
-  const double r = rsqrt_nr(fmin(fmax(u, 1.0e-30), 1.0e30));
+  const double r = rsqrt_nr(u > 1.0e-30 && u < 1.0e30 ? u : 1.0);
   return u > 0.0 ? 1.5 * k.ctf * u * r : 0.0;
 }
 
@@ -391,6 +402,38 @@ __device__ __forceinline__ void mu_point(const DensParams& d, const EvalK& k, co
   }
 }
 
+// The 3D gradient-corrected form of mu_points (below), HB as for grad3_n.
+template <bool HB, int NPT, typename R>
+__device__ __forceinline__ void mu_points_grad3(const EvalK& k, const double* cmu, int nc, const R (&vr)[NPT],
+                                                const R (&lr)[NPT], const R (&gr)[NPT], const bool (&ok)[NPT],
+                                                double (&acc)[kMuAcc]) {
+  double v[NPT], A[NPT], B[NPT];
+#pragma unroll
+  for (int i = 0; i < NPT; ++i) {
+    v[i] = (double)vr[i];
+    A[i] = k.cg * (double)lr[i];
+    B[i] = HB ? k.cg2 * (double)gr[i] : 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < NPT; ++i) {
+    double sl;
+    const double n0 = grad3_n_slope<HB>(k, cmu[0] - v[i], A[i], B[i], sl);
+    acc[0] += ok[i] ? n0 : 0.0;
+    acc[kMuCand] += ok[i] ? sl : 0.0;
+  }
+#pragma unroll
+  for (int c = 1; c < kMuCand; ++c) {
+    if (c >= nc) break;
+    double t = 0.0;
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+      const double x = grad3_n<HB>(k, cmu[c] - v[i], A[i], B[i]);
+      t += ok[i] ? x : 0.0;
+    }
+    acc[c] += t;
+  }
+}
+
 // mu_point for the NPT points of a lane's trip (ok[i]: point i exists):
 // the candidate loop is the outer one, so the points' evaluations are NPT
 // independent chains.
@@ -398,37 +441,25 @@ template <int FK, int NPT, typename R>
 __device__ __forceinline__ void mu_points(const DensParams& d, const EvalK& k, const double* cmu, int nc,
                                           const R (&vr)[NPT], const R (&lr)[NPT], const R (&gr)[NPT],
                                           const bool (&ok)[NPT], double (&acc)[kMuAcc], const double* kx) {
-  if constexpr (FK == 1 || FK == 2) {
-    double v[NPT], A[NPT], B[NPT];
+  if constexpr (FK == 1) {
+    // the reference's small-gradient branch has no |grad V|^2 term
+    if (k.cg2 == 0.0) mu_points_grad3<false, NPT>(k, cmu, nc, vr, lr, gr, ok, acc);
+    else mu_points_grad3<true, NPT>(k, cmu, nc, vr, lr, gr, ok, acc);
+  } else if constexpr (FK == 2) {
+    double v[NPT];
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) v[i] = (double)vr[i];
 #pragma unroll
     for (int i = 0; i < NPT; ++i) {
-      v[i] = (double)vr[i];
-      A[i] = k.cg * (double)lr[i];
-      B[i] = k.cg2 * (double)gr[i];
-    }
-#pragma unroll
-    for (int i = 0; i < NPT; ++i) {
-      double n0, sl;
-      if constexpr (FK == 1) {
-        n0 = grad3_n_slope(k, cmu[0] - v[i], A[i], B[i], sl);
-      } else {
-        n0 = tf3_n(k, cmu[0] - v[i]);
-        sl = tf3_slope(k, cmu[0] - v[i]);
-      }
-      acc[0] += ok[i] ? n0 : 0.0;
-      acc[kMuCand] += ok[i] ? sl : 0.0;
+      acc[0] += ok[i] ? tf3_n(k, cmu[0] - v[i]) : 0.0;
+      acc[kMuCand] += ok[i] ? tf3_slope(k, cmu[0] - v[i]) : 0.0;
     }
 #pragma unroll
     for (int c = 1; c < kMuCand; ++c) {
       if (c >= nc) break;
       double t = 0.0;
 #pragma unroll
-      for (int i = 0; i < NPT; ++i) {
-        double x;
-        if constexpr (FK == 1) x = grad3_n(k, cmu[c] - v[i], A[i], B[i]);
-        else x = tf3_n(k, cmu[c] - v[i]);
-        t += ok[i] ? x : 0.0;
-      }
+      for (int i = 0; i < NPT; ++i) t += ok[i] ? tf3_n(k, cmu[c] - v[i]) : 0.0;
       acc[c] += t;
     }
   } else {
