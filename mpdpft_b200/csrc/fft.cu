@@ -1478,7 +1478,7 @@ static int launch_plane_inv(Ctx& c, void* const* in, int nin, int epi, R* out0, 
     if (epi == EPI_COULOMB_V) b += (3.0 + ((a.contact_self || a.dirac) ? 1.0 : 0.0)) * c.field_bytes();
     c.note("k_plane_inv", b);
   }
-  plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s), epi == EPI_GRAD), c.stream, a);
+  plane_dispatch<R>(false, f.s, plane_inv_smem<R>(f.s, plane_nly<R>(f.s), plane_nlz<R>(f.s), epi == EPI_GRAD || epi == EPI_COULOMB || epi == EPI_COULOMB_V), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }

@@ -93,7 +93,7 @@ inline bool plane_size_instantiated(int s) {
 
 // Shared-memory bytes: the spectrum plane (which first holds the real plane),
 // the two Stockham tiles, twiddles, and the |grad|^2 accumulator (inverse,
-// EPI_GRAD).
+// EPI_GRAD) or the epilogue tile (inverse, Coulomb epilogues).
 template <typename R>
 __host__ __device__ constexpr size_t plane_tile(int S, int NLY, int NLZ) {
   return (size_t)S * (NLY + 1) > (size_t)(S / 2) * (NLZ + 1) ? (size_t)S * (NLY + 1) : (size_t)(S / 2) * (NLZ + 1);
@@ -103,8 +103,8 @@ __host__ __device__ constexpr size_t plane_fwd_smem(int S, int NLY, int NLZ) {
   return ((size_t)S * (S / 2 + 1) + 2 * plane_tile<R>(S, NLY, NLZ) + 2 * (size_t)S + (size_t)(S / 2)) * 2 * sizeof(R);
 }
 template <typename R>
-__host__ __device__ constexpr size_t plane_inv_smem(int S, int NLY, int NLZ, bool grad) {
-  return plane_fwd_smem<R>(S, NLY, NLZ) + (grad ? (size_t)S * S * sizeof(R) : 0);
+__host__ __device__ constexpr size_t plane_inv_smem(int S, int NLY, int NLZ, bool acc) {
+  return plane_fwd_smem<R>(S, NLY, NLZ) + (acc ? (size_t)S * S * sizeof(R) : 0);
 }
 
 // y transforms of columns 0 .. s/2 - 1 of the plane [y][kz], NLY at a time,
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
   C* tw_s = B + TILE;
   C* tw_n = tw_s + S;
   C* tw_m = tw_n + S;
-  R* acc = reinterpret_cast<R*>(tw_m + M);  // [y][z] (EPI_GRAD)
+  R* acc = reinterpret_cast<R*>(tw_m + M);  // [y][z] (EPI_GRAD); the epilogue tile (Coulomb epilogues)
   __shared__ unsigned long long bar;
   __shared__ double s_f0[kPlaneThreads / 32];
   const int xi = blockIdx.x;
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
         const C O = cmul(cconj(tw_n[q]), D);       // 2 O_q
         return C{E.x - O.y, E.y + O.x};            // 2 (E_q + i O_q)
       };
-      auto store = [&](int m, int l, C z) {
+      auto emit = [&](int m, int l, C z) {
         const int y = y0 + l;
         const R x0 = z.x * R(a.scale), x1 = z.y * R(a.scale);
         const long p0 = ((long)xi * S + y) * S + 2 * m;
@@ -344,7 +344,18 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(ZArgs<R> a) {
           *reinterpret_cast<C*>(a.rout[0] + p0) = C{x0, x1};
         }
       };
-      fft_lines<C, M, NLZ, true>(A, B, tw_m, +1, load, store);
+      if constexpr (coul) {
+        // the Coulomb epilogues run once per point pair after the transform
+        // (from the tile T [l][m], in acc), not inlined at every radix
+        // output of its last stage
+        C* T = reinterpret_cast<C*>(acc);
+        auto store = [&](int m, int l, C z) { T[l * M + m] = z; };
+        fft_lines<C, M, NLZ, true>(A, B, tw_m, +1, load, store);
+        for (int w = threadIdx.x; w < NLZ * M; w += blockDim.x) emit(w % M, w / M, T[w]);
+        __syncthreads();
+      } else {
+        fft_lines<C, M, NLZ, true>(A, B, tw_m, +1, load, emit);
+      }
     }
     // every read of `plane` is done before the next transfer overwrites it
     fence_proxy_async_smem();
