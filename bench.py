@@ -78,13 +78,17 @@ def measured_peaks():
 
 
 def traffic_from_profiles(stage):
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    """DRAM bytes per launch of `stage` from profiles/traffic.txt (lines
+    "kernel bytes"; # comments), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    v = d.get(stage)
-    return None if v is None else float(v)
+        for line in f:
+            parts = line.split("#", 1)[0].split()
+            if len(parts) == 2 and parts[0] == stage:
+                return float(parts[1])
+    return None
 
 
 class ClockSampler:
