@@ -376,11 +376,17 @@ int mpdpft_step_phase_times(mpdpft_ctx* ctx, double* us, int n);
 
 /* FFT path of the context (no counterpart in the reference, which plans
  * FFTW once, mpDPFT.cpp:6313-6335): *path 1 = x-plane kernels, 0 = one pass
- * per axis; the autotuner's timings of one iteration's transforms both ways
- * (ms; 0 when not measured); *how 0 = one path only, 1 = measured by this
- * context, 2 = taken from an earlier context of the same kind, 3 = forced by
- * MPDPFT_FFT_PATH. */
+ * per axis; the autotuner's best timings of one iteration's transforms on
+ * each path over the tile widths it tried (ms; 0 when not measured); *how
+ * 0 = nothing to choose, 1 = measured by this context, 2 = taken from an
+ * earlier context of the same kind, 3 = path forced by MPDPFT_FFT_PATH. */
 int mpdpft_fft_config(mpdpft_ctx* ctx, int* path, double* ms_plane, double* ms_pass, int* how);
+
+/* Tile widths the autotuner chose (3D grids): lines per tile of the Y and X
+ * passes (FP32 16 or 8, FP64 8 or 4; fewer where s/2 is not a multiple)
+ * and rows per block of the Z passes (16 or 8).  Results do not depend on
+ * them; MPDPFT_FFT_TILES=<lines>,<rows> forces them. */
+int mpdpft_fft_tiles(mpdpft_ctx* ctx, int* axis_lines, int* z_rows);
 
 /* Adjoint of the converged SC fixed point (no counterpart in the reference,
  * whose optimisation drivers take finite differences of whole solves,

@@ -280,6 +280,11 @@ int mpdpft_fft_config(mpdpft_ctx* ctx, int* path, double* ms_plane, double* ms_p
   return ctx->impl.fft_config(path, ms_plane, ms_pass, how);
 }
 
+int mpdpft_fft_tiles(mpdpft_ctx* ctx, int* axis_lines, int* z_rows) {
+  CHECK_CTX(ctx);
+  return ctx->impl.fft_tiles(axis_lines, z_rows);
+}
+
 int mpdpft_adjoint(mpdpft_ctx* ctx, const double* dl_dn, double* dl_dvext, int layout, int mem, double tol,
                    int max_iter, int* iterations, double* residual) {
   CHECK_CTX(ctx);

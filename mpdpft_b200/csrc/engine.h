@@ -148,6 +148,7 @@ struct Ctx {
   int fft_setup();
   int fft_autotune();  // plane or pass path for 3D transforms (timed, cached per kind)
   int fft_config(int* path, double* ms_plane, double* ms_pass, int* how);
+  int fft_tiles(int* axis_lines, int* z_rows);
   void fft_release();
   int issue_fft_terms();                      // Coulomb terms + V assembly + DelField(V)
   int issue_coulomb(const void* dens, void* out, int for_energy);

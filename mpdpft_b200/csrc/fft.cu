@@ -18,6 +18,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <array>
+#include <cstdio>
 #include <map>
 #include <mutex>
 #include <set>
@@ -1137,7 +1139,8 @@ int Ctx::fft_setup() {
   for (int i = 0; i < nspec_buf; ++i)
     if ((st = alloc(&f.spec[i], csz * f.nspec))) return st;
   if ((st = alloc(&f.rtmp, rsize * geom.n))) return st;
-  if ((st = alloc((void**)&f.zpart, sizeof(double) * (f.zblocks + 1)))) return st;
+  // (room for the autotuner's narrower z tiles: 8 rows per block)
+  if ((st = alloc((void**)&f.zpart, sizeof(double) * ((f.rows + 7) / 8 + 1)))) return st;
   if ((st = alloc((void**)&f.vmax, sizeof(unsigned long long)))) return st;
   f.vblocks = grid_blocks(geom.n);
   if ((st = alloc((void**)&f.vres_part, sizeof(double) * f.vblocks * kMaxS))) return st;
@@ -1221,7 +1224,8 @@ static int launch_z_r2c(Ctx& c, const R* in, int pro, int nsrc, const double* qc
   const size_t smem = r2c_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_R2C]++;
   c.note("k_z_r2c", nsrc * c.field_bytes() + c.spec_bytes());
-  if (f.zl != 16 || !launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
+  if (!(f.zl == 16 ? launch_z_r2c_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a)
+                   : f.zl == 8 && launch_z_r2c_ct<R, 8>(f.M, f.zblocks, smem, c.stream, a)))
     launch_k(k_z_r2c<R, 0, 0>, dim3(f.zblocks), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1257,7 +1261,8 @@ static int launch_z_c2r(Ctx& c, void* const* in, int nin, int epi, R* out0, R* o
   const size_t smem = c2r_smem<R>(f);
   c.cnt[MPDPFT_STAGE_FFT_Z_C2R]++;
   c.note("k_z_c2r", nin * c.spec_bytes() + ((out0 ? 1 : 0) + (out1 ? 1 : 0)) * c.field_bytes());
-  if (f.zl != 16 || !launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a))
+  if (!(f.zl == 16 ? launch_z_c2r_ct<R, 16>(f.M, f.zblocks, smem, c.stream, a)
+                   : f.zl == 8 && launch_z_c2r_ct<R, 8>(f.M, f.zblocks, smem, c.stream, a)))
     launch_k(k_z_c2r<R, 0, 0>, dim3(f.zblocks), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1307,7 +1312,9 @@ static int launch_y(Ctx& c, void* const* data, int nfield, int dir) {
   const size_t smem = (2 * (size_t)f.s * (f.tk + 1) + f.s) * sizeof(typename Cx<R>::T);
   c.cnt[MPDPFT_STAGE_FFT_Y]++;
   c.note("k_axis_c2c", 2.0 * nfield * c.spec_bytes());
-  if (f.tk != ct_width<R>() || !launch_axis_ct<R, ct_width<R>()>(f.s, grid, smem, c.stream, a))
+  constexpr int W = ct_width<R>();
+  if (!(f.tk == W ? launch_axis_ct<R, W>(f.s, grid, smem, c.stream, a)
+                  : f.tk == W / 2 && launch_axis_ct<R, W / 2>(f.s, grid, smem, c.stream, a)))
     launch_k(k_axis_c2c<R, 0, 0>, dim3(grid), dim3(kFftThreads), smem, c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1349,13 +1356,24 @@ static bool x_ct_fits(const FftPlan& f) {
   return x_smem_ct<R>(f) + sizeof(MulTables<R, 512, 16>) <= 227 * 1024;
 }
 
+// The compile-time x round trip for the plan's tile width (the width of
+// ct_width or half of it); false: the runtime kernel runs instead.
+template <typename R>
+static bool launch_x_tiles(const FftPlan& f, unsigned grid, cudaStream_t st, const AxisArgs<R>& a) {
+  constexpr int W = ct_width<R>();
+  if (!x_ct_fits<R>(f)) return false;
+  if (f.tk == W) return launch_x_ct<R, W>(f.s, grid, x_smem_ct<R>(f), st, a);
+  if (f.tk == W / 2) return launch_x_ct<R, W / 2>(f.s, grid, x_smem_ct<R>(f), st, a);
+  return false;
+}
+
 template <typename R>
 static int launch_x_args(Ctx& c, const AxisArgs<R>& a) {
   FftPlan& f = *c.fft;
   const unsigned grid = x_grid<R>(a);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
   c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
-  if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
+  if (!launch_x_tiles<R>(f, grid, c.stream, a))
     launch_k(k_x_roundtrip<R, 0, 0>, dim3(grid), dim3(kFftThreads), x_smem_rt<R>(f), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -1368,7 +1386,7 @@ static int launch_x(Ctx& c, void* in, void* const* out, int nout, int mul, doubl
   const unsigned grid = x_grid<R>(a);
   c.cnt[MPDPFT_STAGE_FFT_X]++;
   c.note("k_x_roundtrip", (1.0 + a.nout) * c.spec_bytes());
-  if (f.tk != ct_width<R>() || !x_ct_fits<R>(f) || !launch_x_ct<R, ct_width<R>()>(f.s, grid, x_smem_ct<R>(f), c.stream, a))
+  if (!launch_x_tiles<R>(f, grid, c.stream, a))
     launch_k(k_x_roundtrip<R, 0, 0>, dim3(grid), dim3(kFftThreads), x_smem_rt<R>(f), c.stream, a);
   CU(cudaGetLastError());
   return MPDPFT_OK;
@@ -2337,6 +2355,11 @@ int Ctx::coulomb_field(const void* in, void* out) {
 // transforms of one SC iteration (DelField of every species and the Coulomb
 // terms) both ways on its own buffers and keeps the faster; later contexts
 // of the same kind reuse the choice.  MPDPFT_FFT_PATH=plane|pass forces a path.
+// Every 3D grid also tunes the tile widths: lines per tile of the Y and X
+// passes (16 or 8 in FP32, 8 or 4 in FP64) and rows per block of the Z
+// passes (16 or 8, pass path); each width has compile-time kernels, and a
+// line's arithmetic does not depend on the width, so every configuration
+// gives the same bits.  MPDPFT_FFT_TILES=<lines>,<rows> forces the widths.
 template <typename R>
 static int tune_transforms(Ctx& c) {
   int st;
@@ -2359,34 +2382,71 @@ static int tune_transforms(Ctx& c) {
 int Ctx::fft_autotune() {
   FftPlan& F = *fft;
   F.tuned = 0;
-  if (F.dim != 3 || !F.plane || !(gradient || has_coulomb)) return MPDPFT_OK;  // one path only
+  if (F.dim != 3 || !(gradient || has_coulomb)) return MPDPFT_OK;  // no transforms in the iteration
+  // candidate configurations: path (plane where instantiated, pass) x tile
+  // width of the Y/X passes (tk0, tk0/2) x rows per block of the Z passes
+  // (16, 8; pass path only)
+  struct Cfg { bool plane; int tk, zl; };
+  const int tk0 = F.tk;
+  Cfg cfg[6];
+  int ncfg = 0;
   const char* env = std::getenv("MPDPFT_FFT_PATH");
-  if (env && (!std::strcmp(env, "pass") || !std::strcmp(env, "plane"))) {
-    F.plane = !std::strcmp(env, "plane");
-    F.tuned = 3;
-    return MPDPFT_OK;
+  const bool forced = env && (!std::strcmp(env, "pass") || !std::strcmp(env, "plane"));
+  for (int path = 0; path < 2; ++path) {
+    const bool plane = path == 0;
+    if (plane && !F.plane) continue;
+    if (forced && plane != !std::strcmp(env, "plane")) continue;
+    for (int t = 0; t < 2; ++t) {
+      const int tk = t ? tk0 / 2 : tk0;
+      if (tk < 4 && t) continue;
+      for (int z = 0; z < (plane ? 1 : 2); ++z) cfg[ncfg++] = Cfg{plane, tk, z ? 8 : 16};
+    }
   }
-  using Key = std::tuple<int, size_t, int, int, int>;
+  // MPDPFT_FFT_TILES=<tk>,<zl> keeps only that tile configuration
+  const char* tiles = std::getenv("MPDPFT_FFT_TILES");
+  int want_tk = 0, want_zl = 0;
+  if (tiles && std::sscanf(tiles, "%d,%d", &want_tk, &want_zl) == 2) {
+    int k = 0;
+    for (int i = 0; i < ncfg; ++i)
+      if (cfg[i].tk == want_tk && (cfg[i].plane || cfg[i].zl == want_zl)) cfg[k++] = cfg[i];
+    ncfg = k;
+    if (ncfg == 0) return set_error(MPDPFT_ERR_ARG, "MPDPFT_FFT_TILES: no such configuration for this grid");
+  }
+  auto apply = [&](const Cfg& c) {
+    F.plane = c.plane;
+    F.tk = c.tk;
+    F.zl = c.zl;
+    F.zblocks = (int)((F.rows + F.zl - 1) / F.zl);
+  };
+  using Key = std::tuple<int, size_t, int, int, int, int, int>;
   static std::mutex mu;
-  static std::map<Key, std::pair<double, double>> cache;
-  const Key key{F.s, rsize, gradient ? 1 : 0, has_coulomb, S};
+  static std::map<Key, std::array<double, 5>> cache;  // plane ms, pass ms, plane, tk, zl
+  const Key key{F.s, rsize, gradient ? 1 : 0, has_coulomb, S, forced ? 1 + (env[1] == 'l') : 0, want_tk * 64 + want_zl};
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) {
-      F.tune_ms[0] = it->second.first;
-      F.tune_ms[1] = it->second.second;
-      F.plane = F.tune_ms[0] <= F.tune_ms[1];
-      F.tuned = 2;
+      F.tune_ms[0] = it->second[0];
+      F.tune_ms[1] = it->second[1];
+      apply(Cfg{it->second[2] != 0.0, (int)it->second[3], (int)it->second[4]});
+      F.tuned = forced ? 3 : 2;
       return MPDPFT_OK;
     }
+  }
+  if (ncfg == 1) {  // nothing to choose
+    apply(cfg[0]);
+    F.tuned = forced ? 3 : 0;
+    return MPDPFT_OK;
   }
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   int st = MPDPFT_OK;
-  for (int path = 0; path < 2 && !st; ++path) {
-    F.plane = path == 0;
+  double best = 1e300;
+  int ibest = 0;
+  F.tune_ms[0] = F.tune_ms[1] = 0.0;
+  for (int i = 0; i < ncfg && !st; ++i) {
+    apply(cfg[i]);
     for (int rep = 0; rep < 2 && !st; ++rep)  // warm-up
       st = rsize == sizeof(double) ? tune_transforms<double>(*this) : tune_transforms<float>(*this);
     if (st) break;
@@ -2398,16 +2458,26 @@ int Ctx::fft_autotune() {
     if (cudaEventSynchronize(e1) != cudaSuccess) st = set_error(MPDPFT_ERR_CUDA, "autotuner timing");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    F.tune_ms[path] = ms / reps;
+    const double t = ms / reps;
+    double& slot = F.tune_ms[cfg[i].plane ? 0 : 1];
+    if (slot == 0.0 || t < slot) slot = t;
+    if (t < best) { best = t; ibest = i; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int i = 0; i < 6; ++i) cnt[i] = 0;
   if (st) return st;
-  F.plane = F.tune_ms[0] <= F.tune_ms[1];
-  F.tuned = 1;
+  apply(cfg[ibest]);
+  F.tuned = forced ? 3 : 1;
   std::lock_guard<std::mutex> lock(mu);
-  cache[key] = {F.tune_ms[0], F.tune_ms[1]};
+  cache[key] = {F.tune_ms[0], F.tune_ms[1], F.plane ? 1.0 : 0.0, (double)F.tk, (double)F.zl};
+  return MPDPFT_OK;
+}
+
+int Ctx::fft_tiles(int* axis_lines, int* z_rows) {
+  if (!fft) return set_error(MPDPFT_ERR_ARG, "no FFT plan");
+  if (axis_lines) *axis_lines = fft->tk;
+  if (z_rows) *z_rows = fft->zl;
   return MPDPFT_OK;
 }
 

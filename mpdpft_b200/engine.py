@@ -31,7 +31,7 @@ EXPORTS = [
     "mpdpft_energy", "mpdpft_profile_stage", "mpdpft_iteration_launches", "mpdpft_step_phase_times",
     "mpdpft_batch_create", "mpdpft_batch_destroy", "mpdpft_batch_set_external_potential", "mpdpft_batch_sc_init",
     "mpdpft_batch_sc_step", "mpdpft_batch_sc_run", "mpdpft_batch_get_field", "mpdpft_batch_get_log",
-    "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei", "mpdpft_fft_config",
+    "mpdpft_batch_sync", "mpdpft_adjoint", "mpdpft_adjoint_nuclei", "mpdpft_fft_config", "mpdpft_fft_tiles",
     "mpdpft_set_limits", "mpdpft_integrate_noalloc", "mpdpft_iteration_profile",
     "mpdpft_read_input", "mpdpft_params_from_input", "mpdpft_write_field_files", "mpdpft_interpolate_v_file",
 ]
@@ -104,6 +104,7 @@ def load(path=LIB_PATH):
     L.mpdpft_batch_get_log.argtypes = [vp, C.c_int, C.POINTER(abi.IterLog), C.c_int, C.POINTER(C.c_int)]
     L.mpdpft_batch_sync.argtypes = [vp]
     L.mpdpft_fft_config.argtypes = [vp, C.POINTER(C.c_int), _dp, _dp, C.POINTER(C.c_int)]
+    L.mpdpft_fft_tiles.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.mpdpft_adjoint.argtypes = [vp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), _dp]
     L.mpdpft_adjoint_nuclei.argtypes = [vp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_double, _dp]
     for name in EXPORTS:
@@ -372,6 +373,13 @@ class Engine:
         a, b = C.c_double(), C.c_double()
         self._check(self.lib.mpdpft_fft_config(self.h, C.byref(path), C.byref(a), C.byref(b), C.byref(how)))
         return path.value, a.value, b.value, how.value
+
+    def fft_tiles(self):
+        """(lines per tile of the Y/X passes, rows per block of the Z passes)
+        the FFT autotuner chose."""
+        t, z = C.c_int(), C.c_int()
+        self._check(self.lib.mpdpft_fft_tiles(self.h, C.byref(t), C.byref(z)))
+        return t.value, z.value
 
     def adjoint(self, dl_dn, tol=1e-10, max_iter=300, check=True):
         """dL/dV_ext of the converged solve for dL/dn (periodic layout):
