@@ -220,7 +220,9 @@ int mpdpft_sc_run(mpdpft_ctx* ctx, const double* const* v0, int layout, int mem,
   // result->seconds: the whole solve, the initial densities (sc_init: V_0
   // import, DelField, the first mu search) included
   const auto t0 = std::chrono::steady_clock::now();
-  int st = ctx->impl.sc_init(v0, layout, mem);
+  // (the loop reads the state after the initial densities itself: a device
+  // abort there ends the loop before its first iteration and is reported)
+  int st = ctx->impl.sc_init(v0, layout, mem, /*check=*/false);
   if (st) return st;
   st = ctx->impl.sc_run(result, log, log_cap, /*use_graph=*/1);
   if (result) result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

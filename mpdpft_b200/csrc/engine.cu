@@ -736,7 +736,7 @@ int Ctx::status_from_state(const ScState& h) {
   return MPDPFT_OK;
 }
 
-int Ctx::sc_init(const double* const* v0, int layout, int mem) {
+int Ctx::sc_init(const double* const* v0, int layout, int mem, bool check) {
   int st;
   if ((st = reset_state())) return st;
   for (int s = 0; s < S; ++s) {
@@ -766,12 +766,11 @@ int Ctx::sc_init(const double* const* v0, int layout, int mem) {
     if ((st = issue_delfield_of_V())) return st;
   }
   if ((st = launch_step(1))) return st;  // initial densities (mpDPFT.cpp:195)
-  CU(cudaStreamSynchronize(stream));
-  ScState h;
-  if ((st = read_state(&h))) return st;
-  if ((st = status_from_state(h))) return st;
   initialised = true;
-  return MPDPFT_OK;
+  if (!check) return MPDPFT_OK;
+  ScState h;
+  if ((st = read_state(&h))) return st;  // (synchronises the stream)
+  return status_from_state(h);
 }
 
 void Ctx::drop_graphs() {

@@ -123,7 +123,9 @@ struct Ctx {
   StepArgs<R> step_args(int mode);
   int launch_step(int mode, int parts = 7);  // parts: 1 mu, 2 density, 4 mixing kernel
   int issue_iteration();
-  int sc_init(const double* const* v0, int layout, int mem);
+  // check: wait for the initial densities and report a device abort now
+  // (false when the SC loop follows at once and reads the state itself)
+  int sc_init(const double* const* v0, int layout, int mem, bool check = true);
   int sc_step(int use_graph);
   void drop_graphs();
   void check_graphs();  // drop captured graphs whose kernel parameters changed
