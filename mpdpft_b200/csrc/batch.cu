@@ -420,7 +420,7 @@ int Batch::sc_init(const double* const* v0, int layout, int mem) {
           Ctx& c = *members[i];
           const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? c.n_ref : c.geom.n;
           for (int s = 0; s < S; ++s)
-            if (v0[(size_t)i * S + s]) std::memcpy(c.host_stage(s), v0[(size_t)i * S + s], sizeof(double) * cnt);
+            if (v0[(size_t)i * S + s]) copy_to_pinned(c.host_stage(s), v0[(size_t)i * S + s], cnt);
         }
       });
     for (std::thread& th : pool) th.join();

@@ -8,9 +8,16 @@
 // stream; the SC iteration is one persistent kernel (plus the FFT kernels for
 // Coulomb and gradient terms) and is replayed as a CUDA graph.
 #include <cuda_runtime.h>
+#if defined(__x86_64__) && defined(__SSE2__)
+#include <immintrin.h>
+#endif
+#include <cstdint>
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -257,6 +264,9 @@ void Ctx::release() {
   for (void* p : allocations) cudaFree(p);
   allocations.clear();
   if (pinned) { cudaFreeHost(pinned); pinned = nullptr; }
+  for (cudaEvent_t e : copy_events) cudaEventDestroy(e);
+  copy_events.clear();
+  copy_pool.reset();
   if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
 }
 
@@ -513,39 +523,150 @@ int Ctx::read_state(ScState* h) {
 // caller synchronises the stream before that half is used again.
 double* Ctx::host_stage(int slot) { return (double*)pinned + (slot ? std::max(n_ref, geom.n) : 0); }
 
-// Host copy of a large grid by several threads (one thread copies well
-// under the bandwidth of the host's memory).
-static void par_memcpy(void* dst, const void* src, size_t bytes) {
-  const size_t min_part = (size_t)1 << 20;
-  size_t nt = std::min<size_t>(8, std::max<size_t>(1, std::thread::hardware_concurrency()));
-  nt = std::min(nt, bytes / min_part);
-  if (nt <= 1) { std::memcpy(dst, src, bytes); return; }
-  const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
-  std::vector<std::thread> pool;
-  for (size_t t = 1; t < nt; ++t) {
-    const size_t b = t * part;
-    if (b >= bytes) break;
-    pool.emplace_back([=] { std::memcpy((char*)dst + b, (const char*)src + b, std::min(part, bytes - b)); });
+// Grids between a caller's host array and the device in kCopyChunk pieces,
+// pipelined over the context's host copy threads (CopyPool, started once):
+// on import the workers copy chunks into the pinned buffer and the calling
+// thread queues each chunk's DMA as soon as it is copied (in chunk order);
+// on export the calling thread queues every chunk's DMA with an event after
+// it, waits for the events in order and releases each chunk to the workers,
+// which copy it out.  Only the calling thread makes CUDA calls.
+constexpr long kCopyChunk = 1L << 16;  // doubles (512 KB)
+
+// n doubles into pinned staging memory with non-temporal stores where the
+// host has them (x86-64): cached stores leave the staged grid dirty in the
+// host's caches, and the DMA that reads it next then ran at a fifth of the
+// speed it has from memory (measured on the B200 host: 16.8 MB in 1.5 ms vs
+// 0.3 ms).
+void copy_to_pinned(double* dst, const double* src, long n) {
+#if defined(__x86_64__) && defined(__SSE2__)
+  if (((uintptr_t)dst & 15) == 0) {
+    long i = 0;
+    for (; i + 2 <= n; i += 2) _mm_stream_si128((__m128i*)(dst + i), _mm_loadu_si128((const __m128i*)(src + i)));
+    for (; i < n; ++i) dst[i] = src[i];
+    _mm_sfence();
+    return;
   }
-  std::memcpy(dst, src, std::min(part, bytes));
-  for (std::thread& th : pool) th.join();
+#endif
+  std::memcpy(dst, src, sizeof(double) * n);
+}
+
+CopyPool::CopyPool() {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = std::max(1, std::min(8, hw - 1));
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([this, t] {
+      unsigned seen = 0;
+      for (;;) {
+        std::function<void(int)> f;
+        {
+          std::unique_lock<std::mutex> l(m);
+          cv.wait(l, [&] { return stop || gen != seen; });
+          if (stop) return;
+          seen = gen;
+          f = job;
+        }
+        f(t);
+        std::lock_guard<std::mutex> l(m);
+        if (--pending == 0) done.notify_all();
+      }
+    });
+}
+
+CopyPool::~CopyPool() {
+  {
+    std::lock_guard<std::mutex> l(m);
+    stop = true;
+  }
+  cv.notify_all();
+  for (std::thread& x : th) x.join();
+}
+
+void CopyPool::begin(std::function<void(int)> f) {
+  {
+    std::lock_guard<std::mutex> l(m);
+    job = std::move(f);
+    pending = nt;
+    ++gen;
+  }
+  cv.notify_all();
+}
+
+void CopyPool::wait() {
+  std::unique_lock<std::mutex> l(m);
+  done.wait(l, [&] { return pending == 0; });
+}
+
+int Ctx::host_to_device(double* dstage, double* hs, const double* src, long cnt) {
+  const long nchunk = (cnt + kCopyChunk - 1) / kCopyChunk;
+  if (!copy_pool) copy_pool.reset(new CopyPool());
+  CopyPool& P = *copy_pool;
+  std::vector<std::atomic<int>> ready(nchunk);
+  for (auto& r : ready) r.store(0);
+  const int nt = P.nt;
+  P.begin([&](int t) {
+    for (long k = t; k < nchunk; k += nt) {
+      const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
+      copy_to_pinned(hs + off, src + off, len);
+      ready[k].store(1, std::memory_order_release);
+    }
+  });
+  int st = MPDPFT_OK;
+  for (long k = 0; k < nchunk; ++k) {
+    while (!ready[k].load(std::memory_order_acquire)) std::this_thread::yield();
+    const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
+    if (!st && cudaMemcpyAsync(dstage + off, hs + off, sizeof(double) * len, cudaMemcpyHostToDevice, stream) !=
+                   cudaSuccess)
+      st = set_error(MPDPFT_ERR_CUDA, "host to device copy");
+  }
+  P.wait();
+  return st;
+}
+
+int Ctx::device_to_host(double* dst, double* hs, const double* dsrc, long cnt) {
+  const long nchunk = (cnt + kCopyChunk - 1) / kCopyChunk;
+  while ((long)copy_events.size() < nchunk) {
+    cudaEvent_t e;
+    CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    copy_events.push_back(e);
+  }
+  for (long k = 0; k < nchunk; ++k) {
+    const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
+    CU(cudaMemcpyAsync(hs + off, dsrc + off, sizeof(double) * len, cudaMemcpyDeviceToHost, stream));
+    CU(cudaEventRecord(copy_events[k], stream));
+  }
+  if (!copy_pool) copy_pool.reset(new CopyPool());
+  CopyPool& P = *copy_pool;
+  std::vector<std::atomic<int>> ready(nchunk);  // 1: copied to the host, 2: failed
+  for (auto& r : ready) r.store(0);
+  const int nt = P.nt;
+  P.begin([&](int t) {
+    for (long k = t; k < nchunk; k += nt) {
+      int r;
+      while (!(r = ready[k].load(std::memory_order_acquire))) std::this_thread::yield();
+      if (r != 1) continue;
+      const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
+      std::memcpy(dst + off, hs + off, sizeof(double) * len);
+    }
+  });
+  int st = MPDPFT_OK;
+  for (long k = 0; k < nchunk; ++k) {
+    const bool ok = !st && cudaEventSynchronize(copy_events[k]) == cudaSuccess;
+    if (!ok && !st) st = set_error(MPDPFT_ERR_CUDA, "device to host copy");
+    ready[k].store(ok ? 1 : 2, std::memory_order_release);
+  }
+  P.wait();
+  return st;
 }
 
 int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slot, bool sync) {
   if (!src) return set_error(MPDPFT_ERR_ARG, "null input array");
   if (mem != MPDPFT_MEM_HOST) return import_staged(src, dst, layout, slot, sync);
-  // host grids cross in 4 MB chunks: the host copies chunk k into the pinned
-  // buffer while the DMA of chunk k - 1 runs
+  // host grids cross in chunks, copied and sent by several host threads
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
-  double* hs = host_stage(slot);
   double* dstage = d_io + (slot ? std::max(n_ref, geom.n) : 0);  // d_io holds two grids
-  const long chunk = 1L << 19;
-  for (long off = 0; off < cnt; off += chunk) {
-    const long len = std::min(chunk, cnt - off);
-    par_memcpy(hs + off, src + off, sizeof(double) * len);
-    CU(cudaMemcpyAsync(dstage + off, hs + off, sizeof(double) * len, cudaMemcpyHostToDevice, stream));
-  }
-  int st = import_staged(dstage, dst, layout, slot, false);
+  int st = host_to_device(dstage, host_stage(slot), src, cnt);
+  if (st) return st;
+  st = import_staged(dstage, dst, layout, slot, false);
   if (st) return st;
   if (sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
   return MPDPFT_OK;
@@ -603,11 +724,7 @@ int Ctx::export_field(const void* src, double* dst, int layout, int mem) {
   if (rsize == sizeof(double)) k_export<double><<<blocks, kThreads, 0, stream>>>((const double*)src, ddst, geom, layout);
   else k_export<float><<<blocks, kThreads, 0, stream>>>((const float*)src, ddst, geom, layout);
   CU(cudaGetLastError());
-  if (mem == MPDPFT_MEM_HOST) {
-    CU(cudaMemcpyAsync(pinned, d_io, sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream));
-    CU(cudaStreamSynchronize(stream));
-    par_memcpy(dst, pinned, sizeof(double) * cnt);
-  }
+  if (mem == MPDPFT_MEM_HOST) return device_to_host(dst, (double*)pinned, d_io, cnt);
   return MPDPFT_OK;
 }
 

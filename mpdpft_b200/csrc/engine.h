@@ -2,7 +2,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mpdpft_gpu.h"
@@ -16,6 +21,29 @@ extern thread_local std::string g_last_error;
 
 struct FftPlan;  // fft.cu
 struct Adjoint;  // adjoint.cu
+
+// n doubles from a caller's array into pinned staging memory (engine.cu).
+void copy_to_pinned(double* dst, const double* src, long n);
+
+// Host threads for the copies between callers' host arrays and the pinned
+// staging buffer (engine.cu): begin() hands every worker t the job f(t)
+// and returns; wait() returns when all have finished it.
+struct CopyPool {
+  int nt = 1;
+  CopyPool();
+  ~CopyPool();
+  void begin(std::function<void(int)> f);
+  void wait();
+
+ private:
+  std::vector<std::thread> th;
+  std::mutex m;
+  std::condition_variable cv, done;
+  std::function<void(int)> job;
+  unsigned gen = 0;
+  int pending = 0;
+  bool stop = false;
+};
 
 // kinds of Ctx::spectral
 enum { SPEC_DERIV = 0, SPEC_SMOOTH = 1, SPEC_COULOMB = 2 };
@@ -75,6 +103,8 @@ struct Ctx {
   const double* vres_part_ext = nullptr;
   int vres_blocks_ext = 0;
   void* pinned = nullptr;
+  std::vector<cudaEvent_t> copy_events;  // per-chunk events of device_to_host
+  std::unique_ptr<CopyPool> copy_pool;    // host copy threads, started at the first host copy
   size_t pinned_bytes = 0;
   std::vector<void*> allocations;
   cudaGraph_t graph = nullptr;          // one SC iteration (mpdpft_sc_step)
@@ -151,6 +181,10 @@ struct Ctx {
   int fft_autotune();  // plane or pass path for 3D transforms (timed, cached per kind)
   int fft_config(int* path, double* ms_plane, double* ms_pass, int* how);
   int fft_tiles(int* axis_lines, int* z_rows);
+  // cnt doubles between a host array and device memory through the pinned
+  // buffer hs, pipelined over several host threads
+  int host_to_device(double* dstage, double* hs, const double* src, long cnt);
+  int device_to_host(double* dst, double* hs, const double* dsrc, long cnt);
   void fft_release();
   int issue_fft_terms();                      // Coulomb terms + V assembly + DelField(V)
   int issue_coulomb(const void* dens, void* out, int for_energy);

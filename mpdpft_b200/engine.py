@@ -311,8 +311,13 @@ class Engine:
     def stream(self):
         return self.lib.mpdpft_ctx_stream(self.h)
 
-    def field(self, which, s, layout=abi.LAYOUT_PERIODIC):
-        out = np.empty(self._count(layout))
+    def field(self, which, s, layout=abi.LAYOUT_PERIODIC, out=None):
+        """One field of the current state as float64 (into `out`, a
+        contiguous float64 array of the grid's size, when given)."""
+        if out is None:
+            out = np.empty(self._count(layout))
+        elif out.dtype != np.float64 or out.size != self._count(layout) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array of the grid's size")
         self._check(self.lib.mpdpft_get_field(self.h, which, s, _ptr(out), layout, abi.MEM_HOST))
         return out
 
