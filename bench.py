@@ -418,6 +418,10 @@ def time_to_converge(sg, device):
         torch.cuda.synchronize(device)
         with engine.Engine(p, device=device) as e:
             e.sc_run(vext, v0)  # warm-up solve (graph instantiation, clocks)
+            path, ms_plane, ms_pass, how = e.fft_config()
+            tiles = e.fft_tiles()
+            out["fft_%s" % name] = {"path": "plane" if path else "pass", "ms_plane": ms_plane, "ms_pass": ms_pass,
+                                    "axis_lines": tiles[0], "z_rows": tiles[1]}
             best_host = None
             for _ in range(3):
                 res, log, st = e.sc_run(None, v0)
