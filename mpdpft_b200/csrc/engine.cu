@@ -52,8 +52,8 @@ int set_error(int status, const std::string& msg) {
   } while (0)
 
 // ------------------------------------------------------------- kernels ----
-template <typename R>
-__global__ void k_import(const double* __restrict__ src, R* __restrict__ dst, Geom g, int layout) {
+template <typename R, typename S = double>
+__global__ void k_import(const S* __restrict__ src, R* __restrict__ dst, Geom g, int layout) {
   const long n = g.n;
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     long q = p;
@@ -72,8 +72,8 @@ __global__ void k_import(const double* __restrict__ src, R* __restrict__ dst, Ge
   }
 }
 
-template <typename R>
-__global__ void k_export(const R* __restrict__ src, double* __restrict__ dst, Geom g, int layout) {
+template <typename R, typename D = double>
+__global__ void k_export(const R* __restrict__ src, D* __restrict__ dst, Geom g, int layout) {
   long total = g.n;
   const long el = g.s + 1;
   if (layout == MPDPFT_LAYOUT_REFERENCE) total = (g.dim == 3) ? el * el * el : el * el;
@@ -89,7 +89,7 @@ __global__ void k_export(const R* __restrict__ src, double* __restrict__ dst, Ge
         p = (t % g.s) * g.s + k;
       }
     }
-    dst[q] = (double)src[p];
+    dst[q] = (D)src[p];
   }
 }
 
@@ -479,7 +479,8 @@ int Ctx::init(const mpdpft_params& params, int dev) {
   }
   part_vals = std::max(kNPart, kNEnergy);
   if ((st = alloc((void**)&d_part, sizeof(double) * (size_t)std::max(step_blocks, kMaxBlocks) * part_vals))) return st;
-  pinned_bytes = sizeof(double) * (size_t)std::max(n_ref, geom.n) * 2;
+  // two halves, the second starting on a 16-byte boundary (streaming stores)
+  pinned_bytes = sizeof(double) * (size_t)((std::max(n_ref, geom.n) + 1) & ~1L) * 2;
   CU(cudaMallocHost(&pinned, pinned_bytes));
   CU(cudaMemsetAsync(d_V, 0, field * S, stream));
   CU(cudaMemsetAsync(d_vext, 0, field * S, stream));
@@ -521,7 +522,7 @@ int Ctx::read_state(ScState* h) {
 // compute-precision device array dst.  Host data is staged through half
 // `slot` (0 or 1) of the pinned buffer and of d_io; with sync = false the
 // caller synchronises the stream before that half is used again.
-double* Ctx::host_stage(int slot) { return (double*)pinned + (slot ? std::max(n_ref, geom.n) : 0); }
+double* Ctx::host_stage(int slot) { return (double*)pinned + (slot ? ((std::max(n_ref, geom.n) + 1) & ~1L) : 0); }
 
 // Grids between a caller's host array and the device in kCopyChunk pieces,
 // pipelined over the context's host copy threads (CopyPool, started once):
@@ -548,6 +549,24 @@ void copy_to_pinned(double* dst, const double* src, long n) {
   }
 #endif
   std::memcpy(dst, src, sizeof(double) * n);
+}
+
+// n doubles rounded to float (round to nearest, as the device conversion)
+// into pinned staging memory, with non-temporal stores as copy_to_pinned.
+static void convert_to_pinned(float* dst, const double* src, long n) {
+#if defined(__x86_64__) && defined(__SSE2__)
+  if (((uintptr_t)dst & 15) == 0) {
+    long i = 0;
+    for (; i + 4 <= n; i += 4) {
+      const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(src + i)), hi = _mm_cvtpd_ps(_mm_loadu_pd(src + i + 2));
+      _mm_stream_ps(dst + i, _mm_movelh_ps(lo, hi));
+    }
+    for (; i < n; ++i) dst[i] = (float)src[i];
+    _mm_sfence();
+    return;
+  }
+#endif
+  for (long i = 0; i < n; ++i) dst[i] = (float)src[i];
 }
 
 CopyPool::CopyPool() {
@@ -596,17 +615,28 @@ void CopyPool::wait() {
   done.wait(l, [&] { return pending == 0; });
 }
 
-int Ctx::host_to_device(double* dstage, double* hs, const double* src, long cnt) {
+static void stage_chunk(double* dst, const double* src, long n) { copy_to_pinned(dst, src, n); }
+static void stage_chunk(float* dst, const double* src, long n) { convert_to_pinned(dst, src, n); }
+static void unstage_chunk(double* dst, const double* src, long n) { std::memcpy(dst, src, sizeof(double) * n); }
+static void unstage_chunk(double* dst, const float* src, long n) {
+  for (long i = 0; i < n; ++i) dst[i] = (double)src[i];
+}
+
+// cnt values of a caller's double array into device memory as T (double,
+// or float for FP32 fields: rounded on the host, half the bytes over the
+// link) through the pinned buffer hs.
+template <typename T>
+static int stage_in(Ctx& c, T* dstage, T* hs, const double* src, long cnt) {
   const long nchunk = (cnt + kCopyChunk - 1) / kCopyChunk;
-  if (!copy_pool) copy_pool.reset(new CopyPool());
-  CopyPool& P = *copy_pool;
+  if (!c.copy_pool) c.copy_pool.reset(new CopyPool());
+  CopyPool& P = *c.copy_pool;
   std::vector<std::atomic<int>> ready(nchunk);
   for (auto& r : ready) r.store(0);
   const int nt = P.nt;
   P.begin([&](int t) {
     for (long k = t; k < nchunk; k += nt) {
       const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
-      copy_to_pinned(hs + off, src + off, len);
+      stage_chunk(hs + off, src + off, len);
       ready[k].store(1, std::memory_order_release);
     }
   });
@@ -614,7 +644,7 @@ int Ctx::host_to_device(double* dstage, double* hs, const double* src, long cnt)
   for (long k = 0; k < nchunk; ++k) {
     while (!ready[k].load(std::memory_order_acquire)) std::this_thread::yield();
     const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
-    if (!st && cudaMemcpyAsync(dstage + off, hs + off, sizeof(double) * len, cudaMemcpyHostToDevice, stream) !=
+    if (!st && cudaMemcpyAsync(dstage + off, hs + off, sizeof(T) * len, cudaMemcpyHostToDevice, c.stream) !=
                    cudaSuccess)
       st = set_error(MPDPFT_ERR_CUDA, "host to device copy");
   }
@@ -622,20 +652,22 @@ int Ctx::host_to_device(double* dstage, double* hs, const double* src, long cnt)
   return st;
 }
 
-int Ctx::device_to_host(double* dst, double* hs, const double* dsrc, long cnt) {
+// cnt values of type T in device memory out to a caller's double array.
+template <typename T>
+static int stage_out(Ctx& c, double* dst, T* hs, const T* dsrc, long cnt) {
   const long nchunk = (cnt + kCopyChunk - 1) / kCopyChunk;
-  while ((long)copy_events.size() < nchunk) {
+  while ((long)c.copy_events.size() < nchunk) {
     cudaEvent_t e;
     CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    copy_events.push_back(e);
+    c.copy_events.push_back(e);
   }
   for (long k = 0; k < nchunk; ++k) {
     const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
-    CU(cudaMemcpyAsync(hs + off, dsrc + off, sizeof(double) * len, cudaMemcpyDeviceToHost, stream));
-    CU(cudaEventRecord(copy_events[k], stream));
+    CU(cudaMemcpyAsync(hs + off, dsrc + off, sizeof(T) * len, cudaMemcpyDeviceToHost, c.stream));
+    CU(cudaEventRecord(c.copy_events[k], c.stream));
   }
-  if (!copy_pool) copy_pool.reset(new CopyPool());
-  CopyPool& P = *copy_pool;
+  if (!c.copy_pool) c.copy_pool.reset(new CopyPool());
+  CopyPool& P = *c.copy_pool;
   std::vector<std::atomic<int>> ready(nchunk);  // 1: copied to the host, 2: failed
   for (auto& r : ready) r.store(0);
   const int nt = P.nt;
@@ -645,17 +677,25 @@ int Ctx::device_to_host(double* dst, double* hs, const double* dsrc, long cnt) {
       while (!(r = ready[k].load(std::memory_order_acquire))) std::this_thread::yield();
       if (r != 1) continue;
       const long off = k * kCopyChunk, len = std::min(kCopyChunk, cnt - off);
-      std::memcpy(dst + off, hs + off, sizeof(double) * len);
+      unstage_chunk(dst + off, hs + off, len);
     }
   });
   int st = MPDPFT_OK;
   for (long k = 0; k < nchunk; ++k) {
-    const bool ok = !st && cudaEventSynchronize(copy_events[k]) == cudaSuccess;
+    const bool ok = !st && cudaEventSynchronize(c.copy_events[k]) == cudaSuccess;
     if (!ok && !st) st = set_error(MPDPFT_ERR_CUDA, "device to host copy");
     ready[k].store(ok ? 1 : 2, std::memory_order_release);
   }
   P.wait();
   return st;
+}
+
+int Ctx::host_to_device(double* dstage, double* hs, const double* src, long cnt) {
+  return stage_in<double>(*this, dstage, hs, src, cnt);
+}
+
+int Ctx::device_to_host(double* dst, double* hs, const double* dsrc, long cnt) {
+  return stage_out<double>(*this, dst, hs, dsrc, cnt);
 }
 
 int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slot, bool sync) {
@@ -664,8 +704,16 @@ int Ctx::import_field(const double* src, void* dst, int layout, int mem, int slo
   // host grids cross in chunks, copied and sent by several host threads
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
   double* dstage = d_io + (slot ? std::max(n_ref, geom.n) : 0);  // d_io holds two grids
-  int st = host_to_device(dstage, host_stage(slot), src, cnt);
-  if (st) return st;
+  int st;
+  if (rsize == sizeof(float)) {  // FP32 fields: rounded on the host, half the bytes over the link
+    float* fstage = reinterpret_cast<float*>(dstage);
+    if ((st = stage_in<float>(*this, fstage, reinterpret_cast<float*>(host_stage(slot)), src, cnt))) return st;
+    k_import<float, float><<<grid_blocks(geom.n), kThreads, 0, stream>>>(fstage, (float*)dst, geom, layout);
+    CU(cudaGetLastError());
+    if (sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
+    return MPDPFT_OK;
+  }
+  if ((st = host_to_device(dstage, host_stage(slot), src, cnt))) return st;
   st = import_staged(dstage, dst, layout, slot, false);
   if (st) return st;
   if (sync) CU(cudaStreamSynchronize(stream));  // pinned buffer reuse
@@ -721,6 +769,12 @@ int Ctx::export_field(const void* src, double* dst, int layout, int mem) {
   const long cnt = layout == MPDPFT_LAYOUT_REFERENCE ? n_ref : geom.n;
   double* ddst = mem == MPDPFT_MEM_HOST ? d_io : dst;
   const int blocks = grid_blocks(cnt);
+  if (mem == MPDPFT_MEM_HOST && rsize == sizeof(float)) {  // FP32 fields cross as floats
+    float* fstage = reinterpret_cast<float*>(d_io);
+    k_export<float, float><<<blocks, kThreads, 0, stream>>>((const float*)src, fstage, geom, layout);
+    CU(cudaGetLastError());
+    return stage_out<float>(*this, dst, reinterpret_cast<float*>(pinned), fstage, cnt);
+  }
   if (rsize == sizeof(double)) k_export<double><<<blocks, kThreads, 0, stream>>>((const double*)src, ddst, geom, layout);
   else k_export<float><<<blocks, kThreads, 0, stream>>>((const float*)src, ddst, geom, layout);
   CU(cudaGetLastError());
