@@ -1215,8 +1215,8 @@ int Ctx::fill_result(mpdpft_result* r, const ScState& h) {
 // stream; energy_finish forms the energies from them on the host.
 int Ctx::energy_issue(const ScState& h, double* e_dev, bool g2_current) {
   int st;
-  double* d_mu = d_io;  // scratch
-  CU(cudaMemcpyAsync(d_mu, h.mu, sizeof(double) * kMaxS, cudaMemcpyHostToDevice, stream));
+  double* d_mu = d_io;  // scratch: mu of the state h was read from (still on the device)
+  CU(cudaMemcpyAsync(d_mu, d_state->mu, sizeof(double) * kMaxS, cudaMemcpyDeviceToDevice, stream));
   const void* dens = (char*)d_nin + (size_t)h.slot * S * geom.n * rsize;
   if (gradient && geom.dim == 2 && !need_g2 && !g2_current) {
     // the 2D kinetic energy reads |grad V|^2, which the iterations' DelField
