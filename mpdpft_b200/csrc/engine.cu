@@ -96,28 +96,53 @@ __global__ void k_export(const R* __restrict__ src, D* __restrict__ dst, Geom g,
 // Energy integrands (GetEnergy, mpDPFT.cpp:5414-5436), one block partial per
 // accumulator: per species [0] int (mu-V)_+^{(D+2)/2}, [1] int Vext n,
 // [2] int n^2, [3] int n_+^{1+1/D}, [4] int n vh/2; pairs [16+...] int n_s n_s'.
-template <typename R>
-__global__ void k_energy(Geom g, int S, const R* V, const R* vext, const R* dens, const R* vh,
-                         const double* mu, double* part) {
-  double acc[kNEnergy];
+// NS = S at compile time: only the accumulators of NS species are held
+// (the row's other entries are written as 0), and the powers are products
+// with one square or cube root instead of pow.
+template <typename R, int NS>
+__global__ void k_energy(Geom g, const R* V, const R* vext, const R* dens, const R* vh, const double* mu,
+                         double* part) {
+  constexpr int NP = NS * (NS - 1) / 2;
+  constexpr int NA = 5 * NS + (NP > 0 ? NP : 1);
+  double acc[NA];
 #pragma unroll
-  for (int j = 0; j < kNEnergy; ++j) acc[j] = 0.0;
+  for (int j = 0; j < NA; ++j) acc[j] = 0.0;
   const long n = g.n;
-  const double ex = 0.5 * (g.dim + 2);
+  const bool d3 = g.dim == 3;
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
-    for (int s = 0; s < S; ++s) {
+    double nsv[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
       const long q = (long)s * n + p;
-      double u = mu[s] - (double)V[q];
-      double ns = (double)dens[q];
-      acc[5 * s + 0] += u > 0.0 ? pow(u, ex) : 0.0;
+      const double u = mu[s] - (double)V[q];
+      const double ns = (double)dens[q];
+      nsv[s] = ns;
+      acc[5 * s + 0] += u > 0.0 ? (d3 ? u * u * sqrt(u) : u * u) : 0.0;
       acc[5 * s + 1] += (double)vext[q] * ns;
       acc[5 * s + 2] += ns * ns;
-      acc[5 * s + 3] += ns > 0.0 ? pow(ns, 1.0 + 1.0 / g.dim) : 0.0;
+      acc[5 * s + 3] += ns > 0.0 ? (d3 ? ns * cbrt(ns) : ns * sqrt(ns)) : 0.0;
       if (vh) acc[5 * s + 4] += 0.5 * ns * (double)vh[q];
-      for (int t = s + 1; t < S; ++t) acc[5 * kMaxS + s * kMaxS + t] += ns * (double)dens[(long)t * n + p];
     }
+    int k = 5 * NS;
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int t = s + 1; t < NS; ++t) acc[k++] += nsv[s] * nsv[t];
   }
-  block_reduce_store<kNEnergy>(acc, part + (long)blockIdx.x * kNEnergy);
+  __shared__ double red[NA];
+  block_reduce_store<NA>(acc, red);
+  __syncthreads();
+  double* out = part + (long)blockIdx.x * kNEnergy;
+  for (int v = threadIdx.x; v < kNEnergy; v += blockDim.x) {
+    double x = 0.0;
+    if (v < 5 * kMaxS) {
+      if (v / 5 < NS) x = red[v];
+    } else if (v < kEkinOff) {
+      const int s = (v - 5 * kMaxS) / kMaxS, t = (v - 5 * kMaxS) % kMaxS;
+      if (s < t && t < NS) x = red[5 * NS + s * NS - s * (s + 1) / 2 + (t - s - 1)];
+    }
+    out[v] = x;
+  }
 }
 
 // Kinetic energy integrands of the gradient-corrected density, per species
@@ -1213,6 +1238,18 @@ int Ctx::fill_result(mpdpft_result* r, const ScState& h) {
 // of the last density evaluation, as in the reference's ExportData.
 // energy_issue leaves the kNEnergy integrals (times dvol) at e_dev on the
 // stream; energy_finish forms the energies from them on the host.
+template <typename R>
+void Ctx::launch_energy(int blocks, const void* dens, const double* d_mu) {
+  const R* vh = has_coulomb ? (const R*)d_vh : nullptr;
+  auto go = [&](auto kern) {
+    kern<<<blocks, kThreads, 0, stream>>>(geom, (const R*)d_V, (const R*)d_vext, (const R*)dens, vh, d_mu, d_part);
+  };
+  if (S == 1) go(k_energy<R, 1>);
+  else if (S == 2) go(k_energy<R, 2>);
+  else if (S == 3) go(k_energy<R, 3>);
+  else go(k_energy<R, 4>);
+}
+
 int Ctx::energy_issue(const ScState& h, double* e_dev, bool g2_current) {
   int st;
   double* d_mu = d_io;  // scratch: mu of the state h was read from (still on the device)
@@ -1230,14 +1267,8 @@ int Ctx::energy_issue(const ScState& h, double* e_dev, bool g2_current) {
     if ((st = issue_coulomb(dens, d_vh, /*for_energy=*/1))) return st;
   }
   const int blocks = grid_blocks(geom.n);
-  if (rsize == sizeof(double))
-    k_energy<double><<<blocks, kThreads, 0, stream>>>(geom, S, (const double*)d_V, (const double*)d_vext,
-                                                       (const double*)dens, has_coulomb ? (const double*)d_vh : nullptr,
-                                                       d_mu, d_part);
-  else
-    k_energy<float><<<blocks, kThreads, 0, stream>>>(geom, S, (const float*)d_V, (const float*)d_vext,
-                                                     (const float*)dens, has_coulomb ? (const float*)d_vh : nullptr,
-                                                     d_mu, d_part);
+  if (rsize == sizeof(double)) launch_energy<double>(blocks, dens, d_mu);
+  else launch_energy<float>(blocks, dens, d_mu);
   k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, kNEnergy, geom.dvol, e_dev);
   CU(cudaGetLastError());
   if (gradient) return ekin_issue(dens, d_mu, e_dev, 4, e_dev + kEkinOff);

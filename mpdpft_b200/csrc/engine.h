@@ -168,6 +168,8 @@ struct Ctx {
   int energy_issue(const ScState& h, double* e_dev, bool g2_current = false);
   void energy_finish(mpdpft_result* r, const double* E);
   int ekin_issue(const void* dens, const double* d_mu, const double* e_dev, int maxit, double* out);
+  template <typename R>
+  void launch_energy(int blocks, const void* dens, const double* d_mu);
   int integrate_device(const void* f, double* out);
   // standalone operators
   int op_mu_search(int s, const double* v, double target, double* mu_io, double* ab_out, int* trials,
