@@ -223,15 +223,21 @@ __global__ void k_ekin_grad(Geom g, int S, double gdeg, double thr, int maxit, d
   block_reduce_store<2 * kMaxS>(acc, part + (long)blockIdx.x * 2 * kMaxS);
 }
 
-// out[v] = scale * sum over rows b < nb of part[b * nv + v], one block, in
-// a fixed order.
+// out[v] = scale * sum over rows b < nb of part[b * nv + v]: block v sums
+// column v (each thread a strided share of the rows, then a fixed-order
+// tree), so the result is the same in every run.  Launch with nv blocks.
 __global__ void k_sum_rows(const double* part, int nb, int nv, double scale, double* out) {
-  const int lane = threadIdx.x & 31;
-  for (int v = threadIdx.x >> 5; v < nv; v += blockDim.x >> 5) {
-    double t = 0.0;
-    for (int b = lane; b < nb; b += 32) t += part[(long)b * nv + v];
-    t = warp_sum(t);
-    if (lane == 0) out[v] = t * scale;
+  __shared__ double sh[32];
+  const int v = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double t = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) t += part[(long)b * nv + v];
+  t = warp_sum(t);
+  if (lane == 0) sh[w] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) x += sh[i];
+    out[v] = x * scale;
   }
 }
 
@@ -1269,7 +1275,7 @@ int Ctx::energy_issue(const ScState& h, double* e_dev, bool g2_current) {
   const int blocks = grid_blocks(geom.n);
   if (rsize == sizeof(double)) launch_energy<double>(blocks, dens, d_mu);
   else launch_energy<float>(blocks, dens, d_mu);
-  k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, kNEnergy, geom.dvol, e_dev);
+  k_sum_rows<<<kNEnergy, kThreads, 0, stream>>>(d_part, blocks, kNEnergy, geom.dvol, e_dev);
   CU(cudaGetLastError());
   if (gradient) return ekin_issue(dens, d_mu, e_dev, 4, e_dev + kEkinOff);
   return MPDPFT_OK;
@@ -1290,7 +1296,7 @@ int Ctx::ekin_issue(const void* dens, const double* d_mu, const double* e_dev, i
     k_ekin_grad<float><<<blocks, kThreads, 0, stream>>>(geom, S, P.degeneracy, thr, maxit, P.internal_acc, area_pref,
                                                         (const float*)d_V, (const float*)d_lap, (const float*)d_g2,
                                                         (const float*)dens, d_mu, e_dev, d_part);
-  k_sum_rows<<<1, kThreads, 0, stream>>>(d_part, blocks, 2 * kMaxS, geom.dvol, out);
+  k_sum_rows<<<2 * kMaxS, kThreads, 0, stream>>>(d_part, blocks, 2 * kMaxS, geom.dvol, out);
   CU(cudaGetLastError());
   return MPDPFT_OK;
 }
